@@ -1,0 +1,610 @@
+/*
+ * oracle/dem_oracle.c -- plain-C restatement of sphere's per-timestep DEM
+ * step (the time-loop body of src/device.cu:731-1109).
+ *
+ * TEST INFRASTRUCTURE ONLY: the checker for the CUDA path, never the path
+ * itself.  It is loaded by tests/, __graft_entry__.smoke() and the CPU
+ * baseline of bench.py.  Its results are pinned against the reference's own
+ * kernel bodies (oracle/_ref, built by oracle/Makefile) and against the
+ * fixtures under tests/golden/.
+ *
+ * Every floating-point expression keeps the reference's operation order,
+ * because the CUDA path is checked against this file bit for bit:
+ *   - double arithmetic with no contraction (build with -ffp-contract=off,
+ *     the reference is built with --fmad=false, src/CMakeLists.txt:16-22);
+ *   - length() narrows to float and calls sqrtf (src/vector_arithmetic.h:317);
+ *   - float literals (0.001f, 4.0f) are widened exactly as in the reference.
+ * Float-to-integer conversions follow the device semantics (saturating), the
+ * behaviour of the GPU build the reference targets.
+ */
+#include "oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+/* PI of src/constants.h:14 (not M_PI) */
+static const double REF_PI = 3.14159265358979;
+
+typedef struct { double x, y, z; } v3;
+
+static inline v3 mk(double x, double y, double z) { v3 r = {x, y, z}; return r; }
+static inline v3 add(v3 a, v3 b) { return mk(a.x + b.x, a.y + b.y, a.z + b.z); }
+static inline v3 sub(v3 a, v3 b) { return mk(a.x - b.x, a.y - b.y, a.z - b.z); }
+/* scalar * vector: (s*a.x, ...) as vector_arithmetic.h:153-156 */
+static inline v3 smul(double s, v3 a) { return mk(s * a.x, s * a.y, s * a.z); }
+/* vector * scalar: (a.x*s, ...) as vector_arithmetic.h:149-152 */
+static inline v3 muls(v3 a, double s) { return mk(a.x * s, a.y * s, a.z * s); }
+static inline v3 divs(v3 a, double s) { return mk(a.x / s, a.y / s, a.z / s); }
+static inline v3 adds(v3 a, double s) { return mk(a.x + s, a.y + s, a.z + s); }
+static inline double dot(v3 a, v3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+/* src/vector_arithmetic.h:317-320: sqrtf of the narrowed dot product */
+static inline double vlen(v3 a) { return (double)sqrtf((float)dot(a, a)); }
+static inline v3 cross(v3 a, v3 b)
+{
+    return mk(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+static inline v3 ld3(const double *p) { return mk(p[0], p[1], p[2]); }
+
+/* device float->unsigned conversion (saturating, NaN -> 0) */
+static inline uint32_t sat_u32(double f)
+{
+    if (!(f > 0.0)) return 0u;
+    if (f >= 4294967295.0) return 0xffffffffu;
+    return (uint32_t)f;
+}
+/* device float->int conversion (saturating, NaN -> 0) */
+static inline int32_t sat_i32(double f)
+{
+    if (f != f) return 0;
+    if (f <= -2147483648.0) return INT32_MIN;
+    if (f >= 2147483647.0) return INT32_MAX;
+    return (int32_t)f;
+}
+static inline int32_t wrap_add(int32_t a, int32_t b) { return (int32_t)((uint32_t)a + (uint32_t)b); }
+
+/* (x - origo) / (L / num), floored: src/sorting.cuh:12-14, contactsearch.cuh:336-338 */
+static inline double cell_floor(const orc_scene *s, int d, double xd)
+{
+    return floor((xd - s->origo[d]) / (s->L[d] / (double)s->num[d]));
+}
+
+/* calcCellID, src/sorting.cuh:7-19 (unsigned arithmetic, wraps mod 2^32) */
+static uint32_t cell_id(const orc_scene *s, const double *x)
+{
+    uint32_t ix = sat_u32(cell_floor(s, 0, x[0]));
+    uint32_t iy = sat_u32(cell_floor(s, 1, x[1]));
+    uint32_t iz = sat_u32(cell_floor(s, 2, x[2]));
+    return (iz * s->num[1]) * s->num[0] + iy * s->num[0] + ix;
+}
+
+/* findDistMod, src/contactsearch.cuh:12-74.  Returns -1 when the target cell
+ * lies outside a non-periodic boundary; otherwise wraps periodic axes and
+ * accumulates the +/-L shift into *dm. */
+static int dist_mod(const orc_scene *s, int32_t c[3], v3 *dm)
+{
+    const uint32_t nx = s->num[0], ny = s->num[1], nz = s->num[2];
+    if (s->periodic == 1) {
+        if (c[0] < 0) { c[0] = (int32_t)(nx - 1); *dm = add(*dm, mk(s->L[0], 0.0, 0.0)); }
+        if ((uint32_t)c[0] == nx) { c[0] = 0; *dm = sub(*dm, mk(s->L[0], 0.0, 0.0)); }
+        if (c[1] < 0) { c[1] = (int32_t)(ny - 1); *dm = add(*dm, mk(0.0, s->L[1], 0.0)); }
+        if ((uint32_t)c[1] == ny) { c[1] = 0; *dm = sub(*dm, mk(0.0, s->L[1], 0.0)); }
+    } else if (s->periodic == 2) {
+        if (c[0] < 0) { c[0] = (int32_t)(nx - 1); *dm = add(*dm, mk(s->L[0], 0.0, 0.0)); }
+        if ((uint32_t)c[0] == nx) { c[0] = 0; *dm = sub(*dm, mk(s->L[0], 0.0, 0.0)); }
+        if (c[1] < 0 || (uint32_t)c[1] == ny) return -1;
+    } else {
+        if (c[0] < 0 || (uint32_t)c[0] == nx) return -1;
+        if (c[1] < 0 || (uint32_t)c[1] == ny) return -1;
+    }
+    if (c[2] < 0 || (uint32_t)c[2] == nz) return -1;
+    return 0;
+}
+
+/* working arrays that live across steps */
+typedef struct {
+    uint32_t np, ncells;
+    uint32_t *cellid;   /* per original index */
+    uint32_t *count;    /* ncells + 1 (last bucket: out-of-grid keys) */
+    double *x_s, *vel_s, *angvel_s; /* sorted copies, 4 doubles each */
+    double *wf_pp;      /* wall-0 force per original index */
+} work_t;
+
+static void work_free(work_t *w)
+{
+    free(w->cellid); free(w->count); free(w->x_s); free(w->vel_s);
+    free(w->angvel_s); free(w->wf_pp);
+    memset(w, 0, sizeof(*w));
+}
+
+static int work_alloc(work_t *w, uint32_t np, uint32_t ncells)
+{
+    memset(w, 0, sizeof(*w));
+    w->np = np; w->ncells = ncells;
+    w->cellid = (uint32_t *)malloc(sizeof(uint32_t) * (size_t)np);
+    w->count = (uint32_t *)malloc(sizeof(uint32_t) * ((size_t)ncells + 1));
+    w->x_s = (double *)malloc(sizeof(double) * 4 * (size_t)np);
+    w->vel_s = (double *)malloc(sizeof(double) * 4 * (size_t)np);
+    w->angvel_s = (double *)malloc(sizeof(double) * 4 * (size_t)np);
+    w->wf_pp = (double *)calloc((size_t)np, sizeof(double));
+    if (!w->cellid || !w->count || !w->x_s || !w->vel_s || !w->angvel_s || !w->wf_pp) {
+        work_free(w);
+        return -1;
+    }
+    return 0;
+}
+
+/* ---- cell list: calcParticleCellID + stable sort + reorderArrays ------- */
+/* src/sorting.cuh:24-43 (cell of every particle), src/device.cu:763-765
+ * (stable sort of (cellID, index); a counting sort is stable by
+ * construction), src/device.cu:776-777 (cellStart := 0xffffffff) and
+ * src/sorting.cuh:49-121 (cellStart/cellEnd and the gathered copies). */
+static int build_cells(orc_scene *s, work_t *w)
+{
+    const uint32_t np = s->np, nc = w->ncells;
+    int err = 0;
+    for (uint32_t i = 0; i < np; ++i) {
+        uint32_t c = cell_id(s, &s->x[4 * (size_t)i]);
+        if (c >= nc) { err |= ORC_ERR_OUT_OF_GRID; c = nc; }
+        w->cellid[i] = c;
+    }
+    memset(w->count, 0, sizeof(uint32_t) * ((size_t)nc + 1));
+    for (uint32_t i = 0; i < np; ++i) w->count[w->cellid[i]]++;
+    uint32_t run = 0;
+    for (uint32_t c = 0; c <= nc; ++c) { uint32_t k = w->count[c]; w->count[c] = run; run += k; }
+    for (uint32_t i = 0; i < np; ++i) {
+        uint32_t c = w->cellid[i];
+        uint32_t k = w->count[c]++;
+        s->perm[k] = i;
+        s->cell_sorted[k] = (c == nc) ? 0xffffffffu : cell_id(s, &s->x[4 * (size_t)i]);
+    }
+    for (uint32_t c = 0; c < nc; ++c) s->cell_start[c] = 0xffffffffu;
+    for (uint32_t k = 0; k < np; ++k) {
+        uint32_t c = w->cellid[s->perm[k]];
+        uint32_t prev = k > 0 ? w->cellid[s->perm[k - 1]] : 0;
+        if (c < nc && (k == 0 || c != prev)) s->cell_start[c] = k;
+        if (k > 0 && c != prev && prev < nc) s->cell_end[prev] = k;
+        if (k == np - 1 && c < nc) s->cell_end[c] = k + 1;
+        const size_t o = 4 * (size_t)s->perm[k];
+        memcpy(&w->x_s[4 * (size_t)k], &s->x[o], 4 * sizeof(double));
+        memcpy(&w->vel_s[4 * (size_t)k], &s->vel[o], 4 * sizeof(double));
+        memcpy(&w->angvel_s[4 * (size_t)k], &s->angvel[o], 4 * sizeof(double));
+    }
+    return err;
+}
+
+/* ---- topology: src/contactsearch.cuh:181-355 ---------------------------- */
+static int topology_one(orc_scene *s, work_t *w, uint32_t a)
+{
+    const uint32_t np = s->np;
+    const double *xa = &w->x_s[4 * (size_t)a];
+    const double ra = xa[3];
+    const uint32_t a_orig = s->perm[a];
+    uint32_t *row = &s->contacts[(size_t)a_orig * ORC_NC];
+    double *dmrow = &s->distmod[(size_t)a_orig * ORC_NC * 4];
+    int err = 0;
+    int nc = 0;
+    int32_t gp[3];
+    for (int d = 0; d < 3; ++d) gp[d] = sat_i32(cell_floor(s, d, xa[d]));
+    for (int oz = -1; oz < 2; ++oz)
+        for (int oy = -1; oy < 2; ++oy)
+            for (int ox = -1; ox < 2; ++ox) {
+                int32_t c[3] = {wrap_add(gp[0], ox), wrap_add(gp[1], oy), wrap_add(gp[2], oz)};
+                v3 dm = mk(0.0, 0.0, 0.0);
+                if (dist_mod(s, c, &dm) == -1) continue;
+                uint32_t cid = (uint32_t)c[0] + (uint32_t)c[1] * s->num[0]
+                    + (s->num[0] * s->num[1]) * (uint32_t)c[2];
+                if (cid >= w->ncells) { err |= ORC_ERR_OUT_OF_GRID; continue; }
+                uint32_t start = s->cell_start[cid];
+                if (start == 0xffffffffu) continue;
+                uint32_t end = s->cell_end[cid];
+                for (uint32_t b = start; b < end; ++b) {
+                    if (b == a) continue;
+                    const double *xb = &w->x_s[4 * (size_t)b];
+                    const double rb = xb[3];
+                    const uint32_t b_orig = s->perm[b];
+                    v3 xab = add(mk(xa[0] - xb[0], xa[1] - xb[1], xa[2] - xb[2]), dm);
+                    double len = vlen(xab);
+                    double delta = len - (ra + rb);
+                    if (delta < 0.0f) {
+                        /* slot choice, contactsearch.cuh:252-265: a slot that
+                         * already holds b wins; otherwise the last empty slot;
+                         * otherwise position nc */
+                        int cpos = nc;
+                        for (int i = 0; i < ORC_NC; ++i) {
+                            uint32_t v = row[i];
+                            if (v == np) cpos = i;
+                            else if (v == b_orig) { cpos = i; break; }
+                        }
+                        if (cpos >= ORC_NC) {
+                            err |= ORC_ERR_NC_OVERFLOW;
+                        } else {
+                            row[cpos] = b_orig;
+                            double *d = &dmrow[4 * cpos];
+                            d[0] = dm.x; d[1] = dm.y; d[2] = dm.z; d[3] = rb;
+                        }
+                        ++nc;
+                        if (nc > ORC_NC) break; /* returns from this cell only */
+                    }
+                }
+            }
+    return err;
+}
+
+/* ---- contact laws: src/contactmodels.cuh -------------------------------- */
+
+/* contactLinear_wall, src/contactmodels.cuh:10-109 */
+static double contact_wall(const orc_scene *s, v3 *F, v3 *T, double *p,
+                           double ra, const double *vel_a, const double *angvel_a,
+                           v3 n, double delta, double wvel)
+{
+    v3 linvel = ld3(vel_a), angvel = ld3(angvel_a);
+    v3 vel = adds(add(linvel, smul(ra, cross(n, angvel))), wvel);
+    double vel_n = dot(vel, n);
+    v3 vel_t = sub(vel, muls(n, dot(vel, n)));
+    double vel_t_length = vlen(vel_t);
+    v3 f_n = smul(-s->k_n * delta - s->gamma_wn * vel_n, n);
+    if (dot(f_n, n) < 0.0f) f_n = mk(0.0, 0.0, 0.0);
+    double f_n_length = vlen(f_n);
+    v3 f_t = mk(0.0, 0.0, 0.0);
+    v3 T_res = mk(0.0, 0.0, 0.0);
+    if (vel_t_length > 0.f) {
+        double f_t_visc = s->gamma_wt * vel_t_length;
+        double f_t_limit;
+        if (vel_t_length > 0.001f) f_t_limit = s->mu_wd * f_n_length;
+        else f_t_limit = s->mu_ws * f_n_length;
+        if (f_t_visc < f_t_limit) f_t = divs(smul(-1.0f * f_t_visc, vel_t), vel_t_length);
+        else f_t = divs(smul(-1.0f * f_t_limit, vel_t), vel_t_length);
+    }
+    *F = add(*F, add(f_n, f_t));
+    *T = add(*T, add(smul(-ra, cross(n, f_t)), T_res));
+    *p += f_n_length / (4.0f * REF_PI * ra * ra);
+    return dot(f_n, n);
+}
+
+/* contactLinear, src/contactmodels.cuh:283-493 (contact model 2) */
+static void contact_linear(const orc_scene *s, v3 *F, v3 *T, double *es_dot,
+                           double *ev_dot, double *p, uint32_t b_orig,
+                           const double *vel_a4, v3 angvel_a, double ra, double rb,
+                           v3 x, double x_length, double delta, double *dt4)
+{
+    const double dt = s->dt;
+    v3 vel_b = ld3(&s->vel[4 * (size_t)b_orig]);
+    v3 angvel_b = ld3(&s->angvel[4 * (size_t)b_orig]);
+    v3 dt0u = ld3(dt4);
+    v3 n = divs(x, x_length);
+    v3 vel_linear = mk(vel_a4[0] - vel_b.x, vel_a4[1] - vel_b.y, vel_a4[2] - vel_b.z);
+    v3 vel = add(add(vel_linear, smul(ra + delta / 2.0, cross(n, angvel_a))),
+                 smul(rb + delta / 2.0, cross(n, angvel_b)));
+    double vel_n = -dot(vel_linear, n);
+    v3 vel_t = sub(vel, muls(n, dot(n, vel)));
+    double vel_t_length = vlen(vel_t);
+    v3 delta_t0 = sub(dt0u, muls(n, dot(n, dt0u)));
+    double delta_t0_length = vlen(delta_t0);
+    v3 delta_t = mk(0.0, 0.0, 0.0); /* left unset by the reference when unused */
+    v3 f_n = smul(-s->k_n * delta - s->gamma_n * vel_n, n);
+    *ev_dot += s->gamma_n * vel_n * vel_n;
+    if (dot(f_n, n) < 0.0f) f_n = mk(0.0, 0.0, 0.0);
+    double f_n_length = vlen(f_n);
+    v3 f_c = smul(-s->kappa * (double)sqrtf((float)(ra * rb)), n);
+    v3 f_t = mk(0.0, 0.0, 0.0);
+    if (delta_t0_length > 0.0 || vel_t_length > 0.0) {
+        delta_t = add(delta_t0, muls(vel_t, dt));
+        v3 f_t_elast = smul(-s->k_t, delta_t);
+        v3 f_t_visc = smul(-s->gamma_t, vel_t);
+        f_t = add(f_t_elast, f_t_visc);
+        double f_t_length = vlen(f_t);
+        double f_t_limit = s->mu_s * vlen(sub(f_n, f_c));
+        delta_t = add(delta_t0, muls(vel_t, dt));
+        if (f_t_length > f_t_limit) {
+            v3 t = divs(f_t, vlen(f_t));
+            f_t = smul(f_t_limit, t);
+            delta_t = smul(-1.0 / s->k_t,
+                           add(smul(s->mu_d * vlen(sub(f_n, f_c)), t), smul(s->gamma_t, vel_t)));
+            *es_dot += vlen(muls(smul(vlen(f_t), vel_t), dt)) / dt;
+        }
+    }
+    *F = add(*F, add(add(f_n, f_t), f_c));
+    *T = add(*T, cross(smul(-(ra + delta * 0.5), n), f_t));
+    *p += f_n_length / (4.0f * REF_PI * ra * ra);
+    dt4[0] = delta_t.x; dt4[1] = delta_t.y; dt4[2] = delta_t.z; dt4[3] = 0.0f;
+}
+
+/* ---- interact: src/contactsearch.cuh:369-689 (contact models 2/3) ------- */
+static void interact_one(orc_scene *s, work_t *w, uint32_t a)
+{
+    const uint32_t np = s->np;
+    const uint32_t a_orig = s->perm[a];
+    const double *xa = &w->x_s[4 * (size_t)a];
+    const double ra = xa[3];
+    const v3 origo = mk(s->origo[0], s->origo[1], s->origo[2]);
+    const v3 L = mk(s->L[0], s->L[1], s->L[2]);
+    /* default walls, contactsearch.cuh:416-427 */
+    double wnx[5][4] = {{0.0, 0.0, -1.0, L.z}, {-1.0, 0.0, 0.0, L.x}, {1.0, 0.0, 0.0, 0.0},
+                        {0.0, -1.0, 0.0, L.y}, {0.0, 1.0, 0.0, 0.0}};
+    double wmvfd[5][4] = {{0}};
+    for (uint32_t k = 0; k < s->nw && k < 5; ++k) {
+        memcpy(wnx[k], &s->walls_nx[4 * k], 4 * sizeof(double));
+        memcpy(wmvfd[k], &s->walls_mvfd[4 * k], 4 * sizeof(double));
+    }
+    double es_dot = 0.0f, ev_dot = 0.0f, p = 0.0f;
+    v3 F = mk(0.0, 0.0, 0.0), T = mk(0.0, 0.0, 0.0);
+    const double *vel_a = &w->vel_s[4 * (size_t)a];
+    const double *angvel_a4 = &w->angvel_s[4 * (size_t)a];
+    v3 angvel_a = ld3(angvel_a4);
+    if (s->contactmodel == 2) {
+        for (int i = 0; i < ORC_NC; ++i) {
+            size_t mp = (size_t)a_orig * ORC_NC + (size_t)i;
+            uint32_t b_orig = s->contacts[mp];
+            double *dt4 = &s->delta_t[4 * mp];
+            if (b_orig != np) {
+                const double *dm = &s->distmod[4 * mp];
+                const double *xb = &s->x[4 * (size_t)b_orig];
+                double rb = xb[3];
+                v3 xab = mk(xa[0] - xb[0] + dm[0], xa[1] - xb[1] + dm[1], xa[2] - xb[2] + dm[2]);
+                double xlen = vlen(xab);
+                double delta_n = xlen - (ra + rb);
+                if (delta_n < 0.0f) {
+                    contact_linear(s, &F, &T, &es_dot, &ev_dot, &p, b_orig, vel_a, angvel_a,
+                                   ra, rb, xab, xlen, delta_n, dt4);
+                } else {
+                    s->contacts[mp] = np;
+                    dt4[0] = dt4[1] = dt4[2] = dt4[3] = 0.0;
+                }
+            } else {
+                dt4[0] = dt4[1] = dt4[2] = dt4[3] = 0.0;
+            }
+        }
+    }
+    /* walls, contactsearch.cuh:578-663 */
+    double w0f = 0.0;
+    double dw;
+    dw = wnx[0][3] - (xa[2] + ra);
+    if (dw < 0.0f)
+        w0f = contact_wall(s, &F, &T, &p, ra, vel_a, angvel_a4, ld3(wnx[0]), dw, wmvfd[0][1]);
+    dw = xa[2] - ra - origo.z;
+    if (dw < 0.0f)
+        (void)contact_wall(s, &F, &T, &p, ra, vel_a, angvel_a4, mk(0.0, 0.0, 1.0), dw, 0.0f);
+    if (s->periodic == 0) {
+        dw = wnx[1][3] - (xa[0] + ra);
+        if (dw < 0.0f) (void)contact_wall(s, &F, &T, &p, ra, vel_a, angvel_a4, ld3(wnx[1]), dw, wmvfd[1][1]);
+        dw = xa[0] - ra - wnx[2][3];
+        if (dw < 0.0f) (void)contact_wall(s, &F, &T, &p, ra, vel_a, angvel_a4, ld3(wnx[2]), dw, wmvfd[2][1]);
+        dw = wnx[3][3] - (xa[1] + ra);
+        if (dw < 0.0f) (void)contact_wall(s, &F, &T, &p, ra, vel_a, angvel_a4, ld3(wnx[3]), dw, wmvfd[3][1]);
+        dw = xa[1] - ra - wnx[4][3];
+        if (dw < 0.0f) (void)contact_wall(s, &F, &T, &p, ra, vel_a, angvel_a4, ld3(wnx[4]), dw, wmvfd[4][1]);
+    } else if (s->periodic == 2) {
+        dw = wnx[3][3] - (xa[1] + ra);
+        if (dw < 0.0f) (void)contact_wall(s, &F, &T, &p, ra, vel_a, angvel_a4, ld3(wnx[3]), dw, wmvfd[3][1]);
+        dw = xa[1] - ra - wnx[4][3];
+        if (dw < 0.0f) (void)contact_wall(s, &F, &T, &p, ra, vel_a, angvel_a4, ld3(wnx[4]), dw, wmvfd[4][1]);
+    }
+    /* writes at the original index, contactsearch.cuh:670-687 */
+    double *f = &s->force[4 * (size_t)a_orig];
+    double *t = &s->torque[4 * (size_t)a_orig];
+    f[0] = F.x; f[1] = F.y; f[2] = F.z; f[3] = 0.0f;
+    t[0] = T.x; t[1] = T.y; t[2] = T.z; t[3] = 0.0f;
+    s->es_dot[a_orig] = es_dot;
+    s->ev_dot[a_orig] = ev_dot;
+    s->es[a_orig] += es_dot * s->dt;
+    s->ev[a_orig] += ev_dot * s->dt;
+    s->p[a_orig] = p;
+    w->wf_pp[a_orig] = w0f;
+}
+
+/* ---- bondsLinear: src/cohesion.cuh:8-233, bonds in index order ---------- */
+static void bond_one(orc_scene *s, uint32_t idx)
+{
+    const double dt = s->dt;
+    uint32_t bi = s->bonds[2 * (size_t)idx], bj = s->bonds[2 * (size_t)idx + 1];
+    if (!(bi < s->np)) return;
+    const double *d0 = &s->bonds_delta[4 * (size_t)idx];
+    const double *o0 = &s->bonds_omega[4 * (size_t)idx];
+    v3 delta0_t = ld3(d0);
+    const double delta0_n = d0[3];
+    v3 omega0_t = ld3(o0);
+    const double omega0_n = o0[3];
+    const double *xi = &s->x[4 * (size_t)bi], *xj = &s->x[4 * (size_t)bj];
+    const double *vi = &s->vel[4 * (size_t)bi], *vj = &s->vel[4 * (size_t)bj];
+    v3 wi = ld3(&s->angvel[4 * (size_t)bi]), wj = ld3(&s->angvel[4 * (size_t)bj]);
+    const double R_bar = s->lambda_bar * fmin(xi[3], xj[3]);
+    const double A = REF_PI * R_bar * R_bar;
+    const double I = 0.25 * REF_PI * R_bar * R_bar * R_bar * R_bar;
+    const double J = I * 2.0;
+    const v3 x = mk(xi[0] - xj[0], xi[1] - xj[1], xi[2] - xj[2]);
+    const double x_length = vlen(x);
+    const double overlap = fmin(0.0, x_length - (xi[3] + xj[3]));
+    v3 n = divs(x, x_length);
+    delta0_t = sub(delta0_t, muls(n, dot(n, delta0_t)));
+    const v3 ddelta = muls(add(add(mk(vi[0] - vj[0], vi[1] - vj[1], vi[2] - vj[2]),
+                                   smul(xi[3] + overlap / 2.0, cross(n, wi))),
+                               smul(xj[3] + overlap / 2.0, cross(n, wj))),
+                           dt);
+    const double ddelta_n = -dot(ddelta, n);
+    const double delta_n = delta0_n + ddelta_n;
+    const v3 ddelta_t = sub(ddelta, muls(n, dot(n, ddelta)));
+    const v3 delta_t = add(delta0_t, ddelta_t);
+    const v3 f_n = smul(s->k_n * A * delta_n + s->gamma_n * ddelta_n / dt, n);
+    const v3 f_t = sub(smul(-s->k_t * A, delta_t), divs(smul(s->gamma_t, ddelta_t), dt));
+    const v3 f = add(f_n, f_t);
+    const v3 mn = mk(-n.x, -n.y, -n.z);
+    omega0_t = sub(omega0_t, muls(mn, dot(omega0_t, mn)));
+    const v3 domega = muls(mk(wj.x - wi.x, wj.y - wi.y, wj.z - wi.z), dt);
+    const double domega_n = dot(domega, mn);
+    const double omega_n = omega0_n + domega_n;
+    const v3 domega_t = sub(domega, smul(domega_n, mn));
+    const v3 omega_t = add(omega0_t, domega_t);
+    const v3 t_n = smul(-s->k_t * J * omega_n, mn);
+    const v3 t_t = smul(-s->k_n * I, omega_t);
+    const v3 t_j = add(t_n, t_t);
+    const double sigma_max = vlen(f_n) / A + vlen(t_t) * R_bar / I;
+    const double tau_max = vlen(f_t) / A + vlen(t_n) * R_bar / J;
+    if (sigma_max >= s->sigma_b || tau_max >= s->tau_b) {
+        s->bonds[2 * (size_t)idx] = s->nb0;
+        return;
+    }
+    double *bd = &s->bonds_delta[4 * (size_t)idx], *bo = &s->bonds_omega[4 * (size_t)idx];
+    bd[0] = delta_t.x; bd[1] = delta_t.y; bd[2] = delta_t.z; bd[3] = delta_n;
+    bo[0] = omega_t.x; bo[1] = omega_t.y; bo[2] = omega_t.z; bo[3] = omega_n;
+    double *fi = &s->force[4 * (size_t)bi], *fj = &s->force[4 * (size_t)bj];
+    double *ti = &s->torque[4 * (size_t)bi], *tj = &s->torque[4 * (size_t)bj];
+    fi[0] += f.x; fi[1] += f.y; fi[2] += f.z; fi[3] += 0.0;
+    fj[0] -= f.x; fj[1] -= f.y; fj[2] -= f.z; fj[3] -= 0.0;
+    ti[0] -= t_j.x; ti[1] -= t_j.y; ti[2] -= t_j.z; ti[3] -= 0.0;
+    tj[0] += t_j.x; tj[1] += t_j.y; tj[2] += t_j.z; tj[3] += 0.0;
+}
+
+/* ---- integrate: src/integration.cuh:9-187 ------------------------------- */
+static void integrate_one(orc_scene *s, work_t *w, uint32_t k)
+{
+    const uint32_t o = s->perm[k];
+    const size_t q = 4 * (size_t)o;
+    const double *force = &s->force[q], *torque = &s->torque[q];
+    double angpos[4], acc[4], angacc[4], vel0[4], angvel0[4], x[4], vel[4], angvel[4];
+    memcpy(angpos, &s->angpos[q], sizeof angpos);
+    memcpy(acc, &s->acc[q], sizeof acc);
+    memcpy(angacc, &s->angacc[q], sizeof angacc);
+    memcpy(vel0, &s->vel0[q], sizeof vel0);
+    memcpy(angvel0, &s->angvel0[q], sizeof angvel0);
+    memcpy(x, &w->x_s[4 * (size_t)k], sizeof x);
+    memcpy(vel, &w->vel_s[4 * (size_t)k], sizeof vel);
+    memcpy(angvel, &w->angvel_s[4 * (size_t)k], sizeof angvel);
+    const double radius = x[3];
+    double xysum[2] = {0.0f, 0.0f};
+    const double dt = s->dt;
+    const double m = 4.0 / 3.0 * REF_PI * radius * radius * radius * s->rho;
+    acc[0] = force[0] / m;
+    acc[1] = force[1] / m;
+    acc[2] = force[2] / m;
+    angacc[0] = torque[0] * 1.0 / (2.0 / 5.0 * m * radius * radius);
+    angacc[1] = torque[1] * 1.0 / (2.0 / 5.0 * m * radius * radius);
+    angacc[2] = torque[2] * 1.0 / (2.0 / 5.0 * m * radius * radius);
+    acc[0] += s->g[0];
+    acc[1] += s->g[1];
+    acc[2] += s->g[2];
+    if (vel[3] > 0.0f) {
+        acc[0] = 0.0;
+        acc[1] = 0.0;
+        acc[2] -= s->g[2];
+        angacc[0] = angacc[1] = angacc[2] = angacc[3] = 0.0f;
+    }
+    if (s->periodic == 1) {
+        if (x[0] < s->origo[0]) x[0] += s->L[0];
+        if (x[0] > s->L[0]) x[0] -= s->L[0];
+        if (x[1] < s->origo[1]) x[1] += s->L[1];
+        if (x[1] > s->L[1]) x[1] -= s->L[1];
+    } else if (s->periodic == 2) {
+        if (x[0] < s->origo[0]) x[0] += s->L[0];
+        if (x[0] > s->L[0]) x[0] -= s->L[0];
+    }
+    for (int d = 0; d < 3; ++d) vel0[d] += acc[d] * dt;
+    for (int d = 0; d < 3; ++d) angvel0[d] += angacc[d] * dt;
+    for (int d = 0; d < 3; ++d) x[d] += vel0[d] * dt;
+    for (int d = 0; d < 3; ++d) angpos[d] += angvel0[d] * dt;
+    for (int d = 0; d < 3; ++d) vel[d] = vel0[d] + 0.5 * acc[d] * dt;
+    for (int d = 0; d < 3; ++d) angvel[d] = angvel0[d] + 0.5 * angacc[d] * dt;
+    xysum[0] += vel[0] * dt;
+    xysum[1] += vel[1] * dt;
+    s->xysum[2 * (size_t)o] += xysum[0];
+    s->xysum[2 * (size_t)o + 1] += xysum[1];
+    memcpy(&s->acc[q], acc, sizeof acc);
+    memcpy(&s->angacc[q], angacc, sizeof angacc);
+    memcpy(&s->angvel[q], angvel, sizeof angvel);
+    memcpy(&s->angvel0[q], angvel0, sizeof angvel0);
+    memcpy(&s->vel[q], vel, sizeof vel);
+    memcpy(&s->vel0[q], vel0, sizeof vel0);
+    memcpy(&s->angpos[q], angpos, sizeof angpos);
+    memcpy(&s->x[q], x, sizeof x);
+}
+
+/* ---- summation + integrateWalls: src/integration.cuh:191-295 ------------ */
+/* The wall-0 force is summed exactly as the reference GPU kernels do: blocks
+ * of 256 particles reduced by a halving tree (integration.cuh:197-216), then
+ * the block partials added in block order (integration.cuh:249-252). */
+static double wall_force_sum(const work_t *w)
+{
+    const uint32_t np = w->np;
+    const uint32_t nblk = (np + 255u) / 256u;
+    double total = 0.0;
+    double cache[256];
+    for (uint32_t b = 0; b < nblk; ++b) {
+        for (uint32_t t = 0; t < 256; ++t) {
+            uint32_t idx = b * 256u + t;
+            double temp = 0.0f;
+            if (idx < np) temp += w->wf_pp[idx];
+            cache[t] = temp;
+        }
+        for (uint32_t i = 128; i != 0; i /= 2)
+            for (uint32_t t = 0; t < i; ++t) cache[t] += cache[t + i];
+        total += cache[0];
+    }
+    return total;
+}
+
+static void integrate_walls(orc_scene *s, const work_t *w, double t_current)
+{
+    if (s->nw == 0) return;
+    const double fsum = wall_force_sum(w);
+    for (uint32_t i = 0; i < s->nw; ++i) {
+        double *nx = &s->walls_nx[4 * i], *mvfd = &s->walls_mvfd[4 * i];
+        int wmode = s->wmode[i];
+        double vel0 = s->walls_vel0[i];
+        if (wmode == 0) continue;
+        mvfd[2] = 0.0;
+        mvfd[2] += fsum;
+        const double dt = s->dt;
+        double sigma_0 = mvfd[3] + s->devs_A * sin(2.0 * 3.141596654 * s->devs_f * t_current);
+        double N = -sigma_0 * s->L[0] * s->L[1];
+        double acc = (mvfd[2] + N) / mvfd[0];
+        if (wmode == 2) acc = 0.0;
+        vel0 += acc * dt;
+        nx[3] += vel0 * dt;
+        mvfd[1] = vel0 + 0.5 * acc * dt;
+        s->walls_vel0[i] = vel0;
+    }
+}
+
+int orc_kind(void) { return 1; }
+
+int orc_threads(int nthreads)
+{
+#ifdef _OPENMP
+    return nthreads > 0 ? nthreads : omp_get_max_threads();
+#else
+    (void)nthreads;
+    return 1;
+#endif
+}
+
+int orc_step(orc_scene *s, uint64_t nsteps, int nthreads)
+{
+    if (!s || s->np == 0 || s->nw > ORC_MAXWALLS) return ORC_ERR_BAD_INPUT;
+    if (s->contactmodel != 2) return ORC_ERR_BAD_INPUT;
+    const uint64_t nc64 = (uint64_t)s->num[0] * s->num[1] * s->num[2];
+    if (nc64 == 0 || nc64 >= 0xffffffffull) return ORC_ERR_BAD_INPUT;
+    work_t w;
+    if (work_alloc(&w, s->np, (uint32_t)nc64) != 0) return ORC_ERR_BAD_INPUT;
+    const int nt = orc_threads(nthreads);
+    int err = 0;
+    for (uint64_t step = 0; step < nsteps; ++step) {
+        err |= build_cells(s, &w);
+        int e_topo = 0;
+#pragma omp parallel for num_threads(nt) schedule(dynamic, 256) reduction(| : e_topo)
+        for (int64_t a = 0; a < (int64_t)s->np; ++a) e_topo |= topology_one(s, &w, (uint32_t)a);
+        err |= e_topo;
+#pragma omp parallel for num_threads(nt) schedule(dynamic, 256)
+        for (int64_t a = 0; a < (int64_t)s->np; ++a) interact_one(s, &w, (uint32_t)a);
+        for (uint32_t b = 0; b < s->nb0; ++b) bond_one(s, b);
+#pragma omp parallel for num_threads(nt) schedule(static)
+        for (int64_t k = 0; k < (int64_t)s->np; ++k) integrate_one(s, &w, (uint32_t)k);
+        integrate_walls(s, &w, s->t_current);
+        s->t_current += s->dt;
+    }
+    if (s->wall0_force) memcpy(s->wall0_force, w.wf_pp, sizeof(double) * s->np);
+    work_free(&w);
+    return err;
+}

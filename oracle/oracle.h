@@ -1,0 +1,82 @@
+/*
+ * oracle/oracle.h -- C interface shared by the two CPU oracles of the sphere
+ * DEM step.
+ *
+ * TEST INFRASTRUCTURE ONLY.  Two libraries export this interface:
+ *   oracle/liborc.so      -- dem_oracle.c, a plain-C restatement of the
+ *                            reference algorithm;
+ *   oracle/_ref/libref.so -- the reference's own kernel bodies
+ *                            (src/sorting.cuh, src/contactsearch.cuh,
+ *                            src/contactmodels.cuh, src/cohesion.cuh,
+ *                            src/integration.cuh) compiled as host C++ under a
+ *                            shim, driven in the order of src/device.cu:731-1109.
+ * Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg load
+ * them, as checkers.  The product path never links or calls either.
+ *
+ * All arrays use the reference's host layout (array-of-structs, "Float4" =
+ * four doubles): Kinematics/Energies/Walls in src/datatypes.h:17-105.
+ */
+#ifndef SPHERE_ORACLE_H_
+#define SPHERE_ORACLE_H_
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ORC_NC 32       /* contact slots per particle, src/constants.h:24 */
+#define ORC_MAXWALLS 6  /* src/constants.h:11 */
+
+/* status codes (bit flags, OR-ed over the run) */
+#define ORC_OK 0
+#define ORC_ERR_NC_OVERFLOW 1   /* a contact would be written past slot NC-1 */
+#define ORC_ERR_OUT_OF_GRID 2   /* a cell index fell outside [0, ncells) */
+#define ORC_ERR_BAD_INPUT 4
+
+typedef struct orc_scene {
+    /* sizes and switches */
+    uint32_t np, nw, nb0, contactmodel;
+    int32_t periodic;
+    uint32_t num[3];
+    double origo[3], L[3];
+    double dt, t_current;
+    /* Params (src/datatypes.h:74-101) */
+    double g[3], k_n, k_t, k_r, gamma_n, gamma_t, gamma_r, mu_s, mu_d, mu_r;
+    double gamma_wn, gamma_wt, mu_ws, mu_wd, rho, kappa, db, V_b;
+    double lambda_bar, sigma_b, tau_b, devs_A, devs_f;
+    int32_t wmode[ORC_MAXWALLS];
+    /* per particle: 4 doubles each (xysum: 2) */
+    double *x, *vel, *vel0, *acc, *force, *angpos, *angvel, *angvel0,
+        *angacc, *torque, *xysum;
+    double *es_dot, *es, *ev_dot, *ev, *p;
+    /* contact bookkeeping: np*NC slots (distmod/delta_t 4 doubles each) */
+    uint32_t *contacts;
+    double *distmod, *delta_t;
+    /* bonds: nb0 pairs, 4 doubles of history each */
+    uint32_t *bonds;
+    double *bonds_delta, *bonds_omega;
+    /* walls: nw entries */
+    double *walls_nx, *walls_mvfd, *walls_vel0;
+    /* cell list of the most recent step (outputs): sorted cell ids and the
+     * sorted-to-original permutation (np each); cell start/end (ncells each) */
+    uint32_t *cell_sorted, *perm, *cell_start, *cell_end;
+    /* wall-0 force of every particle in the most recent step (np) */
+    double *wall0_force;
+} orc_scene;
+
+/* Advance the scene by nsteps time steps.  nthreads <= 0 uses the OpenMP
+ * default.  Returns the OR of the ORC_ERR_* flags raised (0 when clean). */
+int orc_step(orc_scene *s, uint64_t nsteps, int nthreads);
+
+/* Which oracle this is: 1 = plain-C restatement, 2 = reference kernels. */
+int orc_kind(void);
+
+/* Number of OpenMP threads a parallel region gets with nthreads as above. */
+int orc_threads(int nthreads);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,122 @@
+"""ctypes binding of the CPU oracles (TEST INFRASTRUCTURE ONLY).
+
+Loads ``oracle/liborc.so`` (the plain-C restatement, ``kind == 1``) or
+``oracle/_ref/libref.so`` (the reference's kernel bodies, ``kind == 2``) and
+steps a ``sphere_b200.state.HostState`` in place.  Only tests/, the smoke
+check and bench.py's CPU-baseline leg import this module.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB_ORC = HERE / "liborc.so"
+LIB_REF = HERE / "_ref" / "libref.so"
+
+ERR_NC_OVERFLOW = 1
+ERR_OUT_OF_GRID = 2
+ERR_BAD_INPUT = 4
+
+_dp = C.POINTER(C.c_double)
+_up = C.POINTER(C.c_uint32)
+
+
+class OrcScene(C.Structure):
+    _fields_ = [
+        ("np", C.c_uint32), ("nw", C.c_uint32), ("nb0", C.c_uint32), ("contactmodel", C.c_uint32),
+        ("periodic", C.c_int32), ("num", C.c_uint32 * 3),
+        ("origo", C.c_double * 3), ("L", C.c_double * 3),
+        ("dt", C.c_double), ("t_current", C.c_double),
+        ("g", C.c_double * 3),
+        ("k_n", C.c_double), ("k_t", C.c_double), ("k_r", C.c_double),
+        ("gamma_n", C.c_double), ("gamma_t", C.c_double), ("gamma_r", C.c_double),
+        ("mu_s", C.c_double), ("mu_d", C.c_double), ("mu_r", C.c_double),
+        ("gamma_wn", C.c_double), ("gamma_wt", C.c_double), ("mu_ws", C.c_double),
+        ("mu_wd", C.c_double), ("rho", C.c_double), ("kappa", C.c_double), ("db", C.c_double),
+        ("V_b", C.c_double), ("lambda_bar", C.c_double), ("sigma_b", C.c_double),
+        ("tau_b", C.c_double), ("devs_A", C.c_double), ("devs_f", C.c_double),
+        ("wmode", C.c_int32 * 6),
+        ("x", _dp), ("vel", _dp), ("vel0", _dp), ("acc", _dp), ("force", _dp), ("angpos", _dp),
+        ("angvel", _dp), ("angvel0", _dp), ("angacc", _dp), ("torque", _dp), ("xysum", _dp),
+        ("es_dot", _dp), ("es", _dp), ("ev_dot", _dp), ("ev", _dp), ("p", _dp),
+        ("contacts", _up), ("distmod", _dp), ("delta_t", _dp),
+        ("bonds", _up), ("bonds_delta", _dp), ("bonds_omega", _dp),
+        ("walls_nx", _dp), ("walls_mvfd", _dp), ("walls_vel0", _dp),
+        ("cell_sorted", _up), ("perm", _up), ("cell_start", _up), ("cell_end", _up),
+        ("wall0_force", _dp),
+    ]
+
+
+def build(ref: bool = True) -> None:
+    """Build the oracle libraries with oracle/Makefile (``ref`` needs the
+    reference checkout; it is skipped when that is absent)."""
+    subprocess.run(["make", "-s", "-C", str(HERE), "orc"], check=True)
+    if ref:
+        subprocess.run(["make", "-s", "-C", str(HERE), "ref"], check=False)
+
+
+def load(kind: str = "orc"):
+    path = LIB_ORC if kind == "orc" else LIB_REF
+    if not path.exists():
+        raise FileNotFoundError(f"oracle library {path} is not built (run make -C oracle)")
+    lib = C.CDLL(str(path))
+    lib.orc_step.argtypes = [C.POINTER(OrcScene), C.c_uint64, C.c_int]
+    lib.orc_step.restype = C.c_int
+    lib.orc_kind.restype = C.c_int
+    lib.orc_threads.argtypes = [C.c_int]
+    lib.orc_threads.restype = C.c_int
+    return lib
+
+
+class OracleRun:
+    """Owns the scratch/output arrays of one oracle scene."""
+
+    def __init__(self, lib, cfg, st):
+        self.lib, self.cfg, self.st = lib, cfg, st
+        n = cfg.np
+        self.cell_sorted = np.zeros(n, np.uint32)
+        self.perm = np.zeros(n, np.uint32)
+        self.cell_start = np.zeros(cfg.ncells, np.uint32)
+        self.cell_end = np.zeros(cfg.ncells, np.uint32)
+        self.wall0_force = np.zeros(n)
+        self._keep = []
+        s = OrcScene()
+        s.np, s.nw, s.nb0, s.contactmodel = cfg.np, cfg.nw, cfg.nb0, cfg.contactmodel
+        s.periodic = cfg.periodic
+        s.num[:] = [int(v) for v in cfg.num]
+        s.origo[:] = [float(v) for v in cfg.origo]
+        s.L[:] = [float(v) for v in cfg.L]
+        s.dt = cfg.dt
+        s.g[:] = [float(v) for v in cfg.g]
+        for k, v in cfg.params.items():
+            setattr(s, k, float(v))
+        s.wmode[:] = [int(v) for v in cfg.wmode]
+        for name in ("x", "vel", "vel0", "acc", "force", "angpos", "angvel", "angvel0", "angacc",
+                     "torque", "xysum", "es_dot", "es", "ev_dot", "ev", "p", "distmod", "delta_t",
+                     "bonds_delta", "bonds_omega", "walls_nx", "walls_mvfd", "walls_vel0"):
+            setattr(s, name, self._ptr(getattr(st, name), np.float64))
+        for name in ("contacts", "bonds"):
+            setattr(s, name, self._ptr(getattr(st, name), np.uint32))
+        s.cell_sorted = self._ptr(self.cell_sorted, np.uint32)
+        s.perm = self._ptr(self.perm, np.uint32)
+        s.cell_start = self._ptr(self.cell_start, np.uint32)
+        s.cell_end = self._ptr(self.cell_end, np.uint32)
+        s.wall0_force = self._ptr(self.wall0_force, np.float64)
+        self.scene = s
+
+    def _ptr(self, a, dtype):
+        assert a.dtype == dtype and a.flags.c_contiguous, (a.dtype, a.flags)
+        if a.size == 0:
+            a = np.zeros(1, dtype)
+            self._keep.append(a)
+        return a.ctypes.data_as(_dp if dtype == np.float64 else _up)
+
+    def step(self, nsteps: int, nthreads: int = 0) -> int:
+        self.scene.t_current = self.st.t_current
+        rc = self.lib.orc_step(C.byref(self.scene), nsteps, nthreads)
+        self.st.t_current = self.scene.t_current
+        return rc

@@ -1,0 +1,308 @@
+"""Seeded synthetic scenes for the DEM hot path.
+
+Each builder returns a ``Spherebin`` (reference binary layout) built from a
+``numpy.random.default_rng(seed)``; no dataset is involved.  The workloads:
+
+``settling``      10,000 monodisperse spheres (r = 0.01 m, rho = 2600) on a
+                  jittered cubic lattice (spacing 2.2 r, 20 x 20 x 25,
+                  jitter U(+-0.1 r)) in a 0.5 x 0.5 x 2 m box with the
+                  reference's implicit frictional walls, gravity -9.81 m/s^2,
+                  linear-viscoelastic contacts (kn = kt = 1e6 N/m,
+                  gamma_n = 100 N s/m, mu = 0.5), dt = 1e-6 s, grid 24 x 24 x 96.
+``polydisperse``  1,000,000 spheres, radii log-normal (median 1 mm,
+                  sigma 0.2, clipped to 0.5-2 mm), random sequential placement
+                  in a periodic-x/y 0.2 x 0.2 x 0.4 m domain, a top wall at
+                  max(z + r) loaded at 20 kPa, contact parameters of
+                  ``settling`` plus mu_r = 0.01 (unused by contact model 2),
+                  dt = 2e-7 s, grid 50 x 50 x 100.
+``bonded``        uniform radii 0.9-1.1 mm on a jittered FCC lattice with a
+                  bond between every lattice-neighbour pair, both x ends
+                  pulled apart at 0.01 m/s (``fixvel``).
+``collision``     small dense scenes with random velocities and spins, used
+                  by the parity tests because every step makes and breaks
+                  contacts and slides.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from .spherebin import Spherebin, V_sphere
+
+
+def _contact_params(sb: Spherebin, k_n=1e6, k_t=1e6, gamma_n=100.0, gamma_t=0.0, mu=0.5,
+                    gamma_w=100.0, mu_r=0.0):
+    sb.k_n, sb.k_t, sb.k_r = float(k_n), float(k_t), 0.0
+    sb.gamma_n, sb.gamma_t, sb.gamma_r = float(gamma_n), float(gamma_t), 0.0
+    sb.mu_s = sb.mu_d = sb.mu_ws = sb.mu_wd = float(mu)
+    sb.mu_r = float(mu_r)
+    sb.gamma_wn = sb.gamma_wt = float(gamma_w)
+    sb.rho = 2600.0
+    sb.contactmodel = 2
+    sb.kappa = sb.db = sb.V_b = 0.0
+
+
+def settling(seed=0, nx=20, ny=20, nz=25, r=0.01, sid="settling") -> Spherebin:
+    rng = np.random.default_rng(seed)
+    n = nx * ny * nz
+    sb = Spherebin(np_=n, nw=0, sid=sid)
+    spacing = 2.2 * r
+    i = np.arange(n)
+    lat = np.stack([i % nx, (i // nx) % ny, i // (nx * ny)], axis=1).astype(float)
+    sb.x = 0.03 + lat * spacing + rng.uniform(-0.1 * r, 0.1 * r, size=(n, 3))
+    sb.radius = np.full(n, r)
+    sb.origo = np.zeros(3)
+    sb.L = np.array([0.5, 0.5, 2.0])
+    sb.num = np.array([24, 24, 96], dtype=np.uint32)
+    sb.periodic = 0
+    sb.g = np.array([0.0, 0.0, -9.81])
+    _contact_params(sb)
+    sb.time_dt = 1e-6
+    sb.time_total = 1000 * sb.time_dt
+    sb.time_file_dt = sb.time_total
+    return sb
+
+
+def _lognormal_radii(rng, n, median=1e-3, sigma=0.2, lo=0.5e-3, hi=2e-3):
+    return np.clip(np.exp(rng.normal(math.log(median), sigma, n)), lo, hi)
+
+
+def rsa_place(rng, radii, L, periodic_xy=True, cap=24, batch=16384, max_rounds=100000):
+    """Random sequential placement of spheres with the given radii in the box
+    [0, L): particles are placed in index order, each at uniformly random
+    positions until it overlaps no placed sphere (periodic images in x/y,
+    hard floor/ceiling in z).  Returns positions (n, 3)."""
+    n = len(radii)
+    r_max = float(radii.max())
+    h = 2.0 * r_max
+    g = np.maximum(np.floor(np.asarray(L) / h).astype(int), 3)
+    cs = np.asarray(L) / g
+    ncell = int(g[0] * g[1] * g[2])
+    members = np.full((ncell + 1, cap), -1, dtype=np.int64)   # last row: sentinel
+    counts = np.zeros(ncell + 1, dtype=np.int64)
+    pos = np.zeros((n, 3))
+    placed = np.zeros(n, dtype=bool)
+    pending = np.arange(n)
+    offs = np.array([(dx, dy, dz) for dz in (-1, 0, 1) for dy in (-1, 0, 1) for dx in (-1, 0, 1)])
+    Larr = np.asarray(L, float)
+    for _ in range(max_rounds):
+        if pending.size == 0:
+            break
+        idx = pending[:batch]
+        rr = radii[idx]
+        m = idx.size
+        cand = np.empty((m, 3))
+        cand[:, 0] = rng.random(m) * Larr[0]
+        cand[:, 1] = rng.random(m) * Larr[1]
+        cand[:, 2] = rr + rng.random(m) * (Larr[2] - 2 * rr)
+        cc = np.minimum((cand / cs).astype(int), g - 1)
+        nb = cc[:, None, :] + offs[None, :, :]
+        if periodic_xy:
+            nb[..., 0] %= g[0]
+            nb[..., 1] %= g[1]
+        bad = (nb[..., 2] < 0) | (nb[..., 2] >= g[2]) | (nb[..., 0] < 0) | (nb[..., 0] >= g[0]) \
+            | (nb[..., 1] < 0) | (nb[..., 1] >= g[1])
+        cid = nb[..., 0] + g[0] * (nb[..., 1] + g[1] * nb[..., 2])
+        cid = np.where(bad, ncell, cid)
+        mem = members[cid].reshape(m, -1)                      # (m, 27*cap)
+        valid = mem >= 0
+        mj = np.where(valid, mem, 0)
+        d = cand[:, None, :] - pos[mj]
+        if periodic_xy:
+            for ax in (0, 1):
+                d[..., ax] -= Larr[ax] * np.round(d[..., ax] / Larr[ax])
+        dist2 = np.einsum("ijk,ijk->ij", d, d)
+        lim = (rr[:, None] + radii[mj]) ** 2
+        ok = ~np.any(valid & (dist2 < lim), axis=1)
+        # conflicts inside the batch: an accepted candidate that overlaps an
+        # earlier accepted candidate of the same batch is rejected
+        acc = np.nonzero(ok)[0]
+        if acc.size > 1:
+            ca = cand[acc]
+            ra = rr[acc]
+            ccell = np.minimum((ca / cs).astype(int), g - 1)
+            key = ccell[:, 0] + g[0] * (ccell[:, 1] + g[1] * ccell[:, 2])
+            order = np.argsort(key, kind="stable")
+            skey = key[order]
+            keep = np.ones(acc.size, dtype=bool)
+            nbk = ccell[:, None, :] + offs[None, :, :]
+            if periodic_xy:
+                nbk[..., 0] %= g[0]
+                nbk[..., 1] %= g[1]
+            badk = (nbk[..., 2] < 0) | (nbk[..., 2] >= g[2]) | (nbk[..., 0] < 0) \
+                | (nbk[..., 0] >= g[0]) | (nbk[..., 1] < 0) | (nbk[..., 1] >= g[1])
+            kid = nbk[..., 0] + g[0] * (nbk[..., 1] + g[1] * nbk[..., 2])
+            lo = np.searchsorted(skey, kid, "left")
+            hi = np.searchsorted(skey, kid, "right")
+            lo = np.where(badk, 0, lo)
+            hi = np.where(badk, 0, hi)
+            cnt = (hi - lo).ravel()
+            src = np.repeat(np.repeat(np.arange(acc.size), 27), cnt)
+            start = np.repeat(lo.ravel(), cnt)
+            within = np.arange(cnt.sum()) - np.repeat(np.cumsum(cnt) - cnt, cnt)
+            other = order[start + within]
+            sel = other < src
+            src, other = src[sel], other[sel]
+            dd = ca[src] - ca[other]
+            if periodic_xy:
+                for ax in (0, 1):
+                    dd[:, ax] -= Larr[ax] * np.round(dd[:, ax] / Larr[ax])
+            hit = np.einsum("ij,ij->i", dd, dd) < (ra[src] + ra[other]) ** 2
+            keep[np.unique(src[hit])] = False
+            acc = acc[keep]
+        new = idx[acc]
+        pos[new] = cand[acc]
+        placed[new] = True
+        ccell = np.minimum((cand[acc] / cs).astype(int), g - 1)
+        key = ccell[:, 0] + g[0] * (ccell[:, 1] + g[1] * ccell[:, 2])
+        for k_, p_ in zip(key, new):
+            c = counts[k_]
+            if c >= cap:
+                raise RuntimeError("rsa_place: cell capacity exceeded; raise cap")
+            members[k_, c] = p_
+            counts[k_] = c + 1
+        pending = np.concatenate([pending[batch:], np.setdiff1d(idx, new, assume_unique=True)])
+    if not placed.all():
+        raise RuntimeError("rsa_place: could not place every sphere")
+    return pos
+
+
+def polydisperse(n=1_000_000, seed=0, L=(0.2, 0.2, 0.4), num=(50, 50, 100),
+                 devs=20e3, sid="polydisperse") -> Spherebin:
+    rng = np.random.default_rng(seed)
+    sb = Spherebin(np_=n, nw=1, sid=sid)
+    sb.radius = _lognormal_radii(rng, n)
+    sb.x = rsa_place(rng, sb.radius, L)
+    sb.origo = np.zeros(3)
+    sb.L = np.array(L, float)
+    sb.num = np.array(num, dtype=np.uint32)
+    sb.periodic = 1
+    sb.g = np.array([0.0, 0.0, -9.81])
+    _contact_params(sb, mu_r=0.01)
+    # stress-controlled top wall at max(z + r) (python/sphere.py:1266-1306)
+    sb.nw = 1
+    sb.wmode = np.array([1], dtype=np.int32)
+    sb.w_n = np.array([[0.0, 0.0, -1.0]])
+    sb.w_x = np.array([float(np.max(sb.x[:, 2] + sb.radius))])
+    cellsize = sb.L[0] / sb.num[0]
+    sb.w_m = np.array([sb.rho * n * math.pi * (cellsize / 2.0) ** 3])
+    sb.w_vel = np.zeros(1)
+    sb.w_force = np.zeros(1)
+    sb.w_devs = np.array([devs])
+    sb.time_dt = 2e-7
+    sb.time_total = 1e4 * sb.time_dt
+    sb.time_file_dt = sb.time_total
+    return sb
+
+
+def bonded(seed=0, nx=40, ny=20, nz=20, r_lo=0.9e-3, r_hi=1.1e-3, pull=0.01,
+           sigma_b=2e7, tau_b=2e7, sid="bonded") -> Spherebin:
+    """FCC lattice (spacing 2.1 r_hi) with bonds between nearest lattice
+    neighbours; the first and last x layer move apart at +-pull/2."""
+    rng = np.random.default_rng(seed)
+    a = 2.1 * r_hi * math.sqrt(2.0)   # cubic FCC cell edge, neighbour distance 2.1 r_hi
+    basis = np.array([[0, 0, 0], [0.5, 0.5, 0], [0.5, 0, 0.5], [0, 0.5, 0.5]])
+    cells = np.stack(np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij"),
+                     axis=-1).reshape(-1, 3)
+    pts = (cells[:, None, :] + basis[None, :, :]).reshape(-1, 3) * a
+    order = np.lexsort((pts[:, 0], pts[:, 1], pts[:, 2]))
+    pts = pts[order]
+    n = len(pts)
+    sb = Spherebin(np_=n, nw=0, sid=sid)
+    sb.radius = rng.uniform(r_lo, r_hi, n)
+    margin = 4 * r_hi
+    sb.x = pts + margin + rng.uniform(-0.02 * r_lo, 0.02 * r_lo, size=(n, 3))
+    ext = pts.max(axis=0) + 2 * margin
+    cell = 2.2 * r_hi
+    num = np.ceil(ext / cell).astype(np.uint32)
+    sb.origo = np.zeros(3)
+    sb.L = num * cell
+    sb.num = num
+    sb.periodic = 0
+    sb.g = np.zeros(3)
+    _contact_params(sb, k_n=1e6, k_t=1e6, gamma_n=0.0, mu=0.5)
+    # bonds: lattice neighbours at the FCC nearest-neighbour distance
+    nn = a / math.sqrt(2.0)
+    key = np.floor(sb.x / cell).astype(np.int64)
+    kid = key[:, 0] + num[0] * (key[:, 1] + num[1] * key[:, 2])
+    srt = np.argsort(kid, kind="stable")
+    skid = kid[srt]
+    pairs = []
+    for dz in (-1, 0, 1):
+        for dy in (-1, 0, 1):
+            for dx in (-1, 0, 1):
+                nk = (key[:, 0] + dx) + num[0] * ((key[:, 1] + dy) + num[1] * (key[:, 2] + dz))
+                lo = np.searchsorted(skid, nk, "left")
+                hi = np.searchsorted(skid, nk, "right")
+                cnt = hi - lo
+                src = np.repeat(np.arange(n), cnt)
+                oth = srt[np.repeat(lo, cnt) + (np.arange(cnt.sum()) - np.repeat(np.cumsum(cnt) - cnt, cnt))]
+                sel = oth > src
+                src, oth = src[sel], oth[sel]
+                d = np.linalg.norm(sb.x[src] - sb.x[oth], axis=1)
+                ok = d < 1.05 * (sb.radius[src] + sb.radius[oth])
+                ok &= d < 1.2 * nn
+                pairs.append(np.stack([src[ok], oth[ok]], axis=1))
+    bonds = np.unique(np.concatenate(pairs), axis=0).astype(np.uint32)
+    sb.bonds = bonds
+    nb0 = len(bonds)
+    sb.lambda_bar = 1.0
+    sb.bonds_delta_n = np.zeros(nb0)
+    sb.bonds_delta_t = np.zeros((nb0, 3))
+    sb.bonds_omega_n = np.zeros(nb0)
+    sb.bonds_omega_t = np.zeros((nb0, 3))
+    sb.sigma_b, sb.tau_b = float(sigma_b), float(tau_b)
+    xmin, xmax = sb.x[:, 0].min(), sb.x[:, 0].max()
+    left = sb.x[:, 0] < xmin + 0.5 * a
+    right = sb.x[:, 0] > xmax - 0.5 * a
+    sb.fixvel[left | right] = 1.0
+    sb.vel[left, 0] = -0.5 * pull
+    sb.vel[right, 0] = 0.5 * pull
+    m_min = float(V_sphere(r_lo)) * sb.rho
+    sb.time_dt = 1e-7
+    sb.time_total = 1000 * sb.time_dt
+    sb.time_file_dt = sb.time_total
+    _ = m_min
+    return sb
+
+
+def collision(n=2000, seed=0, periodic=0, box=(0.06, 0.06, 0.06), r=(0.8e-3, 1.6e-3),
+              phi_target=0.45, nw=0, vmax=0.5, wmax=200.0, g=(0.0, 0.0, -9.81),
+              k_n=2e4, k_t=2e4, gamma_n=0.05, gamma_t=0.01, mu=0.4, dt=2e-6,
+              sid="collision") -> Spherebin:
+    """Jittered lattice with some overlap, random velocities and spins:
+    contacts open, close and slide from the first step on.  The box is sized
+    so no particle reaches a periodic boundary within a few hundred steps."""
+    rng = np.random.default_rng(seed)
+    radii = rng.uniform(r[0], r[1], n)
+    vol = float(np.sum(V_sphere(radii)))
+    side = (vol / phi_target) ** (1.0 / 3.0)
+    m = int(math.ceil(n ** (1.0 / 3.0)))
+    spacing = side / m
+    i = np.arange(n)
+    lat = np.stack([i % m, (i // m) % m, i // (m * m)], axis=1).astype(float)
+    Lb = np.asarray(box, float)
+    center = 0.5 * Lb
+    x = center - 0.5 * side + (lat + 0.5) * spacing + rng.uniform(-0.15, 0.15, (n, 3)) * spacing
+    sb = Spherebin(np_=n, nw=nw, sid=sid)
+    sb.radius = radii
+    sb.x = x
+    sb.vel = rng.uniform(-vmax, vmax, (n, 3))
+    sb.angvel = rng.uniform(-wmax, wmax, (n, 3))
+    sb.origo = np.zeros(3)
+    sb.L = Lb
+    cell = 2.0 * r[1]
+    sb.num = np.floor(Lb / cell).astype(np.uint32)
+    sb.periodic = int(periodic)
+    sb.g = np.asarray(g, float)
+    _contact_params(sb, k_n=k_n, k_t=k_t, gamma_n=gamma_n, gamma_t=gamma_t, mu=mu, gamma_w=0.05)
+    if nw:
+        sb.wmode = np.ones(nw, dtype=np.int32)
+        sb.w_x = np.array([float(np.max(sb.x[:, 2] + sb.radius)) + 0.2e-3] + [0.0] * (nw - 1))[:nw]
+        sb.w_m = np.full(nw, 1e-3)
+        sb.w_devs = np.full(nw, 50.0)
+    sb.time_dt = dt
+    sb.time_total = 100 * dt
+    sb.time_file_dt = sb.time_total
+    return sb
