@@ -1,0 +1,139 @@
+/*
+ * sphk.h -- C ABI of libsphk, the B200 (sm_100a) DEM step of sphere.
+ *
+ * The reference has no in-process interface for this path: its DEM class
+ * (src/sphere.h:12-322) owns the state and drives the GPU from
+ * DEM::startTime() (src/device.cu:576-1299), and Python reaches it through
+ * binary files and a subprocess (python/sphere.py:1629-1655).  Each entry
+ * point below replaces one step of that class, so the DEM class
+ * (sphere_b200/csrc/host/sphere.cpp) and any FFI can sit on top:
+ *
+ *   sph_create       DEM::initializeGPU + transferToConstantDeviceMemory +
+ *                    allocateGlobalDeviceMemory   (src/device.cu:34-84,201-324)
+ *   sph_upload       DEM::transferToGlobalDeviceMemory (src/device.cu:394-488)
+ *   sph_step         n iterations of the time loop body (src/device.cu:731-1109)
+ *   sph_sync         the checkForCudaErrors after each kernel (src/utility.cu:9-28)
+ *   sph_download     DEM::transferFromGlobalDeviceMemory (src/device.cu:490-572)
+ *   sph_get_contacts the CONTACTINFO dump of slots (src/device.cu:1148-1176)
+ *   sph_get_cells    the sorted arrays of the last step (src/device.cu:747-800)
+ *   sph_destroy      DEM::freeGlobalDeviceMemory (src/device.cu:326-391)
+ *
+ * Conventions: plain C types only; every entry point returns an int status,
+ * SPH_OK (0) or a negative SPH_ERR_* code; the message of the last failure
+ * is available from sph_last_error().  Host arrays use the reference's host
+ * layout: "4 doubles per particle" rows (Float4, src/datatypes.h:17-33),
+ * particle order = the caller's particle index.  A context is bound to one
+ * device and is not thread safe; distinct contexts are independent.
+ */
+#ifndef SPHK_H_
+#define SPHK_H_
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SPHK_VERSION 1
+#define SPHK_NC 32        /* contact slots per particle (src/constants.h:24) */
+#define SPHK_MAXWALLS 6   /* src/constants.h:11 */
+
+#define SPH_OK 0
+#define SPH_ERR_CUDA (-1)         /* a CUDA call failed (see sph_last_error) */
+#define SPH_ERR_NC_OVERFLOW (-2)  /* a particle found more than SPHK_NC contacts */
+#define SPH_ERR_OUT_OF_GRID (-3)  /* a particle left the cell grid */
+#define SPH_ERR_TIMEOUT (-4)      /* a bounded device wait gave up */
+#define SPH_ERR_BAD_INPUT (-5)    /* invalid argument or configuration */
+#define SPH_ERR_BOND_ALIAS (-6)   /* a broken bond's marker (nb0 < np) aliases a particle */
+#define SPH_ERR_NOMEM (-7)        /* device allocation failed */
+
+typedef struct sph_ctx sph_ctx;
+
+/* Static configuration: the Grid, Params and Walls fields of the input file
+ * (src/datatypes.h:43-101) plus the time step.  Mirrors readbin's fields. */
+typedef struct sph_config {
+    uint32_t np, nw, nb0, contactmodel;
+    int32_t periodic;
+    uint32_t num[3];
+    double origo[3], L[3];
+    double dt;
+    double g[3], k_n, k_t, k_r, gamma_n, gamma_t, gamma_r, mu_s, mu_d, mu_r;
+    double gamma_wn, gamma_wt, mu_ws, mu_wd, rho, kappa, db, V_b;
+    double lambda_bar, sigma_b, tau_b, devs_A, devs_f;
+    int32_t wmode[SPHK_MAXWALLS];
+    int32_t device;              /* CUDA device ordinal */
+} sph_config;
+
+/* Host-side state, reference layout.  On upload, NULL pointers take the
+ * reference's initial values: vel0 := vel and angvel0 := angvel
+ * (src/device.cu:413-424), acc/angacc := 0, contacts := empty (np) with zero
+ * history, walls_vel0 := walls_mvfd[].y (src/device.cu:461-464). */
+typedef struct sph_host_state {
+    double *x;        /* np*4: x, y, z, radius */
+    double *xysum;    /* np*2 */
+    double *vel;      /* np*4: vx, vy, vz, fixvel */
+    double *vel0;     /* np*4 or NULL */
+    double *acc;      /* np*4 or NULL (w lane not kept) */
+    double *force;    /* np*4 */
+    double *angpos;   /* np*4 */
+    double *angvel;   /* np*4 */
+    double *angvel0;  /* np*4 or NULL */
+    double *angacc;   /* np*4 or NULL (w lane not kept) */
+    double *torque;   /* np*4 */
+    double *es_dot, *es, *ev_dot, *ev, *p;   /* np each */
+    uint32_t *contacts;   /* np*SPHK_NC or NULL; value np marks an empty slot */
+    double *distmod;      /* np*SPHK_NC*4 or NULL: periodic shift (0 or +-L) + radius */
+    double *delta_t;      /* np*SPHK_NC*4 or NULL: tangential spring history */
+    uint32_t *bonds;      /* nb0*2 */
+    double *bonds_delta;  /* nb0*4: tangential xyz, normal w */
+    double *bonds_omega;  /* nb0*4 */
+    double *walls_nx;     /* nw*4: normal xyz, position w */
+    double *walls_mvfd;   /* nw*4: mass, velocity, force, deviatoric stress */
+    double *walls_vel0;   /* nw or NULL */
+    double t_current;     /* simulation time */
+} sph_host_state;
+
+/* Counters of the current state. */
+typedef struct sph_stats {
+    uint64_t active_contacts;   /* occupied slots over all particles (directed) */
+    uint64_t steps;             /* steps taken since upload */
+    uint64_t relayouts;         /* storage re-orderings performed */
+    uint64_t device_bytes;      /* device memory held by the context */
+} sph_stats;
+
+/* Options for sph_set_option. */
+#define SPH_OPT_RELAYOUT_EVERY 1  /* re-sort storage every n steps (0: at upload only) */
+#define SPH_OPT_GRAPH_STEPS 2     /* steps captured per CUDA graph (1..64, default 8) */
+
+int sph_version(void);
+int sph_create(const sph_config *cfg, sph_ctx **out);
+int sph_set_option(sph_ctx *ctx, int option, int64_t value);
+int sph_upload(sph_ctx *ctx, const sph_host_state *st);
+/* Enqueue nsteps time steps on `stream` (a cudaStream_t, NULL: the context's
+ * own stream).  Asynchronous: device errors surface at sph_sync. */
+int sph_step(sph_ctx *ctx, uint64_t nsteps, void *stream);
+/* Wait for all work and report the first device-side error (sticky). */
+int sph_sync(sph_ctx *ctx);
+int sph_download(sph_ctx *ctx, sph_host_state *st);
+/* Contact slots in the reference layout (np*SPHK_NC; distmod/delta_t
+ * np*SPHK_NC*4).  Any pointer may be NULL.  distmod of empty slots is 0. */
+int sph_get_contacts(sph_ctx *ctx, uint32_t *contacts, double *distmod, double *delta_t);
+/* The cell list used by the most recent step: sorted cell ids and the
+ * sorted->particle permutation (np each), cellStart/cellEnd (ncells each;
+ * cellStart = 0xffffffff for empty cells, cellEnd defined for occupied ones). */
+int sph_get_cells(sph_ctx *ctx, uint32_t *cell_sorted, uint32_t *perm, uint32_t *cell_start,
+                  uint32_t *cell_end);
+/* Wall-0 force of every particle in the most recent step (np doubles). */
+int sph_get_wall_forces(sph_ctx *ctx, double *wall0_force);
+int sph_get_stats(sph_ctx *ctx, sph_stats *out);
+/* Re-sort particle storage into the current cell order (locality only;
+ * results are unchanged). */
+int sph_relayout(sph_ctx *ctx);
+const char *sph_last_error(const sph_ctx *ctx);
+int sph_destroy(sph_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

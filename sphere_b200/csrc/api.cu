@@ -1,0 +1,693 @@
+// api.cu -- the C ABI of libsphk (include/sphk.h): contexts, host<->device
+// transfer in the reference's host layout, and stepping through CUDA graphs.
+#include "sphk_internal.cuh"
+#include "../../include/sphk.h"
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+namespace sphk {
+void launch_step(const Dev &d, uint32_t np, int a, int write_outputs, cudaStream_t st);
+void launch_bonds(const Dev &d, uint32_t nb0, int a, cudaStream_t st);
+void launch_walls(const Dev &d, uint32_t np, uint32_t nw, cudaStream_t st);
+void launch_cell_init(const Dev &d, uint32_t np, int a, cudaStream_t st);
+void launch_rebuild(const Dev &d, uint32_t np, uint32_t ncells, cudaStream_t st);
+unsigned int scan_tile_count(uint32_t ncells);
+void relayout(const Dev &d, uint32_t np, int a, void *scratch, cudaStream_t st);
+}  // namespace sphk
+
+using namespace sphk;
+
+struct sph_ctx {
+    Dev d{};
+    Params hp{};
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int a = 0;                       // buffer holding the current state
+    uint64_t steps = 0, relayouts = 0, since_relayout = 0;
+    double t_host = 0.0;
+    int64_t relayout_every = 0;
+    int graph_steps = 8;
+    bool uploaded = false;
+    void *scratch = nullptr;
+    size_t scratch_bytes = 0;
+    std::vector<void *> allocs;
+    size_t device_bytes = 0;
+    cudaGraphExec_t g_multi[2] = {nullptr, nullptr};
+    cudaGraphExec_t g_single[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+    int graphs_for_k = 0;
+    std::string err;
+    int sticky = SPH_OK;
+};
+
+namespace {
+
+int fail(sph_ctx *c, int code, const std::string &msg)
+{
+    if (c) {
+        c->err = msg;
+        if (c->sticky == SPH_OK && code != SPH_ERR_BAD_INPUT) c->sticky = code;
+    }
+    return code;
+}
+
+#define CK(call)                                                                      \
+    do {                                                                              \
+        cudaError_t e_ = (call);                                                      \
+        if (e_ != cudaSuccess)                                                        \
+            return fail(c, SPH_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+template <typename T>
+int dalloc(sph_ctx *c, T **p, size_t count)
+{
+    const size_t bytes = sizeof(T) * (count ? count : 1);
+    void *q = nullptr;
+    cudaError_t e = cudaMalloc(&q, bytes);
+    if (e != cudaSuccess) return fail(c, SPH_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    e = cudaMemset(q, 0, bytes);
+    if (e != cudaSuccess) return fail(c, SPH_ERR_CUDA, std::string("cudaMemset: ") + cudaGetErrorString(e));
+    c->allocs.push_back(q);
+    c->device_bytes += bytes;
+    *p = static_cast<T *>(q);
+    return SPH_OK;
+}
+
+int status_to_code(uint32_t st)
+{
+    if (st & ST_NC_OVERFLOW) return SPH_ERR_NC_OVERFLOW;
+    if (st & ST_OUT_OF_GRID) return SPH_ERR_OUT_OF_GRID;
+    if (st & ST_TIMEOUT) return SPH_ERR_TIMEOUT;
+    if (st & ST_BOND_ALIAS) return SPH_ERR_BOND_ALIAS;
+    return SPH_OK;
+}
+
+const char *status_msg(int code)
+{
+    switch (code) {
+    case SPH_ERR_NC_OVERFLOW: return "a particle has more than 32 contacts (NC overflow)";
+    case SPH_ERR_OUT_OF_GRID:
+        return "one or more particles moved outside the grid; is the time step too large?";
+    case SPH_ERR_TIMEOUT: return "a bounded device wait gave up";
+    case SPH_ERR_BOND_ALIAS: return "a bond broke while nb0 < np: its marker aliases particle nb0";
+    default: return "";
+    }
+}
+
+// ---- device -> host conversion kernels ------------------------------------
+template <typename T>
+__global__ void k_to_user(const T *src, T *dst, const uint32_t *sidx, uint32_t n)
+{
+    const uint32_t u = blockIdx.x * blockDim.x + threadIdx.x;
+    if (u < n) dst[u] = src[sidx[u]];
+}
+
+__global__ void k_rows_to_user(Dev d, uint32_t *contacts, double4 *distmod, double4 *delta_t,
+                               int A)
+{
+    const Params &P = *d.prm;
+    const uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= (uint64_t)P.np * NC) return;
+    const uint32_t u = (uint32_t)(e / NC), i = (uint32_t)(e % NC);
+    const uint32_t s = d.sidx[u];
+    const bool occ = (d.cmask[s] >> i) & 1u;
+    const uint32_t v = d.contacts[(size_t)s * NC + i];
+    if (contacts) contacts[e] = occ ? d.uid[v] : P.np;
+    if (distmod) {
+        double4 o = make_double4(0.0, 0.0, 0.0, 0.0);
+        if (occ) {
+            const ulonglong2 c = d.dmc[s];
+            const uint32_t code = (uint32_t)((i < 16 ? (c.x >> (4 * i)) : (c.y >> (4 * (i - 16)))) & 0xFull);
+            const d3 dm = decode_dm(code, P);
+            o = make_double4(dm.x, dm.y, dm.z, d.xr[A][v].w);
+        }
+        distmod[e] = o;
+    }
+    if (delta_t) delta_t[e] = d.delta_t[(size_t)s * NC + i];
+}
+
+__global__ void k_cells_out(Dev d, uint32_t *cell_sorted, uint32_t *perm, uint32_t *cstart,
+                            uint32_t *cend)
+{
+    const Params &P = *d.prm;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < P.ncells) {
+        const uint32_t b = d.cell_start[i], e = d.cell_start[i + 1];
+        cstart[i] = (b == e) ? 0xffffffffu : b;
+        cend[i] = (b == e) ? 0u : e;
+        for (uint32_t k = b; k < e; ++k) cell_sorted[k] = i;
+    }
+    if (i == P.ncells) {
+        for (uint32_t k = d.cell_start[i]; k < d.cell_start[i + 1]; ++k) cell_sorted[k] = 0xffffffffu;
+    }
+    if (i < P.np) perm[i] = d.uid[d.cellorder[i]];
+}
+
+__global__ void k_count_contacts(const uint32_t *cmask, uint32_t np, unsigned long long *out)
+{
+    uint32_t acc = 0;
+    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < np; s += gridDim.x * blockDim.x)
+        acc += __popc(cmask[s]);
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31u) == 0 && acc) atomicAdd(out, (unsigned long long)acc);
+}
+
+int sync_status(sph_ctx *c)
+{
+    CK(cudaStreamSynchronize(c->stream));
+    uint32_t st = 0;
+    CK(cudaMemcpy(&st, c->d.status, sizeof(st), cudaMemcpyDeviceToHost));
+    const int code = status_to_code(st);
+    if (code != SPH_OK) return fail(c, code, status_msg(code));
+    return SPH_OK;
+}
+
+void enqueue_one_step(sph_ctx *c, int a, int write_outputs, cudaStream_t st)
+{
+    launch_rebuild(c->d, c->hp.np, c->hp.ncells, st);
+    launch_bonds(c->d, c->hp.nb0, a, st);
+    launch_step(c->d, c->hp.np, a, write_outputs, st);
+    launch_walls(c->d, c->hp.np, c->hp.nw, st);
+}
+
+int capture(sph_ctx *c, cudaGraphExec_t *out, int a, int nsteps, int write_last)
+{
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    int aa = a;
+    for (int i = 0; i < nsteps; ++i) {
+        enqueue_one_step(c, aa, (write_last && i == nsteps - 1) ? 1 : 0, c->stream);
+        aa ^= 1;
+    }
+    CK(cudaStreamEndCapture(c->stream, &g));
+    cudaError_t e = cudaGraphInstantiate(out, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess)
+        return fail(c, SPH_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+    return SPH_OK;
+}
+
+void drop_graphs(sph_ctx *c)
+{
+    for (auto &g : c->g_multi)
+        if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+    for (auto &row : c->g_single)
+        for (auto &g : row)
+            if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+    c->graphs_for_k = 0;
+}
+
+int ensure_graphs(sph_ctx *c)
+{
+    if (c->graphs_for_k == c->graph_steps && c->g_single[0][0]) return SPH_OK;
+    drop_graphs(c);
+    for (int a = 0; a < 2; ++a) {
+        int rc;
+        if ((rc = capture(c, &c->g_multi[a], a, c->graph_steps, 0)) != SPH_OK) return rc;
+        for (int w = 0; w < 2; ++w)
+            if ((rc = capture(c, &c->g_single[a][w], a, 1, w)) != SPH_OK) return rc;
+    }
+    c->graphs_for_k = c->graph_steps;
+    return SPH_OK;
+}
+
+int do_relayout(sph_ctx *c, cudaStream_t st)
+{
+    // the cell list must describe the current positions before storage follows it
+    launch_rebuild(c->d, c->hp.np, c->hp.ncells, st);
+    relayout(c->d, c->hp.np, c->a, c->scratch, st);
+    CK(cudaGetLastError());
+    c->relayouts++;
+    c->since_relayout = 0;
+    return SPH_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int sph_version(void) { return SPHK_VERSION; }
+
+const char *sph_last_error(const sph_ctx *c) { return c ? c->err.c_str() : "null context"; }
+
+int sph_create(const sph_config *cfg, sph_ctx **out)
+{
+    if (!cfg || !out) return SPH_ERR_BAD_INPUT;
+    sph_ctx *c = new sph_ctx();
+    *out = c;
+    const uint64_t ncells = (uint64_t)cfg->num[0] * cfg->num[1] * cfg->num[2];
+    std::string why;
+    if (cfg->np == 0) why = "np must be positive";
+    else if (cfg->nw > SPHK_MAXWALLS) why = "nw exceeds MAXWALLS (6)";
+    else if (ncells == 0 || ncells >= 0xfffffff0ull) why = "grid.num must be positive and below 2^32 cells";
+    else if (cfg->contactmodel != 2) why = "only contact model 2 (contactLinear) is implemented";
+    else if (!(cfg->dt > 0.0)) why = "dt must be positive";
+    else if ((uint64_t)cfg->np * NC >= 0xffffffffull) why = "np too large";
+    if (!why.empty()) {
+        c->err = why;
+        return SPH_ERR_BAD_INPUT;
+    }
+    c->device = cfg->device;
+    CK(cudaSetDevice(c->device));
+    CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    Params &P = c->hp;
+    P.np = cfg->np; P.nw = cfg->nw; P.nb0 = cfg->nb0; P.contactmodel = cfg->contactmodel;
+    P.periodic = cfg->periodic;
+    double ext = 0.0;
+    for (int k = 0; k < 3; ++k) {
+        P.num[k] = cfg->num[k];
+        P.origo[k] = cfg->origo[k];
+        P.L[k] = cfg->L[k];
+        P.cellsize[k] = cfg->L[k] / (double)cfg->num[k];
+        P.g[k] = cfg->g[k];
+        ext = std::fmax(ext, std::fmax(std::fabs(cfg->origo[k]), std::fabs(cfg->L[k])));
+    }
+    P.ncells = (uint32_t)ncells;
+    P.dt = cfg->dt;
+    P.k_n = cfg->k_n; P.k_t = cfg->k_t; P.k_r = cfg->k_r;
+    P.gamma_n = cfg->gamma_n; P.gamma_t = cfg->gamma_t; P.gamma_r = cfg->gamma_r;
+    P.mu_s = cfg->mu_s; P.mu_d = cfg->mu_d; P.mu_r = cfg->mu_r;
+    P.gamma_wn = cfg->gamma_wn; P.gamma_wt = cfg->gamma_wt;
+    P.mu_ws = cfg->mu_ws; P.mu_wd = cfg->mu_wd; P.rho = cfg->rho;
+    P.kappa = cfg->kappa; P.db = cfg->db; P.V_b = cfg->V_b;
+    P.lambda_bar = cfg->lambda_bar; P.sigma_b = cfg->sigma_b; P.tau_b = cfg->tau_b;
+    P.devs_A = cfg->devs_A; P.devs_f = cfg->devs_f;
+    for (int k = 0; k < MAXWALLS; ++k) P.wmode[k] = cfg->wmode[k];
+    // float rounding of coordinates is below 2^-24 |x|; particles near the
+    // domain stay within a few domain extents, so 1e-6 * 4 * extent is a
+    // generous bound on the cull's absolute error
+    P.cull_eps = (float)(4e-6 * (ext > 0.0 ? ext : 1.0));
+
+    const size_t np = cfg->np;
+    Dev &d = c->d;
+    int rc = SPH_OK;
+#define AL(ptr, n) if ((rc = dalloc(c, &(ptr), (n))) != SPH_OK) return rc;
+    for (int b = 0; b < 2; ++b) {
+        AL(d.xr[b], np); AL(d.vel[b], np); AL(d.angvel[b], np); AL(d.xf[b], np);
+    }
+    AL(d.vel0, np); AL(d.angvel0, np); AL(d.angpos, np); AL(d.xysum, np); AL(d.esv, np);
+    AL(d.force, np); AL(d.torque, np); AL(d.acc, np); AL(d.angacc, np); AL(d.edp, np);
+    AL(d.uid, np); AL(d.sidx, np); AL(d.cell, np);
+    AL(d.contacts, np * NC); AL(d.dmc, np); AL(d.delta_t, np * NC); AL(d.cmask, np);
+    AL(d.cell_start, (size_t)ncells + 2); AL(d.cellorder, np); AL(d.cell_fill, (size_t)ncells + 1);
+    AL(d.scan_tiles, scan_tile_count(P.ncells));
+    AL(d.wf_pp, np); AL(d.wtouch, np); AL(d.wf_partial, div_up(np, 256));
+    AL(d.walls, 1);
+    AL(d.bonds, cfg->nb0); AL(d.bonds_delta, cfg->nb0); AL(d.bonds_omega, cfg->nb0);
+    AL(d.bond_f, cfg->nb0); AL(d.bond_t, cfg->nb0); AL(d.bond_xu, cfg->nb0);
+    AL(d.bond_ptr, np + 1); AL(d.bond_list, 2 * (size_t)cfg->nb0);
+    AL(d.status, 1); AL(d.rebuild, 1); AL(d.prm, 1);
+    c->scratch_bytes = np * NC * sizeof(double4) + np * sizeof(uint32_t) + 256;
+    char *sc = nullptr;
+    AL(sc, c->scratch_bytes);
+    c->scratch = sc;
+#undef AL
+    CK(cudaMemcpy(d.prm, &P, sizeof(Params), cudaMemcpyHostToDevice));
+    return SPH_OK;
+}
+
+int sph_set_option(sph_ctx *c, int option, int64_t value)
+{
+    if (!c) return SPH_ERR_BAD_INPUT;
+    if (option == SPH_OPT_RELAYOUT_EVERY && value >= 0) {
+        c->relayout_every = value;
+        return SPH_OK;
+    }
+    if (option == SPH_OPT_GRAPH_STEPS && value >= 1 && value <= 64) {
+        c->graph_steps = (int)value;
+        return SPH_OK;
+    }
+    return fail(c, SPH_ERR_BAD_INPUT, "unknown option or value");
+}
+
+int sph_upload(sph_ctx *c, const sph_host_state *h)
+{
+    if (!c || !h || !h->x || !h->vel || !h->xysum || !h->force || !h->angpos || !h->angvel ||
+        !h->torque || !h->es_dot || !h->es || !h->ev_dot || !h->ev || !h->p)
+        return fail(c, SPH_ERR_BAD_INPUT, "sph_upload: missing required array");
+    const Params &P = c->hp;
+    if (P.nw > 0 && (!h->walls_nx || !h->walls_mvfd))
+        return fail(c, SPH_ERR_BAD_INPUT, "sph_upload: walls_nx/walls_mvfd required when nw > 0");
+    if (P.nb0 > 0 && (!h->bonds || !h->bonds_delta || !h->bonds_omega))
+        return fail(c, SPH_ERR_BAD_INPUT, "sph_upload: bond arrays required when nb0 > 0");
+    CK(cudaSetDevice(c->device));
+    const size_t np = P.np, nb0 = P.nb0;
+    Dev &d = c->d;
+    const int A = 0;
+    c->a = A;
+    // kinematics (identity storage order for now)
+    std::vector<double> buf(np * 4);
+    std::vector<float> xf(np * 4);
+    CK(cudaMemcpy(d.xr[A], h->x, np * 32, cudaMemcpyHostToDevice));
+    for (size_t i = 0; i < np * 4; ++i) xf[i] = (float)h->x[i];
+    CK(cudaMemcpy(d.xf[A], xf.data(), np * 16, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(d.vel[A], h->vel, np * 32, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(d.vel0, h->vel0 ? h->vel0 : h->vel, np * 32, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(d.angvel[A], h->angvel, np * 32, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(d.angvel0, h->angvel0 ? h->angvel0 : h->angvel, np * 32, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(d.angpos, h->angpos, np * 32, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(d.force, h->force, np * 32, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(d.torque, h->torque, np * 32, cudaMemcpyHostToDevice));
+    if (h->acc) {
+        for (size_t i = 0; i < np; ++i) {
+            for (int k = 0; k < 3; ++k) buf[4 * i + k] = h->acc[4 * i + k];
+            buf[4 * i + 3] = 0.0;
+        }
+        CK(cudaMemcpy(d.acc, buf.data(), np * 32, cudaMemcpyHostToDevice));
+    } else {
+        CK(cudaMemset(d.acc, 0, np * 32));
+    }
+    if (h->angacc) {
+        for (size_t i = 0; i < np; ++i) {
+            for (int k = 0; k < 3; ++k) buf[4 * i + k] = h->angacc[4 * i + k];
+            buf[4 * i + 3] = 0.0;
+        }
+        CK(cudaMemcpy(d.angacc, buf.data(), np * 32, cudaMemcpyHostToDevice));
+    } else {
+        CK(cudaMemset(d.angacc, 0, np * 32));
+    }
+    CK(cudaMemcpy(d.xysum, h->xysum, np * 16, cudaMemcpyHostToDevice));
+    {
+        std::vector<double> esv(np * 2), edp(np * 4);
+        for (size_t i = 0; i < np; ++i) {
+            esv[2 * i] = h->es[i];
+            esv[2 * i + 1] = h->ev[i];
+            edp[4 * i] = h->es_dot[i];
+            edp[4 * i + 1] = h->ev_dot[i];
+            edp[4 * i + 2] = h->p[i];
+            edp[4 * i + 3] = 0.0;
+        }
+        CK(cudaMemcpy(d.esv, esv.data(), np * 16, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(d.edp, edp.data(), np * 32, cudaMemcpyHostToDevice));
+    }
+    {
+        std::vector<uint32_t> ident(np);
+        for (size_t i = 0; i < np; ++i) ident[i] = (uint32_t)i;
+        CK(cudaMemcpy(d.uid, ident.data(), np * 4, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(d.sidx, ident.data(), np * 4, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(d.cellorder, ident.data(), np * 4, cudaMemcpyHostToDevice));
+    }
+    // contact slots: partners, periodic-shift codes, occupancy, history
+    {
+        std::vector<uint32_t> rows(np * NC, (uint32_t)np);
+        std::vector<unsigned long long> dmc(np * 2, 0ull);
+        std::vector<uint32_t> cmask(np, 0u);
+        std::vector<double> dts(np * NC * 4, 0.0);
+        if (h->contacts) {
+            for (size_t i = 0; i < np; ++i) {
+                for (int k = 0; k < NC; ++k) {
+                    const uint32_t v = h->contacts[i * NC + k];
+                    if (v >= np) continue;
+                    rows[i * NC + k] = v;
+                    cmask[i] |= 1u << k;
+                    uint32_t code = 0;
+                    if (h->distmod) {
+                        const double dx = h->distmod[(i * NC + k) * 4];
+                        const double dy = h->distmod[(i * NC + k) * 4 + 1];
+                        if (dx == P.L[0]) code |= 1u; else if (dx == -P.L[0]) code |= 2u;
+                        else if (dx != 0.0) return fail(c, SPH_ERR_BAD_INPUT, "distmod.x must be 0 or +-L[0]");
+                        if (dy == P.L[1]) code |= 4u; else if (dy == -P.L[1]) code |= 8u;
+                        else if (dy != 0.0) return fail(c, SPH_ERR_BAD_INPUT, "distmod.y must be 0 or +-L[1]");
+                    }
+                    dmc[2 * i + (k >> 4)] |= (unsigned long long)code << (4 * (k & 15));
+                    if (h->delta_t)
+                        for (int q = 0; q < 4; ++q) dts[(i * NC + k) * 4 + q] = h->delta_t[(i * NC + k) * 4 + q];
+                }
+            }
+        }
+        CK(cudaMemcpy(d.contacts, rows.data(), np * NC * 4, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(d.dmc, dmc.data(), np * 16, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(d.cmask, cmask.data(), np * 4, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(d.delta_t, dts.data(), np * NC * 32, cudaMemcpyHostToDevice));
+    }
+    // walls
+    {
+        Walls W{};
+        for (uint32_t k = 0; k < P.nw; ++k) {
+            W.nx[k] = make_double4(h->walls_nx[4 * k], h->walls_nx[4 * k + 1], h->walls_nx[4 * k + 2], h->walls_nx[4 * k + 3]);
+            W.mvfd[k] = make_double4(h->walls_mvfd[4 * k], h->walls_mvfd[4 * k + 1], h->walls_mvfd[4 * k + 2], h->walls_mvfd[4 * k + 3]);
+            W.vel0[k] = h->walls_vel0 ? h->walls_vel0[k] : h->walls_mvfd[4 * k + 1];
+        }
+        W.t_current = h->t_current;
+        W.done_blocks = 0;
+        CK(cudaMemcpy(d.walls, &W, sizeof(W), cudaMemcpyHostToDevice));
+    }
+    CK(cudaMemset(d.wf_pp, 0, np * sizeof(double)));
+    CK(cudaMemset(d.wtouch, 0, np));
+    // bonds and their per-particle lists (by user index, in bond order)
+    if (nb0 > 0) {
+        std::vector<uint32_t> ptr(np + 1, 0), list;
+        for (size_t b = 0; b < nb0; ++b) {
+            const uint32_t x = h->bonds[2 * b], y = h->bonds[2 * b + 1];
+            if (y >= np) return fail(c, SPH_ERR_BAD_INPUT, "bond partner index out of range");
+            if (x < np) ptr[x + 1]++;
+            ptr[y + 1]++;
+        }
+        for (size_t i = 0; i < np; ++i) ptr[i + 1] += ptr[i];
+        list.resize(ptr[np]);
+        std::vector<uint32_t> fill(ptr.begin(), ptr.end() - 1);
+        for (size_t b = 0; b < nb0; ++b) {
+            const uint32_t x = h->bonds[2 * b], y = h->bonds[2 * b + 1];
+            if (x < np) list[fill[x]++] = (uint32_t)(b << 1);
+            list[fill[y]++] = (uint32_t)((b << 1) | 1u);
+        }
+        CK(cudaMemcpy(d.bond_ptr, ptr.data(), (np + 1) * 4, cudaMemcpyHostToDevice));
+        if (!list.empty())
+            CK(cudaMemcpy(d.bond_list, list.data(), list.size() * 4, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(d.bonds, h->bonds, nb0 * 8, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(d.bonds_delta, h->bonds_delta, nb0 * 32, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(d.bonds_omega, h->bonds_omega, nb0 * 32, cudaMemcpyHostToDevice));
+    }
+    CK(cudaMemset(d.status, 0, 4));
+    const uint32_t one = 1;
+    CK(cudaMemcpy(d.rebuild, &one, 4, cudaMemcpyHostToDevice));
+    c->sticky = SPH_OK;
+    c->err.clear();
+    c->t_host = h->t_current;
+    c->steps = 0;
+    // cell list of the initial positions, then storage in cell order
+    launch_cell_init(d, P.np, A, c->stream);
+    CK(cudaGetLastError());
+    int rc = do_relayout(c, c->stream);
+    if (rc != SPH_OK) return rc;
+    c->uploaded = true;
+    return sync_status(c);
+}
+
+int sph_step(sph_ctx *c, uint64_t nsteps, void *stream)
+{
+    if (!c || !c->uploaded) return fail(c, SPH_ERR_BAD_INPUT, "sph_step before sph_upload");
+    if (c->sticky != SPH_OK) return c->sticky;
+    if (nsteps == 0) return SPH_OK;
+    CK(cudaSetDevice(c->device));
+    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : c->stream;
+    int rc = ensure_graphs(c);
+    if (rc != SPH_OK) return rc;
+    const uint64_t K = (uint64_t)c->graph_steps;
+    uint64_t i = 0;
+    while (i < nsteps) {
+        if (c->relayout_every > 0 && c->since_relayout >= (uint64_t)c->relayout_every) {
+            if ((rc = do_relayout(c, st)) != SPH_OK) return rc;
+        }
+        uint64_t room = nsteps - i;
+        if (c->relayout_every > 0) {
+            const uint64_t left = (uint64_t)c->relayout_every - c->since_relayout;
+            if (left < room) room = left;
+        }
+        const bool last_chunk = (i + room == nsteps);
+        // multi-step graphs while more than one graph's worth remains
+        while (room > K || (room == K && !last_chunk)) {
+            CK(cudaGraphLaunch(c->g_multi[c->a], st));
+            c->a ^= (int)(K & 1u);
+            room -= K; i += K; c->since_relayout += K; c->steps += K;
+            for (uint64_t k = 0; k < K; ++k) c->t_host += c->hp.dt;
+        }
+        while (room > 0) {
+            const int w = (room == 1 && last_chunk) ? 1 : 0;
+            CK(cudaGraphLaunch(c->g_single[c->a][w], st));
+            c->a ^= 1;
+            room -= 1; i += 1; c->since_relayout += 1; c->steps += 1;
+            c->t_host += c->hp.dt;
+        }
+    }
+    return SPH_OK;
+}
+
+int sph_sync(sph_ctx *c)
+{
+    if (!c) return SPH_ERR_BAD_INPUT;
+    CK(cudaSetDevice(c->device));
+    CK(cudaDeviceSynchronize());
+    if (c->sticky != SPH_OK) return c->sticky;
+    return sync_status(c);
+}
+
+int sph_download(sph_ctx *c, sph_host_state *h)
+{
+    if (!c || !h || !c->uploaded) return fail(c, SPH_ERR_BAD_INPUT, "sph_download: bad arguments");
+    CK(cudaSetDevice(c->device));
+    CK(cudaDeviceSynchronize());
+    const Params &P = c->hp;
+    const uint32_t np = P.np;
+    Dev &d = c->d;
+    const int A = c->a;
+    const unsigned int grid = div_up(np, 256);
+    double4 *t4 = static_cast<double4 *>(c->scratch);
+    auto get4 = [&](const double4 *src, double *dst) -> int {
+        if (!dst) return SPH_OK;
+        k_to_user<double4><<<grid, 256, 0, c->stream>>>(src, t4, d.sidx, np);
+        CK(cudaMemcpyAsync(dst, t4, (size_t)np * 32, cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        return SPH_OK;
+    };
+    int rc;
+    if ((rc = get4(d.xr[A], h->x)) || (rc = get4(d.vel[A], h->vel)) || (rc = get4(d.vel0, h->vel0)) ||
+        (rc = get4(d.acc, h->acc)) || (rc = get4(d.force, h->force)) || (rc = get4(d.angpos, h->angpos)) ||
+        (rc = get4(d.angvel[A], h->angvel)) || (rc = get4(d.angvel0, h->angvel0)) ||
+        (rc = get4(d.angacc, h->angacc)) || (rc = get4(d.torque, h->torque)))
+        return rc;
+    {
+        double2 *t2 = static_cast<double2 *>(c->scratch);
+        std::vector<double> tmp((size_t)np * 2);
+        k_to_user<double2><<<grid, 256, 0, c->stream>>>(d.xysum, t2, d.sidx, np);
+        CK(cudaMemcpyAsync(tmp.data(), t2, (size_t)np * 16, cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        if (h->xysum) memcpy(h->xysum, tmp.data(), (size_t)np * 16);
+        k_to_user<double2><<<grid, 256, 0, c->stream>>>(d.esv, t2, d.sidx, np);
+        CK(cudaMemcpyAsync(tmp.data(), t2, (size_t)np * 16, cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        for (uint32_t i = 0; i < np; ++i) {
+            if (h->es) h->es[i] = tmp[2 * i];
+            if (h->ev) h->ev[i] = tmp[2 * i + 1];
+        }
+        std::vector<double> e4((size_t)np * 4);
+        k_to_user<double4><<<grid, 256, 0, c->stream>>>(d.edp, t4, d.sidx, np);
+        CK(cudaMemcpyAsync(e4.data(), t4, (size_t)np * 32, cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        for (uint32_t i = 0; i < np; ++i) {
+            if (h->es_dot) h->es_dot[i] = e4[4 * i];
+            if (h->ev_dot) h->ev_dot[i] = e4[4 * i + 1];
+            if (h->p) h->p[i] = e4[4 * i + 2];
+        }
+    }
+    if (h->contacts || h->distmod || h->delta_t) {
+        rc = sph_get_contacts(c, h->contacts, h->distmod, h->delta_t);
+        if (rc != SPH_OK) return rc;
+    }
+    if (P.nb0 > 0) {
+        if (h->bonds) CK(cudaMemcpy(h->bonds, d.bonds, (size_t)P.nb0 * 8, cudaMemcpyDeviceToHost));
+        if (h->bonds_delta) CK(cudaMemcpy(h->bonds_delta, d.bonds_delta, (size_t)P.nb0 * 32, cudaMemcpyDeviceToHost));
+        if (h->bonds_omega) CK(cudaMemcpy(h->bonds_omega, d.bonds_omega, (size_t)P.nb0 * 32, cudaMemcpyDeviceToHost));
+    }
+    Walls W{};
+    CK(cudaMemcpy(&W, d.walls, sizeof(W), cudaMemcpyDeviceToHost));
+    for (uint32_t k = 0; k < P.nw; ++k) {
+        if (h->walls_nx) memcpy(&h->walls_nx[4 * k], &W.nx[k], 32);
+        if (h->walls_mvfd) memcpy(&h->walls_mvfd[4 * k], &W.mvfd[k], 32);
+        if (h->walls_vel0) h->walls_vel0[k] = W.vel0[k];
+    }
+    h->t_current = c->t_host;
+    return SPH_OK;
+}
+
+int sph_get_contacts(sph_ctx *c, uint32_t *contacts, double *distmod, double *delta_t)
+{
+    if (!c || !c->uploaded) return fail(c, SPH_ERR_BAD_INPUT, "sph_get_contacts before upload");
+    CK(cudaSetDevice(c->device));
+    CK(cudaDeviceSynchronize());
+    const uint32_t np = c->hp.np;
+    const size_t n = (size_t)np * NC;
+    uint32_t *dc = nullptr;
+    double4 *ddm = nullptr, *ddt = nullptr;
+    CK(cudaMallocAsync(&dc, n * 4, c->stream));
+    CK(cudaMallocAsync(&ddm, n * 32, c->stream));
+    CK(cudaMallocAsync(&ddt, n * 32, c->stream));
+    k_rows_to_user<<<div_up(n, 256), 256, 0, c->stream>>>(c->d, dc, ddm, ddt, c->a);
+    if (contacts) CK(cudaMemcpyAsync(contacts, dc, n * 4, cudaMemcpyDeviceToHost, c->stream));
+    if (distmod) CK(cudaMemcpyAsync(distmod, ddm, n * 32, cudaMemcpyDeviceToHost, c->stream));
+    if (delta_t) CK(cudaMemcpyAsync(delta_t, ddt, n * 32, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaFreeAsync(dc, c->stream));
+    CK(cudaFreeAsync(ddm, c->stream));
+    CK(cudaFreeAsync(ddt, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return SPH_OK;
+}
+
+int sph_get_cells(sph_ctx *c, uint32_t *cell_sorted, uint32_t *perm, uint32_t *cell_start,
+                  uint32_t *cell_end)
+{
+    if (!c || !c->uploaded) return fail(c, SPH_ERR_BAD_INPUT, "sph_get_cells before upload");
+    CK(cudaSetDevice(c->device));
+    CK(cudaDeviceSynchronize());
+    const uint32_t np = c->hp.np, nc = c->hp.ncells;
+    uint32_t *b = nullptr;
+    const size_t words = (size_t)np * 2 + (size_t)nc * 2;
+    CK(cudaMallocAsync(&b, words * 4, c->stream));
+    uint32_t *cs = b, *pm = b + np, *st = b + 2 * (size_t)np, *en = st + nc;
+    const unsigned int n = (np > nc + 1 ? np : nc + 1);
+    k_cells_out<<<div_up(n, 256), 256, 0, c->stream>>>(c->d, cs, pm, st, en);
+    if (cell_sorted) CK(cudaMemcpyAsync(cell_sorted, cs, (size_t)np * 4, cudaMemcpyDeviceToHost, c->stream));
+    if (perm) CK(cudaMemcpyAsync(perm, pm, (size_t)np * 4, cudaMemcpyDeviceToHost, c->stream));
+    if (cell_start) CK(cudaMemcpyAsync(cell_start, st, (size_t)nc * 4, cudaMemcpyDeviceToHost, c->stream));
+    if (cell_end) CK(cudaMemcpyAsync(cell_end, en, (size_t)nc * 4, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaFreeAsync(b, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return SPH_OK;
+}
+
+int sph_get_wall_forces(sph_ctx *c, double *wall0_force)
+{
+    if (!c || !c->uploaded || !wall0_force) return fail(c, SPH_ERR_BAD_INPUT, "bad arguments");
+    CK(cudaSetDevice(c->device));
+    CK(cudaDeviceSynchronize());
+    CK(cudaMemcpy(wall0_force, c->d.wf_pp, (size_t)c->hp.np * 8, cudaMemcpyDeviceToHost));
+    return SPH_OK;
+}
+
+int sph_get_stats(sph_ctx *c, sph_stats *out)
+{
+    if (!c || !out) return SPH_ERR_BAD_INPUT;
+    CK(cudaSetDevice(c->device));
+    memset(out, 0, sizeof(*out));
+    if (c->uploaded) {
+        unsigned long long *cnt = nullptr;
+        CK(cudaMallocAsync(&cnt, 8, c->stream));
+        CK(cudaMemsetAsync(cnt, 0, 8, c->stream));
+        k_count_contacts<<<592, 256, 0, c->stream>>>(c->d.cmask, c->hp.np, cnt);
+        unsigned long long v = 0;
+        CK(cudaMemcpyAsync(&v, cnt, 8, cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaFreeAsync(cnt, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        out->active_contacts = v;
+    }
+    out->steps = c->steps;
+    out->relayouts = c->relayouts;
+    out->device_bytes = c->device_bytes;
+    return SPH_OK;
+}
+
+int sph_relayout(sph_ctx *c)
+{
+    if (!c || !c->uploaded) return fail(c, SPH_ERR_BAD_INPUT, "sph_relayout before upload");
+    CK(cudaSetDevice(c->device));
+    int rc = do_relayout(c, c->stream);
+    if (rc != SPH_OK) return rc;
+    return sync_status(c);
+}
+
+int sph_destroy(sph_ctx *c)
+{
+    if (!c) return SPH_OK;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    drop_graphs(c);
+    for (void *p : c->allocs) cudaFree(p);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return SPH_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,155 @@
+// sphk_internal.cuh -- device-side layout and exact-order arithmetic shared by
+// the kernels of libsphk (the B200 DEM step).
+//
+// Numerics.  Every kernel here must reproduce the reference's double-precision
+// results bit for bit (src/CMakeLists.txt:16-22 builds the reference with
+// --fmad=false).  libsphk is therefore compiled with --fmad=false, and the
+// helpers below keep the operand order of the reference's vector operators
+// (src/vector_arithmetic.h): scalar*vector is (s*a.x, s*a.y, s*a.z),
+// vector*scalar is (a.x*s, ...), dot() sums left to right, and length()
+// narrows the dot product to float and takes a correctly rounded float square
+// root (src/vector_arithmetic.h:317-320).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace sphk {
+
+constexpr int NC = 32;           // contact slots per particle, src/constants.h:24
+constexpr int MAXWALLS = 6;      // src/constants.h:11
+constexpr double REF_PI = 3.14159265358979;   // src/constants.h:14
+
+// device status bits (OR-ed into Ctx::status)
+constexpr uint32_t ST_NC_OVERFLOW = 1u;   // a contact would land past slot NC-1
+constexpr uint32_t ST_OUT_OF_GRID = 2u;   // a cell index fell outside the grid
+constexpr uint32_t ST_BOND_ALIAS = 4u;    // a broken bond's marker aliases a particle
+constexpr uint32_t ST_TIMEOUT = 8u;       // a bounded device wait gave up
+
+struct d3 { double x, y, z; };
+
+__device__ __forceinline__ d3 mk(double x, double y, double z) { return d3{x, y, z}; }
+__device__ __forceinline__ d3 add(d3 a, d3 b) { return mk(a.x + b.x, a.y + b.y, a.z + b.z); }
+__device__ __forceinline__ d3 sub(d3 a, d3 b) { return mk(a.x - b.x, a.y - b.y, a.z - b.z); }
+__device__ __forceinline__ d3 smul(double s, d3 a) { return mk(s * a.x, s * a.y, s * a.z); }
+__device__ __forceinline__ d3 muls(d3 a, double s) { return mk(a.x * s, a.y * s, a.z * s); }
+__device__ __forceinline__ d3 divs(d3 a, double s) { return mk(a.x / s, a.y / s, a.z / s); }
+__device__ __forceinline__ d3 adds(d3 a, double s) { return mk(a.x + s, a.y + s, a.z + s); }
+__device__ __forceinline__ double dot(d3 a, d3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ d3 cross(d3 a, d3 b)
+{
+    return mk(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+// length(): float square root of the narrowed dot product
+__device__ __forceinline__ double flen(d3 a)
+{
+    return (double)__fsqrt_rn(__double2float_rn(dot(a, a)));
+}
+__device__ __forceinline__ double fsqrt_of(double v) { return (double)__fsqrt_rn(__double2float_rn(v)); }
+__device__ __forceinline__ d3 xyz(double4 v) { return mk(v.x, v.y, v.z); }
+
+// Static scene parameters, resident in device memory for the whole run.
+struct Params {
+    uint32_t np, nw, nb0, contactmodel;
+    int32_t periodic;
+    uint32_t num[3];
+    uint32_t ncells;
+    double origo[3], L[3], cellsize[3];   // cellsize = L / num, computed once
+    double dt;
+    double g[3], k_n, k_t, k_r, gamma_n, gamma_t, gamma_r, mu_s, mu_d, mu_r;
+    double gamma_wn, gamma_wt, mu_ws, mu_wd, rho, kappa, db, V_b;
+    double lambda_bar, sigma_b, tau_b, devs_A, devs_f;
+    int32_t wmode[MAXWALLS];
+    float cull_eps;     // absolute FP32 slack of the neighbour cull (metres)
+};
+
+// Wall state (src/datatypes.h:95-100), device resident.
+struct Walls {
+    double4 nx[MAXWALLS];     // normal xyz, position w
+    double4 mvfd[MAXWALLS];   // mass, velocity, force, deviatoric stress
+    double vel0[MAXWALLS];    // half-step velocities
+    double t_current;         // simulation time at the start of the next step
+    uint32_t done_blocks;     // last-block counter of the wall reduction
+    uint32_t pad;
+};
+
+// Device pointers of one simulation.  Per-particle arrays are indexed by the
+// storage index s (particles are kept in cell order); uid[s] is the caller's
+// particle index and sidx[uid] its inverse.  Contact rows store partners as
+// storage indices, np marks an empty slot.
+struct Dev {
+    // double-buffered kinematics read by neighbours: [0]/[1]
+    double4 *xr[2];       // x, y, z, radius
+    double4 *vel[2];      // vx, vy, vz, fixvel
+    double4 *angvel[2];   // wx, wy, wz, (w lane carried)
+    float4 *xf[2];        // float copy of xr for the neighbour cull
+    // private per-particle state (updated in place)
+    double4 *vel0, *angvel0, *angpos;
+    double2 *xysum;
+    double2 *esv;         // es, ev
+    // per-step outputs
+    double4 *force, *torque, *acc, *angacc;
+    double4 *edp;         // es_dot, ev_dot, p, 0
+    uint32_t *uid, *sidx;
+    uint32_t *cell;       // cell id (calcCellID semantics) of the current positions
+    // contacts
+    uint32_t *contacts;   // [np][NC]
+    ulonglong2 *dmc;      // [np] 4-bit periodic shift code of each of the NC slots
+    double4 *delta_t;     // [np][NC]
+    uint32_t *cmask;      // [np] occupied-slot bit mask
+    // cell list (cell order sorted by uid inside each cell)
+    uint32_t *cell_start; // [ncells + 2]
+    uint32_t *cellorder;  // [np]
+    uint32_t *cell_fill;  // [ncells + 1] scratch
+    uint32_t *scan_tiles; // scratch for the scan
+    // walls
+    double *wf_pp;        // [np] wall-0 force by uid
+    uint8_t *wtouch;      // [np] by storage index: wall-0 force was nonzero
+    double *wf_partial;   // [ceil(np/256)]
+    Walls *walls;
+    // bonds (user indices, as the reference stores them)
+    uint2 *bonds;
+    double4 *bonds_delta, *bonds_omega;
+    double4 *bond_f, *bond_t;   // per-bond force on x and torque on y
+    uint32_t *bond_xu;          // user index that received +f this step, or ~0u
+    uint32_t *bond_ptr;         // [np + 1] CSR by uid
+    uint32_t *bond_list;        // [2 nb0] (bond << 1) | role (0: x, 1: y)
+    // status
+    uint32_t *status;
+    uint32_t *rebuild;          // cell list must be rebuilt before the next step
+    Params *prm;
+};
+
+// periodic shift code: bits 0-1 x (1: +L, 2: -L), bits 2-3 y
+__device__ __forceinline__ d3 decode_dm(uint32_t code, const Params &P)
+{
+    // reproduces (0,0,0) += (L,0,0) / -= (L,0,0) etc. of findDistMod
+    double dx = 0.0, dy = 0.0, dz = 0.0;
+    if (code & 1u) { dx = dx + P.L[0]; dy = dy + 0.0; dz = dz + 0.0; }
+    if (code & 2u) { dx = dx - P.L[0]; dy = dy - 0.0; dz = dz - 0.0; }
+    if (code & 4u) { dx = dx + 0.0; dy = dy + P.L[1]; dz = dz + 0.0; }
+    if (code & 8u) { dx = dx - 0.0; dy = dy - P.L[1]; dz = dz - 0.0; }
+    return mk(dx, dy, dz);
+}
+
+// (x - origo) / (L / num), floored (src/sorting.cuh:12-14)
+__device__ __forceinline__ double cell_floor(const Params &P, int d, double v)
+{
+    return floor((v - P.origo[d]) / P.cellsize[d]);
+}
+
+// calcCellID with the device's saturating float->unsigned conversion
+__device__ __forceinline__ uint32_t cell_id(const Params &P, double x, double y, double z)
+{
+    uint32_t ix = __double2uint_rz(cell_floor(P, 0, x));
+    uint32_t iy = __double2uint_rz(cell_floor(P, 1, y));
+    uint32_t iz = __double2uint_rz(cell_floor(P, 2, z));
+    return (iz * P.num[1]) * P.num[0] + iy * P.num[0] + ix;
+}
+
+inline unsigned int div_up(unsigned long long a, unsigned int b)
+{
+    return (unsigned int)((a + b - 1) / b);
+}
+
+}  // namespace sphk

@@ -1,0 +1,442 @@
+// step.cu -- the fused per-particle DEM step of libsphk.
+//
+// One launch performs, for every particle, what the reference does in four
+// kernels (src/device.cu:805-1058):
+//   topology   contact detection into persistent slots, contactsearch.cuh:181-355
+//   interact   contact forces over the slots, then the walls, :369-689
+//   (bonds)    the per-bond forces of bondsLinear (cohesion.cuh:8-233), computed
+//              by bonds.cu and gathered here per particle in bond order
+//   integrate  half-step leapfrog, integration.cuh:9-187
+// It reads the kinematics of step n from buffer A and writes step n+1 to
+// buffer B, so neighbours always see start-of-step values and no particle
+// waits on another.  Particles are stored in cell order, so the 27-cell
+// neighbourhood of a warp is a few contiguous runs of memory.
+//
+// Parity: every expression keeps the reference's operation order; see
+// sphk_internal.cuh.  The neighbour candidates are first culled with a
+// conservative FP32 distance test (Params::cull_eps bounds the float
+// rounding), then the reference's own predicate
+// float_sqrt(dot) - (ra + rb) < 0 decides.
+#include "sphk_internal.cuh"
+
+namespace sphk {
+
+constexpr int STEP_BLOCK = 128;
+
+// contactLinear_wall, src/contactmodels.cuh:10-109
+__device__ __forceinline__ double contact_wall(const Params &P, d3 &F, d3 &T, double &p,
+                                               double ra, double4 vel_a, double4 angvel_a,
+                                               d3 n, double delta, double wvel)
+{
+    const d3 linvel = xyz(vel_a), angvel = xyz(angvel_a);
+    const d3 vel = adds(add(linvel, smul(ra, cross(n, angvel))), wvel);
+    const double vel_n = dot(vel, n);
+    const d3 vel_t = sub(vel, muls(n, dot(vel, n)));
+    const double vel_t_length = flen(vel_t);
+    d3 f_n = smul(-P.k_n * delta - P.gamma_wn * vel_n, n);
+    if (dot(f_n, n) < 0.0f) f_n = mk(0.0, 0.0, 0.0);
+    const double f_n_length = flen(f_n);
+    d3 f_t = mk(0.0, 0.0, 0.0);
+    const d3 T_res = mk(0.0, 0.0, 0.0);
+    if (vel_t_length > 0.f) {
+        const double f_t_visc = P.gamma_wt * vel_t_length;
+        double f_t_limit;
+        if (vel_t_length > 0.001f) f_t_limit = P.mu_wd * f_n_length;
+        else f_t_limit = P.mu_ws * f_n_length;
+        if (f_t_visc < f_t_limit) f_t = divs(smul(-1.0f * f_t_visc, vel_t), vel_t_length);
+        else f_t = divs(smul(-1.0f * f_t_limit, vel_t), vel_t_length);
+    }
+    F = add(F, add(f_n, f_t));
+    T = add(T, add(smul(-ra, cross(n, f_t)), T_res));
+    p += f_n_length / (4.0f * REF_PI * ra * ra);
+    return dot(f_n, n);
+}
+
+// contactLinear, src/contactmodels.cuh:283-493 (contact model 2)
+__device__ __forceinline__ void contact_linear(const Params &P, d3 &F, d3 &T, double &es_dot,
+                                               double &ev_dot, double &p, double4 vel_a,
+                                               d3 angvel_a, double4 vel_b4, double4 angvel_b4,
+                                               double ra, double rb, d3 x, double x_length,
+                                               double delta, double4 &dt4)
+{
+    const double dt = P.dt;
+    const d3 vel_b = xyz(vel_b4), angvel_b = xyz(angvel_b4);
+    const d3 dt0u = xyz(dt4);
+    const d3 n = divs(x, x_length);
+    const d3 vel_linear = mk(vel_a.x - vel_b.x, vel_a.y - vel_b.y, vel_a.z - vel_b.z);
+    const d3 vel = add(add(vel_linear, smul(ra + delta / 2.0, cross(n, angvel_a))),
+                       smul(rb + delta / 2.0, cross(n, angvel_b)));
+    const double vel_n = -dot(vel_linear, n);
+    const d3 vel_t = sub(vel, muls(n, dot(n, vel)));
+    const double vel_t_length = flen(vel_t);
+    const d3 delta_t0 = sub(dt0u, muls(n, dot(n, dt0u)));
+    const double delta_t0_length = flen(delta_t0);
+    d3 delta_t = mk(0.0, 0.0, 0.0);   // the reference leaves it unset when unused
+    d3 f_n = smul(-P.k_n * delta - P.gamma_n * vel_n, n);
+    ev_dot += P.gamma_n * vel_n * vel_n;
+    if (dot(f_n, n) < 0.0f) f_n = mk(0.0, 0.0, 0.0);
+    const double f_n_length = flen(f_n);
+    const d3 f_c = smul(-P.kappa * fsqrt_of(ra * rb), n);
+    d3 f_t = mk(0.0, 0.0, 0.0);
+    if (delta_t0_length > 0.0 || vel_t_length > 0.0) {
+        delta_t = add(delta_t0, muls(vel_t, dt));
+        const d3 f_t_elast = smul(-P.k_t, delta_t);
+        const d3 f_t_visc = smul(-P.gamma_t, vel_t);
+        f_t = add(f_t_elast, f_t_visc);
+        const double f_t_length = flen(f_t);
+        const double f_t_limit = P.mu_s * flen(sub(f_n, f_c));
+        if (f_t_length > f_t_limit) {
+            const d3 t = divs(f_t, flen(f_t));
+            f_t = smul(f_t_limit, t);
+            delta_t = smul(-1.0 / P.k_t,
+                           add(smul(P.mu_d * flen(sub(f_n, f_c)), t), smul(P.gamma_t, vel_t)));
+            es_dot += flen(muls(smul(flen(f_t), vel_t), dt)) / dt;
+        }
+    }
+    F = add(F, add(add(f_n, f_t), f_c));
+    T = add(T, cross(smul(-(ra + delta * 0.5), n), f_t));
+    p += f_n_length / (4.0f * REF_PI * ra * ra);
+    dt4 = make_double4(delta_t.x, delta_t.y, delta_t.z, 0.0f);
+}
+
+__device__ __forceinline__ uint32_t dm_get(unsigned long long lo, unsigned long long hi, int i)
+{
+    return (uint32_t)((i < 16 ? (lo >> (4 * i)) : (hi >> (4 * (i - 16)))) & 0xFull);
+}
+__device__ __forceinline__ void dm_set(unsigned long long &lo, unsigned long long &hi, int i,
+                                       uint32_t code)
+{
+    if (i < 16) {
+        lo = (lo & ~(0xFull << (4 * i))) | ((unsigned long long)code << (4 * i));
+    } else {
+        hi = (hi & ~(0xFull << (4 * (i - 16)))) | ((unsigned long long)code << (4 * (i - 16)));
+    }
+}
+
+struct StepArgs {
+    Dev d;
+    int a;              // read buffer (start of step); the kernel writes buffer 1-a
+    int write_outputs;  // store force/torque/acc/angacc/edp of this step
+};
+
+__global__ void __launch_bounds__(STEP_BLOCK)
+k_step(StepArgs args)
+{
+    __shared__ uint32_t srow[NC * STEP_BLOCK];
+    const Dev &d = args.d;
+    const Params &P = *d.prm;
+    const uint32_t np = P.np;
+    const int tid = threadIdx.x;
+    const uint32_t s = blockIdx.x * STEP_BLOCK + tid;
+    if (s >= np) return;
+    const int A = args.a, B = 1 - args.a;
+    uint32_t err = 0;
+
+    const double4 xa = d.xr[A][s];
+    const double ra = xa.w;
+    const float4 xaf = d.xf[A][s];
+
+    // ---- load the slot row (partners as storage indices) -------------------
+    uint32_t occ = d.cmask[s];
+    const uint32_t occ0 = occ;
+    unsigned long long dm_lo = 0, dm_hi = 0;
+    if (occ) {
+        const uint4 *row = reinterpret_cast<const uint4 *>(d.contacts + (size_t)s * NC);
+#pragma unroll
+        for (int q = 0; q < NC / 4; ++q) {
+            uint4 v = row[q];
+            srow[(4 * q + 0) * STEP_BLOCK + tid] = v.x;
+            srow[(4 * q + 1) * STEP_BLOCK + tid] = v.y;
+            srow[(4 * q + 2) * STEP_BLOCK + tid] = v.z;
+            srow[(4 * q + 3) * STEP_BLOCK + tid] = v.w;
+        }
+        const ulonglong2 c = d.dmc[s];
+        dm_lo = c.x;
+        dm_hi = c.y;
+    }
+    const unsigned long long dm_lo0 = dm_lo, dm_hi0 = dm_hi;
+    bool row_dirty = false;
+
+    // ---- topology: 27-cell sweep, z/y/x order, candidates in uid order ----
+    {
+        int32_t gp[3];
+        gp[0] = __double2int_rz(cell_floor(P, 0, xa.x));
+        gp[1] = __double2int_rz(cell_floor(P, 1, xa.y));
+        gp[2] = __double2int_rz(cell_floor(P, 2, xa.z));
+        const float Lf0 = (float)P.L[0], Lf1 = (float)P.L[1];
+        const float eps = P.cull_eps;
+        int nc = 0;
+        for (int oz = -1; oz < 2; ++oz)
+            for (int oy = -1; oy < 2; ++oy)
+                for (int ox = -1; ox < 2; ++ox) {
+                    int32_t cx = (int32_t)((uint32_t)gp[0] + (uint32_t)ox);
+                    int32_t cy = (int32_t)((uint32_t)gp[1] + (uint32_t)oy);
+                    int32_t cz = (int32_t)((uint32_t)gp[2] + (uint32_t)oz);
+                    uint32_t code = 0;
+                    // findDistMod, src/contactsearch.cuh:12-74
+                    if (P.periodic == 1) {
+                        if (cx < 0) { cx = (int32_t)(P.num[0] - 1); code |= 1u; }
+                        if ((uint32_t)cx == P.num[0]) { cx = 0; code |= 2u; }
+                        if (cy < 0) { cy = (int32_t)(P.num[1] - 1); code |= 4u; }
+                        if ((uint32_t)cy == P.num[1]) { cy = 0; code |= 8u; }
+                    } else if (P.periodic == 2) {
+                        if (cx < 0) { cx = (int32_t)(P.num[0] - 1); code |= 1u; }
+                        if ((uint32_t)cx == P.num[0]) { cx = 0; code |= 2u; }
+                        if (cy < 0 || (uint32_t)cy == P.num[1]) continue;
+                    } else {
+                        if (cx < 0 || (uint32_t)cx == P.num[0]) continue;
+                        if (cy < 0 || (uint32_t)cy == P.num[1]) continue;
+                    }
+                    if (cz < 0 || (uint32_t)cz == P.num[2]) continue;
+                    const uint32_t cid = (uint32_t)cx + (uint32_t)cy * P.num[0]
+                        + (P.num[0] * P.num[1]) * (uint32_t)cz;
+                    if (cid >= P.ncells) { err |= ST_OUT_OF_GRID; continue; }
+                    const uint32_t beg = d.cell_start[cid], end = d.cell_start[cid + 1];
+                    if (beg == end) continue;
+                    const float sx = (code & 1u) ? Lf0 : ((code & 2u) ? -Lf0 : 0.0f);
+                    const float sy = (code & 4u) ? Lf1 : ((code & 8u) ? -Lf1 : 0.0f);
+                    const d3 dm = decode_dm(code, P);
+                    for (uint32_t k = beg; k < end; ++k) {
+                        const uint32_t t = __ldg(&d.cellorder[k]);
+                        if (t == s) continue;
+                        const float4 xbf = __ldg(&d.xf[A][t]);
+                        const float fx = (xaf.x - xbf.x) + sx;
+                        const float fy = (xaf.y - xbf.y) + sy;
+                        const float fz = xaf.z - xbf.z;
+                        const float d2 = __fmaf_rn(fx, fx, __fmaf_rn(fy, fy, fz * fz));
+                        const float rr = (xaf.w + xbf.w) * 1.000004f + eps;
+                        if (d2 >= rr * rr) continue;
+                        const double4 xb = d.xr[A][t];
+                        const d3 xab = add(mk(xa.x - xb.x, xa.y - xb.y, xa.z - xb.z), dm);
+                        const double len = flen(xab);
+                        const double delta = len - (ra + xb.w);
+                        if (!(delta < 0.0f)) continue;
+                        // slot choice, src/contactsearch.cuh:252-271
+                        int cpos = -1;
+                        for (uint32_t m = occ; m; m &= m - 1) {
+                            const int i = __ffs(m) - 1;
+                            if (srow[i * STEP_BLOCK + tid] == t) { cpos = i; break; }
+                        }
+                        if (cpos < 0) {
+                            const uint32_t empty = ~occ;
+                            cpos = empty ? 31 - __clz(empty) : nc;
+                        }
+                        if (cpos < NC) {
+                            if (!((occ >> cpos) & 1u)) {
+                                occ |= 1u << cpos;
+                            }
+                            srow[cpos * STEP_BLOCK + tid] = t;
+                            dm_set(dm_lo, dm_hi, cpos, code);
+                            row_dirty = true;
+                        } else {
+                            err |= ST_NC_OVERFLOW;
+                        }
+                        ++nc;
+                        if (nc > NC) break;
+                    }
+                }
+    }
+
+    // ---- interact: slots in order, then walls ------------------------------
+    const double4 vel_a = d.vel[A][s];
+    const double4 angvel_a4 = d.angvel[A][s];
+    const d3 angvel_a = xyz(angvel_a4);
+    d3 F = mk(0.0, 0.0, 0.0), T = mk(0.0, 0.0, 0.0);
+    double es_dot = 0.0f, ev_dot = 0.0f, p = 0.0f;
+    if (P.contactmodel == 2) {
+        double4 *dtrow = d.delta_t + (size_t)s * NC;
+        for (uint32_t m = occ; m; m &= m - 1) {
+            const int i = __ffs(m) - 1;
+            const uint32_t t = srow[i * STEP_BLOCK + tid];
+            const d3 dm = decode_dm(dm_get(dm_lo, dm_hi, i), P);
+            const double4 xb = d.xr[A][t];
+            const double rb = xb.w;
+            const d3 xab = mk(xa.x - xb.x + dm.x, xa.y - xb.y + dm.y, xa.z - xb.z + dm.z);
+            const double xlen = flen(xab);
+            const double delta_n = xlen - (ra + rb);
+            if (delta_n < 0.0f) {
+                double4 dt4 = dtrow[i];
+                contact_linear(P, F, T, es_dot, ev_dot, p, vel_a, angvel_a, d.vel[A][t],
+                               d.angvel[A][t], ra, rb, xab, xlen, delta_n, dt4);
+                dtrow[i] = dt4;
+            } else {
+                occ &= ~(1u << i);
+                srow[i * STEP_BLOCK + tid] = np;
+                dtrow[i] = make_double4(0.0, 0.0, 0.0, 0.0);
+                row_dirty = true;
+            }
+        }
+    }
+    // walls, src/contactsearch.cuh:578-663 (defaults :416-427)
+    double w0f = 0.0;
+    {
+        const Walls &W = *d.walls;
+        double4 wnx[5] = {make_double4(0.0f, 0.0f, -1.0f, P.L[2]), make_double4(-1.0f, 0.0f, 0.0f, P.L[0]),
+                          make_double4(1.0f, 0.0f, 0.0f, 0.0f), make_double4(0.0f, -1.0f, 0.0f, P.L[1]),
+                          make_double4(0.0f, 1.0f, 0.0f, 0.0f)};
+        double wv[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+        for (int k = 0; k < 5; ++k)
+            if ((uint32_t)k < P.nw) { wnx[k] = W.nx[k]; wv[k] = W.mvfd[k].y; }
+        double dw;
+        dw = wnx[0].w - (xa.z + ra);
+        if (dw < 0.0f) w0f = contact_wall(P, F, T, p, ra, vel_a, angvel_a4, xyz(wnx[0]), dw, wv[0]);
+        dw = xa.z - ra - P.origo[2];
+        if (dw < 0.0f) (void)contact_wall(P, F, T, p, ra, vel_a, angvel_a4, mk(0.0, 0.0, 1.0), dw, 0.0f);
+        if (P.periodic == 0) {
+            dw = wnx[1].w - (xa.x + ra);
+            if (dw < 0.0f) (void)contact_wall(P, F, T, p, ra, vel_a, angvel_a4, xyz(wnx[1]), dw, wv[1]);
+            dw = xa.x - ra - wnx[2].w;
+            if (dw < 0.0f) (void)contact_wall(P, F, T, p, ra, vel_a, angvel_a4, xyz(wnx[2]), dw, wv[2]);
+        }
+        if (P.periodic == 0 || P.periodic == 2) {
+            dw = wnx[3].w - (xa.y + ra);
+            if (dw < 0.0f) (void)contact_wall(P, F, T, p, ra, vel_a, angvel_a4, xyz(wnx[3]), dw, wv[3]);
+            dw = xa.y - ra - wnx[4].w;
+            if (dw < 0.0f) (void)contact_wall(P, F, T, p, ra, vel_a, angvel_a4, xyz(wnx[4]), dw, wv[4]);
+        }
+    }
+
+    // ---- write back the slot row --------------------------------------------
+    if (row_dirty || occ != occ0) {
+        uint4 *row = reinterpret_cast<uint4 *>(d.contacts + (size_t)s * NC);
+#pragma unroll
+        for (int q = 0; q < NC / 4; ++q) {
+            uint4 v;
+            v.x = ((occ >> (4 * q + 0)) & 1u) ? srow[(4 * q + 0) * STEP_BLOCK + tid] : np;
+            v.y = ((occ >> (4 * q + 1)) & 1u) ? srow[(4 * q + 1) * STEP_BLOCK + tid] : np;
+            v.z = ((occ >> (4 * q + 2)) & 1u) ? srow[(4 * q + 2) * STEP_BLOCK + tid] : np;
+            v.w = ((occ >> (4 * q + 3)) & 1u) ? srow[(4 * q + 3) * STEP_BLOCK + tid] : np;
+            row[q] = v;
+        }
+        d.cmask[s] = occ;
+        if (dm_lo != dm_lo0 || dm_hi != dm_hi0)
+            d.dmc[s] = make_ulonglong2(dm_lo, dm_hi);
+    }
+
+    const uint32_t u = d.uid[s];
+    // ---- bonds: per-bond contributions in bond order (bondsLinear's serial
+    // scatter order, cohesion.cuh:220-226) ------------------------------------
+    if (P.nb0 > 0) {
+        const uint32_t e0 = d.bond_ptr[u], e1 = d.bond_ptr[u + 1];
+        for (uint32_t e = e0; e < e1; ++e) {
+            const uint32_t ent = d.bond_list[e];
+            const uint32_t b = ent >> 1;
+            const uint32_t xu = d.bond_xu[b];
+            if (xu == 0xffffffffu) continue;
+            const double4 f = d.bond_f[b];
+            const double4 tj = d.bond_t[b];
+            if ((ent & 1u) == 0u) {
+                if (xu != u) continue;
+                F = mk(F.x + f.x, F.y + f.y, F.z + f.z);
+                T = mk(T.x - tj.x, T.y - tj.y, T.z - tj.z);
+            } else {
+                F = mk(F.x - f.x, F.y - f.y, F.z - f.z);
+                T = mk(T.x + tj.x, T.y + tj.y, T.z + tj.z);
+            }
+        }
+    }
+
+    // ---- outputs of interact ------------------------------------------------
+    const double dt = P.dt;
+    {
+        const double2 e = d.esv[s];
+        d.esv[s] = make_double2(e.x + es_dot * dt, e.y + ev_dot * dt);
+    }
+    if (P.nw > 0) {
+        const uint8_t touched = d.wtouch[s];
+        if (w0f != 0.0 || touched) {
+            d.wf_pp[u] = w0f;
+            d.wtouch[s] = (w0f != 0.0) ? 1 : 0;
+        }
+    }
+
+    // ---- integrate, src/integration.cuh:9-187 -------------------------------
+    double4 x = xa, vel = vel_a, angvel = angvel_a4;
+    double4 angpos = d.angpos[s], vel0 = d.vel0[s], angvel0 = d.angvel0[s];
+    const double radius = x.w;
+    const double m = 4.0 / 3.0 * REF_PI * radius * radius * radius * P.rho;
+    double4 acc, angacc;
+    acc.x = F.x / m;
+    acc.y = F.y / m;
+    acc.z = F.z / m;
+    acc.w = 0.0;
+    angacc.x = T.x * 1.0 / (2.0 / 5.0 * m * radius * radius);
+    angacc.y = T.y * 1.0 / (2.0 / 5.0 * m * radius * radius);
+    angacc.z = T.z * 1.0 / (2.0 / 5.0 * m * radius * radius);
+    angacc.w = 0.0;
+    acc.x += P.g[0];
+    acc.y += P.g[1];
+    acc.z += P.g[2];
+    if (vel.w > 0.0f) {
+        acc.x = 0.0;
+        acc.y = 0.0;
+        acc.z -= P.g[2];
+        angacc = make_double4(0.0f, 0.0f, 0.0f, 0.0f);
+    }
+    if (P.periodic == 1) {
+        if (x.x < P.origo[0]) x.x += P.L[0];
+        if (x.x > P.L[0]) x.x -= P.L[0];
+        if (x.y < P.origo[1]) x.y += P.L[1];
+        if (x.y > P.L[1]) x.y -= P.L[1];
+    } else if (P.periodic == 2) {
+        if (x.x < P.origo[0]) x.x += P.L[0];
+        if (x.x > P.L[0]) x.x -= P.L[0];
+    }
+    vel0.x += acc.x * dt;
+    vel0.y += acc.y * dt;
+    vel0.z += acc.z * dt;
+    angvel0.x += angacc.x * dt;
+    angvel0.y += angacc.y * dt;
+    angvel0.z += angacc.z * dt;
+    x.x += vel0.x * dt;
+    x.y += vel0.y * dt;
+    x.z += vel0.z * dt;
+    angpos.x += angvel0.x * dt;
+    angpos.y += angvel0.y * dt;
+    angpos.z += angvel0.z * dt;
+    vel.x = vel0.x + 0.5 * acc.x * dt;
+    vel.y = vel0.y + 0.5 * acc.y * dt;
+    vel.z = vel0.z + 0.5 * acc.z * dt;
+    angvel.x = angvel0.x + 0.5 * angacc.x * dt;
+    angvel.y = angvel0.y + 0.5 * angacc.y * dt;
+    angvel.z = angvel0.z + 0.5 * angacc.z * dt;
+    double2 xys = make_double2(0.0f, 0.0f);
+    xys.x += vel.x * dt;
+    xys.y += vel.y * dt;
+    {
+        const double2 o = d.xysum[s];
+        d.xysum[s] = make_double2(o.x + xys.x, o.y + xys.y);
+    }
+    d.xr[B][s] = x;
+    d.vel[B][s] = vel;
+    d.angvel[B][s] = angvel;
+    d.xf[B][s] = make_float4((float)x.x, (float)x.y, (float)x.z, (float)x.w);
+    d.vel0[s] = vel0;
+    d.angvel0[s] = angvel0;
+    d.angpos[s] = angpos;
+    if (args.write_outputs) {
+        d.force[s] = make_double4(F.x, F.y, F.z, 0.0f);
+        d.torque[s] = make_double4(T.x, T.y, T.z, 0.0f);
+        d.acc[s] = acc;
+        d.angacc[s] = angacc;
+        d.edp[s] = make_double4(es_dot, ev_dot, p, 0.0);
+    }
+
+    // ---- cell of the new position, for the next step's cell list -----------
+    uint32_t c = cell_id(P, x.x, x.y, x.z);
+    if (c >= P.ncells) { err |= ST_OUT_OF_GRID; c = P.ncells; }
+    if (c != d.cell[s]) {
+        d.cell[s] = c;
+        *d.rebuild = 1u;
+    }
+    if (err) atomicOr(d.status, err);
+}
+
+void launch_step(const Dev &d, uint32_t np, int a, int write_outputs, cudaStream_t st)
+{
+    StepArgs args{d, a, write_outputs};
+    k_step<<<div_up(np, STEP_BLOCK), STEP_BLOCK, 0, st>>>(args);
+}
+
+}  // namespace sphk

@@ -198,10 +198,12 @@ def polydisperse(n=1_000_000, seed=0, L=(0.2, 0.2, 0.4), num=(50, 50, 100),
 
 def bonded(seed=0, nx=40, ny=20, nz=20, r_lo=0.9e-3, r_hi=1.1e-3, pull=0.01,
            sigma_b=2e7, tau_b=2e7, sid="bonded") -> Spherebin:
-    """FCC lattice (spacing 2.1 r_hi) with bonds between nearest lattice
-    neighbours; the first and last x layer move apart at +-pull/2."""
+    """FCC lattice with the nearest-neighbour distance equal to the mean
+    diameter (a close packing: pairs with ri + rj above it overlap), bonds
+    between all pairs closer than 1.05 (ri + rj); the first and last x layer
+    move apart at +-pull/2."""
     rng = np.random.default_rng(seed)
-    a = 2.1 * r_hi * math.sqrt(2.0)   # cubic FCC cell edge, neighbour distance 2.1 r_hi
+    a = (r_lo + r_hi) * math.sqrt(2.0)   # cubic FCC cell edge; neighbour distance r_lo + r_hi
     basis = np.array([[0, 0, 0], [0.5, 0.5, 0], [0.5, 0, 0.5], [0, 0.5, 0.5]])
     cells = np.stack(np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij"),
                      axis=-1).reshape(-1, 3)
@@ -299,7 +301,7 @@ def collision(n=2000, seed=0, periodic=0, box=(0.06, 0.06, 0.06), r=(0.8e-3, 1.6
     _contact_params(sb, k_n=k_n, k_t=k_t, gamma_n=gamma_n, gamma_t=gamma_t, mu=mu, gamma_w=0.05)
     if nw:
         sb.wmode = np.ones(nw, dtype=np.int32)
-        sb.w_x = np.array([float(np.max(sb.x[:, 2] + sb.radius)) + 0.2e-3] + [0.0] * (nw - 1))[:nw]
+        sb.w_x = np.array([float(np.max(sb.x[:, 2] + sb.radius)) - 0.05e-3] + [0.0] * (nw - 1))[:nw]
         sb.w_m = np.full(nw, 1e-3)
         sb.w_devs = np.full(nw, 50.0)
     sb.time_dt = dt

@@ -1,0 +1,256 @@
+"""ctypes binding of libsphk (include/sphk.h) and the host-side ``Simulation``.
+
+``Simulation`` is the in-process counterpart of what the reference's ``DEM``
+object does between ``readbin`` and ``writebin`` (``src/sphere.h:244-273``):
+it owns one device context, uploads a ``HostState`` in the reference's host
+layout, runs time steps on the GPU and downloads the state.  There is no
+CPU fallback: constructing a ``Simulation`` without the built library or
+without a CUDA device raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import re
+from pathlib import Path
+
+import numpy as np
+
+from .state import NC, HostState, SceneConfig
+
+PKG = Path(__file__).resolve().parent
+LIB_PATH = PKG / "lib" / "libsphk.so"
+HEADER = PKG.parent / "include" / "sphk.h"
+
+SPH_OK = 0
+ERRORS = {
+    -1: "SPH_ERR_CUDA", -2: "SPH_ERR_NC_OVERFLOW", -3: "SPH_ERR_OUT_OF_GRID",
+    -4: "SPH_ERR_TIMEOUT", -5: "SPH_ERR_BAD_INPUT", -6: "SPH_ERR_BOND_ALIAS", -7: "SPH_ERR_NOMEM",
+}
+OPT_RELAYOUT_EVERY = 1
+OPT_GRAPH_STEPS = 2
+
+_dp = C.POINTER(C.c_double)
+_up = C.POINTER(C.c_uint32)
+
+
+class SphConfig(C.Structure):
+    _fields_ = [
+        ("np", C.c_uint32), ("nw", C.c_uint32), ("nb0", C.c_uint32), ("contactmodel", C.c_uint32),
+        ("periodic", C.c_int32), ("num", C.c_uint32 * 3),
+        ("origo", C.c_double * 3), ("L", C.c_double * 3), ("dt", C.c_double),
+        ("g", C.c_double * 3),
+        ("k_n", C.c_double), ("k_t", C.c_double), ("k_r", C.c_double),
+        ("gamma_n", C.c_double), ("gamma_t", C.c_double), ("gamma_r", C.c_double),
+        ("mu_s", C.c_double), ("mu_d", C.c_double), ("mu_r", C.c_double),
+        ("gamma_wn", C.c_double), ("gamma_wt", C.c_double), ("mu_ws", C.c_double),
+        ("mu_wd", C.c_double), ("rho", C.c_double), ("kappa", C.c_double), ("db", C.c_double),
+        ("V_b", C.c_double), ("lambda_bar", C.c_double), ("sigma_b", C.c_double),
+        ("tau_b", C.c_double), ("devs_A", C.c_double), ("devs_f", C.c_double),
+        ("wmode", C.c_int32 * 6), ("device", C.c_int32),
+    ]
+
+
+class SphHostState(C.Structure):
+    _fields_ = [(n, _dp) for n in ("x", "xysum", "vel", "vel0", "acc", "force", "angpos", "angvel",
+                                   "angvel0", "angacc", "torque", "es_dot", "es", "ev_dot", "ev", "p")]
+    _fields_ += [("contacts", _up), ("distmod", _dp), ("delta_t", _dp), ("bonds", _up),
+                 ("bonds_delta", _dp), ("bonds_omega", _dp), ("walls_nx", _dp), ("walls_mvfd", _dp),
+                 ("walls_vel0", _dp), ("t_current", C.c_double)]
+
+
+class SphStats(C.Structure):
+    _fields_ = [("active_contacts", C.c_uint64), ("steps", C.c_uint64),
+                ("relayouts", C.c_uint64), ("device_bytes", C.c_uint64)]
+
+
+class SphError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+_lib = None
+
+
+def exported_symbols():
+    """Function names declared in include/sphk.h."""
+    return re.findall(r"^\s*(?:int|const char \*)\s*(sph_\w+)\s*\(", HEADER.read_text(), re.M)
+
+
+def load_library(path: os.PathLike | None = None):
+    """Load libsphk.so; raises if it has not been built (no fallback)."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = Path(path) if path else LIB_PATH
+    if not p.exists():
+        raise FileNotFoundError(f"{p} is not built; run `python -m sphere_b200.build`")
+    lib = C.CDLL(str(p))
+    vp = C.c_void_p
+    sig = {
+        "sph_version": ([], C.c_int),
+        "sph_create": ([C.POINTER(SphConfig), C.POINTER(vp)], C.c_int),
+        "sph_set_option": ([vp, C.c_int, C.c_int64], C.c_int),
+        "sph_upload": ([vp, C.POINTER(SphHostState)], C.c_int),
+        "sph_step": ([vp, C.c_uint64, vp], C.c_int),
+        "sph_sync": ([vp], C.c_int),
+        "sph_download": ([vp, C.POINTER(SphHostState)], C.c_int),
+        "sph_get_contacts": ([vp, _up, _dp, _dp], C.c_int),
+        "sph_get_cells": ([vp, _up, _up, _up, _up], C.c_int),
+        "sph_get_wall_forces": ([vp, _dp], C.c_int),
+        "sph_get_stats": ([vp, C.POINTER(SphStats)], C.c_int),
+        "sph_relayout": ([vp], C.c_int),
+        "sph_last_error": ([vp], C.c_char_p),
+        "sph_destroy": ([vp], C.c_int),
+    }
+    for name, (args, res) in sig.items():
+        f = getattr(lib, name)
+        f.argtypes = args
+        f.restype = res
+    if path is None:
+        _lib = lib
+    return lib
+
+
+def make_config(cfg: SceneConfig, device: int = 0) -> SphConfig:
+    c = SphConfig()
+    c.np, c.nw, c.nb0, c.contactmodel = cfg.np, cfg.nw, cfg.nb0, cfg.contactmodel
+    c.periodic = cfg.periodic
+    c.num[:] = [int(v) for v in cfg.num]
+    c.origo[:] = [float(v) for v in cfg.origo]
+    c.L[:] = [float(v) for v in cfg.L]
+    c.dt = cfg.dt
+    c.g[:] = [float(v) for v in cfg.g]
+    for k, v in cfg.params.items():
+        setattr(c, k, float(v))
+    c.wmode[:] = [int(v) for v in cfg.wmode]
+    c.device = int(device)
+    return c
+
+
+def _ptr(a, dtype, keep):
+    if a is None:
+        return None
+    assert a.dtype == dtype and a.flags.c_contiguous, (a.dtype, a.flags.c_contiguous)
+    if a.size == 0:
+        a = np.zeros(1, dtype)
+        keep.append(a)
+    return a.ctypes.data_as(_dp if dtype == np.float64 else _up)
+
+
+def _host_struct(st: HostState, keep) -> SphHostState:
+    h = SphHostState()
+    for n in ("x", "xysum", "vel", "vel0", "acc", "force", "angpos", "angvel", "angvel0", "angacc",
+              "torque", "es_dot", "es", "ev_dot", "ev", "p", "distmod", "delta_t", "bonds_delta",
+              "bonds_omega", "walls_nx", "walls_mvfd", "walls_vel0"):
+        setattr(h, n, _ptr(getattr(st, n), np.float64, keep))
+    h.contacts = _ptr(st.contacts, np.uint32, keep)
+    h.bonds = _ptr(st.bonds, np.uint32, keep)
+    h.t_current = float(st.t_current)
+    return h
+
+
+class Simulation:
+    """One DEM simulation resident on a GPU."""
+
+    def __init__(self, cfg: SceneConfig, device: int = 0, graph_steps: int | None = None,
+                 relayout_every: int | None = None):
+        self.lib = load_library()
+        self.cfg = cfg
+        self._ctx = C.c_void_p()
+        conf = make_config(cfg, device)
+        rc = self.lib.sph_create(C.byref(conf), C.byref(self._ctx))
+        self._check(rc)
+        if graph_steps is not None:
+            self._check(self.lib.sph_set_option(self._ctx, OPT_GRAPH_STEPS, int(graph_steps)))
+        if relayout_every is not None:
+            self._check(self.lib.sph_set_option(self._ctx, OPT_RELAYOUT_EVERY, int(relayout_every)))
+
+    def _check(self, rc):
+        if rc != SPH_OK:
+            msg = self.lib.sph_last_error(self._ctx) if self._ctx else b""
+            raise SphError(rc, (msg or b"").decode())
+
+    def upload(self, st: HostState):
+        keep = []
+        h = _host_struct(st, keep)
+        self._check(self.lib.sph_upload(self._ctx, C.byref(h)))
+
+    def step(self, nsteps: int, stream=None):
+        """Enqueue nsteps steps (asynchronous); ``stream`` is a raw cudaStream_t."""
+        s = C.c_void_p(stream) if stream else None
+        self._check(self.lib.sph_step(self._ctx, int(nsteps), s))
+
+    def sync(self):
+        self._check(self.lib.sph_sync(self._ctx))
+
+    def download(self, st: HostState | None = None) -> HostState:
+        if st is None:
+            st = empty_state(self.cfg)
+        keep = []
+        h = _host_struct(st, keep)
+        self._check(self.lib.sph_download(self._ctx, C.byref(h)))
+        st.t_current = h.t_current
+        return st
+
+    def contacts(self):
+        n = self.cfg.np
+        c = np.zeros((n, NC), np.uint32)
+        dm = np.zeros((n, NC, 4))
+        dt = np.zeros((n, NC, 4))
+        self._check(self.lib.sph_get_contacts(self._ctx, c.ctypes.data_as(_up),
+                                              dm.ctypes.data_as(_dp), dt.ctypes.data_as(_dp)))
+        return c, dm, dt
+
+    def cells(self):
+        n, ncell = self.cfg.np, self.cfg.ncells
+        cs = np.zeros(n, np.uint32)
+        pm = np.zeros(n, np.uint32)
+        st = np.zeros(ncell, np.uint32)
+        en = np.zeros(ncell, np.uint32)
+        self._check(self.lib.sph_get_cells(self._ctx, *(a.ctypes.data_as(_up) for a in (cs, pm, st, en))))
+        return cs, pm, st, en
+
+    def wall_forces(self):
+        out = np.zeros(self.cfg.np)
+        self._check(self.lib.sph_get_wall_forces(self._ctx, out.ctypes.data_as(_dp)))
+        return out
+
+    def stats(self) -> dict:
+        s = SphStats()
+        self._check(self.lib.sph_get_stats(self._ctx, C.byref(s)))
+        return {k: int(getattr(s, k)) for k, _ in SphStats._fields_}
+
+    def relayout(self):
+        self._check(self.lib.sph_relayout(self._ctx))
+
+    def close(self):
+        if self._ctx:
+            self.lib.sph_destroy(self._ctx)
+            self._ctx = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+def empty_state(cfg: SceneConfig) -> HostState:
+    n, nw, nb0 = cfg.np, cfg.nw, cfg.nb0
+    z4 = lambda: np.zeros((n, 4))
+    return HostState(x=z4(), xysum=np.zeros((n, 2)), vel=z4(), vel0=z4(), acc=z4(), force=z4(),
+                     angpos=z4(), angvel=z4(), angvel0=z4(), angacc=z4(), torque=z4(),
+                     es_dot=np.zeros(n), es=np.zeros(n), ev_dot=np.zeros(n), ev=np.zeros(n),
+                     p=np.zeros(n), contacts=np.zeros((n, NC), np.uint32),
+                     distmod=np.zeros((n, NC, 4)), delta_t=np.zeros((n, NC, 4)),
+                     bonds=np.zeros((nb0, 2), np.uint32), bonds_delta=np.zeros((nb0, 4)),
+                     bonds_omega=np.zeros((nb0, 4)), walls_nx=np.zeros((nw, 4)),
+                     walls_mvfd=np.zeros((nw, 4)), walls_vel0=np.zeros(nw))

@@ -1,0 +1,151 @@
+"""Parity of the CUDA path (libsphk through its C ABI) with the CPU oracle
+and with the golden fixtures made from the reference's own kernels.
+
+The bar is bit-exactness for everything: cell ids, permutation, contact
+slots, tangential history, forces, positions and walls.  Scenes are small
+enough for the oracle to finish in seconds."""
+import json
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from helpers import (BOND_FIELDS, OUTPUT_FIELDS, STATE_FIELDS, WALL_FIELDS, active_distmod,
+                     mismatches, run_oracle)
+from sphere_b200 import scenes
+from sphere_b200.spherebin import readbin
+from sphere_b200.sphk import SphError, Simulation
+from sphere_b200.state import config_from_spherebin, state_from_spherebin
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = Path(__file__).resolve().parent / "golden"
+ALL = STATE_FIELDS + OUTPUT_FIELDS + ("acc", "angacc", "contacts", "delta_t") + WALL_FIELDS
+
+SCENES = {
+    "box": lambda: scenes.collision(n=1500, seed=31, periodic=0),
+    "periodic_xy": lambda: scenes.collision(n=1500, seed=32, periodic=1),
+    "periodic_x_wall": lambda: scenes.collision(n=1200, seed=33, periodic=2, nw=1),
+    "box_wall": lambda: scenes.collision(n=2000, seed=34, periodic=0, nw=1),
+    "bonded": lambda: scenes.bonded(nx=4, ny=3, nz=3, sigma_b=1e30, tau_b=1e30),
+}
+
+
+def run_gpu(sb, chunks, **kw):
+    cfg = config_from_spherebin(sb)
+    with Simulation(cfg, **kw) as sim:
+        sim.upload(state_from_spherebin(sb))
+        for n in chunks:
+            sim.step(n)
+        sim.sync()
+        st = sim.download()
+        cells = sim.cells()
+        stats = sim.stats()
+    return st, cells, stats
+
+
+@pytest.mark.parametrize("name", sorted(SCENES))
+@pytest.mark.parametrize("chunks", [(40,), (1, 7, 13, 19)], ids=["one_call", "four_calls"])
+def test_gpu_matches_oracle_bit_for_bit(oracle_libs, name, chunks):
+    sb = SCENES[name]()
+    rc, want, orun = run_oracle(oracle_libs["orc"], sb, sum(chunks))
+    assert rc == 0
+    got, (cell_sorted, perm, cstart, cend), stats = run_gpu(sb, chunks)
+    fields = ALL + (BOND_FIELDS if sb.nb0 else ())
+    assert mismatches(got, want, fields) == []
+    assert np.array_equal(active_distmod(got, sb.np), active_distmod(want, sb.np))
+    assert got.t_current == want.t_current
+    # the cell list of the last step: cell ids, permutation, start/end
+    assert np.array_equal(perm, orun.perm)
+    assert np.array_equal(cell_sorted, orun.cell_sorted)
+    assert np.array_equal(cstart, orun.cell_start)
+    occ = orun.cell_start != 0xFFFFFFFF
+    assert np.array_equal(cend[occ], orun.cell_end[occ])
+    assert stats["active_contacts"] == int((want.contacts != sb.np).sum())
+
+
+def _golden_cases():
+    idx = GOLDEN / "index.json"
+    return json.loads(idx.read_text())["cases"] if idx.exists() else []
+
+
+@pytest.mark.parametrize("case", _golden_cases(), ids=lambda c: c["name"])
+def test_gpu_matches_golden_fixtures(case):
+    sb = readbin(GOLDEN / case["input"])
+    want = np.load(GOLDEN / case["expected"])
+    steps = case["steps"]
+    got, (_, perm, _, _), _ = run_gpu(sb, (steps,))
+    for f in want.files:
+        if f == "perm":
+            value = perm
+        elif f == "delta_t_active":
+            value = got.delta_t[got.contacts != sb.np]
+        else:
+            value = getattr(got, f)
+        assert np.asarray(value).tobytes() == want[f].tobytes(), f
+
+
+def test_relayout_does_not_change_results(oracle_libs):
+    sb = scenes.collision(n=1500, seed=41, periodic=1)
+    a, _, _ = run_gpu(sb, (30,))
+    b, _, stats = run_gpu(sb, (30,), relayout_every=4)
+    assert stats["relayouts"] >= 7
+    assert mismatches(a, b, ALL) == []
+
+
+@pytest.mark.parametrize("graph_steps", [1, 3, 16])
+def test_graph_batching_does_not_change_results(graph_steps):
+    sb = scenes.collision(n=800, seed=42, periodic=0, nw=1)
+    a, _, _ = run_gpu(sb, (37,), graph_steps=8)
+    b, _, _ = run_gpu(sb, (37,), graph_steps=graph_steps)
+    assert mismatches(a, b, ALL) == []
+
+
+def test_null_step_known_answer():
+    """tests/io_tests.py:27-33: with no gravity and no contacts the state after
+    the run is identical to the input except for the time fields."""
+    sb = readbin(GOLDEN / "io_null_step.bin")
+    got, _, _ = run_gpu(sb, (3,))
+    st0 = state_from_spherebin(sb)
+    for f in ("x", "vel", "angvel", "angpos", "xysum", "es", "ev", "walls_nx", "walls_mvfd"):
+        assert np.array_equal(getattr(got, f), getattr(st0, f)), f
+
+
+def test_nc_overflow_is_reported(oracle_libs):
+    """A large sphere overlapped by more than 32 small ones: the reference
+    writes past the slot row; here the step reports SPH_ERR_NC_OVERFLOW."""
+    from sphere_b200.spherebin import Spherebin
+    rng = np.random.default_rng(5)
+    n_small = 40
+    sb = Spherebin(np_=n_small + 1, nw=0, sid="overflow")
+    dirs = rng.normal(size=(n_small, 3))
+    dirs /= np.linalg.norm(dirs, axis=1)[:, None]
+    center = np.array([0.05, 0.05, 0.05])
+    sb.x = np.vstack([center, center + dirs * 0.0108])
+    sb.radius = np.concatenate([[0.01], np.full(n_small, 1e-3)])
+    sb.origo = np.zeros(3)
+    sb.L = np.full(3, 0.1)
+    sb.num = np.array([4, 4, 4], dtype=np.uint32)
+    sb.k_n = sb.k_t = 1e3
+    sb.time_dt = 1e-6
+    rc, _, _ = run_oracle(oracle_libs["orc"], sb, 1)
+    assert rc & 1
+    cfg = config_from_spherebin(sb)
+    with Simulation(cfg) as sim:
+        sim.upload(state_from_spherebin(sb))
+        sim.step(1)
+        with pytest.raises(SphError) as e:
+            sim.sync()
+        assert e.value.code == -2
+
+
+def test_out_of_grid_is_reported():
+    sb = scenes.collision(n=64, seed=6, periodic=0)
+    sb.vel[0] = [0.0, 0.0, 500.0]      # leaves the grid within a few steps
+    cfg = config_from_spherebin(sb)
+    with Simulation(cfg) as sim:
+        sim.upload(state_from_spherebin(sb))
+        sim.step(200)
+        with pytest.raises(SphError) as e:
+            sim.sync()
+        assert e.value.code == -3

@@ -1,0 +1,94 @@
+"""Pin the plain-C oracle (oracle/dem_oracle.c) to the reference's own kernel
+bodies (oracle/_ref/libref.so) and to the committed golden fixtures."""
+import json
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import pyoracle
+from helpers import BOND_FIELDS, OUTPUT_FIELDS, STATE_FIELDS, WALL_FIELDS, mismatches, run_oracle
+from sphere_b200 import scenes
+from sphere_b200.spherebin import readbin
+from sphere_b200.state import config_from_spherebin, state_from_spherebin
+
+GOLDEN = Path(__file__).resolve().parent / "golden"
+ALL = STATE_FIELDS + OUTPUT_FIELDS + ("acc", "angacc", "contacts", "delta_t") + WALL_FIELDS
+
+SCENES = {
+    "box": lambda: scenes.collision(n=1200, seed=11, periodic=0),
+    "periodic_xy": lambda: scenes.collision(n=1200, seed=12, periodic=1),
+    "periodic_x_wall": lambda: scenes.collision(n=1000, seed=13, periodic=2, nw=1),
+    "box_wall": lambda: scenes.collision(n=1500, seed=14, periodic=0, nw=1),
+    "bonded": lambda: scenes.bonded(nx=4, ny=3, nz=3, sigma_b=1e30, tau_b=1e30),
+}
+
+
+def _need_ref(oracle_libs):
+    if "ref" not in oracle_libs:
+        pytest.skip("reference harness not built (reference checkout absent)")
+
+
+@pytest.mark.parametrize("name", sorted(SCENES))
+def test_restatement_matches_reference_kernels(oracle_libs, name):
+    _need_ref(oracle_libs)
+    sb = SCENES[name]()
+    rc1, a, ra = run_oracle(oracle_libs["orc"], sb, 40, nthreads=4)
+    rc2, b, rb = run_oracle(oracle_libs["ref"], sb, 40, nthreads=4)
+    assert rc1 == 0 and rc2 == 0
+    fields = ALL + (BOND_FIELDS if sb.nb0 else ())
+    assert mismatches(a, b, fields) == []
+    assert np.array_equal(ra.perm, rb.perm)
+    assert np.array_equal(ra.cell_sorted, rb.cell_sorted)
+    assert np.array_equal(ra.cell_start, rb.cell_start)
+    occupied = ra.cell_start != 0xFFFFFFFF
+    assert np.array_equal(ra.cell_end[occupied], rb.cell_end[occupied])
+    # the scene exercised what it is meant to: contacts with slip, or bonds
+    if sb.nb0:
+        assert np.count_nonzero(a.bonds_delta) > 0
+    else:
+        assert (a.contacts != sb.np).sum() > 100
+        assert np.count_nonzero(a.es_dot) > 0
+
+
+def test_threaded_block_summation_equals_ordered_form(oracle_libs):
+    """The reference's summation() run with real 256-thread blocks gives the
+    same wall force as the harness's order-equivalent evaluation."""
+    _need_ref(oracle_libs)
+    lib = oracle_libs["ref"]
+    sb = scenes.collision(n=700, seed=21, periodic=0, nw=1)
+    lib.orc_set_threaded_summation_max.argtypes = [pyoracle.C.c_uint]
+    lib.orc_set_threaded_summation_max(0)
+    _, a, _ = run_oracle(lib, sb, 3)
+    lib.orc_set_threaded_summation_max(1 << 30)
+    try:
+        _, b, _ = run_oracle(lib, sb, 3)
+    finally:
+        lib.orc_set_threaded_summation_max(0)
+    assert np.any(a.walls_mvfd[:, 2] != 0.0)
+    assert mismatches(a, b, WALL_FIELDS + ("x",)) == []
+
+
+def _golden_cases():
+    idx = GOLDEN / "index.json"
+    if not idx.exists():
+        return []
+    return json.loads(idx.read_text())["cases"]
+
+
+@pytest.mark.parametrize("case", _golden_cases(), ids=lambda c: c["name"])
+def test_oracle_matches_golden_fixtures(oracle_libs, case):
+    sb = readbin(GOLDEN / case["input"])
+    want = np.load(GOLDEN / case["expected"])
+    rc, st, run = run_oracle(oracle_libs["orc"], sb, case["steps"])
+    assert rc == 0
+    for f in want.files:
+        if f == "perm":
+            got = run.perm
+        elif f == "contacts_active":
+            got = st.contacts != sb.np
+        elif f == "delta_t_active":
+            got = st.delta_t[st.contacts != sb.np]
+        else:
+            got = getattr(st, f)
+        assert np.array_equal(np.asarray(got), want[f]), f
