@@ -1,0 +1,355 @@
+#!/usr/bin/env python
+"""Throughput of the sphere DEM time step on B200.
+
+Metric: particle-steps/s of the FP64 DEM step (contact search, contact and
+wall forces, integration, wall update) on the 1,000,000-sphere polydisperse
+workload: log-normal radii (median 1 mm, sigma 0.2, clipped 0.5-2 mm), random
+sequential placement in a periodic-x/y 0.2 x 0.2 x 0.4 m domain, top wall at
+20 kPa, dt = 2e-7 s, grid 50 x 50 x 100 (seeded synthetic input; no dataset).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl sphk|reference]
+
+A step is one time step of the whole scene.  ``value`` is device-timed
+throughput with the state resident in HBM (CUDA events on the launching
+stream around exactly K steps; the ~1.5 GB state exceeds the 126 MB L2, so no
+flush is needed).  ``e2e`` is the same metric through the C ABI with host
+buffers: upload of the pinned host state, K steps, download of the state.
+With N > 1 every rank runs an independent replica (own seed): the DEM step of
+one scene has no cross-rank exchange here, so scaling is weak and no
+collective sits on the data path; timing is the max over ranks.
+``--impl reference`` times the reference's own kernel bodies (oracle/_ref,
+compiled as host C++) on the host cores over a bounded sample of the same
+workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "particle-steps/s at 1M FP64 spheres"
+UNIT = "particle-steps/s"
+WORKLOAD = ("polydisperse settling: 1,000,000 log-normal spheres (median 1 mm, sigma 0.2, "
+            "0.5-2 mm), RSA in periodic-x/y 0.2x0.2x0.4 m, 20 kPa top wall, FP64, dt 2e-7 s, "
+            "grid 50x50x100, contact model 2")
+
+
+def parse():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=50)
+    ap.add_argument("--impl", choices=("sphk", "reference"), default="sphk")
+    ap.add_argument("--n", type=int, default=1_000_000, help="particles (default: the 1M workload)")
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0,
+                    help="bound on the timed CPU-baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def scene(n: int, seed: int):
+    from sphere_b200 import scenes
+    if n == 1_000_000:
+        return scenes.polydisperse(seed=seed)
+    # the same workload at another size: keep the number density and cell size
+    s = (n / 1_000_000) ** (1.0 / 3.0)
+    L = (0.2 * s, 0.2 * s, 0.4 * s)
+    num = tuple(max(3, int(round(v / 0.004))) for v in L)
+    return scenes.polydisperse(n=n, seed=seed, L=L, num=num)
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local = int(os.environ.get("LOCAL_RANK", rank))
+    return rank, world, local
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during timing."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-i", str(self.gpu)],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except FileNotFoundError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": 0}
+        sm.sort()
+        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peak_hbm():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic(np_):
+    """DRAM bytes per launch of the step kernel from the committed ncu summary
+    (profiles/), scaled to this particle count; None when absent."""
+    p = ROOT / "profiles" / "k_step_polydisperse.md"
+    if not p.exists():
+        return None
+    for ln in p.read_text().splitlines():
+        if ln.startswith("dram_bytes_per_particle:"):
+            return float(ln.split(":")[1]) * np_
+    return None
+
+
+def algorithmic_bytes(np_, ncells, contacts, nbonds=0):
+    """Compulsory HBM bytes of one step: 368 B of particle state per particle,
+    16 B of sort key/permutation, 16 B per cell of start/end, 52 B per active
+    directed contact (partner 4 + history read 24 + write 24), 136 B per bond."""
+    step_kernel = 368 * np_ + 52 * contacts
+    whole = step_kernel + 16 * np_ + 16 * ncells + 136 * nbonds
+    return step_kernel, whole
+
+
+def cpu_reference_run(sb, warmup, max_steps, seconds, kind_pref="reference"):
+    """Time the reference's kernel bodies (oracle/_ref) -- or, where they are
+    not built, the plain-C oracle -- on the host cores over a bounded sample:
+    `warmup` untimed steps, then steps until `max_steps` or `seconds`."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import pyoracle
+    from sphere_b200.state import config_from_spherebin, state_from_spherebin
+    kind = "reference" if (kind_pref == "reference" and pyoracle.LIB_REF.exists()) else "port"
+    lib = pyoracle.load("ref" if kind == "reference" else "orc")
+    cfg = config_from_spherebin(sb)
+    run = pyoracle.OracleRun(lib, cfg, state_from_spherebin(sb))
+    threads = lib.orc_threads(0)
+    if warmup:
+        rc = run.step(warmup, 0)
+        if rc:
+            raise RuntimeError(f"CPU oracle returned {rc}")
+    done, t0 = 0, time.perf_counter()
+    while done < max_steps and (time.perf_counter() - t0) < seconds:
+        rc = run.step(1, 0)
+        if rc:
+            raise RuntimeError(f"CPU oracle returned {rc}")
+        done += 1
+    el = time.perf_counter() - t0
+    return {"value": cfg.np * done / el, "unit": UNIT, "cores": int(threads), "kind": kind,
+            "sample": f"{done} timed steps (after {warmup} warm-up) of the {cfg.np}-sphere "
+                      f"workload, {el:.1f} s, OpenMP over particles"}
+
+
+def gpu_arm(args, rank, world, local):
+    import numpy as np
+    import torch
+    from sphere_b200.sphk import Simulation
+    from sphere_b200.state import config_from_spherebin, state_from_spherebin
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    sb = scene(args.n, args.seed + 1000 * rank)
+    cfg = config_from_spherebin(sb)
+    st0 = state_from_spherebin(sb)
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        import torch.distributed as dist
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    stream = torch.cuda.Stream()
+    sim = Simulation(cfg, device=local)
+    sim.upload(st0)
+    sim.step(args.warmup, stream=stream.cuda_stream)
+    torch.cuda.synchronize()
+    sim.sync()
+
+    # ---- device-resident throughput: exactly K steps between events -------
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    with ClockSampler(local) as clocks:
+        start.record(stream)
+        sim.step(args.steps, stream=stream.cuda_stream)
+        end.record(stream)
+        end.synchronize()
+    barrier()
+    sim.sync()
+    ms = max_over_ranks(start.elapsed_time(end))
+    stats = sim.stats()
+
+    # ---- per-phase device time (profile mode, events between phases) ------
+    nprof = min(args.steps, 200)
+    sim.set_profile(True)
+    sim.profile(reset=True)
+    sim.step(nprof)
+    sim.sync()
+    prof = sim.profile(reset=True)
+    sim.set_profile(False)
+    sim.close()
+
+    # ---- end to end through the C ABI with pinned host buffers ------------
+    def pinned(a):
+        t = torch.empty(a.shape, dtype=torch.from_numpy(a[:0]).dtype, pin_memory=True)
+        out = t.numpy()
+        out[...] = a
+        return out, t
+    keep = []
+    st_h = st0.copy()
+    for f, v in list(st_h.__dict__.items()):
+        if isinstance(v, np.ndarray) and v.size:
+            arr, t = pinned(v)
+            keep.append(t)
+            setattr(st_h, f, arr)
+    st_out = st_h.copy()
+    for f, v in list(st_out.__dict__.items()):
+        if isinstance(v, np.ndarray) and v.size:
+            arr, t = pinned(v)
+            keep.append(t)
+            setattr(st_out, f, arr)
+    sim2 = Simulation(cfg, device=local)
+    h2d = sum(getattr(st_h, f).nbytes for f in ("x", "xysum", "vel", "vel0", "force", "angpos",
+                                               "angvel", "angvel0", "torque", "es_dot", "es",
+                                               "ev_dot", "ev", "p", "walls_nx", "walls_mvfd"))
+    d2h = h2d + sum(getattr(st_out, f).nbytes for f in ("acc", "angacc", "contacts", "distmod",
+                                                         "delta_t"))
+    barrier()
+    t0 = time.perf_counter()
+    sim2.upload(st_h)
+    sim2.step(args.steps)
+    sim2.sync()
+    sim2.download(st_out)
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    sim2.close()
+
+    n_total = cfg.np * world
+    value = n_total * args.steps / (ms * 1e-3)
+    e2e_value = n_total * args.steps / e2e_s
+    step_ms = prof["step"] / max(1, prof["steps"])
+    C = stats["active_contacts"]
+    b_step, b_whole = algorithmic_bytes(cfg.np, cfg.ncells, C, cfg.nb0)
+    peak, peak_kind = measured_peak_hbm()
+    achieved = b_step / (step_ms * 1e-3) / 1e9
+    kernels_per_step = 5 + (1 if cfg.nb0 else 0) + 1 + (1 if cfg.nw else 0)
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "particles_per_gpu": cfg.np, "ncells": cfg.ncells,
+                   "dt": cfg.dt, "active_contacts": C, "l2": "state (~1.5 GB) exceeds L2",
+                   "parallelism": "independent replicas" if world > 1 else "single GPU",
+                   "graph_steps": 8},
+        "e2e": {"value": e2e_value, "unit": UNIT,
+                "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
+                "seconds": e2e_s},
+        "gpu_launches": kernels_per_step * args.steps,
+        "roofline": {"bound": "hbm", "kernel": "k_step", "achieved": achieved, "peak": peak,
+                     "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
+                     "traffic": ncu_traffic(cfg.np),
+                     "algorithmic_bytes_per_launch": b_step,
+                     "launch_ms": step_ms,
+                     "whole_step_algorithmic_bytes": b_whole,
+                     "whole_step_frac": (b_whole / (ms / args.steps * 1e-3) / 1e9) / peak},
+        "phase_ms_per_step": {k: prof[k] / max(1, prof["steps"]) for k in ("cells", "bonds", "step", "walls")},
+        "clocks": clocks.summary(),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_reference_run(sb, 1, 1000, args.cpu_seconds)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+    return out
+
+
+def reference_arm(args, rank, world):
+    if rank != 0:
+        return None
+    sb = scene(args.n, args.seed)
+    base = cpu_reference_run(sb, min(args.warmup, 1), args.steps, 60.0)
+    return {
+        "metric": METRIC, "value": base["value"], "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+        "config": {"workload": WORKLOAD, "particles_per_gpu": sb.np, "parallelism": "host cores"},
+        "cpu_baseline": base,
+        "e2e": {"value": base["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        out = reference_arm(args, rank, world)
+    else:
+        from sphere_b200 import build
+        if rank == 0:
+            build.build()
+        out = gpu_arm(args, rank, world, local)
+    if rank == 0 and out is not None:
+        print(json.dumps(out))
+
+
+if __name__ == "__main__":
+    main()

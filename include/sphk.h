@@ -104,6 +104,16 @@ typedef struct sph_stats {
 /* Options for sph_set_option. */
 #define SPH_OPT_RELAYOUT_EVERY 1  /* re-sort storage every n steps (0: at upload only) */
 #define SPH_OPT_GRAPH_STEPS 2     /* steps captured per CUDA graph (1..64, default 8) */
+#define SPH_OPT_PROFILE 3         /* 1: launch kernels one by one with CUDA events around
+                                     each phase (the reference's PROFILING switch,
+                                     src/debug.h:7, src/device.cu:86-102); 0: graphs */
+
+/* Phases timed in profile mode. */
+#define SPH_PHASE_CELLS 0   /* cell list rebuild (hash histogram, scan, scatter, sort) */
+#define SPH_PHASE_BONDS 1   /* per-bond forces */
+#define SPH_PHASE_STEP 2    /* fused contact search + forces + integration */
+#define SPH_PHASE_WALLS 3   /* wall force reduction + wall integration */
+#define SPH_NPHASES 4
 
 int sph_version(void);
 int sph_create(const sph_config *cfg, sph_ctx **out);
@@ -126,6 +136,9 @@ int sph_get_cells(sph_ctx *ctx, uint32_t *cell_sorted, uint32_t *perm, uint32_t 
 /* Wall-0 force of every particle in the most recent step (np doubles). */
 int sph_get_wall_forces(sph_ctx *ctx, double *wall0_force);
 int sph_get_stats(sph_ctx *ctx, sph_stats *out);
+/* Accumulated milliseconds per phase (SPH_NPHASES doubles) and the number of
+ * profiled steps since the last reset; reset != 0 clears the counters. */
+int sph_get_profile(sph_ctx *ctx, double *ms, uint64_t *steps, int reset);
 /* Re-sort particle storage into the current cell order (locality only;
  * results are unchanged). */
 int sph_relayout(sph_ctx *ctx);

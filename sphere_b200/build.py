@@ -23,6 +23,7 @@ ROOT = PKG.parent
 CSRC = PKG / "csrc"
 LIB = PKG / "lib" / "libsphk.so"
 CLI = PKG / "bin" / "sphere"
+SCENEGEN = PKG / "lib" / "libscenegen.so"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC = os.environ.get("NVCC", shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc")
 CUDA_HOME = Path(NVCC).resolve().parent.parent
@@ -85,9 +86,19 @@ def build_cli(force=False) -> Path:
     return CLI
 
 
+def build_scenegen(force=False) -> Path:
+    src = CSRC / "host" / "scenegen.c"
+    if not force and not _stale(SCENEGEN, [src]):
+        return SCENEGEN
+    SCENEGEN.parent.mkdir(parents=True, exist_ok=True)
+    _run(["gcc", "-O2", "-fPIC", "-shared", "-std=c11", str(src), "-o", str(SCENEGEN), "-lm"])
+    return SCENEGEN
+
+
 def build(force=False, verbose_ptxas=False):
     build_lib(force=force, verbose_ptxas=verbose_ptxas)
     build_cli(force=force)
+    build_scenegen(force=force)
 
 
 if __name__ == "__main__":

@@ -41,6 +41,11 @@ struct sph_ctx {
     int graphs_for_k = 0;
     std::string err;
     int sticky = SPH_OK;
+    // profile mode: events bracket each phase of each step
+    bool profile = false;
+    std::vector<cudaEvent_t> ev;          // 5 events per profiled step
+    double prof_ms[SPH_NPHASES] = {0, 0, 0, 0};
+    uint64_t prof_steps = 0;
 };
 
 namespace {
@@ -214,6 +219,33 @@ int ensure_graphs(sph_ctx *c)
     return SPH_OK;
 }
 
+// profile mode: one step with events between the phases
+int profiled_step(sph_ctx *c, int a, int write_outputs, cudaStream_t st)
+{
+    if (c->ev.empty()) {
+        c->ev.resize(5);
+        for (auto &e : c->ev) CK(cudaEventCreate(&e));
+    }
+    CK(cudaEventRecord(c->ev[0], st));
+    launch_rebuild(c->d, c->hp.np, c->hp.ncells, st);
+    CK(cudaEventRecord(c->ev[1], st));
+    launch_bonds(c->d, c->hp.nb0, a, st);
+    CK(cudaEventRecord(c->ev[2], st));
+    launch_step(c->d, c->hp.np, a, write_outputs, st);
+    CK(cudaEventRecord(c->ev[3], st));
+    launch_walls(c->d, c->hp.np, c->hp.nw, st);
+    CK(cudaEventRecord(c->ev[4], st));
+    CK(cudaGetLastError());
+    CK(cudaEventSynchronize(c->ev[4]));
+    for (int k = 0; k < SPH_NPHASES; ++k) {
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, c->ev[k], c->ev[k + 1]));
+        c->prof_ms[k] += ms;
+    }
+    c->prof_steps++;
+    return SPH_OK;
+}
+
 int do_relayout(sph_ctx *c, cudaStream_t st)
 {
     // the cell list must describe the current positions before storage follows it
@@ -314,6 +346,10 @@ int sph_set_option(sph_ctx *c, int option, int64_t value)
     if (!c) return SPH_ERR_BAD_INPUT;
     if (option == SPH_OPT_RELAYOUT_EVERY && value >= 0) {
         c->relayout_every = value;
+        return SPH_OK;
+    }
+    if (option == SPH_OPT_PROFILE && (value == 0 || value == 1)) {
+        c->profile = value != 0;
         return SPH_OK;
     }
     if (option == SPH_OPT_GRAPH_STEPS && value >= 1 && value <= 64) {
@@ -484,7 +520,20 @@ int sph_step(sph_ctx *c, uint64_t nsteps, void *stream)
     if (nsteps == 0) return SPH_OK;
     CK(cudaSetDevice(c->device));
     cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : c->stream;
-    int rc = ensure_graphs(c);
+    int rc;
+    if (c->profile) {
+        for (uint64_t i = 0; i < nsteps; ++i) {
+            if (c->relayout_every > 0 && c->since_relayout >= (uint64_t)c->relayout_every)
+                if ((rc = do_relayout(c, st)) != SPH_OK) return rc;
+            if ((rc = profiled_step(c, c->a, i + 1 == nsteps, st)) != SPH_OK) return rc;
+            c->a ^= 1;
+            c->since_relayout++;
+            c->steps++;
+            c->t_host += c->hp.dt;
+        }
+        return SPH_OK;
+    }
+    rc = ensure_graphs(c);
     if (rc != SPH_OK) return rc;
     const uint64_t K = (uint64_t)c->graph_steps;
     uint64_t i = 0;
@@ -669,6 +718,18 @@ int sph_get_stats(sph_ctx *c, sph_stats *out)
     return SPH_OK;
 }
 
+int sph_get_profile(sph_ctx *c, double *ms, uint64_t *steps, int reset)
+{
+    if (!c) return SPH_ERR_BAD_INPUT;
+    for (int k = 0; k < SPH_NPHASES; ++k) {
+        if (ms) ms[k] = c->prof_ms[k];
+        if (reset) c->prof_ms[k] = 0.0;
+    }
+    if (steps) *steps = c->prof_steps;
+    if (reset) c->prof_steps = 0;
+    return SPH_OK;
+}
+
 int sph_relayout(sph_ctx *c)
 {
     if (!c || !c->uploaded) return fail(c, SPH_ERR_BAD_INPUT, "sph_relayout before upload");
@@ -684,6 +745,7 @@ int sph_destroy(sph_ctx *c)
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
     drop_graphs(c);
+    for (auto e : c->ev) cudaEventDestroy(e);
     for (void *p : c->allocs) cudaFree(p);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;

@@ -68,103 +68,38 @@ def _lognormal_radii(rng, n, median=1e-3, sigma=0.2, lo=0.5e-3, hi=2e-3):
     return np.clip(np.exp(rng.normal(math.log(median), sigma, n)), lo, hi)
 
 
-def rsa_place(rng, radii, L, periodic_xy=True, cap=24, batch=16384, max_rounds=100000):
+def _scenegen():
+    import ctypes as C
+    from pathlib import Path
+    from . import build
+    path = build.build_scenegen()
+    lib = C.CDLL(str(path))
+    lib.rsa_place.argtypes = [C.c_int64, C.POINTER(C.c_double), C.POINTER(C.c_int64),
+                              C.POINTER(C.c_double), C.c_int, C.c_uint64, C.c_int64,
+                              C.POINTER(C.c_double)]
+    lib.rsa_place.restype = C.c_int
+    return lib
+
+
+def rsa_place(rng, radii, L, periodic_xy=True, max_trials=10_000_000):
     """Random sequential placement of spheres with the given radii in the box
-    [0, L): particles are placed in index order, each at uniformly random
-    positions until it overlaps no placed sphere (periodic images in x/y,
-    hard floor/ceiling in z).  Returns positions (n, 3)."""
-    n = len(radii)
-    r_max = float(radii.max())
-    h = 2.0 * r_max
-    g = np.maximum(np.floor(np.asarray(L) / h).astype(int), 3)
-    cs = np.asarray(L) / g
-    ncell = int(g[0] * g[1] * g[2])
-    members = np.full((ncell + 1, cap), -1, dtype=np.int64)   # last row: sentinel
-    counts = np.zeros(ncell + 1, dtype=np.int64)
-    pos = np.zeros((n, 3))
-    placed = np.zeros(n, dtype=bool)
-    pending = np.arange(n)
-    offs = np.array([(dx, dy, dz) for dz in (-1, 0, 1) for dy in (-1, 0, 1) for dx in (-1, 0, 1)])
-    Larr = np.asarray(L, float)
-    for _ in range(max_rounds):
-        if pending.size == 0:
-            break
-        idx = pending[:batch]
-        rr = radii[idx]
-        m = idx.size
-        cand = np.empty((m, 3))
-        cand[:, 0] = rng.random(m) * Larr[0]
-        cand[:, 1] = rng.random(m) * Larr[1]
-        cand[:, 2] = rr + rng.random(m) * (Larr[2] - 2 * rr)
-        cc = np.minimum((cand / cs).astype(int), g - 1)
-        nb = cc[:, None, :] + offs[None, :, :]
-        if periodic_xy:
-            nb[..., 0] %= g[0]
-            nb[..., 1] %= g[1]
-        bad = (nb[..., 2] < 0) | (nb[..., 2] >= g[2]) | (nb[..., 0] < 0) | (nb[..., 0] >= g[0]) \
-            | (nb[..., 1] < 0) | (nb[..., 1] >= g[1])
-        cid = nb[..., 0] + g[0] * (nb[..., 1] + g[1] * nb[..., 2])
-        cid = np.where(bad, ncell, cid)
-        mem = members[cid].reshape(m, -1)                      # (m, 27*cap)
-        valid = mem >= 0
-        mj = np.where(valid, mem, 0)
-        d = cand[:, None, :] - pos[mj]
-        if periodic_xy:
-            for ax in (0, 1):
-                d[..., ax] -= Larr[ax] * np.round(d[..., ax] / Larr[ax])
-        dist2 = np.einsum("ijk,ijk->ij", d, d)
-        lim = (rr[:, None] + radii[mj]) ** 2
-        ok = ~np.any(valid & (dist2 < lim), axis=1)
-        # conflicts inside the batch: an accepted candidate that overlaps an
-        # earlier accepted candidate of the same batch is rejected
-        acc = np.nonzero(ok)[0]
-        if acc.size > 1:
-            ca = cand[acc]
-            ra = rr[acc]
-            ccell = np.minimum((ca / cs).astype(int), g - 1)
-            key = ccell[:, 0] + g[0] * (ccell[:, 1] + g[1] * ccell[:, 2])
-            order = np.argsort(key, kind="stable")
-            skey = key[order]
-            keep = np.ones(acc.size, dtype=bool)
-            nbk = ccell[:, None, :] + offs[None, :, :]
-            if periodic_xy:
-                nbk[..., 0] %= g[0]
-                nbk[..., 1] %= g[1]
-            badk = (nbk[..., 2] < 0) | (nbk[..., 2] >= g[2]) | (nbk[..., 0] < 0) \
-                | (nbk[..., 0] >= g[0]) | (nbk[..., 1] < 0) | (nbk[..., 1] >= g[1])
-            kid = nbk[..., 0] + g[0] * (nbk[..., 1] + g[1] * nbk[..., 2])
-            lo = np.searchsorted(skey, kid, "left")
-            hi = np.searchsorted(skey, kid, "right")
-            lo = np.where(badk, 0, lo)
-            hi = np.where(badk, 0, hi)
-            cnt = (hi - lo).ravel()
-            src = np.repeat(np.repeat(np.arange(acc.size), 27), cnt)
-            start = np.repeat(lo.ravel(), cnt)
-            within = np.arange(cnt.sum()) - np.repeat(np.cumsum(cnt) - cnt, cnt)
-            other = order[start + within]
-            sel = other < src
-            src, other = src[sel], other[sel]
-            dd = ca[src] - ca[other]
-            if periodic_xy:
-                for ax in (0, 1):
-                    dd[:, ax] -= Larr[ax] * np.round(dd[:, ax] / Larr[ax])
-            hit = np.einsum("ij,ij->i", dd, dd) < (ra[src] + ra[other]) ** 2
-            keep[np.unique(src[hit])] = False
-            acc = acc[keep]
-        new = idx[acc]
-        pos[new] = cand[acc]
-        placed[new] = True
-        ccell = np.minimum((cand[acc] / cs).astype(int), g - 1)
-        key = ccell[:, 0] + g[0] * (ccell[:, 1] + g[1] * ccell[:, 2])
-        for k_, p_ in zip(key, new):
-            c = counts[k_]
-            if c >= cap:
-                raise RuntimeError("rsa_place: cell capacity exceeded; raise cap")
-            members[k_, c] = p_
-            counts[k_] = c + 1
-        pending = np.concatenate([pending[batch:], np.setdiff1d(idx, new, assume_unique=True)])
-    if not placed.all():
-        raise RuntimeError("rsa_place: could not place every sphere")
+    [0, L): largest spheres first (ties in index order), each at uniformly
+    random positions until it overlaps no placed sphere (periodic images in
+    x/y, hard floor/ceiling in z).  The placement runs in native code
+    (csrc/host/scenegen.c) from a seed drawn from ``rng``.  Returns (n, 3)."""
+    import ctypes as C
+    radii = np.ascontiguousarray(radii, dtype=np.float64)
+    Larr = np.ascontiguousarray(L, dtype=np.float64)
+    pos = np.zeros((len(radii), 3))
+    seed = int(rng.integers(0, 2**63 - 1))
+    order = np.ascontiguousarray(np.argsort(-radii, kind="stable"), dtype=np.int64)
+    dp = C.POINTER(C.c_double)
+    rc = _scenegen().rsa_place(len(radii), radii.ctypes.data_as(dp),
+                               order.ctypes.data_as(C.POINTER(C.c_int64)), Larr.ctypes.data_as(dp),
+                               1 if periodic_xy else 0, seed, int(max_trials),
+                               pos.ctypes.data_as(dp))
+    if rc != 0:
+        raise RuntimeError(f"rsa_place failed ({rc}): the packing is too dense for RSA")
     return pos
 
 

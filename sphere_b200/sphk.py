@@ -29,6 +29,8 @@ ERRORS = {
 }
 OPT_RELAYOUT_EVERY = 1
 OPT_GRAPH_STEPS = 2
+OPT_PROFILE = 3
+PHASES = ("cells", "bonds", "step", "walls")
 
 _dp = C.POINTER(C.c_double)
 _up = C.POINTER(C.c_uint32)
@@ -101,6 +103,7 @@ def load_library(path: os.PathLike | None = None):
         "sph_get_wall_forces": ([vp, _dp], C.c_int),
         "sph_get_stats": ([vp, C.POINTER(SphStats)], C.c_int),
         "sph_relayout": ([vp], C.c_int),
+        "sph_get_profile": ([vp, _dp, C.POINTER(C.c_uint64), C.c_int], C.c_int),
         "sph_last_error": ([vp], C.c_char_p),
         "sph_destroy": ([vp], C.c_int),
     }
@@ -221,6 +224,17 @@ class Simulation:
         s = SphStats()
         self._check(self.lib.sph_get_stats(self._ctx, C.byref(s)))
         return {k: int(getattr(s, k)) for k, _ in SphStats._fields_}
+
+    def set_profile(self, on: bool):
+        self._check(self.lib.sph_set_option(self._ctx, OPT_PROFILE, 1 if on else 0))
+
+    def profile(self, reset=False) -> dict:
+        ms = (C.c_double * len(PHASES))()
+        n = C.c_uint64()
+        self._check(self.lib.sph_get_profile(self._ctx, ms, C.byref(n), 1 if reset else 0))
+        out = {p: float(ms[i]) for i, p in enumerate(PHASES)}
+        out["steps"] = int(n.value)
+        return out
 
     def relayout(self):
         self._check(self.lib.sph_relayout(self._ctx))

@@ -91,7 +91,8 @@ class HostState:
 
 
 def _c(a, dtype=np.float64):
-    return np.ascontiguousarray(a, dtype=dtype)
+    # always a fresh array: a HostState must never alias its Spherebin
+    return np.array(a, dtype=dtype, copy=True, order="C")
 
 
 def config_from_spherebin(sb: Spherebin) -> SceneConfig:
