@@ -14,7 +14,7 @@ void launch_step(const Dev &d, uint32_t np, int a, int write_outputs, cudaStream
 void launch_bonds(const Dev &d, uint32_t nb0, int a, cudaStream_t st);
 void launch_walls(const Dev &d, uint32_t np, uint32_t nw, cudaStream_t st);
 void launch_cell_init(const Dev &d, uint32_t np, int a, cudaStream_t st);
-void launch_rebuild(const Dev &d, uint32_t np, uint32_t ncells, cudaStream_t st);
+void launch_rebuild(const Dev &d, uint32_t np, uint32_t ncells, int a, cudaStream_t st);
 unsigned int scan_tile_count(uint32_t ncells);
 void relayout(const Dev &d, uint32_t np, int a, void *scratch, cudaStream_t st);
 }  // namespace sphk
@@ -172,7 +172,7 @@ int sync_status(sph_ctx *c)
 
 void enqueue_one_step(sph_ctx *c, int a, int write_outputs, cudaStream_t st)
 {
-    launch_rebuild(c->d, c->hp.np, c->hp.ncells, st);
+    launch_rebuild(c->d, c->hp.np, c->hp.ncells, a, st);
     launch_bonds(c->d, c->hp.nb0, a, st);
     launch_step(c->d, c->hp.np, a, write_outputs, st);
     launch_walls(c->d, c->hp.np, c->hp.nw, st);
@@ -227,7 +227,7 @@ int profiled_step(sph_ctx *c, int a, int write_outputs, cudaStream_t st)
         for (auto &e : c->ev) CK(cudaEventCreate(&e));
     }
     CK(cudaEventRecord(c->ev[0], st));
-    launch_rebuild(c->d, c->hp.np, c->hp.ncells, st);
+    launch_rebuild(c->d, c->hp.np, c->hp.ncells, a, st);
     CK(cudaEventRecord(c->ev[1], st));
     launch_bonds(c->d, c->hp.nb0, a, st);
     CK(cudaEventRecord(c->ev[2], st));
@@ -249,7 +249,7 @@ int profiled_step(sph_ctx *c, int a, int write_outputs, cudaStream_t st)
 int do_relayout(sph_ctx *c, cudaStream_t st)
 {
     // the cell list must describe the current positions before storage follows it
-    launch_rebuild(c->d, c->hp.np, c->hp.ncells, st);
+    launch_rebuild(c->d, c->hp.np, c->hp.ncells, c->a, st);
     relayout(c->d, c->hp.np, c->a, c->scratch, st);
     CK(cudaGetLastError());
     c->relayouts++;
@@ -318,13 +318,13 @@ int sph_create(const sph_config *cfg, sph_ctx **out)
     int rc = SPH_OK;
 #define AL(ptr, n) if ((rc = dalloc(c, &(ptr), (n))) != SPH_OK) return rc;
     for (int b = 0; b < 2; ++b) {
-        AL(d.xr[b], np); AL(d.vel[b], np); AL(d.angvel[b], np); AL(d.xf[b], np);
+        AL(d.xr[b], np); AL(d.vel[b], np); AL(d.angvel[b], np); AL(d.xs[b], np);
     }
     AL(d.vel0, np); AL(d.angvel0, np); AL(d.angpos, np); AL(d.xysum, np); AL(d.esv, np);
     AL(d.force, np); AL(d.torque, np); AL(d.acc, np); AL(d.angacc, np); AL(d.edp, np);
     AL(d.uid, np); AL(d.sidx, np); AL(d.cell, np);
     AL(d.contacts, np * NC); AL(d.dmc, np); AL(d.delta_t, np * NC); AL(d.cmask, np);
-    AL(d.cell_start, (size_t)ncells + 2); AL(d.cellorder, np); AL(d.cell_fill, (size_t)ncells + 1);
+    AL(d.cell_start, (size_t)ncells + 2); AL(d.cellorder, np); AL(d.pos, np); AL(d.cell_fill, (size_t)ncells + 1);
     AL(d.scan_tiles, scan_tile_count(P.ncells));
     AL(d.wf_pp, np); AL(d.wtouch, np); AL(d.wf_partial, div_up(np, 256));
     AL(d.walls, 1);
@@ -376,10 +376,7 @@ int sph_upload(sph_ctx *c, const sph_host_state *h)
     c->a = A;
     // kinematics (identity storage order for now)
     std::vector<double> buf(np * 4);
-    std::vector<float> xf(np * 4);
     CK(cudaMemcpy(d.xr[A], h->x, np * 32, cudaMemcpyHostToDevice));
-    for (size_t i = 0; i < np * 4; ++i) xf[i] = (float)h->x[i];
-    CK(cudaMemcpy(d.xf[A], xf.data(), np * 16, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(d.vel[A], h->vel, np * 32, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(d.vel0, h->vel0 ? h->vel0 : h->vel, np * 32, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(d.angvel[A], h->angvel, np * 32, cudaMemcpyHostToDevice));

@@ -10,10 +10,11 @@
 //   k_scan_*   exclusive scan of the histogram        (two launches, no waits)
 //   k_scatter  each particle claims a position in its cell's range
 //   k_cellsort each cell orders its few members by particle index
+//   k_post_sort inverse order and the float position copy in list order
 // The cell of every particle is computed by the step kernel from its new
 // position, which also raises `rebuild` when any particle changed cell; all
-// four kernels return at once when it is clear, so an unchanged cell list
-// costs four empty launches.
+// the kernels above return at once when it is clear, so an unchanged cell
+// list costs only their empty launches.
 //
 // Particles are stored in cell order (relayout), so neighbours are close in
 // memory; k_relayout_* re-establish that order on demand.
@@ -161,12 +162,25 @@ __global__ void k_cellsort(Dev d)
     }
 }
 
+// inverse of the new order and the float copy of the positions in list order
+__global__ void k_post_sort(Dev d, int A)
+{
+    if (*d.rebuild == 0u) return;
+    const Params &P = *d.prm;
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= P.np) return;
+    const uint32_t s = d.cellorder[k];
+    d.pos[s] = k;
+    const double4 x = d.xr[A][s];
+    d.xs[A][k] = make_float4((float)x.x, (float)x.y, (float)x.z, (float)x.w);
+}
+
 void launch_cell_init(const Dev &d, uint32_t np, int a, cudaStream_t st)
 {
     k_cell_init<<<div_up(np, CELL_BLOCK), CELL_BLOCK, 0, st>>>(d, a);
 }
 
-void launch_rebuild(const Dev &d, uint32_t np, uint32_t ncells, cudaStream_t st)
+void launch_rebuild(const Dev &d, uint32_t np, uint32_t ncells, int a, cudaStream_t st)
 {
     const unsigned int ntiles = div_up((unsigned long long)ncells + 1, SCAN_TILE);
     k_count<<<div_up(np, CELL_BLOCK), CELL_BLOCK, 0, st>>>(d);
@@ -174,6 +188,7 @@ void launch_rebuild(const Dev &d, uint32_t np, uint32_t ncells, cudaStream_t st)
     k_scan_apply<<<ntiles, CELL_BLOCK, 0, st>>>(d);
     k_scatter<<<div_up(np, CELL_BLOCK), CELL_BLOCK, 0, st>>>(d);
     k_cellsort<<<div_up((unsigned long long)ncells + 1, CELL_BLOCK), CELL_BLOCK, 0, st>>>(d);
+    k_post_sort<<<div_up(np, CELL_BLOCK), CELL_BLOCK, 0, st>>>(d, a);
     cudaMemsetAsync(d.rebuild, 0, sizeof(uint32_t), st);
 }
 
@@ -218,12 +233,15 @@ __global__ void k_gather_dt(const double4 *src, double4 *dst, const uint32_t *or
     dst[e] = src[(size_t)order[k] * NC + i];
 }
 
-__global__ void k_relayout_finish(Dev d)
+__global__ void k_relayout_finish(Dev d, int A)
 {
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= d.prm->np) return;
     d.cellorder[k] = k;
+    d.pos[k] = k;
     d.sidx[d.uid[k]] = k;
+    const double4 x = d.xr[A][k];
+    d.xs[A][k] = make_float4((float)x.x, (float)x.y, (float)x.z, (float)x.w);
 }
 
 template <typename T>
@@ -246,7 +264,6 @@ void relayout(const Dev &d, uint32_t np, int a, void *scratch, cudaStream_t st)
     gather_back(d.xr[a], scratch, order, np, st);
     gather_back(d.vel[a], scratch, order, np, st);
     gather_back(d.angvel[a], scratch, order, np, st);
-    gather_back(d.xf[a], scratch, order, np, st);
     gather_back(d.vel0, scratch, order, np, st);
     gather_back(d.angvel0, scratch, order, np, st);
     gather_back(d.angpos, scratch, order, np, st);
@@ -275,7 +292,7 @@ void relayout(const Dev &d, uint32_t np, int a, void *scratch, cudaStream_t st)
         cudaMemcpyAsync(d.delta_t, tmp, sizeof(double4) * (size_t)np * NC,
                         cudaMemcpyDeviceToDevice, st);
     }
-    k_relayout_finish<<<div_up(np, CELL_BLOCK), CELL_BLOCK, 0, st>>>(d);
+    k_relayout_finish<<<div_up(np, CELL_BLOCK), CELL_BLOCK, 0, st>>>(d, a);
 }
 
 }  // namespace sphk

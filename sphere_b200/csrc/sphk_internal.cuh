@@ -82,7 +82,7 @@ struct Dev {
     double4 *xr[2];       // x, y, z, radius
     double4 *vel[2];      // vx, vy, vz, fixvel
     double4 *angvel[2];   // wx, wy, wz, (w lane carried)
-    float4 *xf[2];        // float copy of xr for the neighbour cull
+    float4 *xs[2];        // float copy of xr in cell-list order, for the neighbour cull
     // private per-particle state (updated in place)
     double4 *vel0, *angvel0, *angpos;
     double2 *xysum;
@@ -99,7 +99,8 @@ struct Dev {
     uint32_t *cmask;      // [np] occupied-slot bit mask
     // cell list (cell order sorted by uid inside each cell)
     uint32_t *cell_start; // [ncells + 2]
-    uint32_t *cellorder;  // [np]
+    uint32_t *cellorder;  // [np] cell-list position -> storage index
+    uint32_t *pos;        // [np] storage index -> cell-list position
     uint32_t *cell_fill;  // [ncells + 1] scratch
     uint32_t *scan_tiles; // scratch for the scan
     // walls

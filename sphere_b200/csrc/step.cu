@@ -1,27 +1,33 @@
-// step.cu -- the fused per-particle DEM step of libsphk.
+// step.cu -- the per-particle DEM step of libsphk, in two launches.
 //
-// One launch performs, for every particle, what the reference does in four
-// kernels (src/device.cu:805-1058):
-//   topology   contact detection into persistent slots, contactsearch.cuh:181-355
-//   interact   contact forces over the slots, then the walls, :369-689
-//   (bonds)    the per-bond forces of bondsLinear (cohesion.cuh:8-233), computed
-//              by bonds.cu and gathered here per particle in bond order
-//   integrate  half-step leapfrog, integration.cuh:9-187
-// It reads the kinematics of step n from buffer A and writes step n+1 to
-// buffer B, so neighbours always see start-of-step values and no particle
-// waits on another.  Particles are stored in cell order, so the 27-cell
-// neighbourhood of a warp is a few contiguous runs of memory.
+// k_topo   contact detection into the persistent slots (topology,
+//          src/contactsearch.cuh:181-355).  One thread per cell-list
+//          position.  Candidates come from a float copy of the positions kept
+//          in cell-list order (Dev::xs), so the three cells of each x-row of
+//          the 27-cell stencil are three adjacent runs of one array and a
+//          candidate costs one coalesced 16-byte load; the particle's own slot
+//          row is fetched only when an overlap is found.
+// k_force  everything per particle after it (src/device.cu:829-1058):
+//          contact forces over the slots and the walls (interact,
+//          contactsearch.cuh:369-689), the per-bond forces of bondsLinear
+//          (cohesion.cuh:8-233, computed by bonds.cu and gathered here in bond
+//          order), and the half-step leapfrog (integrate, integration.cuh:9-187).
+//          One thread per storage index, so the particle state streams.
+// Kinematics of step n are read from buffer A and step n+1 is written to
+// buffer B, so neighbours always see start-of-step values.
 //
 // Parity: every expression keeps the reference's operation order; see
-// sphk_internal.cuh.  The neighbour candidates are first culled with a
-// conservative FP32 distance test (Params::cull_eps bounds the float
-// rounding), then the reference's own predicate
-// float_sqrt(dot) - (ra + rb) < 0 decides.
+// sphk_internal.cuh.  Candidates are first culled with a conservative FP32
+// distance test (Params::cull_eps bounds the float rounding), then the
+// reference's own predicate float_sqrt(dot) - (ra + rb) < 0 decides.  The
+// visiting order is the reference's: stencil cells z, y, x, members of a cell
+// by particle index.
 #include "sphk_internal.cuh"
 
 namespace sphk {
 
-constexpr int STEP_BLOCK = 128;
+constexpr int TOPO_BLOCK = 128;
+constexpr int FORCE_BLOCK = 128;
 
 // contactLinear_wall, src/contactmodels.cuh:10-109
 __device__ __forceinline__ double contact_wall(const Params &P, d3 &F, d3 &T, double &p,
@@ -113,142 +119,194 @@ __device__ __forceinline__ void dm_set(unsigned long long &lo, unsigned long lon
     }
 }
 
-struct StepArgs {
+
+// findDistMod for one axis that may be periodic (src/contactsearch.cuh:12-74):
+// wraps -1 -> num-1 (shift +L, code bit lo) and num -> 0 (shift -L, bit hi).
+__device__ __forceinline__ void wrap_axis(int32_t &c, uint32_t num, uint32_t &code,
+                                          uint32_t bit_lo, uint32_t bit_hi)
+{
+    if (c < 0) { c = (int32_t)(num - 1); code |= bit_lo; }
+    if ((uint32_t)c == num) { c = 0; code |= bit_hi; }
+}
+
+__global__ void __launch_bounds__(TOPO_BLOCK)
+k_topo(Dev d, int A)
+{
+    __shared__ uint32_t srow[NC * TOPO_BLOCK];
+    const Params &P = *d.prm;
+    const uint32_t np = P.np;
+    const int tid = threadIdx.x;
+    const uint32_t k = blockIdx.x * TOPO_BLOCK + tid;
+    if (k >= np) return;
+    const uint32_t s = d.cellorder[k];
+    const float4 xaf = d.xs[A][k];
+    const double4 xa = d.xr[A][s];
+    const double ra = xa.w;
+    uint32_t occ = d.cmask[s];
+    const float4 *__restrict__ xs = d.xs[A];
+    bool loaded = false, dirty = false;
+    unsigned long long dm_lo = 0, dm_hi = 0;
+    uint32_t err = 0;
+    int nc = 0;
+    int32_t gp[3];
+    gp[0] = __double2int_rz(cell_floor(P, 0, xa.x));
+    gp[1] = __double2int_rz(cell_floor(P, 1, xa.y));
+    gp[2] = __double2int_rz(cell_floor(P, 2, xa.z));
+    const float Lf0 = (float)P.L[0], Lf1 = (float)P.L[1];
+    const float eps = P.cull_eps;
+    const uint32_t nx = P.num[0], ny = P.num[1], nz = P.num[2];
+
+    // one cell: members in particle-index order; false once nc > NC, which
+    // ends the cell (the reference returns from findContactsInCell)
+    auto scan_cell = [&](uint32_t beg, uint32_t end, uint32_t code) {
+        const float sx = (code & 1u) ? Lf0 : ((code & 2u) ? -Lf0 : 0.0f);
+        const float sy = (code & 4u) ? Lf1 : ((code & 8u) ? -Lf1 : 0.0f);
+        for (uint32_t k2 = beg; k2 < end; ++k2) {
+            if (k2 == k) continue;
+            const float4 xbf = __ldg(&xs[k2]);
+            const float fx = (xaf.x - xbf.x) + sx;
+            const float fy = (xaf.y - xbf.y) + sy;
+            const float fz = xaf.z - xbf.z;
+            const float d2 = __fmaf_rn(fx, fx, __fmaf_rn(fy, fy, fz * fz));
+            const float rr = (xaf.w + xbf.w) * 1.000004f + eps;
+            if (d2 >= rr * rr) continue;
+            const uint32_t t = __ldg(&d.cellorder[k2]);
+            const double4 xb = d.xr[A][t];
+            const d3 dm = decode_dm(code, P);
+            const d3 xab = add(mk(xa.x - xb.x, xa.y - xb.y, xa.z - xb.z), dm);
+            const double delta = flen(xab) - (ra + xb.w);
+            if (!(delta < 0.0f)) continue;
+            if (!loaded) {
+                if (occ) {
+                    const uint4 *row = reinterpret_cast<const uint4 *>(d.contacts + (size_t)s * NC);
+#pragma unroll
+                    for (int q = 0; q < NC / 4; ++q) {
+                        const uint4 v = row[q];
+                        srow[(4 * q + 0) * TOPO_BLOCK + tid] = v.x;
+                        srow[(4 * q + 1) * TOPO_BLOCK + tid] = v.y;
+                        srow[(4 * q + 2) * TOPO_BLOCK + tid] = v.z;
+                        srow[(4 * q + 3) * TOPO_BLOCK + tid] = v.w;
+                    }
+                    const ulonglong2 c2 = d.dmc[s];
+                    dm_lo = c2.x;
+                    dm_hi = c2.y;
+                }
+                loaded = true;
+            }
+            // slot choice, src/contactsearch.cuh:252-271: a slot already
+            // holding t wins, else the last empty slot, else position nc
+            int cpos = -1;
+            for (uint32_t m = occ; m; m &= m - 1) {
+                const int i = __ffs(m) - 1;
+                if (srow[i * TOPO_BLOCK + tid] == t) { cpos = i; break; }
+            }
+            if (cpos < 0) {
+                const uint32_t empty = ~occ;
+                cpos = empty ? 31 - __clz(empty) : nc;
+            }
+            if (cpos < NC) {
+                occ |= 1u << cpos;
+                srow[cpos * TOPO_BLOCK + tid] = t;
+                dm_set(dm_lo, dm_hi, cpos, code);
+                dirty = true;
+            } else {
+                err |= ST_NC_OVERFLOW;
+            }
+            if (++nc > NC) return false;
+        }
+        return true;
+    };
+
+    for (int oz = -1; oz < 2; ++oz) {
+        const int32_t cz = (int32_t)((uint32_t)gp[2] + (uint32_t)oz);
+        if (cz < 0 || (uint32_t)cz == nz) continue;
+        for (int oy = -1; oy < 2; ++oy) {
+            int32_t cy = (int32_t)((uint32_t)gp[1] + (uint32_t)oy);
+            uint32_t ycode = 0;
+            if (P.periodic == 1) {
+                wrap_axis(cy, ny, ycode, 4u, 8u);
+            } else if (cy < 0 || (uint32_t)cy == ny) {
+                continue;
+            }
+            const uint32_t rowbase = (uint32_t)cy * nx + (nx * ny) * (uint32_t)cz;
+            const int32_t c0 = gp[0] - 1;
+            if (c0 >= 0 && (uint32_t)c0 + 2 < nx) {
+                // the three x cells are consecutive ids: one run of xs
+                const uint32_t cid0 = (uint32_t)c0 + rowbase;
+                if (cid0 + 2 >= P.ncells) { err |= ST_OUT_OF_GRID; continue; }
+                const uint32_t b0 = d.cell_start[cid0], b1 = d.cell_start[cid0 + 1];
+                const uint32_t b2 = d.cell_start[cid0 + 2], b3 = d.cell_start[cid0 + 3];
+                scan_cell(b0, b1, ycode);
+                scan_cell(b1, b2, ycode);
+                scan_cell(b2, b3, ycode);
+            } else {
+                for (int ox = -1; ox < 2; ++ox) {
+                    int32_t cx = (int32_t)((uint32_t)gp[0] + (uint32_t)ox);
+                    uint32_t code = ycode;
+                    if (P.periodic == 1 || P.periodic == 2) {
+                        wrap_axis(cx, nx, code, 1u, 2u);
+                    } else if (cx < 0 || (uint32_t)cx == nx) {
+                        continue;
+                    }
+                    const uint32_t cid = (uint32_t)cx + rowbase;
+                    if (cid >= P.ncells) { err |= ST_OUT_OF_GRID; continue; }
+                    scan_cell(d.cell_start[cid], d.cell_start[cid + 1], code);
+                }
+            }
+        }
+    }
+    if (dirty) {
+        uint4 *row = reinterpret_cast<uint4 *>(d.contacts + (size_t)s * NC);
+#pragma unroll
+        for (int q = 0; q < NC / 4; ++q) {
+            uint4 v;
+            v.x = ((occ >> (4 * q + 0)) & 1u) ? srow[(4 * q + 0) * TOPO_BLOCK + tid] : np;
+            v.y = ((occ >> (4 * q + 1)) & 1u) ? srow[(4 * q + 1) * TOPO_BLOCK + tid] : np;
+            v.z = ((occ >> (4 * q + 2)) & 1u) ? srow[(4 * q + 2) * TOPO_BLOCK + tid] : np;
+            v.w = ((occ >> (4 * q + 3)) & 1u) ? srow[(4 * q + 3) * TOPO_BLOCK + tid] : np;
+            row[q] = v;
+        }
+        d.cmask[s] = occ;
+        d.dmc[s] = make_ulonglong2(dm_lo, dm_hi);
+    }
+    if (err) atomicOr(d.status, err);
+}
+
+struct ForceArgs {
     Dev d;
     int a;              // read buffer (start of step); the kernel writes buffer 1-a
     int write_outputs;  // store force/torque/acc/angacc/edp of this step
 };
 
-__global__ void __launch_bounds__(STEP_BLOCK)
-k_step(StepArgs args)
+__global__ void __launch_bounds__(FORCE_BLOCK)
+k_force(ForceArgs args)
 {
-    __shared__ uint32_t srow[NC * STEP_BLOCK];
     const Dev &d = args.d;
     const Params &P = *d.prm;
     const uint32_t np = P.np;
-    const int tid = threadIdx.x;
-    const uint32_t s = blockIdx.x * STEP_BLOCK + tid;
+    const uint32_t s = blockIdx.x * FORCE_BLOCK + threadIdx.x;
     if (s >= np) return;
     const int A = args.a, B = 1 - args.a;
     uint32_t err = 0;
-
     const double4 xa = d.xr[A][s];
     const double ra = xa.w;
-    const float4 xaf = d.xf[A][s];
-
-    // ---- load the slot row (partners as storage indices) -------------------
-    uint32_t occ = d.cmask[s];
-    const uint32_t occ0 = occ;
-    unsigned long long dm_lo = 0, dm_hi = 0;
-    if (occ) {
-        const uint4 *row = reinterpret_cast<const uint4 *>(d.contacts + (size_t)s * NC);
-#pragma unroll
-        for (int q = 0; q < NC / 4; ++q) {
-            uint4 v = row[q];
-            srow[(4 * q + 0) * STEP_BLOCK + tid] = v.x;
-            srow[(4 * q + 1) * STEP_BLOCK + tid] = v.y;
-            srow[(4 * q + 2) * STEP_BLOCK + tid] = v.z;
-            srow[(4 * q + 3) * STEP_BLOCK + tid] = v.w;
-        }
-        const ulonglong2 c = d.dmc[s];
-        dm_lo = c.x;
-        dm_hi = c.y;
-    }
-    const unsigned long long dm_lo0 = dm_lo, dm_hi0 = dm_hi;
-    bool row_dirty = false;
-
-    // ---- topology: 27-cell sweep, z/y/x order, candidates in uid order ----
-    {
-        int32_t gp[3];
-        gp[0] = __double2int_rz(cell_floor(P, 0, xa.x));
-        gp[1] = __double2int_rz(cell_floor(P, 1, xa.y));
-        gp[2] = __double2int_rz(cell_floor(P, 2, xa.z));
-        const float Lf0 = (float)P.L[0], Lf1 = (float)P.L[1];
-        const float eps = P.cull_eps;
-        int nc = 0;
-        for (int oz = -1; oz < 2; ++oz)
-            for (int oy = -1; oy < 2; ++oy)
-                for (int ox = -1; ox < 2; ++ox) {
-                    int32_t cx = (int32_t)((uint32_t)gp[0] + (uint32_t)ox);
-                    int32_t cy = (int32_t)((uint32_t)gp[1] + (uint32_t)oy);
-                    int32_t cz = (int32_t)((uint32_t)gp[2] + (uint32_t)oz);
-                    uint32_t code = 0;
-                    // findDistMod, src/contactsearch.cuh:12-74
-                    if (P.periodic == 1) {
-                        if (cx < 0) { cx = (int32_t)(P.num[0] - 1); code |= 1u; }
-                        if ((uint32_t)cx == P.num[0]) { cx = 0; code |= 2u; }
-                        if (cy < 0) { cy = (int32_t)(P.num[1] - 1); code |= 4u; }
-                        if ((uint32_t)cy == P.num[1]) { cy = 0; code |= 8u; }
-                    } else if (P.periodic == 2) {
-                        if (cx < 0) { cx = (int32_t)(P.num[0] - 1); code |= 1u; }
-                        if ((uint32_t)cx == P.num[0]) { cx = 0; code |= 2u; }
-                        if (cy < 0 || (uint32_t)cy == P.num[1]) continue;
-                    } else {
-                        if (cx < 0 || (uint32_t)cx == P.num[0]) continue;
-                        if (cy < 0 || (uint32_t)cy == P.num[1]) continue;
-                    }
-                    if (cz < 0 || (uint32_t)cz == P.num[2]) continue;
-                    const uint32_t cid = (uint32_t)cx + (uint32_t)cy * P.num[0]
-                        + (P.num[0] * P.num[1]) * (uint32_t)cz;
-                    if (cid >= P.ncells) { err |= ST_OUT_OF_GRID; continue; }
-                    const uint32_t beg = d.cell_start[cid], end = d.cell_start[cid + 1];
-                    if (beg == end) continue;
-                    const float sx = (code & 1u) ? Lf0 : ((code & 2u) ? -Lf0 : 0.0f);
-                    const float sy = (code & 4u) ? Lf1 : ((code & 8u) ? -Lf1 : 0.0f);
-                    const d3 dm = decode_dm(code, P);
-                    for (uint32_t k = beg; k < end; ++k) {
-                        const uint32_t t = __ldg(&d.cellorder[k]);
-                        if (t == s) continue;
-                        const float4 xbf = __ldg(&d.xf[A][t]);
-                        const float fx = (xaf.x - xbf.x) + sx;
-                        const float fy = (xaf.y - xbf.y) + sy;
-                        const float fz = xaf.z - xbf.z;
-                        const float d2 = __fmaf_rn(fx, fx, __fmaf_rn(fy, fy, fz * fz));
-                        const float rr = (xaf.w + xbf.w) * 1.000004f + eps;
-                        if (d2 >= rr * rr) continue;
-                        const double4 xb = d.xr[A][t];
-                        const d3 xab = add(mk(xa.x - xb.x, xa.y - xb.y, xa.z - xb.z), dm);
-                        const double len = flen(xab);
-                        const double delta = len - (ra + xb.w);
-                        if (!(delta < 0.0f)) continue;
-                        // slot choice, src/contactsearch.cuh:252-271
-                        int cpos = -1;
-                        for (uint32_t m = occ; m; m &= m - 1) {
-                            const int i = __ffs(m) - 1;
-                            if (srow[i * STEP_BLOCK + tid] == t) { cpos = i; break; }
-                        }
-                        if (cpos < 0) {
-                            const uint32_t empty = ~occ;
-                            cpos = empty ? 31 - __clz(empty) : nc;
-                        }
-                        if (cpos < NC) {
-                            if (!((occ >> cpos) & 1u)) {
-                                occ |= 1u << cpos;
-                            }
-                            srow[cpos * STEP_BLOCK + tid] = t;
-                            dm_set(dm_lo, dm_hi, cpos, code);
-                            row_dirty = true;
-                        } else {
-                            err |= ST_NC_OVERFLOW;
-                        }
-                        ++nc;
-                        if (nc > NC) break;
-                    }
-                }
-    }
-
-    // ---- interact: slots in order, then walls ------------------------------
     const double4 vel_a = d.vel[A][s];
     const double4 angvel_a4 = d.angvel[A][s];
     const d3 angvel_a = xyz(angvel_a4);
     d3 F = mk(0.0, 0.0, 0.0), T = mk(0.0, 0.0, 0.0);
     double es_dot = 0.0f, ev_dot = 0.0f, p = 0.0f;
-    if (P.contactmodel == 2) {
+
+    // ---- interact: occupied slots in slot order ----------------------------
+    uint32_t occ = d.cmask[s];
+    if (occ && P.contactmodel == 2) {
+        const uint32_t occ0 = occ;
+        const ulonglong2 dmw = d.dmc[s];
+        uint32_t *crow = d.contacts + (size_t)s * NC;
         double4 *dtrow = d.delta_t + (size_t)s * NC;
-        for (uint32_t m = occ; m; m &= m - 1) {
+        for (uint32_t m = occ0; m; m &= m - 1) {
             const int i = __ffs(m) - 1;
-            const uint32_t t = srow[i * STEP_BLOCK + tid];
-            const d3 dm = decode_dm(dm_get(dm_lo, dm_hi, i), P);
+            const uint32_t t = crow[i];
+            const d3 dm = decode_dm(dm_get(dmw.x, dmw.y, i), P);
             const double4 xb = d.xr[A][t];
             const double rb = xb.w;
             const d3 xab = mk(xa.x - xb.x + dm.x, xa.y - xb.y + dm.y, xa.z - xb.z + dm.z);
@@ -260,14 +318,16 @@ k_step(StepArgs args)
                                d.angvel[A][t], ra, rb, xab, xlen, delta_n, dt4);
                 dtrow[i] = dt4;
             } else {
+                // separated: free the slot and zero its history
                 occ &= ~(1u << i);
-                srow[i * STEP_BLOCK + tid] = np;
+                crow[i] = np;
                 dtrow[i] = make_double4(0.0, 0.0, 0.0, 0.0);
-                row_dirty = true;
             }
         }
+        if (occ != occ0) d.cmask[s] = occ;
     }
-    // walls, src/contactsearch.cuh:578-663 (defaults :416-427)
+
+    // ---- walls, src/contactsearch.cuh:578-663 (defaults :416-427) ----------
     double w0f = 0.0;
     {
         const Walls &W = *d.walls;
@@ -297,23 +357,6 @@ k_step(StepArgs args)
         }
     }
 
-    // ---- write back the slot row --------------------------------------------
-    if (row_dirty || occ != occ0) {
-        uint4 *row = reinterpret_cast<uint4 *>(d.contacts + (size_t)s * NC);
-#pragma unroll
-        for (int q = 0; q < NC / 4; ++q) {
-            uint4 v;
-            v.x = ((occ >> (4 * q + 0)) & 1u) ? srow[(4 * q + 0) * STEP_BLOCK + tid] : np;
-            v.y = ((occ >> (4 * q + 1)) & 1u) ? srow[(4 * q + 1) * STEP_BLOCK + tid] : np;
-            v.z = ((occ >> (4 * q + 2)) & 1u) ? srow[(4 * q + 2) * STEP_BLOCK + tid] : np;
-            v.w = ((occ >> (4 * q + 3)) & 1u) ? srow[(4 * q + 3) * STEP_BLOCK + tid] : np;
-            row[q] = v;
-        }
-        d.cmask[s] = occ;
-        if (dm_lo != dm_lo0 || dm_hi != dm_hi0)
-            d.dmc[s] = make_ulonglong2(dm_lo, dm_hi);
-    }
-
     const uint32_t u = d.uid[s];
     // ---- bonds: per-bond contributions in bond order (bondsLinear's serial
     // scatter order, cohesion.cuh:220-226) ------------------------------------
@@ -337,7 +380,6 @@ k_step(StepArgs args)
         }
     }
 
-    // ---- outputs of interact ------------------------------------------------
     const double dt = P.dt;
     {
         const double2 e = d.esv[s];
@@ -411,10 +453,12 @@ k_step(StepArgs args)
     d.xr[B][s] = x;
     d.vel[B][s] = vel;
     d.angvel[B][s] = angvel;
-    d.xf[B][s] = make_float4((float)x.x, (float)x.y, (float)x.z, (float)x.w);
     d.vel0[s] = vel0;
     d.angvel0[s] = angvel0;
     d.angpos[s] = angpos;
+    // float copy for the next step's contact search, at this particle's
+    // cell-list position (rewritten by the rebuild when the order changes)
+    d.xs[B][d.pos[s]] = make_float4((float)x.x, (float)x.y, (float)x.z, (float)x.w);
     if (args.write_outputs) {
         d.force[s] = make_double4(F.x, F.y, F.z, 0.0f);
         d.torque[s] = make_double4(T.x, T.y, T.z, 0.0f);
@@ -435,8 +479,9 @@ k_step(StepArgs args)
 
 void launch_step(const Dev &d, uint32_t np, int a, int write_outputs, cudaStream_t st)
 {
-    StepArgs args{d, a, write_outputs};
-    k_step<<<div_up(np, STEP_BLOCK), STEP_BLOCK, 0, st>>>(args);
+    k_topo<<<div_up(np, TOPO_BLOCK), TOPO_BLOCK, 0, st>>>(d, a);
+    ForceArgs args{d, a, write_outputs};
+    k_force<<<div_up(np, FORCE_BLOCK), FORCE_BLOCK, 0, st>>>(args);
 }
 
 }  // namespace sphk
