@@ -289,7 +289,7 @@ def gpu_arm(args, rank, world, local):
     b_step, b_whole = algorithmic_bytes(cfg.np, cfg.ncells, C, cfg.nb0)
     peak, peak_kind = measured_peak_hbm()
     achieved = b_step / (step_ms * 1e-3) / 1e9
-    kernels_per_step = 5 + (1 if cfg.nb0 else 0) + 1 + (1 if cfg.nw else 0)
+    kernels_per_step = 6 + (1 if cfg.nb0 else 0) + 2 + (1 if cfg.nw else 0)
     out = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
