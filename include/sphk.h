@@ -46,6 +46,7 @@ extern "C" {
 #define SPH_ERR_BAD_INPUT (-5)    /* invalid argument or configuration */
 #define SPH_ERR_BOND_ALIAS (-6)   /* a broken bond's marker (nb0 < np) aliases a particle */
 #define SPH_ERR_NOMEM (-7)        /* device allocation failed */
+#define SPH_ERR_TOO_LARGE (-8)    /* input exceeds the fixed scratch of sph_cell_list_noalloc */
 
 typedef struct sph_ctx sph_ctx;
 
@@ -144,6 +145,32 @@ int sph_get_profile(sph_ctx *ctx, double *ms, uint64_t *steps, int reset);
 int sph_relayout(sph_ctx *ctx);
 const char *sph_last_error(const sph_ctx *ctx);
 int sph_destroy(sph_ctx *ctx);
+
+/* ---- Cell list without device allocation ----------------------------------
+ * No counterpart in the reference: an addition for callers that cannot
+ * allocate device memory -- a plugin whose host owns the device memory pool
+ * through its own allocator and forbids cudaMalloc, or a latency-critical
+ * loop that must not pay the device-wide synchronisation of cudaMalloc and
+ * cudaFree.  Computes, for device-resident positions x_dev (np*4 doubles,
+ * x, y, z, radius, the caller's particle order), the same cell list as
+ * sph_get_cells reports for a context holding those positions: sorted cell
+ * ids and the sorted -> particle permutation (np each), cellStart (0xffffffff
+ * for empty cells) and cellEnd (0 for empty cells), ncells each.  Every
+ * output is a device pointer supplied by the caller; the work is enqueued on
+ * `stream` (a cudaStream_t; NULL is the default stream).  Only cfg->np,
+ * num, origo, L and device are read.
+ * Limits: np <= SPHK_NOALLOC_MAX_PARTICLES and num[0]*num[1]*num[2] <=
+ * SPHK_NOALLOC_MAX_CELLS, otherwise SPH_ERR_TOO_LARGE and nothing is
+ * launched.  It calls no cudaMalloc, cudaFree or allocating library routine:
+ * its scratch is one fixed array of about 8 MB inside the library, held by
+ * every GPU that loads the library until the process exits.  The first call
+ * on a device looks up that array's device address (cudaGetSymbolAddress);
+ * make that first call before any stream capture.  All calls share the
+ * array, so calls that overlap on the GPU race and give wrong results. */
+#define SPHK_NOALLOC_MAX_PARTICLES 1048576u
+#define SPHK_NOALLOC_MAX_CELLS 524288u
+int sph_cell_list_noalloc(const sph_config *cfg, const double *x_dev, uint32_t *cell_sorted,
+                          uint32_t *perm, uint32_t *cell_start, uint32_t *cell_end, void *stream);
 
 #ifdef __cplusplus
 }

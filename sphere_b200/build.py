@@ -28,7 +28,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC = os.environ.get("NVCC", shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc")
 CUDA_HOME = Path(NVCC).resolve().parent.parent
 
-KERNEL_SOURCES = ["api.cu", "step.cu", "cells.cu", "walls.cu", "bonds.cu"]
+KERNEL_SOURCES = ["api.cu", "step.cu", "cells.cu", "walls.cu", "bonds.cu", "noalloc.cu"]
 HOST_SOURCES = ["host/sphere.cpp", "host/file_io.cpp", "host/main.cpp"]
 
 

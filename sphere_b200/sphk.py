@@ -26,6 +26,7 @@ SPH_OK = 0
 ERRORS = {
     -1: "SPH_ERR_CUDA", -2: "SPH_ERR_NC_OVERFLOW", -3: "SPH_ERR_OUT_OF_GRID",
     -4: "SPH_ERR_TIMEOUT", -5: "SPH_ERR_BAD_INPUT", -6: "SPH_ERR_BOND_ALIAS", -7: "SPH_ERR_NOMEM",
+    -8: "SPH_ERR_TOO_LARGE",
 }
 OPT_RELAYOUT_EVERY = 1
 OPT_GRAPH_STEPS = 2
@@ -106,6 +107,7 @@ def load_library(path: os.PathLike | None = None):
         "sph_get_profile": ([vp, _dp, C.POINTER(C.c_uint64), C.c_int], C.c_int),
         "sph_last_error": ([vp], C.c_char_p),
         "sph_destroy": ([vp], C.c_int),
+        "sph_cell_list_noalloc": ([C.POINTER(SphConfig), vp, vp, vp, vp, vp, vp], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)

@@ -1,0 +1,64 @@
+"""sph_cell_list_noalloc: the cell list for callers that cannot allocate
+device memory (a plugin host that owns the device memory pool, or a loop
+that must not pay cudaMalloc's device-wide synchronisation).
+
+The entry point takes device-resident positions and device outputs from the
+caller and uses only a fixed scratch array inside the library.  It must give
+the same cell list as the allocating path (a context's sph_get_cells for the
+same positions), bit for bit, on consecutive calls: the shared scratch keeps
+the previous call's contents and each call must clear what it needs."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from sphere_b200 import scenes, sphk
+from sphere_b200.sphk import Simulation
+from sphere_b200.state import config_from_spherebin, state_from_spherebin
+
+pytestmark = pytest.mark.gpu
+
+
+def _noalloc(lib, cfg, x_dev, np_, ncells, torch):
+    outs = [torch.full((n,), 7, dtype=torch.int32, device="cuda") for n in (np_, np_, ncells, ncells)]
+    conf = sphk.make_config(cfg)
+    stream = torch.cuda.current_stream().cuda_stream
+    rc = lib.sph_cell_list_noalloc(C.byref(conf), C.c_void_p(x_dev.data_ptr()),
+                                   *(C.c_void_p(o.data_ptr()) for o in outs), C.c_void_p(stream))
+    assert rc == 0
+    torch.cuda.synchronize()
+    return [o.cpu().numpy().view(np.uint32) for o in outs]
+
+
+@pytest.mark.parametrize("builder", [
+    lambda: scenes.collision(n=3000, seed=71, periodic=1),
+    lambda: scenes.collision(n=2500, seed=72, periodic=0, nw=1),
+])
+def test_noalloc_cell_list_matches_context_path(builder):
+    torch = pytest.importorskip("torch")
+    sb = builder()
+    cfg = config_from_spherebin(sb)
+    st = state_from_spherebin(sb)
+    with Simulation(cfg) as sim:
+        sim.upload(st)
+        want = sim.cells()
+    lib = sphk.load_library()
+    x_dev = torch.tensor(st.x, dtype=torch.float64, device="cuda").contiguous()
+    first = _noalloc(lib, cfg, x_dev, cfg.np, cfg.ncells, torch)
+    second = _noalloc(lib, cfg, x_dev, cfg.np, cfg.ncells, torch)
+    for got in (first, second):
+        for g, w, name in zip(got, want, ("cell_sorted", "perm", "cell_start", "cell_end")):
+            assert np.array_equal(g, w), name
+
+
+def test_noalloc_rejects_sizes_beyond_its_scratch():
+    lib = sphk.load_library()
+    sb = scenes.collision(n=100, seed=73)
+    conf = sphk.make_config(config_from_spherebin(sb))
+    conf.np = sphk_max = 1048576 + 1
+    dummy = C.c_void_p(1)
+    assert lib.sph_cell_list_noalloc(C.byref(conf), dummy, dummy, dummy, dummy, dummy, None) == -8
+    conf.np = 100
+    conf.num[0], conf.num[1], conf.num[2] = 1024, 1024, 1
+    assert lib.sph_cell_list_noalloc(C.byref(conf), dummy, dummy, dummy, dummy, dummy, None) == -8
+    assert sphk_max > 1048576
