@@ -312,6 +312,7 @@ int sph_create(const sph_config *cfg, sph_ctx **out)
     // domain stay within a few domain extents, so 1e-6 * 4 * extent is a
     // generous bound on the cull's absolute error
     P.cull_eps = (float)(4e-6 * (ext > 0.0 ? ext : 1.0));
+    P.prune_pad = 4.0 * (double)P.cull_eps;
 
     const size_t np = cfg->np;
     Dev &d = c->d;
@@ -326,6 +327,7 @@ int sph_create(const sph_config *cfg, sph_ctx **out)
     AL(d.contacts, np * NC); AL(d.dmc, np); AL(d.delta_t, np * NC); AL(d.cmask, np);
     AL(d.cell_start, (size_t)ncells + 2); AL(d.cellorder, np); AL(d.pos, np); AL(d.cell_fill, (size_t)ncells + 1);
     AL(d.scan_tiles, scan_tile_count(P.ncells));
+    AL(d.alias_any, 1);
     AL(d.wf_pp, np); AL(d.wtouch, np); AL(d.wf_partial, div_up(np, 256));
     AL(d.walls, 1);
     AL(d.bonds, cfg->nb0); AL(d.bonds_delta, cfg->nb0); AL(d.bonds_omega, cfg->nb0);
@@ -377,6 +379,13 @@ int sph_upload(sph_ctx *c, const sph_host_state *h)
     // kinematics (identity storage order for now)
     std::vector<double> buf(np * 4);
     CK(cudaMemcpy(d.xr[A], h->x, np * 32, cudaMemcpyHostToDevice));
+    {
+        // largest radius, for the cell-level distance test of contact search
+        double rmax = 0.0;
+        for (size_t i = 0; i < np; ++i) rmax = std::fmax(rmax, h->x[4 * i + 3]);
+        c->hp.rmax = rmax;
+        CK(cudaMemcpy(d.prm, &c->hp, sizeof(Params), cudaMemcpyHostToDevice));
+    }
     CK(cudaMemcpy(d.vel[A], h->vel, np * 32, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(d.vel0, h->vel0 ? h->vel0 : h->vel, np * 32, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(d.angvel[A], h->angvel, np * 32, cudaMemcpyHostToDevice));

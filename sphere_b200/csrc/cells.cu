@@ -45,6 +45,7 @@ __global__ void k_count(Dev d)
     if (*d.rebuild == 0u) return;
     const Params &P = *d.prm;
     const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s == 0) *d.alias_any = 0u;   // recomputed by k_post_sort
     if (s >= P.np) return;
     atomicAdd(&d.cell_fill[d.cell[s]], 1u);
 }
@@ -173,6 +174,13 @@ __global__ void k_post_sort(Dev d, int A)
     d.pos[s] = k;
     const double4 x = d.xr[A][s];
     d.xs[A][k] = make_float4((float)x.x, (float)x.y, (float)x.z, (float)x.w);
+    // a particle whose floored coordinates leave the grid sits outside its
+    // cell's box (saturated or aliased cell id): contact search must then
+    // not prune cells by geometry
+    const double f0 = cell_floor(P, 0, x.x), f1 = cell_floor(P, 1, x.y), f2 = cell_floor(P, 2, x.z);
+    if (!(f0 >= 0.0 && f0 < (double)P.num[0] && f1 >= 0.0 && f1 < (double)P.num[1] &&
+          f2 >= 0.0 && f2 < (double)P.num[2]))
+        atomicOr(d.alias_any, 1u);
 }
 
 void launch_cell_init(const Dev &d, uint32_t np, int a, cudaStream_t st)

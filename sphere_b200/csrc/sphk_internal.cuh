@@ -61,6 +61,8 @@ struct Params {
     double lambda_bar, sigma_b, tau_b, devs_A, devs_f;
     int32_t wmode[MAXWALLS];
     float cull_eps;     // absolute FP32 slack of the neighbour cull (metres)
+    double rmax;        // largest radius of the scene (set at upload)
+    double prune_pad;   // absolute slack of the cell-level distance test (metres)
 };
 
 // Wall state (src/datatypes.h:95-100), device resident.
@@ -103,6 +105,7 @@ struct Dev {
     uint32_t *pos;        // [np] storage index -> cell-list position
     uint32_t *cell_fill;  // [ncells + 1] scratch
     uint32_t *scan_tiles; // scratch for the scan
+    uint32_t *alias_any;  // some particle sits outside its cell's box (set by the rebuild)
     // walls
     double *wf_pp;        // [np] wall-0 force by uid
     uint8_t *wtouch;      // [np] by storage index: wall-0 force was nonzero

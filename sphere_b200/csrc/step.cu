@@ -217,10 +217,38 @@ k_topo(Dev d, int A)
         return true;
     };
 
+    // Cell-level pruning: a stencil cell whose box lies farther from the
+    // particle than ra + rmax (plus the float slack of the predicate) cannot
+    // hold a contact, and skipping it leaves the visiting order of the
+    // others unchanged.  Used only while the particle's own cell is inside
+    // the grid and every particle sits inside its cell's box (alias_any
+    // clear), so the stencil geometry is the plain one.
+    const bool prune = (*d.alias_any == 0u) && gp[0] >= 0 && (uint32_t)gp[0] < nx &&
+                       gp[1] >= 0 && (uint32_t)gp[1] < ny && gp[2] >= 0 && (uint32_t)gp[2] < nz;
+    // squared distance from the particle to the slab of stencil offset -1/+1
+    // along each axis (offset 0: the particle's own slab, distance 0)
+    double flo[3], fhi[3];
+    {
+        const double xc[3] = {xa.x, xa.y, xa.z};
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+            const double lo = xc[q] - (P.origo[q] + (double)gp[q] * P.cellsize[q]);
+            const double hi = (P.origo[q] + (double)(gp[q] + 1) * P.cellsize[q]) - xc[q];
+            flo[q] = lo > 0.0 ? lo * lo : 0.0;
+            fhi[q] = hi > 0.0 ? hi * hi : 0.0;
+        }
+    }
+    const double reach = (ra + P.rmax) * (1.0 + 1e-5) + P.prune_pad;
+    const double reach2 = prune ? reach * reach : 1e300;
+
     for (int oz = -1; oz < 2; ++oz) {
         const int32_t cz = (int32_t)((uint32_t)gp[2] + (uint32_t)oz);
         if (cz < 0 || (uint32_t)cz == nz) continue;
+        const double dz2 = oz < 0 ? flo[2] : (oz > 0 ? fhi[2] : 0.0);
+        if (dz2 > reach2) continue;
         for (int oy = -1; oy < 2; ++oy) {
+            const double dyz2 = dz2 + (oy < 0 ? flo[1] : (oy > 0 ? fhi[1] : 0.0));
+            if (dyz2 > reach2) continue;
             int32_t cy = (int32_t)((uint32_t)gp[1] + (uint32_t)oy);
             uint32_t ycode = 0;
             if (P.periodic == 1) {
@@ -236,11 +264,12 @@ k_topo(Dev d, int A)
                 if (cid0 + 2 >= P.ncells) { err |= ST_OUT_OF_GRID; continue; }
                 const uint32_t b0 = d.cell_start[cid0], b1 = d.cell_start[cid0 + 1];
                 const uint32_t b2 = d.cell_start[cid0 + 2], b3 = d.cell_start[cid0 + 3];
-                scan_cell(b0, b1, ycode);
+                if (dyz2 + flo[0] <= reach2) scan_cell(b0, b1, ycode);
                 scan_cell(b1, b2, ycode);
-                scan_cell(b2, b3, ycode);
+                if (dyz2 + fhi[0] <= reach2) scan_cell(b2, b3, ycode);
             } else {
                 for (int ox = -1; ox < 2; ++ox) {
+                    if (dyz2 + (ox < 0 ? flo[0] : (ox > 0 ? fhi[0] : 0.0)) > reach2) continue;
                     int32_t cx = (int32_t)((uint32_t)gp[0] + (uint32_t)ox);
                     uint32_t code = ycode;
                     if (P.periodic == 1 || P.periodic == 2) {
@@ -278,7 +307,7 @@ struct ForceArgs {
     int write_outputs;  // store force/torque/acc/angacc/edp of this step
 };
 
-__global__ void __launch_bounds__(FORCE_BLOCK)
+__global__ void __launch_bounds__(FORCE_BLOCK, 4)
 k_force(ForceArgs args)
 {
     const Dev &d = args.d;

@@ -207,10 +207,12 @@ def bonded(seed=0, nx=40, ny=20, nz=20, r_lo=0.9e-3, r_hi=1.1e-3, pull=0.01,
 def collision(n=2000, seed=0, periodic=0, box=(0.06, 0.06, 0.06), r=(0.8e-3, 1.6e-3),
               phi_target=0.45, nw=0, vmax=0.5, wmax=200.0, g=(0.0, 0.0, -9.81),
               k_n=2e4, k_t=2e4, gamma_n=0.05, gamma_t=0.01, mu=0.4, dt=2e-6,
-              sid="collision") -> Spherebin:
+              straddle=False, sid="collision") -> Spherebin:
     """Jittered lattice with some overlap, random velocities and spins:
     contacts open, close and slide from the first step on.  The box is sized
-    so no particle reaches a periodic boundary within a few hundred steps."""
+    so no particle reaches a periodic boundary within a few hundred steps,
+    unless ``straddle`` moves the cluster across the x and y boundaries (with
+    periodic x/y, particles then leave and re-enter the grid every few steps)."""
     rng = np.random.default_rng(seed)
     radii = rng.uniform(r[0], r[1], n)
     vol = float(np.sum(V_sphere(radii)))
@@ -222,6 +224,8 @@ def collision(n=2000, seed=0, periodic=0, box=(0.06, 0.06, 0.06), r=(0.8e-3, 1.6
     Lb = np.asarray(box, float)
     center = 0.5 * Lb
     x = center - 0.5 * side + (lat + 0.5) * spacing + rng.uniform(-0.15, 0.15, (n, 3)) * spacing
+    if straddle:
+        x[:, :2] = np.mod(x[:, :2] + 0.5 * Lb[:2], Lb[:2])
     sb = Spherebin(np_=n, nw=nw, sid=sid)
     sb.radius = radii
     sb.x = x

@@ -28,7 +28,33 @@ SCENES = {
     "periodic_x_wall": lambda: scenes.collision(n=1200, seed=33, periodic=2, nw=1),
     "box_wall": lambda: scenes.collision(n=2000, seed=34, periodic=0, nw=1),
     "bonded": lambda: scenes.bonded(nx=4, ny=3, nz=3, sigma_b=1e30, tau_b=1e30),
+    # the cluster straddles the periodic x/y boundaries: cell ids saturate
+    # and alias while particles cross, which turns the cell-level pruning off
+    "periodic_crossing": lambda: _crossing(),
+    "polydisperse_small": lambda: _small_polydisperse(),
 }
+
+
+def _crossing():
+    sb = scenes.collision(n=1500, seed=35, periodic=1, straddle=True, vmax=3.0)
+    # every 10th particle sits just inside a periodic face and moves out
+    # through it, so positions leave the grid for a step before the wrap
+    rng = np.random.default_rng(36)
+    sel = np.arange(0, sb.np, 10)
+    for j, i in enumerate(sel):
+        ax = j % 2
+        hi = (j // 2) % 2 == 0
+        sb.x[i, ax] = sb.L[ax] - 1e-7 if hi else 1e-7
+        sb.vel[i, ax] = (1.0 if hi else -1.0) * rng.uniform(0.5, 2.0)
+    return sb
+
+
+def _small_polydisperse():
+    # the bench workload at 20,000 spheres with the wall lowered onto the pack
+    sb = scenes.polydisperse(n=20000, seed=5, L=(0.0543, 0.0543, 0.1086), num=(13, 13, 27))
+    sb.w_x = sb.w_x - 0.3e-3
+    sb.vel = np.random.default_rng(6).uniform(-0.05, 0.05, (sb.np, 3))
+    return sb
 
 
 def run_gpu(sb, chunks, **kw):
