@@ -284,7 +284,7 @@ def gpu_arm(args, rank, world, local):
     n_total = cfg.np * world
     value = n_total * args.steps / (ms * 1e-3)
     e2e_value = n_total * args.steps / e2e_s
-    step_ms = prof["step"] / max(1, prof["steps"])
+    step_ms = (prof["topo"] + prof["force"]) / max(1, prof["steps"])
     C = stats["active_contacts"]
     b_step, b_whole = algorithmic_bytes(cfg.np, cfg.ncells, C, cfg.nb0)
     peak, peak_kind = measured_peak_hbm()
@@ -302,14 +302,15 @@ def gpu_arm(args, rank, world, local):
                 "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
                 "seconds": e2e_s},
         "gpu_launches": kernels_per_step * args.steps,
-        "roofline": {"bound": "hbm", "kernel": "k_step", "achieved": achieved, "peak": peak,
+        "roofline": {"bound": "hbm", "kernel": "k_topo+k_force", "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
                      "traffic": ncu_traffic(cfg.np),
                      "algorithmic_bytes_per_launch": b_step,
                      "launch_ms": step_ms,
                      "whole_step_algorithmic_bytes": b_whole,
                      "whole_step_frac": (b_whole / (ms / args.steps * 1e-3) / 1e9) / peak},
-        "phase_ms_per_step": {k: prof[k] / max(1, prof["steps"]) for k in ("cells", "bonds", "step", "walls")},
+        "phase_ms_per_step": {k: prof[k] / max(1, prof["steps"])
+                              for k in ("cells", "bonds", "topo", "force", "walls")},
         "clocks": clocks.summary(),
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -105,6 +105,10 @@ typedef struct sph_stats {
 /* Options for sph_set_option. */
 #define SPH_OPT_RELAYOUT_EVERY 1  /* re-sort storage every n steps (0: at upload only) */
 #define SPH_OPT_GRAPH_STEPS 2     /* steps captured per CUDA graph (1..64, default 8) */
+#define SPH_OPT_VERLET_SKIN 4     /* Verlet skin in thousandths of the largest radius
+                                     (default 100; 0 sweeps the 27-cell stencil every
+                                     step); set before sph_upload.  Results do not depend
+                                     on it, only the cost of contact detection does. */
 #define SPH_OPT_PROFILE 3         /* 1: launch kernels one by one with CUDA events around
                                      each phase (the reference's PROFILING switch,
                                      src/debug.h:7, src/device.cu:86-102); 0: graphs */
@@ -112,9 +116,10 @@ typedef struct sph_stats {
 /* Phases timed in profile mode. */
 #define SPH_PHASE_CELLS 0   /* cell list rebuild (hash histogram, scan, scatter, sort) */
 #define SPH_PHASE_BONDS 1   /* per-bond forces */
-#define SPH_PHASE_STEP 2    /* fused contact search + forces + integration */
-#define SPH_PHASE_WALLS 3   /* wall force reduction + wall integration */
-#define SPH_NPHASES 4
+#define SPH_PHASE_TOPO 2    /* contact detection into the slots */
+#define SPH_PHASE_FORCE 3   /* contact and wall forces + integration */
+#define SPH_PHASE_WALLS 4   /* wall force reduction + wall integration */
+#define SPH_NPHASES 5
 
 int sph_version(void);
 int sph_create(const sph_config *cfg, sph_ctx **out);

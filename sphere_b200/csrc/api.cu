@@ -11,6 +11,8 @@
 
 namespace sphk {
 void launch_step(const Dev &d, uint32_t np, int a, int write_outputs, cudaStream_t st);
+void launch_topo(const Dev &d, uint32_t np, int a, cudaStream_t st);
+void launch_force(const Dev &d, uint32_t np, int a, int write_outputs, cudaStream_t st);
 void launch_bonds(const Dev &d, uint32_t nb0, int a, cudaStream_t st);
 void launch_walls(const Dev &d, uint32_t np, uint32_t nw, cudaStream_t st);
 void launch_cell_init(const Dev &d, uint32_t np, int a, cudaStream_t st);
@@ -30,6 +32,7 @@ struct sph_ctx {
     uint64_t steps = 0, relayouts = 0, since_relayout = 0;
     double t_host = 0.0;
     int64_t relayout_every = 0;
+    double skin_rel = 0.1;           // Verlet skin as a fraction of the largest radius
     int graph_steps = 8;
     bool uploaded = false;
     void *scratch = nullptr;
@@ -44,7 +47,7 @@ struct sph_ctx {
     // profile mode: events bracket each phase of each step
     bool profile = false;
     std::vector<cudaEvent_t> ev;          // 5 events per profiled step
-    double prof_ms[SPH_NPHASES] = {0, 0, 0, 0};
+    double prof_ms[SPH_NPHASES] = {};
     uint64_t prof_steps = 0;
 };
 
@@ -223,7 +226,7 @@ int ensure_graphs(sph_ctx *c)
 int profiled_step(sph_ctx *c, int a, int write_outputs, cudaStream_t st)
 {
     if (c->ev.empty()) {
-        c->ev.resize(5);
+        c->ev.resize(SPH_NPHASES + 1);
         for (auto &e : c->ev) CK(cudaEventCreate(&e));
     }
     CK(cudaEventRecord(c->ev[0], st));
@@ -231,12 +234,14 @@ int profiled_step(sph_ctx *c, int a, int write_outputs, cudaStream_t st)
     CK(cudaEventRecord(c->ev[1], st));
     launch_bonds(c->d, c->hp.nb0, a, st);
     CK(cudaEventRecord(c->ev[2], st));
-    launch_step(c->d, c->hp.np, a, write_outputs, st);
+    launch_topo(c->d, c->hp.np, a, st);
     CK(cudaEventRecord(c->ev[3], st));
-    launch_walls(c->d, c->hp.np, c->hp.nw, st);
+    launch_force(c->d, c->hp.np, a, write_outputs, st);
     CK(cudaEventRecord(c->ev[4], st));
+    launch_walls(c->d, c->hp.np, c->hp.nw, st);
+    CK(cudaEventRecord(c->ev[5], st));
     CK(cudaGetLastError());
-    CK(cudaEventSynchronize(c->ev[4]));
+    CK(cudaEventSynchronize(c->ev[5]));
     for (int k = 0; k < SPH_NPHASES; ++k) {
         float ms = 0.f;
         CK(cudaEventElapsedTime(&ms, c->ev[k], c->ev[k + 1]));
@@ -328,6 +333,8 @@ int sph_create(const sph_config *cfg, sph_ctx **out)
     AL(d.cell_start, (size_t)ncells + 2); AL(d.cellorder, np); AL(d.pos, np); AL(d.cell_fill, (size_t)ncells + 1);
     AL(d.scan_tiles, scan_tile_count(P.ncells));
     AL(d.alias_any, 1);
+    AL(d.vl, np * VL_CAP); AL(d.vl_meta, np * VL_CAP); AL(d.vl_len, np); AL(d.disp, np);
+    AL(d.movers, MOVER_CAP); AL(d.dirty, (size_t)ncells + 1); AL(d.vs, 1);
     AL(d.wf_pp, np); AL(d.wtouch, np); AL(d.wf_partial, div_up(np, 256));
     AL(d.walls, 1);
     AL(d.bonds, cfg->nb0); AL(d.bonds_delta, cfg->nb0); AL(d.bonds_omega, cfg->nb0);
@@ -348,6 +355,11 @@ int sph_set_option(sph_ctx *c, int option, int64_t value)
     if (!c) return SPH_ERR_BAD_INPUT;
     if (option == SPH_OPT_RELAYOUT_EVERY && value >= 0) {
         c->relayout_every = value;
+        return SPH_OK;
+    }
+    if (option == SPH_OPT_VERLET_SKIN && value >= 0 && value <= 1000) {
+        if (c->uploaded) return fail(c, SPH_ERR_BAD_INPUT, "set the Verlet skin before sph_upload");
+        c->skin_rel = (double)value / 1000.0;
         return SPH_OK;
     }
     if (option == SPH_OPT_PROFILE && (value == 0 || value == 1)) {
@@ -384,7 +396,14 @@ int sph_upload(sph_ctx *c, const sph_host_state *h)
         double rmax = 0.0;
         for (size_t i = 0; i < np; ++i) rmax = std::fmax(rmax, h->x[4 * i + 3]);
         c->hp.rmax = rmax;
+        c->hp.skin = c->skin_rel * rmax;
         CK(cudaMemcpy(d.prm, &c->hp, sizeof(Params), cudaMemcpyHostToDevice));
+        Verlet V{};
+        V.step = 1;
+        V.all_rebuild = 1;
+        CK(cudaMemcpy(d.vs, &V, sizeof(V), cudaMemcpyHostToDevice));
+        CK(cudaMemset(d.dirty, 0, ((size_t)c->hp.ncells + 1) * sizeof(uint32_t)));
+        CK(cudaMemset(d.vl_len, VL_NONE, np));
     }
     CK(cudaMemcpy(d.vel[A], h->vel, np * 32, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(d.vel0, h->vel0 ? h->vel0 : h->vel, np * 32, cudaMemcpyHostToDevice));

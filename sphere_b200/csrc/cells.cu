@@ -183,6 +183,48 @@ __global__ void k_post_sort(Dev d, int A)
         atomicOr(d.alias_any, 1u);
 }
 
+// Verlet lists: every cell of the 27-cell neighbourhood of a cell that
+// gained or lost a member is stamped with this step's number; particles in
+// stamped cells re-sweep their stencil (their list's membership or order may
+// have changed).  Periodic axes wrap as in findDistMod.
+__global__ void k_mark_dirty(Dev d)
+{
+    if (*d.rebuild == 0u) return;
+    const Params &P = *d.prm;
+    Verlet &V = *d.vs;
+    const uint32_t n = min(V.nmovers, MOVER_CAP);
+    if (blockIdx.x == 0 && threadIdx.x == 0 && V.movers_overflow) {
+        V.all_rebuild = 1u;
+        V.dmax_bits = 0u;
+    }
+    const uint32_t nx = P.num[0], ny = P.num[1], nz = P.num[2];
+    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < 2 * n; e += gridDim.x * blockDim.x) {
+        const uint2 mv = d.movers[e >> 1];
+        const uint32_t c = (e & 1u) ? mv.y : mv.x;
+        if (c >= P.ncells) continue;
+        const int32_t cx = (int32_t)(c % nx), cy = (int32_t)((c / nx) % ny), cz = (int32_t)(c / (nx * ny));
+        for (int oz = -1; oz < 2; ++oz) {
+            const int32_t z = cz + oz;
+            if (z < 0 || z >= (int32_t)nz) continue;
+            for (int oy = -1; oy < 2; ++oy) {
+                int32_t y = cy + oy;
+                if (y < 0 || y >= (int32_t)ny) {
+                    if (P.periodic != 1) continue;
+                    y = (y + (int32_t)ny) % (int32_t)ny;
+                }
+                for (int ox = -1; ox < 2; ++ox) {
+                    int32_t x = cx + ox;
+                    if (x < 0 || x >= (int32_t)nx) {
+                        if (P.periodic != 1 && P.periodic != 2) continue;
+                        x = (x + (int32_t)nx) % (int32_t)nx;
+                    }
+                    d.dirty[(uint32_t)x + (uint32_t)y * nx + (nx * ny) * (uint32_t)z] = V.step;
+                }
+            }
+        }
+    }
+}
+
 void launch_cell_init(const Dev &d, uint32_t np, int a, cudaStream_t st)
 {
     k_cell_init<<<div_up(np, CELL_BLOCK), CELL_BLOCK, 0, st>>>(d, a);
@@ -197,6 +239,7 @@ void launch_rebuild(const Dev &d, uint32_t np, uint32_t ncells, int a, cudaStrea
     k_scatter<<<div_up(np, CELL_BLOCK), CELL_BLOCK, 0, st>>>(d);
     k_cellsort<<<div_up((unsigned long long)ncells + 1, CELL_BLOCK), CELL_BLOCK, 0, st>>>(d);
     k_post_sort<<<div_up(np, CELL_BLOCK), CELL_BLOCK, 0, st>>>(d, a);
+    k_mark_dirty<<<64, CELL_BLOCK, 0, st>>>(d);
     cudaMemsetAsync(d.rebuild, 0, sizeof(uint32_t), st);
 }
 
@@ -248,6 +291,11 @@ __global__ void k_relayout_finish(Dev d, int A)
     d.cellorder[k] = k;
     d.pos[k] = k;
     d.sidx[d.uid[k]] = k;
+    if (k == 0) {
+        // storage indices changed: every Verlet list is stale
+        d.vs->all_rebuild = 1u;
+        d.vs->dmax_bits = 0u;
+    }
     const double4 x = d.xr[A][k];
     d.xs[A][k] = make_float4((float)x.x, (float)x.y, (float)x.z, (float)x.w);
 }

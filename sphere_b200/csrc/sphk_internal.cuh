@@ -63,6 +63,23 @@ struct Params {
     float cull_eps;     // absolute FP32 slack of the neighbour cull (metres)
     double rmax;        // largest radius of the scene (set at upload)
     double prune_pad;   // absolute slack of the cell-level distance test (metres)
+    double skin;        // Verlet-list skin (metres); 0 disables the lists
+};
+
+constexpr int VL_CAP = 32;              // candidates kept per particle
+constexpr uint8_t VL_NONE = 0xff;       // no usable list: sweep the stencil
+constexpr uint32_t MOVER_CAP = 1u << 16;
+
+// State of the Verlet-list epoch, device resident.  An epoch starts with a
+// full sweep of every particle; lists stay exact while 4 * dmax < skin, where
+// dmax bounds how far any particle moved since the epoch started.
+struct Verlet {
+    uint32_t step;          // number of the step about to run (dirty stamps)
+    uint32_t all_rebuild;   // every particle sweeps in this step
+    uint32_t dmax_bits;     // float bits of the displacement bound (atomicMax)
+    uint32_t nmovers;       // particles that changed cell in the last step
+    uint32_t movers_overflow;
+    uint32_t pad[3];
 };
 
 // Wall state (src/datatypes.h:95-100), device resident.
@@ -106,6 +123,14 @@ struct Dev {
     uint32_t *cell_fill;  // [ncells + 1] scratch
     uint32_t *scan_tiles; // scratch for the scan
     uint32_t *alias_any;  // some particle sits outside its cell's box (set by the rebuild)
+    // Verlet lists
+    uint32_t *vl;         // [np][VL_CAP] candidate storage indices, in visiting order
+    uint16_t *vl_meta;    // [np][VL_CAP] stencil cell (0..26) | shift code << 5
+    uint8_t *vl_len;      // [np] list length or VL_NONE
+    float *disp;          // [np] displacement bound since the epoch started
+    uint2 *movers;        // [MOVER_CAP] (old cell, new cell) of the last step
+    uint32_t *dirty;      // [ncells + 1] step stamp: a neighbour cell changed members
+    Verlet *vs;
     // walls
     double *wf_pp;        // [np] wall-0 force by uid
     uint8_t *wtouch;      // [np] by storage index: wall-0 force was nonzero

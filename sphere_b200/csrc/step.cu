@@ -129,6 +129,81 @@ __device__ __forceinline__ void wrap_axis(int32_t &c, uint32_t num, uint32_t &co
     if ((uint32_t)c == num) { c = 0; code |= bit_hi; }
 }
 
+// Slot state of one particle during contact detection.
+struct TopoSlots {
+    uint32_t occ;                    // occupied-slot mask
+    uint32_t err;
+    unsigned long long dm_lo, dm_hi; // periodic shift code of each slot
+    int nc;                          // contacts found this step
+    bool loaded;                     // row copied to shared memory
+    bool dirty;                      // row changed
+};
+
+// Candidate t (storage index) reached through a stencil cell with shift
+// `code`: the reference's exact overlap predicate, then the slot choice.
+// Returns false once nc > NC, which ends the current cell (the reference
+// returns from findContactsInCell).  Kept out of line: it runs for a few
+// candidates per particle, and inlining it would raise the register count
+// of the whole candidate loop.
+__device__ __noinline__ bool topo_hit(const Dev &d, const Params &P, const double4 *xr,
+                                      uint32_t *srow, int tid, uint32_t s, uint32_t t,
+                                      uint32_t code, double4 xa, TopoSlots &ts)
+{
+    const double4 xb = xr[t];
+    const d3 dm = decode_dm(code, P);
+    const d3 xab = add(mk(xa.x - xb.x, xa.y - xb.y, xa.z - xb.z), dm);
+    const double delta = flen(xab) - (xa.w + xb.w);
+    if (!(delta < 0.0f)) return true;
+    if (!ts.loaded) {
+        if (ts.occ) {
+            const uint4 *row = reinterpret_cast<const uint4 *>(d.contacts + (size_t)s * NC);
+#pragma unroll
+            for (int q = 0; q < NC / 4; ++q) {
+                const uint4 v = row[q];
+                srow[(4 * q + 0) * TOPO_BLOCK + tid] = v.x;
+                srow[(4 * q + 1) * TOPO_BLOCK + tid] = v.y;
+                srow[(4 * q + 2) * TOPO_BLOCK + tid] = v.z;
+                srow[(4 * q + 3) * TOPO_BLOCK + tid] = v.w;
+            }
+            const ulonglong2 c2 = d.dmc[s];
+            ts.dm_lo = c2.x;
+            ts.dm_hi = c2.y;
+        }
+        ts.loaded = true;
+    }
+    // slot choice, src/contactsearch.cuh:252-271: a slot already holding t
+    // wins, else the last empty slot, else position nc
+    int cpos = -1;
+    for (uint32_t m = ts.occ; m; m &= m - 1) {
+        const int i = __ffs(m) - 1;
+        if (srow[i * TOPO_BLOCK + tid] == t) { cpos = i; break; }
+    }
+    if (cpos < 0) {
+        const uint32_t empty = ~ts.occ;
+        cpos = empty ? 31 - __clz(empty) : ts.nc;
+    }
+    if (cpos < NC) {
+        ts.occ |= 1u << cpos;
+        srow[cpos * TOPO_BLOCK + tid] = t;
+        dm_set(ts.dm_lo, ts.dm_hi, cpos, code);
+        ts.dirty = true;
+    } else {
+        ts.err |= ST_NC_OVERFLOW;
+    }
+    return ++ts.nc <= NC;
+}
+
+// k_topo: one thread per cell-list position k, particle s = cellorder[k].
+//
+// List mode: while the particle's Verlet list is valid (no epoch restart, no
+// cell of its neighbourhood changed members this step) only the listed
+// candidates are tested, in their recorded order.  The list holds, in the
+// reference's visiting order, every member of the stencil cells that was
+// within ra + rb + skin when it was recorded; a pair missing from it is at
+// least skin - 4 dmax > 0 apart now, so it cannot overlap.
+//
+// Sweep mode: the 27 stencil cells are scanned as in the reference (z, y, x;
+// members by particle index) and the list is recorded on the way.
 __global__ void __launch_bounds__(TOPO_BLOCK)
 k_topo(Dev d, int A)
 {
@@ -137,155 +212,180 @@ k_topo(Dev d, int A)
     const uint32_t np = P.np;
     const int tid = threadIdx.x;
     const uint32_t k = blockIdx.x * TOPO_BLOCK + tid;
+    if (k == 0) {
+        // the movers of the last step have been consumed by the rebuild
+        d.vs->nmovers = 0u;
+        d.vs->movers_overflow = 0u;
+    }
     if (k >= np) return;
     const uint32_t s = d.cellorder[k];
-    const float4 xaf = d.xs[A][k];
     const double4 xa = d.xr[A][s];
     const double ra = xa.w;
-    uint32_t occ = d.cmask[s];
-    const float4 *__restrict__ xs = d.xs[A];
-    bool loaded = false, dirty = false;
-    unsigned long long dm_lo = 0, dm_hi = 0;
-    uint32_t err = 0;
-    int nc = 0;
+    const double4 *__restrict__ xr = d.xr[A];
+    TopoSlots ts{d.cmask[s], 0u, 0ull, 0ull, 0, false, false};
+    const Verlet &V = *d.vs;
+    const uint32_t nx = P.num[0], ny = P.num[1], nz = P.num[2];
     int32_t gp[3];
     gp[0] = __double2int_rz(cell_floor(P, 0, xa.x));
     gp[1] = __double2int_rz(cell_floor(P, 1, xa.y));
     gp[2] = __double2int_rz(cell_floor(P, 2, xa.z));
-    const float Lf0 = (float)P.L[0], Lf1 = (float)P.L[1];
-    const float eps = P.cull_eps;
-    const uint32_t nx = P.num[0], ny = P.num[1], nz = P.num[2];
+    const bool gp_in = gp[0] >= 0 && (uint32_t)gp[0] < nx && gp[1] >= 0 && (uint32_t)gp[1] < ny &&
+                       gp[2] >= 0 && (uint32_t)gp[2] < nz;
+    const bool use_lists = P.skin > 0.0 && gp_in;
+    const uint8_t len = d.vl_len[s];
+    const bool list_ok = use_lists && !V.all_rebuild && len != VL_NONE &&
+                         d.dirty[d.cell[s]] != V.step;
 
-    // one cell: members in particle-index order; false once nc > NC, which
-    // ends the cell (the reference returns from findContactsInCell)
-    auto scan_cell = [&](uint32_t beg, uint32_t end, uint32_t code) {
-        const float sx = (code & 1u) ? Lf0 : ((code & 2u) ? -Lf0 : 0.0f);
-        const float sy = (code & 4u) ? Lf1 : ((code & 8u) ? -Lf1 : 0.0f);
-        for (uint32_t k2 = beg; k2 < end; ++k2) {
-            if (k2 == k) continue;
-            const float4 xbf = __ldg(&xs[k2]);
-            const float fx = (xaf.x - xbf.x) + sx;
-            const float fy = (xaf.y - xbf.y) + sy;
-            const float fz = xaf.z - xbf.z;
-            const float d2 = __fmaf_rn(fx, fx, __fmaf_rn(fy, fy, fz * fz));
-            const float rr = (xaf.w + xbf.w) * 1.000004f + eps;
-            if (d2 >= rr * rr) continue;
-            const uint32_t t = __ldg(&d.cellorder[k2]);
-            const double4 xb = d.xr[A][t];
-            const d3 dm = decode_dm(code, P);
-            const d3 xab = add(mk(xa.x - xb.x, xa.y - xb.y, xa.z - xb.z), dm);
-            const double delta = flen(xab) - (ra + xb.w);
-            if (!(delta < 0.0f)) continue;
-            if (!loaded) {
-                if (occ) {
-                    const uint4 *row = reinterpret_cast<const uint4 *>(d.contacts + (size_t)s * NC);
+    if (list_ok) {
+        const uint32_t *vl = d.vl + (size_t)s * VL_CAP;
+        const uint16_t *vm = d.vl_meta + (size_t)s * VL_CAP;
+        int skip_slot = -1;
+        for (uint32_t e = 0; e < len; ++e) {
+            const uint32_t meta = vm[e];
+            const int slot = (int)(meta & 31u);
+            if (slot == skip_slot) continue;   // nc > NC: rest of that cell
+            if (!topo_hit(d, P, xr, srow, tid, s, vl[e], meta >> 5, xa, ts)) skip_slot = slot;
+        }
+    } else {
+        const float4 *__restrict__ xs = d.xs[A];
+        const float4 xaf = xs[k];
+        const float Lf0 = (float)P.L[0], Lf1 = (float)P.L[1];
+        const float eps = P.cull_eps;
+        const float skinf = (float)P.skin;
+        uint32_t *vl = d.vl + (size_t)s * VL_CAP;
+        uint16_t *vm = d.vl_meta + (size_t)s * VL_CAP;
+        uint32_t nlist = 0;
+        bool list_overflow = false;
+
+        // A run [beg, end) of cell-list positions (one cell, or the three
+        // cells of an x-row whose inner boundaries are bnd1 <= bnd2, stencil
+        // slots slot0 .. slot0 + 2), culled four candidates at a time so the
+        // four loads are in flight together; hits are handled in list order.
+        auto scan_run = [&](uint32_t beg, uint32_t end, uint32_t code, uint32_t bnd1,
+                            uint32_t bnd2, uint32_t slot0) {
+            const float sx = (code & 1u) ? Lf0 : ((code & 2u) ? -Lf0 : 0.0f);
+            const float sy = (code & 4u) ? Lf1 : ((code & 8u) ? -Lf1 : 0.0f);
+            uint32_t base = beg;
+            while (base < end) {
+                const uint32_t last = end - 1;
+                float4 c[4];
 #pragma unroll
-                    for (int q = 0; q < NC / 4; ++q) {
-                        const uint4 v = row[q];
-                        srow[(4 * q + 0) * TOPO_BLOCK + tid] = v.x;
-                        srow[(4 * q + 1) * TOPO_BLOCK + tid] = v.y;
-                        srow[(4 * q + 2) * TOPO_BLOCK + tid] = v.z;
-                        srow[(4 * q + 3) * TOPO_BLOCK + tid] = v.w;
-                    }
-                    const ulonglong2 c2 = d.dmc[s];
-                    dm_lo = c2.x;
-                    dm_hi = c2.y;
-                }
-                loaded = true;
-            }
-            // slot choice, src/contactsearch.cuh:252-271: a slot already
-            // holding t wins, else the last empty slot, else position nc
-            int cpos = -1;
-            for (uint32_t m = occ; m; m &= m - 1) {
-                const int i = __ffs(m) - 1;
-                if (srow[i * TOPO_BLOCK + tid] == t) { cpos = i; break; }
-            }
-            if (cpos < 0) {
-                const uint32_t empty = ~occ;
-                cpos = empty ? 31 - __clz(empty) : nc;
-            }
-            if (cpos < NC) {
-                occ |= 1u << cpos;
-                srow[cpos * TOPO_BLOCK + tid] = t;
-                dm_set(dm_lo, dm_hi, cpos, code);
-                dirty = true;
-            } else {
-                err |= ST_NC_OVERFLOW;
-            }
-            if (++nc > NC) return false;
-        }
-        return true;
-    };
-
-    // Cell-level pruning: a stencil cell whose box lies farther from the
-    // particle than ra + rmax (plus the float slack of the predicate) cannot
-    // hold a contact, and skipping it leaves the visiting order of the
-    // others unchanged.  Used only while the particle's own cell is inside
-    // the grid and every particle sits inside its cell's box (alias_any
-    // clear), so the stencil geometry is the plain one.
-    const bool prune = (*d.alias_any == 0u) && gp[0] >= 0 && (uint32_t)gp[0] < nx &&
-                       gp[1] >= 0 && (uint32_t)gp[1] < ny && gp[2] >= 0 && (uint32_t)gp[2] < nz;
-    // squared distance from the particle to the slab of stencil offset -1/+1
-    // along each axis (offset 0: the particle's own slab, distance 0)
-    double flo[3], fhi[3];
-    {
-        const double xc[3] = {xa.x, xa.y, xa.z};
+                for (int j = 0; j < 4; ++j) c[j] = __ldg(&xs[min(base + (uint32_t)j, last)]);
+                uint32_t near = 0, hit = 0;
 #pragma unroll
-        for (int q = 0; q < 3; ++q) {
-            const double lo = xc[q] - (P.origo[q] + (double)gp[q] * P.cellsize[q]);
-            const double hi = (P.origo[q] + (double)(gp[q] + 1) * P.cellsize[q]) - xc[q];
-            flo[q] = lo > 0.0 ? lo * lo : 0.0;
-            fhi[q] = hi > 0.0 ? hi * hi : 0.0;
-        }
-    }
-    const double reach = (ra + P.rmax) * (1.0 + 1e-5) + P.prune_pad;
-    const double reach2 = prune ? reach * reach : 1e300;
-
-    for (int oz = -1; oz < 2; ++oz) {
-        const int32_t cz = (int32_t)((uint32_t)gp[2] + (uint32_t)oz);
-        if (cz < 0 || (uint32_t)cz == nz) continue;
-        const double dz2 = oz < 0 ? flo[2] : (oz > 0 ? fhi[2] : 0.0);
-        if (dz2 > reach2) continue;
-        for (int oy = -1; oy < 2; ++oy) {
-            const double dyz2 = dz2 + (oy < 0 ? flo[1] : (oy > 0 ? fhi[1] : 0.0));
-            if (dyz2 > reach2) continue;
-            int32_t cy = (int32_t)((uint32_t)gp[1] + (uint32_t)oy);
-            uint32_t ycode = 0;
-            if (P.periodic == 1) {
-                wrap_axis(cy, ny, ycode, 4u, 8u);
-            } else if (cy < 0 || (uint32_t)cy == ny) {
-                continue;
-            }
-            const uint32_t rowbase = (uint32_t)cy * nx + (nx * ny) * (uint32_t)cz;
-            const int32_t c0 = gp[0] - 1;
-            if (c0 >= 0 && (uint32_t)c0 + 2 < nx) {
-                // the three x cells are consecutive ids: one run of xs
-                const uint32_t cid0 = (uint32_t)c0 + rowbase;
-                if (cid0 + 2 >= P.ncells) { err |= ST_OUT_OF_GRID; continue; }
-                const uint32_t b0 = d.cell_start[cid0], b1 = d.cell_start[cid0 + 1];
-                const uint32_t b2 = d.cell_start[cid0 + 2], b3 = d.cell_start[cid0 + 3];
-                if (dyz2 + flo[0] <= reach2) scan_cell(b0, b1, ycode);
-                scan_cell(b1, b2, ycode);
-                if (dyz2 + fhi[0] <= reach2) scan_cell(b2, b3, ycode);
-            } else {
-                for (int ox = -1; ox < 2; ++ox) {
-                    if (dyz2 + (ox < 0 ? flo[0] : (ox > 0 ? fhi[0] : 0.0)) > reach2) continue;
-                    int32_t cx = (int32_t)((uint32_t)gp[0] + (uint32_t)ox);
-                    uint32_t code = ycode;
-                    if (P.periodic == 1 || P.periodic == 2) {
-                        wrap_axis(cx, nx, code, 1u, 2u);
-                    } else if (cx < 0 || (uint32_t)cx == nx) {
-                        continue;
+                for (int j = 0; j < 4; ++j) {
+                    const float fx = (xaf.x - c[j].x) + sx;
+                    const float fy = (xaf.y - c[j].y) + sy;
+                    const float fz = xaf.z - c[j].z;
+                    const float d2 = __fmaf_rn(fx, fx, __fmaf_rn(fy, fy, fz * fz));
+                    const float rr = (xaf.w + c[j].w) * 1.000004f + eps;
+                    const float rs = (xaf.w + c[j].w + skinf) * 1.000004f + eps;
+                    const uint32_t k2 = base + (uint32_t)j;
+                    const bool ok = k2 < end && k2 != k;
+                    if (ok && d2 < rs * rs) near |= 1u << j;
+                    if (ok && d2 < rr * rr) hit |= 1u << j;
+                }
+                uint32_t next = base + 4;
+                while (near) {
+                    const int j = __ffs(near) - 1;
+                    near &= near - 1;
+                    const uint32_t k2 = base + (uint32_t)j;
+                    const uint32_t t = __ldg(&d.cellorder[k2]);
+                    const uint32_t slot = slot0 + ((k2 < bnd1) ? 0u : ((k2 < bnd2) ? 1u : 2u));
+                    if (!use_lists) {
+                    } else if (nlist < VL_CAP) {
+                        vl[nlist] = t;
+                        vm[nlist] = (uint16_t)(slot | (code << 5));
+                        ++nlist;
+                    } else {
+                        list_overflow = true;
                     }
-                    const uint32_t cid = (uint32_t)cx + rowbase;
-                    if (cid >= P.ncells) { err |= ST_OUT_OF_GRID; continue; }
-                    scan_cell(d.cell_start[cid], d.cell_start[cid + 1], code);
+                    if ((hit >> j) & 1u) {
+                        if (!topo_hit(d, P, xr, srow, tid, s, t, code, xa, ts)) {
+                            // nc > NC: skip the rest of this cell; the list
+                            // would not describe the skipped part
+                            next = (k2 < bnd1) ? bnd1 : ((k2 < bnd2) ? bnd2 : end);
+                            near = 0;
+                            list_overflow = true;
+                        }
+                    }
+                }
+                base = next;
+            }
+        };
+
+        // Cell-level pruning: a stencil cell whose box lies farther from the
+        // particle than ra + rmax + skin (plus the float slack of the
+        // predicate) holds neither a contact nor a list candidate; skipping
+        // it leaves the visiting order of the others unchanged.  Used only
+        // while the particle's own cell is inside the grid and every
+        // particle sits inside its cell's box (alias_any clear).
+        const bool prune = gp_in && (*d.alias_any == 0u);
+        float flo[3], fhi[3];
+        {
+            const double xc[3] = {xa.x, xa.y, xa.z};
+#pragma unroll
+            for (int q = 0; q < 3; ++q) {
+                const double lo = xc[q] - (P.origo[q] + (double)gp[q] * P.cellsize[q]);
+                const double hi = (P.origo[q] + (double)(gp[q] + 1) * P.cellsize[q]) - xc[q];
+                flo[q] = lo > 0.0 ? (float)(lo * lo) * 0.99999f : 0.0f;
+                fhi[q] = hi > 0.0 ? (float)(hi * hi) * 0.99999f : 0.0f;
+            }
+        }
+        const float reach = (float)((ra + P.rmax + P.skin) * (1.0 + 1e-5) + P.prune_pad);
+        const float reach2 = prune ? reach * reach : 3.0e38f;
+
+        for (int oz = -1; oz < 2; ++oz) {
+            const int32_t cz = (int32_t)((uint32_t)gp[2] + (uint32_t)oz);
+            if (cz < 0 || (uint32_t)cz == nz) continue;
+            const float dz2 = oz < 0 ? flo[2] : (oz > 0 ? fhi[2] : 0.0f);
+            if (dz2 > reach2) continue;
+            for (int oy = -1; oy < 2; ++oy) {
+                const float dyz2 = dz2 + (oy < 0 ? flo[1] : (oy > 0 ? fhi[1] : 0.0f));
+                if (dyz2 > reach2) continue;
+                int32_t cy = (int32_t)((uint32_t)gp[1] + (uint32_t)oy);
+                uint32_t ycode = 0;
+                if (P.periodic == 1) {
+                    wrap_axis(cy, ny, ycode, 4u, 8u);
+                } else if (cy < 0 || (uint32_t)cy == ny) {
+                    continue;
+                }
+                const uint32_t rowbase = (uint32_t)cy * nx + (nx * ny) * (uint32_t)cz;
+                const uint32_t slot0 = (uint32_t)((oz + 1) * 9 + (oy + 1) * 3);
+                const int32_t c0 = gp[0] - 1;
+                if (c0 >= 0 && (uint32_t)c0 + 2 < nx) {
+                    // the three x cells are consecutive ids: one run of xs
+                    const uint32_t cid0 = (uint32_t)c0 + rowbase;
+                    if (cid0 + 2 >= P.ncells) { ts.err |= ST_OUT_OF_GRID; continue; }
+                    const uint32_t b0 = d.cell_start[cid0], b1 = d.cell_start[cid0 + 1];
+                    const uint32_t b2 = d.cell_start[cid0 + 2], b3 = d.cell_start[cid0 + 3];
+                    const uint32_t lo = (dyz2 + flo[0] <= reach2) ? b0 : b1;
+                    const uint32_t hi = (dyz2 + fhi[0] <= reach2) ? b3 : b2;
+                    scan_run(lo, hi, ycode, b1, b2, slot0);
+                } else {
+                    for (int ox = -1; ox < 2; ++ox) {
+                        if (dyz2 + (ox < 0 ? flo[0] : (ox > 0 ? fhi[0] : 0.0f)) > reach2) continue;
+                        int32_t cx = (int32_t)((uint32_t)gp[0] + (uint32_t)ox);
+                        uint32_t code = ycode;
+                        if (P.periodic == 1 || P.periodic == 2) {
+                            wrap_axis(cx, nx, code, 1u, 2u);
+                        } else if (cx < 0 || (uint32_t)cx == nx) {
+                            continue;
+                        }
+                        const uint32_t cid = (uint32_t)cx + rowbase;
+                        if (cid >= P.ncells) { ts.err |= ST_OUT_OF_GRID; continue; }
+                        const uint32_t e = d.cell_start[cid + 1];
+                        scan_run(d.cell_start[cid], e, code, e, e, slot0 + (uint32_t)(ox + 1));
+                    }
                 }
             }
         }
+        d.vl_len[s] = (use_lists && !list_overflow) ? (uint8_t)nlist : VL_NONE;
     }
-    if (dirty) {
+
+    if (ts.dirty) {
         uint4 *row = reinterpret_cast<uint4 *>(d.contacts + (size_t)s * NC);
+        const uint32_t occ = ts.occ;
 #pragma unroll
         for (int q = 0; q < NC / 4; ++q) {
             uint4 v;
@@ -296,9 +396,9 @@ k_topo(Dev d, int A)
             row[q] = v;
         }
         d.cmask[s] = occ;
-        d.dmc[s] = make_ulonglong2(dm_lo, dm_hi);
+        d.dmc[s] = make_ulonglong2(ts.dm_lo, ts.dm_hi);
     }
-    if (err) atomicOr(d.status, err);
+    if (ts.err) atomicOr(d.status, ts.err);
 }
 
 struct ForceArgs {
@@ -496,21 +596,48 @@ k_force(ForceArgs args)
         d.edp[s] = make_double4(es_dot, ev_dot, p, 0.0);
     }
 
+    // ---- displacement bound since the Verlet epoch started ----------------
+    Verlet &V = *d.vs;
+    if (P.skin > 0.0) {
+        const double ix = vel0.x * dt, iy = vel0.y * dt, iz = vel0.z * dt;
+        const float inc = __fadd_ru(__fmul_ru((float)sqrt(ix * ix + iy * iy + iz * iz), 1.0001f), 1e-15f);
+        const float dnew = __fadd_ru(V.all_rebuild ? 0.0f : d.disp[s], inc);
+        d.disp[s] = dnew;
+        const uint32_t bits = __reduce_max_sync(__activemask(), __float_as_uint(dnew));
+        if ((threadIdx.x & 31u) == (uint32_t)(__ffs(__activemask()) - 1)) atomicMax(&V.dmax_bits, bits);
+    }
+
     // ---- cell of the new position, for the next step's cell list -----------
     uint32_t c = cell_id(P, x.x, x.y, x.z);
     if (c >= P.ncells) { err |= ST_OUT_OF_GRID; c = P.ncells; }
-    if (c != d.cell[s]) {
+    const uint32_t c_old = d.cell[s];
+    if (c != c_old) {
         d.cell[s] = c;
         *d.rebuild = 1u;
+        if (P.skin > 0.0) {
+            const uint32_t m = atomicAdd(&V.nmovers, 1u);
+            if (m < MOVER_CAP) d.movers[m] = make_uint2(c_old, c);
+            else V.movers_overflow = 1u;
+        }
     }
     if (err) atomicOr(d.status, err);
 }
 
-void launch_step(const Dev &d, uint32_t np, int a, int write_outputs, cudaStream_t st)
+void launch_topo(const Dev &d, uint32_t np, int a, cudaStream_t st)
 {
     k_topo<<<div_up(np, TOPO_BLOCK), TOPO_BLOCK, 0, st>>>(d, a);
+}
+
+void launch_force(const Dev &d, uint32_t np, int a, int write_outputs, cudaStream_t st)
+{
     ForceArgs args{d, a, write_outputs};
     k_force<<<div_up(np, FORCE_BLOCK), FORCE_BLOCK, 0, st>>>(args);
+}
+
+void launch_step(const Dev &d, uint32_t np, int a, int write_outputs, cudaStream_t st)
+{
+    launch_topo(d, np, a, st);
+    launch_force(d, np, a, write_outputs, st);
 }
 
 }  // namespace sphk

@@ -14,62 +14,99 @@ namespace sphk {
 
 constexpr int WALL_BLOCK = 256;
 
+// Verlet epoch decision for the next step: lists stay exact while
+// 4 * dmax < skin; otherwise every particle sweeps and a new epoch starts.
+__device__ void step_tail(const Dev &d)
+{
+    const Params &P = *d.prm;
+    Verlet &V = *d.vs;
+    const float dmax = __uint_as_float(V.dmax_bits);
+    const bool restart = P.skin > 0.0 && 4.0 * (double)dmax >= 0.999 * P.skin;
+    V.all_rebuild = restart ? 1u : 0u;
+    if (restart) V.dmax_bits = 0u;
+    V.step += 1u;
+}
+
+constexpr int REF_BLOCK = 256;               // the reference's summation block
+constexpr int WARPS = WALL_BLOCK / 32;        // reference blocks per CUDA block
+constexpr int FOLD = 16;                      // partials per thread in the fold
+
 __global__ void __launch_bounds__(WALL_BLOCK)
 k_walls(Dev d)
 {
-    __shared__ double cache[WALL_BLOCK];
-    __shared__ double nz[WALL_BLOCK];
+    __shared__ double nz[WALL_BLOCK * FOLD];
+    __shared__ uint32_t warp_tot[WARPS];
     __shared__ int is_last;
-    __shared__ int n_nz;
     const Params &P = *d.prm;
     const uint32_t np = P.np;
-    const unsigned int t = threadIdx.x;
-    const unsigned int nblk = gridDim.x;
-    unsigned int idx = t + blockIdx.x * WALL_BLOCK;
-    double temp = 0.0f;
-    while (idx < np) {
-        temp += d.wf_pp[idx];
-        idx += WALL_BLOCK * nblk;
+    const unsigned int t = threadIdx.x, lane = t & 31u, warp = t >> 5;
+    const uint32_t nref = (np + REF_BLOCK - 1) / REF_BLOCK;
+
+    // One warp evaluates one reference block's halving tree in its exact
+    // pairing order: lane l holds c[l + 32 m], m = 0..7; levels 128, 64 and
+    // 32 pair registers of a lane, levels 16..1 pair lanes (shfl_down).
+    const uint32_t rb = blockIdx.x * WARPS + warp;
+    if (rb < nref) {
+        double c[8];
+#pragma unroll
+        for (int m = 0; m < 8; ++m) {
+            const uint32_t idx = rb * REF_BLOCK + lane + 32u * m;
+            double temp = 0.0f;
+            if (idx < np) temp += d.wf_pp[idx];
+            c[m] = temp;
+        }
+        double a0 = c[0] + c[4], a1 = c[1] + c[5], a2 = c[2] + c[6], a3 = c[3] + c[7];
+        double b0 = a0 + a2, b1 = a1 + a3;
+        double e = b0 + b1;
+#pragma unroll
+        for (int i = 16; i != 0; i /= 2) e += __shfl_down_sync(0xffffffffu, e, i);
+        if (lane == 0) d.wf_partial[rb] = e;
     }
-    cache[t] = temp;
     __syncthreads();
-    for (unsigned int i = WALL_BLOCK / 2; i != 0; i /= 2) {
-        if (t < i) cache[t] += cache[t + i];
-        __syncthreads();
-    }
     if (t == 0) {
-        d.wf_partial[blockIdx.x] = cache[0];
         __threadfence();
         const unsigned int ticket = atomicAdd(&d.walls->done_blocks, 1u);
-        is_last = (ticket == nblk - 1);
+        is_last = (ticket == gridDim.x - 1);
     }
     __syncthreads();
     if (!is_last) return;
     __threadfence();
 
-    // serial fold of the partials in block order (nonzero ones only)
+    // Serial fold of the partials in block order (integration.cuh:249-252),
+    // over the nonzero ones: each round loads WALL_BLOCK * FOLD partials at
+    // once, compacts the nonzero ones in order into shared memory, and one
+    // thread adds them up.
     double sum = 0.0;
-    for (unsigned int base = 0; base < nblk; base += WALL_BLOCK) {
-        const unsigned int b = base + t;
-        const double v = (b < nblk) ? __ldcg(&d.wf_partial[b]) : 0.0;
-        const bool keep = (b < nblk) && (__double_as_longlong(v) != 0ll);
-        // order-preserving compaction of the nonzero partials of this chunk
-        const unsigned int lane = t & 31u, warp = t >> 5;
-        const unsigned int bal = __ballot_sync(0xffffffffu, keep);
-        __shared__ unsigned int wcount[WALL_BLOCK / 32];
-        if (lane == 0) wcount[warp] = __popc(bal);
-        __syncthreads();
-        unsigned int off = 0;
-        for (unsigned int w = 0; w < warp; ++w) off += wcount[w];
-        if (keep) nz[off + __popc(bal & ((1u << lane) - 1u))] = v;
-        if (t == 0) {
-            unsigned int tot = 0;
-            for (unsigned int w = 0; w < WALL_BLOCK / 32; ++w) tot += wcount[w];
-            n_nz = (int)tot;
+    for (uint32_t base = 0; base < nref; base += WALL_BLOCK * FOLD) {
+        double v[FOLD];
+        uint32_t cnt = 0;
+#pragma unroll
+        for (int q = 0; q < FOLD; ++q) {
+            const uint32_t b = base + t * FOLD + q;
+            v[q] = (b < nref) ? __ldcg(&d.wf_partial[b]) : 0.0;
+            cnt += (__double_as_longlong(v[q]) != 0ll) ? 1u : 0u;
         }
+        uint32_t inc = cnt;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= (unsigned)o) inc += y;
+        }
+        if (lane == 31) warp_tot[warp] = inc;
+        __syncthreads();
+        uint32_t off = 0, tot = 0;
+#pragma unroll
+        for (int w = 0; w < WARPS; ++w) {
+            if ((unsigned)w < warp) off += warp_tot[w];
+            tot += warp_tot[w];
+        }
+        off += inc - cnt;
+#pragma unroll
+        for (int q = 0; q < FOLD; ++q)
+            if (__double_as_longlong(v[q]) != 0ll) nz[off++] = v[q];
         __syncthreads();
         if (t == 0)
-            for (int k = 0; k < n_nz; ++k) sum += nz[k];
+            for (uint32_t k = 0; k < tot; ++k) sum += nz[k];
         __syncthreads();
     }
 
@@ -101,13 +138,24 @@ k_walls(Dev d)
     if (t == 0) {
         W.t_current += P.dt;
         W.done_blocks = 0;
+        step_tail(d);
     }
+}
+
+// End of a step without walls: only the Verlet epoch bookkeeping.
+__global__ void k_tail(Dev d)
+{
+    if (threadIdx.x == 0) step_tail(d);
 }
 
 void launch_walls(const Dev &d, uint32_t np, uint32_t nw, cudaStream_t st)
 {
-    if (nw == 0) return;
-    k_walls<<<div_up(np, WALL_BLOCK), WALL_BLOCK, 0, st>>>(d);
+    if (nw == 0) {
+        k_tail<<<1, 32, 0, st>>>(d);
+        return;
+    }
+    const unsigned int nref = div_up(np, REF_BLOCK);
+    k_walls<<<div_up(nref, WARPS), WALL_BLOCK, 0, st>>>(d);
 }
 
 }  // namespace sphk

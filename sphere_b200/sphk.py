@@ -31,7 +31,8 @@ ERRORS = {
 OPT_RELAYOUT_EVERY = 1
 OPT_GRAPH_STEPS = 2
 OPT_PROFILE = 3
-PHASES = ("cells", "bonds", "step", "walls")
+OPT_VERLET_SKIN = 4
+PHASES = ("cells", "bonds", "topo", "force", "walls")
 
 _dp = C.POINTER(C.c_double)
 _up = C.POINTER(C.c_uint32)
@@ -160,7 +161,9 @@ class Simulation:
     """One DEM simulation resident on a GPU."""
 
     def __init__(self, cfg: SceneConfig, device: int = 0, graph_steps: int | None = None,
-                 relayout_every: int | None = None):
+                 relayout_every: int | None = None, verlet_skin: float | None = None):
+        """``verlet_skin``: Verlet-list skin as a fraction of the largest radius
+        (default 0.1; 0 sweeps the full stencil every step)."""
         self.lib = load_library()
         self.cfg = cfg
         self._ctx = C.c_void_p()
@@ -171,6 +174,9 @@ class Simulation:
             self._check(self.lib.sph_set_option(self._ctx, OPT_GRAPH_STEPS, int(graph_steps)))
         if relayout_every is not None:
             self._check(self.lib.sph_set_option(self._ctx, OPT_RELAYOUT_EVERY, int(relayout_every)))
+        if verlet_skin is not None:
+            self._check(self.lib.sph_set_option(self._ctx, OPT_VERLET_SKIN,
+                                                int(round(verlet_skin * 1000))))
 
     def _check(self, rc):
         if rc != SPH_OK:

@@ -90,6 +90,29 @@ def test_gpu_matches_oracle_bit_for_bit(oracle_libs, name, chunks):
     assert stats["active_contacts"] == int((want.contacts != sb.np).sum())
 
 
+@pytest.mark.parametrize("name", ["box", "periodic_crossing", "box_wall", "polydisperse_small"])
+@pytest.mark.parametrize("skin", [0.0, 0.6], ids=["sweep_every_step", "wide_skin"])
+def test_contact_detection_modes_agree_with_oracle(oracle_libs, name, skin):
+    """Verlet lists off (the full 27-cell sweep every step) and with a wide
+    skin give the oracle's results bit for bit."""
+    sb = SCENES[name]()
+    rc, want, _ = run_oracle(oracle_libs["orc"], sb, 30)
+    assert rc == 0
+    got, _, _ = run_gpu(sb, (30,), verlet_skin=skin)
+    assert mismatches(got, want, ALL) == []
+
+
+@pytest.mark.parametrize("name", ["box", "periodic_crossing"])
+def test_verlet_epochs_restart_exactly(oracle_libs, name):
+    """300 steps: the displacement bound restarts the list epoch several
+    times and particles change cells often; results stay bit-exact."""
+    sb = SCENES[name]()
+    rc, want, _ = run_oracle(oracle_libs["orc"], sb, 300)
+    assert rc == 0
+    got, _, _ = run_gpu(sb, (100, 77, 123))
+    assert mismatches(got, want, ALL) == []
+
+
 def _golden_cases():
     idx = GOLDEN / "index.json"
     return json.loads(idx.read_text())["cases"] if idx.exists() else []
