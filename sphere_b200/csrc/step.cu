@@ -29,8 +29,9 @@ namespace sphk {
 constexpr int TOPO_BLOCK = 128;
 constexpr int FORCE_BLOCK = 128;
 
-// contactLinear_wall, src/contactmodels.cuh:10-109
-__device__ __forceinline__ double contact_wall(const Params &P, d3 &F, d3 &T, double &p,
+// contactLinear_wall, src/contactmodels.cuh:10-109.  Out of line: six call
+// sites, taken only by particles touching a wall.
+__device__ __noinline__ double contact_wall(const Params &P, d3 &F, d3 &T, double &p,
                                                double ra, double4 vel_a, double4 angvel_a,
                                                d3 n, double delta, double wvel)
 {
@@ -58,8 +59,9 @@ __device__ __forceinline__ double contact_wall(const Params &P, d3 &F, d3 &T, do
     return dot(f_n, n);
 }
 
-// contactLinear, src/contactmodels.cuh:283-493 (contact model 2)
-__device__ __forceinline__ void contact_linear(const Params &P, d3 &F, d3 &T, double &es_dot,
+// contactLinear, src/contactmodels.cuh:283-493 (contact model 2).  Out of
+// line so that particles without contacts run a lean kernel.
+__device__ __noinline__ void contact_linear(const Params &P, d3 &F, d3 &T, double &es_dot,
                                                double &ev_dot, double &p, double4 vel_a,
                                                d3 angvel_a, double4 vel_b4, double4 angvel_b4,
                                                double ra, double rb, d3 x, double x_length,
@@ -139,21 +141,14 @@ struct TopoSlots {
     bool dirty;                      // row changed
 };
 
-// Candidate t (storage index) reached through a stencil cell with shift
-// `code`: the reference's exact overlap predicate, then the slot choice.
-// Returns false once nc > NC, which ends the current cell (the reference
-// returns from findContactsInCell).  Kept out of line: it runs for a few
-// candidates per particle, and inlining it would raise the register count
-// of the whole candidate loop.
-__device__ __noinline__ bool topo_hit(const Dev &d, const Params &P, const double4 *xr,
-                                      uint32_t *srow, int tid, uint32_t s, uint32_t t,
-                                      uint32_t code, double4 xa, TopoSlots &ts)
+// Overlapping candidate t (storage index) reached through a stencil cell
+// with shift `code`: the slot choice.  Returns false once nc > NC, which ends
+// the current cell (the reference returns from findContactsInCell).  Kept
+// out of line: it runs for the few overlaps of a particle, and inlining it
+// would raise the register count of the whole candidate loop.
+__device__ __noinline__ bool topo_insert(const Dev &d, uint32_t *srow, int tid, uint32_t s,
+                                         uint32_t t, uint32_t code, TopoSlots &ts)
 {
-    const double4 xb = xr[t];
-    const d3 dm = decode_dm(code, P);
-    const d3 xab = add(mk(xa.x - xb.x, xa.y - xb.y, xa.z - xb.z), dm);
-    const double delta = flen(xab) - (xa.w + xb.w);
-    if (!(delta < 0.0f)) return true;
     if (!ts.loaded) {
         if (ts.occ) {
             const uint4 *row = reinterpret_cast<const uint4 *>(d.contacts + (size_t)s * NC);
@@ -191,6 +186,19 @@ __device__ __noinline__ bool topo_hit(const Dev &d, const Params &P, const doubl
         ts.err |= ST_NC_OVERFLOW;
     }
     return ++ts.nc <= NC;
+}
+
+// The reference's overlap predicate, float_sqrt(dot) - (ra + rb) < 0, for
+// candidate t through a stencil cell with shift `code`
+// (src/contactsearch.cuh:233-248).
+__device__ __forceinline__ bool overlaps(const Params &P, const double4 *xr, uint32_t t,
+                                         uint32_t code, double4 xa)
+{
+    const double4 xb = xr[t];
+    const d3 dm = decode_dm(code, P);
+    const d3 xab = add(mk(xa.x - xb.x, xa.y - xb.y, xa.z - xb.z), dm);
+    const double delta = flen(xab) - (xa.w + xb.w);
+    return delta < 0.0f;
 }
 
 // k_topo: one thread per cell-list position k, particle s = cellorder[k].
@@ -244,7 +252,9 @@ k_topo(Dev d, int A)
             const uint32_t meta = vm[e];
             const int slot = (int)(meta & 31u);
             if (slot == skip_slot) continue;   // nc > NC: rest of that cell
-            if (!topo_hit(d, P, xr, srow, tid, s, vl[e], meta >> 5, xa, ts)) skip_slot = slot;
+            const uint32_t t = vl[e], code = meta >> 5;
+            if (overlaps(P, xr, t, code, xa) && !topo_insert(d, srow, tid, s, t, code, ts))
+                skip_slot = slot;
         }
     } else {
         const float4 *__restrict__ xs = d.xs[A];
@@ -301,7 +311,8 @@ k_topo(Dev d, int A)
                         list_overflow = true;
                     }
                     if ((hit >> j) & 1u) {
-                        if (!topo_hit(d, P, xr, srow, tid, s, t, code, xa, ts)) {
+                        if (overlaps(P, xr, t, code, xa) &&
+                            !topo_insert(d, srow, tid, s, t, code, ts)) {
                             // nc > NC: skip the rest of this cell; the list
                             // would not describe the skipped part
                             next = (k2 < bnd1) ? bnd1 : ((k2 < bnd2) ? bnd2 : end);

@@ -102,7 +102,7 @@ def test_contact_detection_modes_agree_with_oracle(oracle_libs, name, skin):
     assert mismatches(got, want, ALL) == []
 
 
-@pytest.mark.parametrize("name", ["box", "periodic_crossing"])
+@pytest.mark.parametrize("name", ["box", "periodic_xy"])
 def test_verlet_epochs_restart_exactly(oracle_libs, name):
     """300 steps: the displacement bound restarts the list epoch several
     times and particles change cells often; results stay bit-exact."""
