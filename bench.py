@@ -253,25 +253,26 @@ def gpu_arm(args, rank, world, local):
         out = t.numpy()
         out[...] = a
         return out, t
+    # the host side holds what the reference's state file holds: contact
+    # slots, half-step velocities and accelerations stay on the device
+    file_fields = ("x", "xysum", "vel", "force", "angpos", "angvel", "torque", "es_dot", "es",
+                   "ev_dot", "ev", "p", "walls_nx", "walls_mvfd", "bonds", "bonds_delta",
+                   "bonds_omega")
     keep = []
-    st_h = st0.copy()
-    for f, v in list(st_h.__dict__.items()):
-        if isinstance(v, np.ndarray) and v.size:
-            arr, t = pinned(v)
-            keep.append(t)
-            setattr(st_h, f, arr)
-    st_out = st_h.copy()
-    for f, v in list(st_out.__dict__.items()):
-        if isinstance(v, np.ndarray) and v.size:
-            arr, t = pinned(v)
-            keep.append(t)
-            setattr(st_out, f, arr)
+    st_h, st_out = st0.copy(), st0.copy()
+    for st in (st_h, st_out):
+        for f, v in list(st.__dict__.items()):
+            if not isinstance(v, np.ndarray):
+                continue
+            if f not in file_fields:
+                setattr(st, f, None)
+            elif v.size:
+                arr, t = pinned(v)
+                keep.append(t)
+                setattr(st, f, arr)
     sim2 = Simulation(cfg, device=local)
-    h2d = sum(getattr(st_h, f).nbytes for f in ("x", "xysum", "vel", "vel0", "force", "angpos",
-                                               "angvel", "angvel0", "torque", "es_dot", "es",
-                                               "ev_dot", "ev", "p", "walls_nx", "walls_mvfd"))
-    d2h = h2d + sum(getattr(st_out, f).nbytes for f in ("acc", "angacc", "contacts", "distmod",
-                                                         "delta_t"))
+    h2d = sum(getattr(st_h, f).nbytes for f in file_fields if getattr(st_h, f) is not None)
+    d2h = h2d
     barrier()
     t0 = time.perf_counter()
     sim2.upload(st_h)

@@ -452,31 +452,35 @@ int sph_upload(sph_ctx *c, const sph_host_state *h)
         CK(cudaMemcpy(d.cellorder, ident.data(), np * 4, cudaMemcpyHostToDevice));
     }
     // contact slots: partners, periodic-shift codes, occupancy, history
-    {
+    if (!h->contacts) {
+        // the reference's initial state: every slot empty, zero history
+        CK(cudaMemset(d.contacts, 0xff, np * NC * 4));   // empty slots are read through cmask only
+        CK(cudaMemset(d.dmc, 0, np * 16));
+        CK(cudaMemset(d.cmask, 0, np * 4));
+        CK(cudaMemset(d.delta_t, 0, np * NC * 32));
+    } else {
         std::vector<uint32_t> rows(np * NC, (uint32_t)np);
         std::vector<unsigned long long> dmc(np * 2, 0ull);
         std::vector<uint32_t> cmask(np, 0u);
         std::vector<double> dts(np * NC * 4, 0.0);
-        if (h->contacts) {
-            for (size_t i = 0; i < np; ++i) {
-                for (int k = 0; k < NC; ++k) {
-                    const uint32_t v = h->contacts[i * NC + k];
-                    if (v >= np) continue;
-                    rows[i * NC + k] = v;
-                    cmask[i] |= 1u << k;
-                    uint32_t code = 0;
-                    if (h->distmod) {
-                        const double dx = h->distmod[(i * NC + k) * 4];
-                        const double dy = h->distmod[(i * NC + k) * 4 + 1];
-                        if (dx == P.L[0]) code |= 1u; else if (dx == -P.L[0]) code |= 2u;
-                        else if (dx != 0.0) return fail(c, SPH_ERR_BAD_INPUT, "distmod.x must be 0 or +-L[0]");
-                        if (dy == P.L[1]) code |= 4u; else if (dy == -P.L[1]) code |= 8u;
-                        else if (dy != 0.0) return fail(c, SPH_ERR_BAD_INPUT, "distmod.y must be 0 or +-L[1]");
-                    }
-                    dmc[2 * i + (k >> 4)] |= (unsigned long long)code << (4 * (k & 15));
-                    if (h->delta_t)
-                        for (int q = 0; q < 4; ++q) dts[(i * NC + k) * 4 + q] = h->delta_t[(i * NC + k) * 4 + q];
+        for (size_t i = 0; i < np; ++i) {
+            for (int k = 0; k < NC; ++k) {
+                const uint32_t v = h->contacts[i * NC + k];
+                if (v >= np) continue;
+                rows[i * NC + k] = v;
+                cmask[i] |= 1u << k;
+                uint32_t code = 0;
+                if (h->distmod) {
+                    const double dx = h->distmod[(i * NC + k) * 4];
+                    const double dy = h->distmod[(i * NC + k) * 4 + 1];
+                    if (dx == P.L[0]) code |= 1u; else if (dx == -P.L[0]) code |= 2u;
+                    else if (dx != 0.0) return fail(c, SPH_ERR_BAD_INPUT, "distmod.x must be 0 or +-L[0]");
+                    if (dy == P.L[1]) code |= 4u; else if (dy == -P.L[1]) code |= 8u;
+                    else if (dy != 0.0) return fail(c, SPH_ERR_BAD_INPUT, "distmod.y must be 0 or +-L[1]");
                 }
+                dmc[2 * i + (k >> 4)] |= (unsigned long long)code << (4 * (k & 15));
+                if (h->delta_t)
+                    for (int q = 0; q < 4; ++q) dts[(i * NC + k) * 4 + q] = h->delta_t[(i * NC + k) * 4 + q];
             }
         }
         CK(cudaMemcpy(d.contacts, rows.data(), np * NC * 4, cudaMemcpyHostToDevice));

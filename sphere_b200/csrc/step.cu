@@ -212,7 +212,7 @@ __device__ __forceinline__ bool overlaps(const Params &P, const double4 *xr, uin
 //
 // Sweep mode: the 27 stencil cells are scanned as in the reference (z, y, x;
 // members by particle index) and the list is recorded on the way.
-__global__ void __launch_bounds__(TOPO_BLOCK)
+__global__ void __launch_bounds__(TOPO_BLOCK, 8)
 k_topo(Dev d, int A)
 {
     __shared__ uint32_t srow[NC * TOPO_BLOCK];
@@ -418,7 +418,7 @@ struct ForceArgs {
     int write_outputs;  // store force/torque/acc/angacc/edp of this step
 };
 
-__global__ void __launch_bounds__(FORCE_BLOCK, 4)
+__global__ void __launch_bounds__(FORCE_BLOCK, 6)
 k_force(ForceArgs args)
 {
     const Dev &d = args.d;
