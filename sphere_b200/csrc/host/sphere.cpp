@@ -1,0 +1,311 @@
+// sphere.cpp -- DEM class: construction, pre-flight checks, parameter report
+// and the time loop, over libsphk's C ABI.
+//
+// Behaviour follows the reference host driver: DEM::DEM (src/sphere.cpp:16-77),
+// checkValues (:104-246), reportValues (:249-341) and DEM::startTime
+// (src/device.cu:576-1299) -- output file numbering, status.dat, the
+// `float` file-interval clock (device.cu:594) and the loop condition
+// time.current <= time.total.  Instead of one launch sequence and one device
+// synchronisation per step, the steps between two output files are handed
+// to sph_step in one call and errors are checked once per output interval.
+#include "sphere.h"
+
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <algorithm>
+#include <iostream>
+
+DEM::DEM(std::string inputbin, const int verbosity, const int checkVals, const int dry,
+         const int initCuda, const int transferConstMem, const int darcyflow)
+    : inputbin_(inputbin), verbose_(verbosity), darcy_(darcyflow)
+{
+    (void)transferConstMem;   // parameters live in per-context device memory
+    const size_t dotpos = inputbin.rfind('.');
+    const size_t slashpos = inputbin.rfind('/');
+    const size_t start = (slashpos == std::string::npos) ? 0 : slashpos + 1;
+    if (dotpos == std::string::npos || dotpos < start) {
+        std::cerr << "Error! Unable to extract simulation id from input file name.\n";
+        sid_ = inputbin.substr(start);
+    } else {
+        sid_ = inputbin.substr(start, dotpos - start);
+    }
+    readbin(inputbin.c_str());
+    if (checkVals == 1) checkValues();
+    if (dry == 1) {
+        reportValues();
+        exit(0);
+    }
+    if (initCuda == 1) initDevice();
+}
+
+DEM::~DEM()
+{
+    if (ctx_) sph_destroy(ctx_);
+    if (verbose_ == 1) std::cout << "Freeing host memory:                             Done" << std::endl;
+}
+
+void DEM::fail(int rc, const char *where)
+{
+    const char *msg = ctx_ ? sph_last_error(ctx_) : "";
+    std::cerr << "\nDevice error detected, checkpoint: " << where << "\nError string: " << msg
+              << " (status " << rc << ")" << std::endl;
+    if (rc == SPH_ERR_OUT_OF_GRID)
+        std::cerr << "One or more particles moved outside the grid.\n"
+                     "This could possibly be caused by a numerical instability.\n"
+                     "Is the computational time step too large?" << std::endl;
+    exit(EXIT_FAILURE);
+}
+
+sph_host_state DEM::hostState()
+{
+    sph_host_state h{};
+    h.x = x_.data();
+    h.xysum = xysum_.data();
+    h.vel = vel_.data();
+    h.force = force_.data();
+    h.angpos = angpos_.data();
+    h.angvel = angvel_.data();
+    h.torque = torque_.data();
+    h.es_dot = es_dot_.data();
+    h.es = es_.data();
+    h.ev_dot = ev_dot_.data();
+    h.ev = ev_.data();
+    h.p = p_.data();
+    h.bonds = bonds_.empty() ? nullptr : bonds_.data();
+    h.bonds_delta = bonds_delta_.empty() ? nullptr : bonds_delta_.data();
+    h.bonds_omega = bonds_omega_.empty() ? nullptr : bonds_omega_.data();
+    h.walls_nx = walls_nx_.empty() ? nullptr : walls_nx_.data();
+    h.walls_mvfd = walls_mvfd_.empty() ? nullptr : walls_mvfd_.data();
+    h.t_current = current_;
+    return h;
+}
+
+void DEM::initDevice()
+{
+    if (nu_ > 0.0) {
+        std::cerr << "Error: fluid coupling (nu > 0, "
+                  << (darcy_ ? "Darcy" : "lattice-Boltzmann")
+                  << ") is not part of this DEM step implementation." << std::endl;
+        exit(1);
+    }
+    cfg_.device = 0;
+    int rc = sph_create(&cfg_, &ctx_);
+    if (rc != SPH_OK) fail(rc, "sph_create");
+    if (verbose_ == 1) std::cout << "  Allocating global device memory:                Done\n";
+    upload();
+}
+
+void DEM::upload()
+{
+    sph_host_state h = hostState();
+    const int rc = sph_upload(ctx_, &h);
+    if (rc != SPH_OK) fail(rc, "sph_upload");
+    if (verbose_ == 1) std::cout << "  Transfering data to the device:                 Done\n";
+}
+
+void DEM::download()
+{
+    sph_host_state h = hostState();
+    const int rc = sph_download(ctx_, &h);
+    if (rc != SPH_OK) fail(rc, "sph_download");
+}
+
+void DEM::checkValues()
+{
+    using std::cerr;
+    if (cfg_.np < 1) {
+        cerr << "Error: np = " << cfg_.np << '\n';
+        exit(1);
+    }
+    if (current_ > total_ || current_ < 0.0) {
+        cerr << "Error: time.current = " << current_ << " s, time.total = " << total_ << " s\n";
+        exit(1);
+    }
+    if (cfg_.origo[0] < 0.0 || cfg_.origo[1] < 0.0 || cfg_.origo[2] < 0.0) {
+        cerr << "Error: Negative values in grid.origo are known to cause problems. \n"
+             << "grid.origo[0] = " << cfg_.origo[0] << " m, grid.origo[1] = " << cfg_.origo[1]
+             << " m, grid.origo[2] = " << cfg_.origo[2] << " m.\n";
+        exit(1);
+    }
+    if (cfg_.L[0] <= 0.0 || cfg_.L[1] <= 0.0 || cfg_.L[2] <= 0.0) {
+        cerr << "Error: grid.L[0] = " << cfg_.L[0] << " m, grid.L[1] = " << cfg_.L[1]
+             << " m, grid.L[2] = " << cfg_.L[2] << " m.\n";
+        exit(1);
+    }
+    if (cfg_.num[0] == 0 || cfg_.num[1] == 0 || cfg_.num[2] == 0) {
+        cerr << "Error: grid.num[0] = " << cfg_.num[0] << ", grid.num[1] = " << cfg_.num[1]
+             << ", grid.num[2] = " << cfg_.num[2] << ".\n";
+        exit(1);
+    }
+    if (cfg_.periodic == 2 && cfg_.num[0] < 3) {
+        cerr << "Error: When 1st dimension boundaries are periodic, "
+             << "there must be at least 3 cells in that dimension.";
+        exit(1);
+    }
+    if (cfg_.periodic == 1 && (cfg_.num[0] < 3 || cfg_.num[1] < 3)) {
+        cerr << "Error: When 1st and 2nd dimension boundaries are periodic, "
+             << "there must be at least 3 cells in each of those dimensions.";
+        exit(1);
+    }
+    for (uint32_t i = 0; i < cfg_.np; ++i) {
+        const double *x = &x_[4 * (size_t)i];
+        if (x[3] <= 0.0) {
+            cerr << "Error: Particle " << i << " has a radius of " << x[3] << " m." << std::endl;
+            exit(1);
+        }
+        if (x[0] < cfg_.origo[0] || x[1] < cfg_.origo[1] || x[2] < cfg_.origo[2] ||
+            x[0] > cfg_.L[0] || x[1] > cfg_.L[1] || x[2] > cfg_.L[2]) {
+            cerr << "Error: Particle " << i << " is outside of the computational grid\n"
+                 << "k.x[i] = [" << x[0] << ", " << x[1] << ", " << x[2] << "]\n"
+                 << "grid.origo = [" << cfg_.origo[0] << ", " << cfg_.origo[1] << ", "
+                 << cfg_.origo[2] << "], grid.L = [" << cfg_.L[0] << ", " << cfg_.L[1] << ", "
+                 << cfg_.L[2] << "]." << std::endl;
+            exit(1);
+        }
+    }
+    if (cfg_.nw > 0) {
+        double z_max = 0.0;
+        for (uint32_t i = 0; i < cfg_.np; ++i) z_max = std::max(z_max, x_[4 * (size_t)i + 2]);
+        if (walls_nx_[3] < z_max) {
+            cerr << "Error: One or more particles have centres above the upper, dynamic wall";
+            exit(1);
+        }
+    }
+    if (cfg_.k_n <= 0.0) {
+        cerr << "Error: k_n = " << cfg_.k_n << " N/m\n";
+        exit(1);
+    }
+    if (cfg_.rho <= 0.0) {
+        cerr << "Error: rho = " << cfg_.rho << " kg/m3\n";
+        exit(1);
+    }
+}
+
+void DEM::reportValues()
+{
+    using std::cout;
+    cout << "  - Number of dimensions: nd = 3\n"
+         << "  - Number of particles:  np = " << cfg_.np << "\n"
+         << "  - Compiled for double precision\n"
+         << "  - Timestep length:      time.dt         = " << dt_ << " s\n"
+         << "  - Start at time:        time.current    = " << current_ << " s\n"
+         << "  - Total sim. time:      time.total      = " << total_ << " s\n"
+         << "  - File output interval: time.file_dt    = " << file_dt_ << " s\n"
+         << "  - Start at step count:  time.step_count = " << step_count_ << std::endl;
+    if (cfg_.contactmodel == 1)
+        cout << "  - Contact model: Linear-elastic-viscous (n), visco-frictional (t)\n";
+    else if (cfg_.contactmodel == 2)
+        cout << "  - Contact model: Linear-elastic-visco-frictional\n";
+    else if (cfg_.contactmodel == 3)
+        cout << "  - Contact model: Nonlinear-elastic-visco-frictional\n";
+    else {
+        std::cerr << "Error: Contact model value (" << cfg_.contactmodel << ") not understood.\n";
+        exit(1);
+    }
+    cout << "  - Number of dynamic walls: " << cfg_.nw << '\n';
+    if (cfg_.periodic == 1)
+        cout << "  - 1st and 2nd dim. boundaries: Periodic\n";
+    else if (cfg_.periodic == 2)
+        cout << "  - 1st dim. boundaries: Visco-frictional walls\n";
+    else
+        cout << "  - 1st and 2nd dim. boundaries: Visco-frictional walls\n";
+    if (cfg_.nw > 0) {
+        cout << "  - Top BC: ";
+        if (cfg_.wmode[0] == 0) cout << "Fixed\n";
+        else if (cfg_.wmode[0] == 1) cout << "Deviatoric stress, " << walls_mvfd_[3] << " Pa\n";
+        else if (cfg_.wmode[0] == 2) cout << "Velocity, " << walls_mvfd_[1] << " m/s\n";
+        else {
+            std::cerr << "Top BC not recognized!\n";
+            exit(1);
+        }
+    }
+    cout << "  - Grid: " << cfg_.num[0] << " * " << cfg_.num[1] << " * " << cfg_.num[2]
+         << " cells\n"
+         << "  - Domain size: " << cfg_.L[0] << " * " << cfg_.L[1] << " * " << cfg_.L[2]
+         << " m\n"
+         << "  - No. of particle bonds: " << cfg_.nb0 << std::endl;
+}
+
+static void write_status(const std::string &sid, double current, double total, uint32_t count)
+{
+    const std::string fn = "output/" + sid + ".status.dat";
+    FILE *fp = fopen(fn.c_str(), "w");
+    if (!fp) {
+        std::cerr << "Could not write " << fn << std::endl;
+        exit(1);
+    }
+    fprintf(fp, "%2.4e %2.4e %d\n", current, 100.0 * current / total, count);
+    fclose(fp);
+}
+
+void DEM::startTime()
+{
+    if (!ctx_) initDevice();
+    writebin(("output/" + sid_ + ".output00000.bin").c_str());
+    write_status(sid_, current_, total_, step_count_);
+    const auto tic = std::chrono::steady_clock::now();
+    float filetimeclock = 0.0f;   // float in the reference (src/device.cu:594)
+    uint64_t pending = 0, iter = 0;
+    char file[512];
+    if (verbose_ == 1) std::cout << "  Current simulation time: " << current_ << " s.";
+    while (current_ <= total_) {
+        ++pending;
+        ++iter;
+        current_ += dt_;
+        filetimeclock += dt_;
+        if (filetimeclock >= file_dt_) {
+            int rc = sph_step(ctx_, pending, nullptr);
+            if (rc == SPH_OK) rc = sph_sync(ctx_);
+            if (rc != SPH_OK) fail(rc, "time loop");
+            pending = 0;
+            download();
+            step_count_ += 1;
+            snprintf(file, sizeof file, "output/%s.output%05d.bin", sid_.c_str(), step_count_);
+            writebin(file);
+            write_status(sid_, current_, total_, step_count_);
+            filetimeclock = 0.0f;
+            if (verbose_ == 1)
+                std::cout << "\r  Current simulation time: " << current_ << "/" << total_
+                          << " s.        " << std::flush;
+        }
+    }
+    if (pending) {
+        int rc = sph_step(ctx_, pending, nullptr);
+        if (rc == SPH_OK) rc = sph_sync(ctx_);
+        if (rc != SPH_OK) fail(rc, "time loop");
+        download();
+    }
+    const double secs =
+        std::chrono::duration<double>(std::chrono::steady_clock::now() - tic).count();
+    if (verbose_ == 1) {
+        std::cout << "\nSimulation ended. Statistics:\n"
+                  << "  - Last output file number: " << step_count_ << "\n"
+                  << "  - Wall time spent: " << secs << " s\n"
+                  << "  - Mean duration of iteration:\n"
+                  << "      " << (iter ? secs / (double)iter : 0.0) << " s" << std::endl;
+    }
+}
+
+void DEM::render(const int, const float, const float, const float, const unsigned int,
+                 const unsigned int)
+{
+    std::cerr << "Error: the ray-traced renderer is not part of this DEM step implementation."
+              << std::endl;
+    exit(1);
+}
+
+void DEM::porosity(const int)
+{
+    std::cerr << "Error: the porosity tool is not part of this DEM step implementation."
+              << std::endl;
+    exit(1);
+}
+
+void DEM::forcechains(const std::string, const int, const double, const double)
+{
+    std::cerr << "Error: the force-chain tool is not part of this DEM step implementation."
+              << std::endl;
+    exit(1);
+}

@@ -1,0 +1,75 @@
+// sphere.h -- the DEM class: the reference's host-side driver API
+// (src/sphere.h:12-322) over libsphk's C ABI (include/sphk.h).
+//
+// Public interface kept from the reference (src/sphere.h:244-273):
+// constructor DEM(inputbin, verbosity, checkVals, dry, initCuda,
+// transferConstMem, darcyflow), readbin, writebin, checkValues,
+// reportValues, startTime, and the destructor.  The state is held in the
+// reference's host layout (Float4 rows, src/datatypes.h:17-33) and moved to
+// and from the device with sph_upload / sph_download.  The renderer, porosity,
+// force-chain and fluid (Darcy/LBM) members of the reference are not part of
+// this DEM step; render(), porosity() and forcechains() report that and exit.
+#ifndef SPHERE_B200_SPHERE_H_
+#define SPHERE_B200_SPHERE_H_
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "sphk.h"
+
+class DEM {
+  public:
+    DEM(std::string inputbin, const int verbosity = 1, const int checkVals = 1,
+        const int dry = 0, const int initCuda = 1, const int transferConstMem = 1,
+        const int darcyflow = 0);
+    ~DEM();
+
+    // binary state file, src/file_io.cpp:29-490
+    void readbin(const char *target);
+    void writebin(const char *target);
+
+    // pre-flight checks and parameter report, src/sphere.cpp:104-341
+    void checkValues();
+    void reportValues();
+
+    // time loop, src/device.cu:576-1299
+    void startTime();
+
+    // outside the DEM step (renderer, analysis tools)
+    void render(const int method = 1, const float maxval = 1.0e3f,
+                const float lower_cutoff = 0.0f, const float focalLength = 1.0f,
+                const unsigned int img_width = 800, const unsigned int img_height = 800);
+    void porosity(const int z_slices = 10);
+    void forcechains(const std::string format = "interactive", const int threedim = 1,
+                     const double lower_cutoff = 0.0, const double upper_cutoff = 1.0e9);
+
+  private:
+    std::string inputbin_, sid_;
+    int verbose_ = 1;
+    int darcy_ = 0;
+
+    // time (src/datatypes.h:62-68)
+    double dt_ = 0.0, current_ = 0.0, total_ = 0.0, file_dt_ = 0.0;
+    uint32_t step_count_ = 0;
+
+    // configuration and state in the reference host layout
+    sph_config cfg_{};
+    std::vector<double> x_, xysum_, vel_, force_, angpos_, angvel_, torque_;
+    std::vector<double> es_dot_, es_, ev_dot_, ev_, p_;
+    std::vector<double> walls_nx_, walls_mvfd_;
+    std::vector<uint32_t> bonds_;
+    std::vector<double> bonds_delta_, bonds_omega_;
+    double nu_ = 0.0;
+    std::vector<char> fluid_trailer_;   // carried unchanged when nu > 0
+
+    sph_ctx *ctx_ = nullptr;
+
+    void initDevice();
+    void upload();
+    void download();
+    void fail(int rc, const char *where);
+    sph_host_state hostState();
+};
+
+#endif
