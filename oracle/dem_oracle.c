@@ -313,9 +313,180 @@ static void contact_linear(const orc_scene *s, v3 *F, v3 *T, double *es_dot,
     dt4[0] = delta_t.x; dt4[1] = delta_t.y; dt4[2] = delta_t.z; dt4[3] = 0.0f;
 }
 
-/* ---- interact: src/contactsearch.cuh:369-689 (contact models 2/3) ------- */
-static void interact_one(orc_scene *s, work_t *w, uint32_t a)
+/* The FP32 transcendentals of the force laws: expf in capillaryCohesion_exp
+ * and powf in contactHertz.  By default each is evaluated as the float
+ * nearest to the double-precision result, which is also what the CUDA path
+ * computes; orc_set_libm_float_math(1) switches to the C library's expf and
+ * powf, which is what the reference's host build calls. */
+static int g_libm_float = 0;
+void orc_set_libm_float_math(int on) { g_libm_float = on; }
+
+static inline double f32_expf(double x)
 {
+    const float xf = (float)x;
+    return g_libm_float ? (double)expf(xf) : (double)(float)exp((double)xf);
+}
+
+static inline double f32_powf(double x, float y)
+{
+    const float xf = (float)x;
+    return g_libm_float ? (double)powf(xf, y) : (double)(float)pow((double)xf, (double)y);
+}
+
+/* contactLinearViscous, src/contactmodels.cuh:114-253 (contact model 1):
+ * no tangential history; the torque is not changed (its update is commented
+ * out in the reference, :244) */
+static void contact_viscous(const orc_scene *s, v3 *F, double *p, const double *vel_a,
+                            const double *vel_b, v3 angvel_a, v3 angvel_b, double ra,
+                            double rb, v3 x_ab, double x_ab_length, double delta, double kappa)
+{
+    v3 n = divs(x_ab, x_ab_length);
+    v3 vel_linear = mk(vel_a[0] - vel_b[0], vel_a[1] - vel_b[1], vel_a[2] - vel_b[2]);
+    v3 vel = add(add(vel_linear, smul(ra + delta / 2.0, cross(n, angvel_a))),
+                 smul(rb + delta / 2.0, cross(n, angvel_b)));
+    double vel_n = dot(vel_linear, n);
+    v3 vel_t = sub(vel, muls(n, dot(vel, n)));
+    double vel_t_length = vlen(vel_t);
+    v3 f_n = smul(-s->k_n * delta - s->gamma_n * vel_n, n);
+    if (dot(f_n, n) < 0.0f) f_n = mk(0.0, 0.0, 0.0);
+    double f_n_length = vlen(f_n);
+    v3 f_c = smul(-kappa * (double)sqrtf((float)(ra * rb)), n);
+    v3 f_t = mk(0.0, 0.0, 0.0);
+    if (vel_t_length > 0.0) {
+        double f_t_visc = s->gamma_t * vel_t_length;
+        double f_t_limit;
+        if (vel_t_length > 0.001f) f_t_limit = s->mu_d * vlen(sub(f_n, f_c));
+        else f_t_limit = s->mu_s * vlen(sub(f_n, f_c));
+        if (f_t_visc < f_t_limit) f_t = divs(smul(-f_t_visc, vel_t), vel_t_length);
+        else f_t = divs(smul(-f_t_limit, vel_t), vel_t_length);
+    }
+    *F = add(*F, add(add(f_n, f_t), f_c));
+    *p += f_n_length / (4.0f * REF_PI * ra * ra);
+}
+
+/* capillaryCohesion_exp, src/cohesion.cuh:314-350 */
+static void capillary_exp(const orc_scene *s, v3 *F, double ra, double rb, double delta,
+                          v3 x_ab, double x_ab_length, double kappa)
+{
+    v3 n = divs(x_ab, x_ab_length);
+    double r;
+    if ((ra / rb) > (rb / ra)) r = ra / rb;
+    else r = rb / ra;
+    double h = -(double)sqrtf((float)r);
+    double R_har = (2.0f * ra * rb) / (ra + rb);
+    double R_geo = (double)sqrtf((float)(ra * rb));
+    double lambda = 0.9f * h * (double)sqrtf((float)(s->V_b / R_har));
+    v3 f_c = smul(-kappa * R_geo * f32_expf(-delta / lambda), n);
+    *F = add(*F, f_c);
+}
+
+/* contactHertz, src/contactmodels.cuh:499-666 (contact model 3).  The
+ * overlap delta is negative here, as in the reference, so the fractional
+ * powers of it are NaN. */
+static void contact_hertz(const orc_scene *s, v3 *F, v3 *T, double *es_dot, double *ev_dot,
+                          double *p, uint32_t b_orig, const double *vel_a4, v3 angvel_a,
+                          double ra, double rb, v3 x, double x_length, double delta,
+                          double *dt4)
+{
+    const double dt = s->dt;
+    v3 vel_b = ld3(&s->vel[4 * (size_t)b_orig]);
+    v3 angvel_b = ld3(&s->angvel[4 * (size_t)b_orig]);
+    v3 dt0u = ld3(dt4);
+    v3 n = divs(x, x_length);
+    v3 vel_linear = mk(vel_a4[0] - vel_b.x, vel_a4[1] - vel_b.y, vel_a4[2] - vel_b.z);
+    v3 vel = add(add(vel_linear, smul(ra + delta / 2.0, cross(n, angvel_a))),
+                 smul(rb + delta / 2.0, cross(n, angvel_b)));
+    v3 angvel_ab = sub(angvel_a, angvel_b);
+    double angvel_ab_length = vlen(angvel_ab);
+    double vel_n = dot(vel_linear, n);
+    v3 vel_t = sub(vel, muls(n, dot(vel, n)));
+    double vel_t_length = vlen(vel_t);
+    v3 delta_t0 = sub(dt0u, muls(n, dot(dt0u, n)));
+    double delta_t0_length = vlen(delta_t0);
+    v3 delta_t = mk(0.0, 0.0, 0.0); /* left unset by the reference when unused */
+    v3 f_n = smul(-s->k_n * f32_powf(delta, 3.0f / 2.0f)
+                      - s->gamma_n * f32_powf(delta, 1.0f / 4.0f) * vel_n, n);
+    *ev_dot += s->gamma_n * vel_n * vel_n;
+    if (dot(f_n, n) < 0.0f) f_n = mk(0.0, 0.0, 0.0);
+    double f_n_length = vlen(f_n);
+    v3 f_c = smul(-s->kappa * (double)sqrtf((float)(ra * rb)), n);
+    v3 f_t = mk(0.0, 0.0, 0.0);
+    v3 T_res = mk(0.0, 0.0, 0.0);
+    if (delta_t0_length > 0.f || vel_t_length > 0.f) {
+        v3 f_t_elast = smul(-s->k_t * f32_powf(delta, 1.0f / 2.0f), delta_t0);
+        v3 f_t_visc = smul(-s->gamma_t * f32_powf(delta, 1.0f / 4.0f), vel_t);
+        double f_t_limit;
+        if (vel_t_length > 0.001f) f_t_limit = s->mu_d * vlen(sub(f_n, f_c));
+        else f_t_limit = s->mu_s * vlen(sub(f_n, f_c));
+        f_t = add(f_t_elast, f_t_visc);
+        double f_t_length = vlen(f_t);
+        if (f_t_length > f_t_limit) {
+            f_t = muls(f_t, f_t_limit / f_t_length);
+            delta_t = divs(add(f_t, smul(s->gamma_t * f32_powf(delta, 1.0f / 4.0f), vel_t)),
+                           -s->k_t * f32_powf(delta, 1.0f / 2.0f));
+            *es_dot += vlen(sub(delta_t0, delta_t)) * s->k_t / dt;
+        } else {
+            delta_t = add(delta_t0, muls(vel_t, dt));
+        }
+    }
+    if (angvel_ab_length > 0.f) {
+        T_res = divs(smul(-1.0f * fmin(s->gamma_r * ra * angvel_ab_length,
+                                       s->mu_r * ra * f_n_length),
+                          angvel_ab),
+                     angvel_ab_length);
+    }
+    *F = add(*F, add(add(f_n, f_t), f_c));
+    *T = add(*T, add(smul(-(ra + delta / 2.0), cross(n, f_t)), T_res));
+    *p += f_n_length / (4.0f * REF_PI * ra * ra);
+    dt4[0] = delta_t.x; dt4[1] = delta_t.y; dt4[2] = delta_t.z; dt4[3] = 0.0f;
+}
+
+/* Model 1 finds and processes contacts in one pass over the 27 stencil cells
+ * (contactsearch.cuh:548-576 and findAndProcessContactsInCell, :81-175),
+ * over the sorted copies. */
+static int sweep_viscous(orc_scene *s, work_t *w, uint32_t a, v3 *F, double *p)
+{
+    const double *xa = &w->x_s[4 * (size_t)a];
+    const double ra = xa[3];
+    const double *vel_a = &w->vel_s[4 * (size_t)a];
+    const v3 angvel_a = ld3(&w->angvel_s[4 * (size_t)a]);
+    int err = 0;
+    int32_t gp[3];
+    for (int d = 0; d < 3; ++d) gp[d] = sat_i32(cell_floor(s, d, xa[d]));
+    for (int oz = -1; oz < 2; ++oz)
+        for (int oy = -1; oy < 2; ++oy)
+            for (int ox = -1; ox < 2; ++ox) {
+                int32_t c[3] = {wrap_add(gp[0], ox), wrap_add(gp[1], oy), wrap_add(gp[2], oz)};
+                v3 dm = mk(0.0, 0.0, 0.0);
+                if (dist_mod(s, c, &dm) == -1) continue;
+                uint32_t cid = (uint32_t)c[0] + (uint32_t)c[1] * s->num[0]
+                    + (s->num[0] * s->num[1]) * (uint32_t)c[2];
+                if (cid >= w->ncells) { err |= ORC_ERR_OUT_OF_GRID; continue; }
+                uint32_t start = s->cell_start[cid];
+                if (start == 0xffffffffu) continue;
+                uint32_t end = s->cell_end[cid];
+                for (uint32_t b = start; b < end; ++b) {
+                    if (b == a) continue;
+                    const double *xb = &w->x_s[4 * (size_t)b];
+                    const double rb = xb[3];
+                    v3 xab = add(mk(xa[0] - xb[0], xa[1] - xb[1], xa[2] - xb[2]), dm);
+                    double len = vlen(xab);
+                    double delta = len - (ra + rb);
+                    if (delta < 0.0f)
+                        contact_viscous(s, F, p, vel_a, &w->vel_s[4 * (size_t)b], angvel_a,
+                                        ld3(&w->angvel_s[4 * (size_t)b]), ra, rb, xab, len,
+                                        delta, s->kappa);
+                    else if (delta < s->db)
+                        capillary_exp(s, F, ra, rb, delta, xab, len, s->kappa);
+                }
+            }
+    return err;
+}
+
+/* ---- interact: src/contactsearch.cuh:369-689 (contact models 2/3) ------- */
+static int interact_one(orc_scene *s, work_t *w, uint32_t a)
+{
+    int err = 0;
     const uint32_t np = s->np;
     const uint32_t a_orig = s->perm[a];
     const double *xa = &w->x_s[4 * (size_t)a];
@@ -335,7 +506,7 @@ static void interact_one(orc_scene *s, work_t *w, uint32_t a)
     const double *vel_a = &w->vel_s[4 * (size_t)a];
     const double *angvel_a4 = &w->angvel_s[4 * (size_t)a];
     v3 angvel_a = ld3(angvel_a4);
-    if (s->contactmodel == 2) {
+    if (s->contactmodel == 2 || s->contactmodel == 3) {
         for (int i = 0; i < ORC_NC; ++i) {
             size_t mp = (size_t)a_orig * ORC_NC + (size_t)i;
             uint32_t b_orig = s->contacts[mp];
@@ -348,8 +519,12 @@ static void interact_one(orc_scene *s, work_t *w, uint32_t a)
                 double xlen = vlen(xab);
                 double delta_n = xlen - (ra + rb);
                 if (delta_n < 0.0f) {
-                    contact_linear(s, &F, &T, &es_dot, &ev_dot, &p, b_orig, vel_a, angvel_a,
-                                   ra, rb, xab, xlen, delta_n, dt4);
+                    if (s->contactmodel == 2)
+                        contact_linear(s, &F, &T, &es_dot, &ev_dot, &p, b_orig, vel_a,
+                                       angvel_a, ra, rb, xab, xlen, delta_n, dt4);
+                    else
+                        contact_hertz(s, &F, &T, &es_dot, &ev_dot, &p, b_orig, vel_a,
+                                      angvel_a, ra, rb, xab, xlen, delta_n, dt4);
                 } else {
                     s->contacts[mp] = np;
                     dt4[0] = dt4[1] = dt4[2] = dt4[3] = 0.0;
@@ -358,6 +533,8 @@ static void interact_one(orc_scene *s, work_t *w, uint32_t a)
                 dt4[0] = dt4[1] = dt4[2] = dt4[3] = 0.0;
             }
         }
+    } else if (s->contactmodel == 1) {
+        err |= sweep_viscous(s, w, a, &F, &p);
     }
     /* walls, contactsearch.cuh:578-663 */
     double w0f = 0.0;
@@ -394,6 +571,7 @@ static void interact_one(orc_scene *s, work_t *w, uint32_t a)
     s->ev[a_orig] += ev_dot * s->dt;
     s->p[a_orig] = p;
     w->wf_pp[a_orig] = w0f;
+    return err;
 }
 
 /* ---- bondsLinear: src/cohesion.cuh:8-233, bonds in index order ---------- */
@@ -583,7 +761,7 @@ int orc_threads(int nthreads)
 int orc_step(orc_scene *s, uint64_t nsteps, int nthreads)
 {
     if (!s || s->np == 0 || s->nw > ORC_MAXWALLS) return ORC_ERR_BAD_INPUT;
-    if (s->contactmodel != 2) return ORC_ERR_BAD_INPUT;
+    if (s->contactmodel < 1 || s->contactmodel > 3) return ORC_ERR_BAD_INPUT;
     const uint64_t nc64 = (uint64_t)s->num[0] * s->num[1] * s->num[2];
     if (nc64 == 0 || nc64 >= 0xffffffffull) return ORC_ERR_BAD_INPUT;
     work_t w;
@@ -592,12 +770,17 @@ int orc_step(orc_scene *s, uint64_t nsteps, int nthreads)
     int err = 0;
     for (uint64_t step = 0; step < nsteps; ++step) {
         err |= build_cells(s, &w);
-        int e_topo = 0;
+        int e_topo = 0, e_int = 0;
+        /* models 2 and 3 keep contact history (device.cu:805) */
+        if (s->contactmodel != 1) {
 #pragma omp parallel for num_threads(nt) schedule(dynamic, 256) reduction(| : e_topo)
-        for (int64_t a = 0; a < (int64_t)s->np; ++a) e_topo |= topology_one(s, &w, (uint32_t)a);
+            for (int64_t a = 0; a < (int64_t)s->np; ++a)
+                e_topo |= topology_one(s, &w, (uint32_t)a);
+        }
         err |= e_topo;
-#pragma omp parallel for num_threads(nt) schedule(dynamic, 256)
-        for (int64_t a = 0; a < (int64_t)s->np; ++a) interact_one(s, &w, (uint32_t)a);
+#pragma omp parallel for num_threads(nt) schedule(dynamic, 256) reduction(| : e_int)
+        for (int64_t a = 0; a < (int64_t)s->np; ++a) e_int |= interact_one(s, &w, (uint32_t)a);
+        err |= e_int;
         for (uint32_t b = 0; b < s->nb0; ++b) bond_one(s, b);
 #pragma omp parallel for num_threads(nt) schedule(static)
         for (int64_t k = 0; k < (int64_t)s->np; ++k) integrate_one(s, &w, (uint32_t)k);

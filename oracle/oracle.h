@@ -74,6 +74,12 @@ int orc_kind(void);
 
 /* Number of OpenMP threads a parallel region gets with nthreads as above. */
 int orc_threads(int nthreads);
+/* FP32 transcendentals of the force laws (expf, powf): 0 (default) evaluates
+ * each as the float nearest to the double-precision result, as the CUDA path
+ * does; 1 calls the C library's expf/powf, as the reference's host build
+ * does.  Not provided by the reference harness (oracle/_ref), which always
+ * calls the C library. */
+void orc_set_libm_float_math(int on);
 
 #ifdef __cplusplus
 }

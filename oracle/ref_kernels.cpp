@@ -95,7 +95,7 @@ static inline void launch1(unsigned int i)
 extern "C" int orc_step(orc_scene *s, uint64_t nsteps, int nthreads)
 {
     if (!s || s->np == 0 || s->nw > ORC_MAXWALLS) return ORC_ERR_BAD_INPUT;
-    if (s->contactmodel != 2) return ORC_ERR_BAD_INPUT;
+    if (s->contactmodel < 1 || s->contactmodel > 3) return ORC_ERR_BAD_INPUT;
     const unsigned int np = s->np;
     const unsigned long long nc64 = (unsigned long long)s->num[0] * s->num[1] * s->num[2];
     if (nc64 == 0 || nc64 >= 0xffffffffull) return ORC_ERR_BAD_INPUT;
@@ -183,8 +183,9 @@ extern "C" int orc_step(orc_scene *s, uint64_t nsteps, int nthreads)
             reorderArrays(s->cell_start, s->cell_end, cellid.data(), index.data(), x, vel,
                           angvel, x_sorted.data(), vel_sorted.data(), angvel_sorted.data());
         }
+        /* contact history only for models 2 and 3 (src/device.cu:805) */
 #pragma omp parallel for num_threads(nt) schedule(dynamic, 256)
-        for (long i = 0; i < (long)np; ++i) {
+        for (long i = 0; i < (long)(s->contactmodel == 1 ? 0u : np); ++i) {
             launch1((unsigned int)i);
             topology(s->cell_start, s->cell_end, index.data(), x_sorted.data(), s->contacts,
                      distmod);

@@ -49,3 +49,33 @@ def relative_error(a, b, scale=None):
     b = np.asarray(b, float)
     s = np.maximum(np.abs(b), 1e-300) if scale is None else scale
     return float(np.max(np.abs(a - b) / s)) if a.size else 0.0
+
+
+def with_model(sb, model, kappa=0.05, V_b=1e-12, db=1e-4):
+    """Switch a scene to contact model 1 (with capillary cohesion: kappa,
+    liquid bridge volume V_b and the cohesion reach db) or model 3."""
+    sb.contactmodel = int(model)
+    if model == 1:
+        sb.kappa, sb.V_b, sb.db = kappa, V_b, db
+    return sb
+
+
+def nan_aware_mismatches(a: HostState, b: HostState, fields):
+    """Like mismatches(), but NaN equals NaN whatever its sign and payload
+    (the CPU and the GPU write different NaN bit patterns)."""
+    bad = []
+    for f in fields:
+        A, B = np.asarray(getattr(a, f)), np.asarray(getattr(b, f))
+        if f in ("acc", "angacc"):
+            A, B = A[:, :3], B[:, :3]
+        if A.dtype.kind != "f":
+            if not bits_equal(A, B):
+                bad.append((f, "int", int(np.count_nonzero(A != B))))
+            continue
+        na, nb = np.isnan(A), np.isnan(B)
+        if not np.array_equal(na, nb):
+            bad.append((f, "nan pattern", int(np.count_nonzero(na != nb))))
+            continue
+        if not bits_equal(np.where(na, 0.0, A), np.where(nb, 0.0, B)):
+            bad.append((f, "values", int(np.count_nonzero(np.where(na, 0.0, A) != np.where(nb, 0.0, B)))))
+    return bad

@@ -7,7 +7,8 @@ import numpy as np
 import pytest
 
 import pyoracle
-from helpers import BOND_FIELDS, OUTPUT_FIELDS, STATE_FIELDS, WALL_FIELDS, mismatches, run_oracle
+from helpers import (BOND_FIELDS, OUTPUT_FIELDS, STATE_FIELDS, WALL_FIELDS, mismatches,
+                     relative_error, run_oracle, with_model)
 from sphere_b200 import scenes
 from sphere_b200.spherebin import readbin
 from sphere_b200.state import config_from_spherebin, state_from_spherebin
@@ -92,3 +93,63 @@ def test_oracle_matches_golden_fixtures(oracle_libs, case):
         else:
             got = getattr(st, f)
         assert np.array_equal(np.asarray(got), want[f]), f
+
+
+MODEL_SCENES = {
+    "box": dict(periodic=0),
+    "periodic_xy": dict(periodic=1),
+    "periodic_x_wall": dict(periodic=2, nw=1),
+}
+
+
+@pytest.mark.parametrize("name", sorted(MODEL_SCENES))
+def test_model1_with_cohesion_matches_reference_kernels(oracle_libs, name):
+    """contactLinearViscous + capillaryCohesion_exp (model 1): bit for bit
+    when the oracle calls the C library's expf, as the reference's host build
+    does."""
+    _need_ref(oracle_libs)
+    orc = oracle_libs["orc"]
+    mk = lambda: with_model(scenes.collision(n=1200, seed=11, **MODEL_SCENES[name]), 1)
+    orc.orc_set_libm_float_math(1)
+    try:
+        rc1, a, ra = run_oracle(orc, mk(), 30, nthreads=4)
+    finally:
+        orc.orc_set_libm_float_math(0)
+    rc2, b, rb = run_oracle(oracle_libs["ref"], mk(), 30, nthreads=4)
+    assert rc1 == 0 and rc2 == 0
+    assert mismatches(a, b, ALL) == []
+    assert np.array_equal(ra.perm, rb.perm)
+    # contacts and cohesion both acted; the slots stay empty in model 1
+    assert np.count_nonzero(a.p) > 100
+    assert (a.contacts == mk().np).all()
+
+
+def test_model1_nearest_float_exp_stays_close(oracle_libs):
+    """With expf evaluated as the float nearest to exp (the CUDA path's
+    choice) the oracle leaves the reference's host build only by the last
+    bits of a few cohesion forces: within 1e-9 relative after 30 steps."""
+    _need_ref(oracle_libs)
+    mk = lambda: with_model(scenes.collision(n=1200, seed=11, periodic=1), 1)
+    rc1, a, _ = run_oracle(oracle_libs["orc"], mk(), 30, nthreads=4)
+    rc2, b, _ = run_oracle(oracle_libs["ref"], mk(), 30, nthreads=4)
+    assert rc1 == 0 and rc2 == 0
+    assert relative_error(a.x[:, :3], b.x[:, :3], scale=np.abs(b.x[:, :3]).max()) < 1e-12
+    vscale = np.abs(b.vel[:, :3]).max()
+    assert relative_error(a.vel[:, :3], b.vel[:, :3], scale=vscale) < 1e-9
+
+
+@pytest.mark.parametrize("name", sorted(MODEL_SCENES))
+def test_model3_matches_reference_kernels(oracle_libs, name):
+    """contactHertz (model 3) raises the negative overlap to fractional
+    powers, so every touching pair gets NaN forces; the oracle reproduces the
+    reference's step, NaN bits included."""
+    _need_ref(oracle_libs)
+    mk = lambda: with_model(scenes.collision(n=1200, seed=11, **MODEL_SCENES[name]), 3)
+    rc1, a, _ = run_oracle(oracle_libs["orc"], mk(), 1, nthreads=4)
+    rc2, b, _ = run_oracle(oracle_libs["ref"], mk(), 1, nthreads=4)
+    assert rc1 == 0 and rc2 == 0
+    assert mismatches(a, b, ALL) == []
+    touching = (a.contacts != mk().np).any(axis=1)
+    assert touching.sum() > 100
+    assert np.isnan(a.force[touching, :3]).all()
+    assert not np.isnan(a.force[~touching, :3]).any()
