@@ -123,6 +123,19 @@ typedef struct sph_stats {
 
 int sph_version(void);
 int sph_create(const sph_config *cfg, sph_ctx **out);
+/* Batched ensemble: ninst independent scenes stepped together by one
+ * context, every kernel launched once over all of them (an addition for the
+ * ensemble workload; the reference runs one scene per process).  Each scene
+ * keeps its own grid, parameters and time step; results for each scene are
+ * those of a context created for it alone, bit for bit.  Host arrays passed
+ * to sph_upload / sph_download hold the scenes end to end: rows of scene 0,
+ * then of scene 1, ...; contact partners are indices within the particle's
+ * own scene (its np marks an empty slot).  Scenes must use contact model 2,
+ * no dynamic walls (nw = 0) and no bonds (nb0 = 0), on one device.  A batched
+ * context takes every other call of this header; sph_get_cells reports the
+ * context-wide cell list (scene i's cells follow scene i-1's; perm holds
+ * context-wide particle indices), and sph_download's t_current is scene 0's. */
+int sph_batch_create(const sph_config *cfgs, uint32_t ninst, sph_ctx **out);
 int sph_set_option(sph_ctx *ctx, int option, int64_t value);
 int sph_upload(sph_ctx *ctx, const sph_host_state *st);
 /* Enqueue nsteps time steps on `stream` (a cudaStream_t, NULL: the context's

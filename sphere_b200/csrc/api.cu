@@ -10,9 +10,9 @@
 #include <vector>
 
 namespace sphk {
-void launch_step(const Dev &d, uint32_t np, int a, int write_outputs, cudaStream_t st);
-void launch_topo(const Dev &d, uint32_t np, int a, cudaStream_t st);
-void launch_force(const Dev &d, uint32_t np, int a, int write_outputs, cudaStream_t st);
+void launch_step(const Dev &d, uint32_t np, int model, int a, int write_outputs, cudaStream_t st);
+void launch_topo(const Dev &d, uint32_t np, bool visc, int a, cudaStream_t st);
+void launch_force(const Dev &d, uint32_t np, int model, int a, int write_outputs, cudaStream_t st);
 void launch_bonds(const Dev &d, uint32_t nb0, int a, cudaStream_t st);
 void launch_walls(const Dev &d, uint32_t np, uint32_t nw, cudaStream_t st);
 void launch_cell_init(const Dev &d, uint32_t np, int a, cudaStream_t st);
@@ -25,7 +25,10 @@ using namespace sphk;
 
 struct sph_ctx {
     Dev d{};
-    Params hp{};
+    Params hp{};                     // the first instance's parameters (all of one scene's)
+    std::vector<Params> hps;         // every instance's parameters
+    uint32_t np_all = 0, ncells_all = 0, ninst = 1;
+    bool batched = false;
     int device = 0;
     cudaStream_t stream = nullptr;
     int a = 0;                       // buffer holding the current state
@@ -116,14 +119,15 @@ __global__ void k_to_user(const T *src, T *dst, const uint32_t *sidx, uint32_t n
 __global__ void k_rows_to_user(Dev d, uint32_t *contacts, double4 *distmod, double4 *delta_t,
                                int A)
 {
-    const Params &P = *d.prm;
     const uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= (uint64_t)P.np * NC) return;
+    if (e >= (uint64_t)d.np_all * NC) return;
     const uint32_t u = (uint32_t)(e / NC), i = (uint32_t)(e % NC);
     const uint32_t s = d.sidx[u];
+    const Params &P = prm_of(d, s);
     const bool occ = (d.cmask[s] >> i) & 1u;
     const uint32_t v = d.contacts[(size_t)s * NC + i];
-    if (contacts) contacts[e] = occ ? d.uid[v] : P.np;
+    // partners as indices within the particle's own scene; np marks empty
+    if (contacts) contacts[e] = occ ? d.uid[v] - P.uid_base : P.np;
     if (distmod) {
         double4 o = make_double4(0.0, 0.0, 0.0, 0.0);
         if (occ) {
@@ -140,18 +144,17 @@ __global__ void k_rows_to_user(Dev d, uint32_t *contacts, double4 *distmod, doub
 __global__ void k_cells_out(Dev d, uint32_t *cell_sorted, uint32_t *perm, uint32_t *cstart,
                             uint32_t *cend)
 {
-    const Params &P = *d.prm;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < P.ncells) {
+    if (i < d.ncells_all) {
         const uint32_t b = d.cell_start[i], e = d.cell_start[i + 1];
         cstart[i] = (b == e) ? 0xffffffffu : b;
         cend[i] = (b == e) ? 0u : e;
         for (uint32_t k = b; k < e; ++k) cell_sorted[k] = i;
     }
-    if (i == P.ncells) {
+    if (i == d.ncells_all) {
         for (uint32_t k = d.cell_start[i]; k < d.cell_start[i + 1]; ++k) cell_sorted[k] = 0xffffffffu;
     }
-    if (i < P.np) perm[i] = d.uid[d.cellorder[i]];
+    if (i < d.np_all) perm[i] = d.uid[d.cellorder[i]];
 }
 
 __global__ void k_count_contacts(const uint32_t *cmask, uint32_t np, unsigned long long *out)
@@ -175,10 +178,10 @@ int sync_status(sph_ctx *c)
 
 void enqueue_one_step(sph_ctx *c, int a, int write_outputs, cudaStream_t st)
 {
-    launch_rebuild(c->d, c->hp.np, c->hp.ncells, a, st);
+    launch_rebuild(c->d, c->np_all, c->ncells_all, a, st);
     launch_bonds(c->d, c->hp.nb0, a, st);
-    launch_step(c->d, c->hp.np, a, write_outputs, st);
-    launch_walls(c->d, c->hp.np, c->hp.nw, st);
+    launch_step(c->d, c->np_all, (int)c->hp.contactmodel, a, write_outputs, st);
+    launch_walls(c->d, c->np_all, c->hp.nw, st);
 }
 
 int capture(sph_ctx *c, cudaGraphExec_t *out, int a, int nsteps, int write_last)
@@ -230,15 +233,15 @@ int profiled_step(sph_ctx *c, int a, int write_outputs, cudaStream_t st)
         for (auto &e : c->ev) CK(cudaEventCreate(&e));
     }
     CK(cudaEventRecord(c->ev[0], st));
-    launch_rebuild(c->d, c->hp.np, c->hp.ncells, a, st);
+    launch_rebuild(c->d, c->np_all, c->ncells_all, a, st);
     CK(cudaEventRecord(c->ev[1], st));
     launch_bonds(c->d, c->hp.nb0, a, st);
     CK(cudaEventRecord(c->ev[2], st));
-    launch_topo(c->d, c->hp.np, a, st);
+    launch_topo(c->d, c->np_all, c->hp.contactmodel == 1, a, st);
     CK(cudaEventRecord(c->ev[3], st));
-    launch_force(c->d, c->hp.np, a, write_outputs, st);
+    launch_force(c->d, c->np_all, (int)c->hp.contactmodel, a, write_outputs, st);
     CK(cudaEventRecord(c->ev[4], st));
-    launch_walls(c->d, c->hp.np, c->hp.nw, st);
+    launch_walls(c->d, c->np_all, c->hp.nw, st);
     CK(cudaEventRecord(c->ev[5], st));
     CK(cudaGetLastError());
     CK(cudaEventSynchronize(c->ev[5]));
@@ -254,8 +257,8 @@ int profiled_step(sph_ctx *c, int a, int write_outputs, cudaStream_t st)
 int do_relayout(sph_ctx *c, cudaStream_t st)
 {
     // the cell list must describe the current positions before storage follows it
-    launch_rebuild(c->d, c->hp.np, c->hp.ncells, c->a, st);
-    relayout(c->d, c->hp.np, c->a, c->scratch, st);
+    launch_rebuild(c->d, c->np_all, c->ncells_all, c->a, st);
+    relayout(c->d, c->np_all, c->a, c->scratch, st);
     CK(cudaGetLastError());
     c->relayouts++;
     c->since_relayout = 0;
@@ -270,27 +273,27 @@ int sph_version(void) { return SPHK_VERSION; }
 
 const char *sph_last_error(const sph_ctx *c) { return c ? c->err.c_str() : "null context"; }
 
-int sph_create(const sph_config *cfg, sph_ctx **out)
+}  // extern "C"
+
+namespace {
+
+// The reasons a scene configuration is refused (empty when it is valid).
+std::string config_problem(const sph_config *cfg)
 {
-    if (!cfg || !out) return SPH_ERR_BAD_INPUT;
-    sph_ctx *c = new sph_ctx();
-    *out = c;
     const uint64_t ncells = (uint64_t)cfg->num[0] * cfg->num[1] * cfg->num[2];
-    std::string why;
-    if (cfg->np == 0) why = "np must be positive";
-    else if (cfg->nw > SPHK_MAXWALLS) why = "nw exceeds MAXWALLS (6)";
-    else if (ncells == 0 || ncells >= 0xfffffff0ull) why = "grid.num must be positive and below 2^32 cells";
-    else if (cfg->contactmodel != 2) why = "only contact model 2 (contactLinear) is implemented";
-    else if (!(cfg->dt > 0.0)) why = "dt must be positive";
-    else if ((uint64_t)cfg->np * NC >= 0xffffffffull) why = "np too large";
-    if (!why.empty()) {
-        c->err = why;
-        return SPH_ERR_BAD_INPUT;
-    }
-    c->device = cfg->device;
-    CK(cudaSetDevice(c->device));
-    CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
-    Params &P = c->hp;
+    if (cfg->np == 0) return "np must be positive";
+    if (cfg->nw > SPHK_MAXWALLS) return "nw exceeds MAXWALLS (6)";
+    if (ncells == 0 || ncells >= 0xfffffff0ull) return "grid.num must be positive and below 2^32 cells";
+    if (cfg->contactmodel < 1 || cfg->contactmodel > 3) return "contact model must be 1, 2 or 3";
+    if (!(cfg->dt > 0.0)) return "dt must be positive";
+    if ((uint64_t)cfg->np * NC >= 0xffffffffull) return "np too large";
+    return "";
+}
+
+// Params of one scene (the rest -- rmax, skin -- is set at upload).
+void fill_params(const sph_config *cfg, Params &P)
+{
+    P = Params{};
     P.np = cfg->np; P.nw = cfg->nw; P.nb0 = cfg->nb0; P.contactmodel = cfg->contactmodel;
     P.periodic = cfg->periodic;
     double ext = 0.0;
@@ -302,7 +305,7 @@ int sph_create(const sph_config *cfg, sph_ctx **out)
         P.g[k] = cfg->g[k];
         ext = std::fmax(ext, std::fmax(std::fabs(cfg->origo[k]), std::fabs(cfg->L[k])));
     }
-    P.ncells = (uint32_t)ncells;
+    P.ncells = cfg->num[0] * cfg->num[1] * cfg->num[2];
     P.dt = cfg->dt;
     P.k_n = cfg->k_n; P.k_t = cfg->k_t; P.k_r = cfg->k_r;
     P.gamma_n = cfg->gamma_n; P.gamma_t = cfg->gamma_t; P.gamma_r = cfg->gamma_r;
@@ -318,9 +321,65 @@ int sph_create(const sph_config *cfg, sph_ctx **out)
     // generous bound on the cull's absolute error
     P.cull_eps = (float)(4e-6 * (ext > 0.0 ? ext : 1.0));
     P.prune_pad = 4.0 * (double)P.cull_eps;
+    // model 1 also acts on pairs with a gap below db (capillary cohesion)
+    P.reach_extra = (cfg->contactmodel == 1 && cfg->db > 0.0) ? cfg->db : 0.0;
+}
 
-    const size_t np = cfg->np;
+// One context over `ninst` scenes laid end to end: particle u of scene i is
+// global particle uid_base(i) + u, its cells are global cells cell_base(i)..
+int create_impl(const sph_config *cfgs, uint32_t ninst, bool batched, sph_ctx **out)
+{
+    sph_ctx *c = new sph_ctx();
+    *out = c;
+    uint64_t np_all = 0, ncells_all = 0, nb0 = 0;
+    for (uint32_t i = 0; i < ninst; ++i) {
+        const sph_config *cfg = &cfgs[i];
+        std::string why = config_problem(cfg);
+        if (why.empty() && batched) {
+            if (cfg->contactmodel != 2) why = "batched scenes use contact model 2";
+            else if (cfg->nw != 0) why = "batched scenes have no dynamic walls (nw = 0)";
+            else if (cfg->nb0 != 0) why = "batched scenes have no bonds (nb0 = 0)";
+            else if (cfg->device != cfgs[0].device) why = "batched scenes share one device";
+        }
+        if (!why.empty()) {
+            c->err = batched ? "scene " + std::to_string(i) + ": " + why : why;
+            return SPH_ERR_BAD_INPUT;
+        }
+        np_all += cfg->np;
+        ncells_all += (uint64_t)cfg->num[0] * cfg->num[1] * cfg->num[2];
+        nb0 += cfg->nb0;
+    }
+    if (np_all * NC >= 0xffffffffull || ncells_all >= 0xfffffff0ull) {
+        c->err = "the scenes together are too large for one context";
+        return SPH_ERR_BAD_INPUT;
+    }
+    c->batched = batched;
+    c->ninst = ninst;
+    c->np_all = (uint32_t)np_all;
+    c->ncells_all = (uint32_t)ncells_all;
+    c->hps.resize(ninst);
+    uint32_t cb = 0, ub = 0;
+    std::vector<uint32_t> cell_bases(ninst + 1);
+    for (uint32_t i = 0; i < ninst; ++i) {
+        fill_params(&cfgs[i], c->hps[i]);
+        c->hps[i].cell_base = cb;
+        c->hps[i].uid_base = ub;
+        cell_bases[i] = cb;
+        cb += c->hps[i].ncells;
+        ub += c->hps[i].np;
+    }
+    cell_bases[ninst] = cb;
+    c->hp = c->hps[0];
+    c->device = cfgs[0].device;
+    CK(cudaSetDevice(c->device));
+    CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+
+    const size_t np = c->np_all;
+    const size_t ncells = c->ncells_all;
     Dev &d = c->d;
+    d.np_all = c->np_all;
+    d.ncells_all = c->ncells_all;
+    d.ninst = ninst;
     int rc = SPH_OK;
 #define AL(ptr, n) if ((rc = dalloc(c, &(ptr), (n))) != SPH_OK) return rc;
     for (int b = 0; b < 2; ++b) {
@@ -330,24 +389,47 @@ int sph_create(const sph_config *cfg, sph_ctx **out)
     AL(d.force, np); AL(d.torque, np); AL(d.acc, np); AL(d.angacc, np); AL(d.edp, np);
     AL(d.uid, np); AL(d.sidx, np); AL(d.cell, np);
     AL(d.contacts, np * NC); AL(d.dmc, np); AL(d.delta_t, np * NC); AL(d.cmask, np);
-    AL(d.cell_start, (size_t)ncells + 2); AL(d.cellorder, np); AL(d.pos, np); AL(d.cell_fill, (size_t)ncells + 1);
-    AL(d.scan_tiles, scan_tile_count(P.ncells));
+    AL(d.cell_start, ncells + 2); AL(d.cellorder, np); AL(d.pos, np); AL(d.cell_fill, ncells + 1);
+    AL(d.scan_tiles, scan_tile_count(c->ncells_all));
     AL(d.alias_any, 1);
     AL(d.vl, np * VL_CAP); AL(d.vl_meta, np * VL_CAP); AL(d.vl_len, np); AL(d.disp, np);
-    AL(d.movers, MOVER_CAP); AL(d.dirty, (size_t)ncells + 1); AL(d.vs, 1);
+    AL(d.movers, MOVER_CAP); AL(d.dirty, ncells + 1); AL(d.vs, 1);
     AL(d.wf_pp, np); AL(d.wtouch, np); AL(d.wf_partial, div_up(np, 256));
     AL(d.walls, 1);
-    AL(d.bonds, cfg->nb0); AL(d.bonds_delta, cfg->nb0); AL(d.bonds_omega, cfg->nb0);
-    AL(d.bond_f, cfg->nb0); AL(d.bond_t, cfg->nb0); AL(d.bond_xu, cfg->nb0);
-    AL(d.bond_ptr, np + 1); AL(d.bond_list, 2 * (size_t)cfg->nb0);
-    AL(d.status, 1); AL(d.rebuild, 1); AL(d.prm, 1);
+    AL(d.bonds, nb0); AL(d.bonds_delta, nb0); AL(d.bonds_omega, nb0);
+    AL(d.bond_f, nb0); AL(d.bond_t, nb0); AL(d.bond_xu, nb0);
+    AL(d.bond_ptr, np + 1); AL(d.bond_list, 2 * (size_t)nb0);
+    if (c->hp.contactmodel == 1) AL(d.c1acc, np);
+    AL(d.status, 1); AL(d.rebuild, 1); AL(d.prm, ninst);
+    if (batched) {
+        AL(d.inst, np);
+        AL(d.inst_cell_base, (size_t)ninst + 1);
+        CK(cudaMemcpy(d.inst_cell_base, cell_bases.data(), ((size_t)ninst + 1) * 4,
+                      cudaMemcpyHostToDevice));
+    }
     c->scratch_bytes = np * NC * sizeof(double4) + np * sizeof(uint32_t) + 256;
     char *sc = nullptr;
     AL(sc, c->scratch_bytes);
     c->scratch = sc;
 #undef AL
-    CK(cudaMemcpy(d.prm, &P, sizeof(Params), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(d.prm, c->hps.data(), sizeof(Params) * ninst, cudaMemcpyHostToDevice));
     return SPH_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int sph_create(const sph_config *cfg, sph_ctx **out)
+{
+    if (!cfg || !out) return SPH_ERR_BAD_INPUT;
+    return create_impl(cfg, 1, false, out);
+}
+
+int sph_batch_create(const sph_config *cfgs, uint32_t ninst, sph_ctx **out)
+{
+    if (!cfgs || !out || ninst == 0) return SPH_ERR_BAD_INPUT;
+    return create_impl(cfgs, ninst, true, out);
 }
 
 int sph_set_option(sph_ctx *c, int option, int64_t value)
@@ -384,25 +466,39 @@ int sph_upload(sph_ctx *c, const sph_host_state *h)
     if (P.nb0 > 0 && (!h->bonds || !h->bonds_delta || !h->bonds_omega))
         return fail(c, SPH_ERR_BAD_INPUT, "sph_upload: bond arrays required when nb0 > 0");
     CK(cudaSetDevice(c->device));
-    const size_t np = P.np, nb0 = P.nb0;
+    const size_t np = c->np_all, nb0 = P.nb0;
     Dev &d = c->d;
     const int A = 0;
     c->a = A;
+    // scene of every particle (particles of scene i follow those of scene i-1)
+    std::vector<uint32_t> inst_of(np, 0u);
+    for (uint32_t i = 0; i < c->ninst; ++i)
+        for (uint32_t u = 0; u < c->hps[i].np; ++u) inst_of[c->hps[i].uid_base + u] = i;
+    if (c->batched) CK(cudaMemcpy(d.inst, inst_of.data(), np * 4, cudaMemcpyHostToDevice));
     // kinematics (identity storage order for now)
     std::vector<double> buf(np * 4);
     CK(cudaMemcpy(d.xr[A], h->x, np * 32, cudaMemcpyHostToDevice));
     {
-        // largest radius, for the cell-level distance test of contact search
-        double rmax = 0.0;
-        for (size_t i = 0; i < np; ++i) rmax = std::fmax(rmax, h->x[4 * i + 3]);
-        c->hp.rmax = rmax;
-        c->hp.skin = c->skin_rel * rmax;
-        CK(cudaMemcpy(d.prm, &c->hp, sizeof(Params), cudaMemcpyHostToDevice));
+        // largest radius of each scene, for the cell-level distance test of
+        // contact search; one Verlet skin for the whole context, from the
+        // largest radius of all
+        double rmax_all = 0.0;
+        for (uint32_t i = 0; i < c->ninst; ++i) {
+            Params &Q = c->hps[i];
+            double rmax = 0.0;
+            for (size_t u = Q.uid_base; u < (size_t)Q.uid_base + Q.np; ++u)
+                rmax = std::fmax(rmax, h->x[4 * u + 3]);
+            Q.rmax = rmax;
+            rmax_all = std::fmax(rmax_all, rmax);
+        }
+        for (auto &Q : c->hps) Q.skin = c->skin_rel * rmax_all;
+        c->hp = c->hps[0];
+        CK(cudaMemcpy(d.prm, c->hps.data(), sizeof(Params) * c->ninst, cudaMemcpyHostToDevice));
         Verlet V{};
         V.step = 1;
         V.all_rebuild = 1;
         CK(cudaMemcpy(d.vs, &V, sizeof(V), cudaMemcpyHostToDevice));
-        CK(cudaMemset(d.dirty, 0, ((size_t)c->hp.ncells + 1) * sizeof(uint32_t)));
+        CK(cudaMemset(d.dirty, 0, ((size_t)c->ncells_all + 1) * sizeof(uint32_t)));
         CK(cudaMemset(d.vl_len, VL_NONE, np));
     }
     CK(cudaMemcpy(d.vel[A], h->vel, np * 32, cudaMemcpyHostToDevice));
@@ -464,18 +560,20 @@ int sph_upload(sph_ctx *c, const sph_host_state *h)
         std::vector<uint32_t> cmask(np, 0u);
         std::vector<double> dts(np * NC * 4, 0.0);
         for (size_t i = 0; i < np; ++i) {
+            // partners are indices within the particle's own scene
+            const Params &Q = c->hps[inst_of[i]];
             for (int k = 0; k < NC; ++k) {
                 const uint32_t v = h->contacts[i * NC + k];
-                if (v >= np) continue;
-                rows[i * NC + k] = v;
+                if (v >= Q.np) continue;
+                rows[i * NC + k] = v + Q.uid_base;
                 cmask[i] |= 1u << k;
                 uint32_t code = 0;
                 if (h->distmod) {
                     const double dx = h->distmod[(i * NC + k) * 4];
                     const double dy = h->distmod[(i * NC + k) * 4 + 1];
-                    if (dx == P.L[0]) code |= 1u; else if (dx == -P.L[0]) code |= 2u;
+                    if (dx == Q.L[0]) code |= 1u; else if (dx == -Q.L[0]) code |= 2u;
                     else if (dx != 0.0) return fail(c, SPH_ERR_BAD_INPUT, "distmod.x must be 0 or +-L[0]");
-                    if (dy == P.L[1]) code |= 4u; else if (dy == -P.L[1]) code |= 8u;
+                    if (dy == Q.L[1]) code |= 4u; else if (dy == -Q.L[1]) code |= 8u;
                     else if (dy != 0.0) return fail(c, SPH_ERR_BAD_INPUT, "distmod.y must be 0 or +-L[1]");
                 }
                 dmc[2 * i + (k >> 4)] |= (unsigned long long)code << (4 * (k & 15));
@@ -534,7 +632,7 @@ int sph_upload(sph_ctx *c, const sph_host_state *h)
     c->t_host = h->t_current;
     c->steps = 0;
     // cell list of the initial positions, then storage in cell order
-    launch_cell_init(d, P.np, A, c->stream);
+    launch_cell_init(d, c->np_all, A, c->stream);
     CK(cudaGetLastError());
     int rc = do_relayout(c, c->stream);
     if (rc != SPH_OK) return rc;
@@ -609,7 +707,7 @@ int sph_download(sph_ctx *c, sph_host_state *h)
     CK(cudaSetDevice(c->device));
     CK(cudaDeviceSynchronize());
     const Params &P = c->hp;
-    const uint32_t np = P.np;
+    const uint32_t np = c->np_all;
     Dev &d = c->d;
     const int A = c->a;
     const unsigned int grid = div_up(np, 256);
@@ -676,7 +774,7 @@ int sph_get_contacts(sph_ctx *c, uint32_t *contacts, double *distmod, double *de
     if (!c || !c->uploaded) return fail(c, SPH_ERR_BAD_INPUT, "sph_get_contacts before upload");
     CK(cudaSetDevice(c->device));
     CK(cudaDeviceSynchronize());
-    const uint32_t np = c->hp.np;
+    const uint32_t np = c->np_all;
     const size_t n = (size_t)np * NC;
     uint32_t *dc = nullptr;
     double4 *ddm = nullptr, *ddt = nullptr;
@@ -700,7 +798,7 @@ int sph_get_cells(sph_ctx *c, uint32_t *cell_sorted, uint32_t *perm, uint32_t *c
     if (!c || !c->uploaded) return fail(c, SPH_ERR_BAD_INPUT, "sph_get_cells before upload");
     CK(cudaSetDevice(c->device));
     CK(cudaDeviceSynchronize());
-    const uint32_t np = c->hp.np, nc = c->hp.ncells;
+    const uint32_t np = c->np_all, nc = c->ncells_all;
     uint32_t *b = nullptr;
     const size_t words = (size_t)np * 2 + (size_t)nc * 2;
     CK(cudaMallocAsync(&b, words * 4, c->stream));
@@ -721,7 +819,7 @@ int sph_get_wall_forces(sph_ctx *c, double *wall0_force)
     if (!c || !c->uploaded || !wall0_force) return fail(c, SPH_ERR_BAD_INPUT, "bad arguments");
     CK(cudaSetDevice(c->device));
     CK(cudaDeviceSynchronize());
-    CK(cudaMemcpy(wall0_force, c->d.wf_pp, (size_t)c->hp.np * 8, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(wall0_force, c->d.wf_pp, (size_t)c->np_all * 8, cudaMemcpyDeviceToHost));
     return SPH_OK;
 }
 
@@ -734,7 +832,7 @@ int sph_get_stats(sph_ctx *c, sph_stats *out)
         unsigned long long *cnt = nullptr;
         CK(cudaMallocAsync(&cnt, 8, c->stream));
         CK(cudaMemsetAsync(cnt, 0, 8, c->stream));
-        k_count_contacts<<<592, 256, 0, c->stream>>>(c->d.cmask, c->hp.np, cnt);
+        k_count_contacts<<<592, 256, 0, c->stream>>>(c->d.cmask, c->np_all, cnt);
         unsigned long long v = 0;
         CK(cudaMemcpyAsync(&v, cnt, 8, cudaMemcpyDeviceToHost, c->stream));
         CK(cudaFreeAsync(cnt, c->stream));

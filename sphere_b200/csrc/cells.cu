@@ -28,14 +28,16 @@ constexpr int SCAN_TILE = CELL_BLOCK * SCAN_ITEMS;   // 2048 counters per block
 
 __global__ void k_cell_init(Dev d, int A)
 {
-    const Params &P = *d.prm;
     const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= P.np) return;
+    if (s >= d.np_all) return;
+    const Params &P = prm_of(d, s);
     const double4 x = d.xr[A][s];
     uint32_t c = cell_id(P, x.x, x.y, x.z);
     if (c >= P.ncells) {
         atomicOr(d.status, ST_OUT_OF_GRID);
-        c = P.ncells;
+        c = d.ncells_all;
+    } else {
+        c += P.cell_base;
     }
     d.cell[s] = c;
 }
@@ -43,10 +45,9 @@ __global__ void k_cell_init(Dev d, int A)
 __global__ void k_count(Dev d)
 {
     if (*d.rebuild == 0u) return;
-    const Params &P = *d.prm;
     const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s == 0) *d.alias_any = 0u;   // recomputed by k_post_sort
-    if (s >= P.np) return;
+    if (s >= d.np_all) return;
     atomicAdd(&d.cell_fill[d.cell[s]], 1u);
 }
 
@@ -79,8 +80,7 @@ __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t &e
 __global__ void k_scan_tiles(Dev d)
 {
     if (*d.rebuild == 0u) return;
-    const Params &P = *d.prm;
-    const uint32_t n = P.ncells + 1;
+    const uint32_t n = d.ncells_all + 1;
     const uint32_t base = blockIdx.x * SCAN_TILE + threadIdx.x * SCAN_ITEMS;
     uint32_t sum = 0;
 #pragma unroll
@@ -96,8 +96,7 @@ __global__ void k_scan_tiles(Dev d)
 __global__ void k_scan_apply(Dev d)
 {
     if (*d.rebuild == 0u) return;
-    const Params &P = *d.prm;
-    const uint32_t n = P.ncells + 1;
+    const uint32_t n = d.ncells_all + 1;
     uint32_t pre = 0;
     for (uint32_t b = threadIdx.x; b < blockIdx.x; b += CELL_BLOCK) pre += d.scan_tiles[b];
     // block reduction of pre
@@ -126,16 +125,15 @@ __global__ void k_scan_apply(Dev d)
         if (base + i < n) d.cell_start[base + i] = run;
         run += v[i];
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) d.cell_start[n] = P.np;
+    if (blockIdx.x == 0 && threadIdx.x == 0) d.cell_start[n] = d.np_all;
 }
 
 // each particle takes a slot of its cell's range; counters return to zero
 __global__ void k_scatter(Dev d)
 {
     if (*d.rebuild == 0u) return;
-    const Params &P = *d.prm;
     const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= P.np) return;
+    if (s >= d.np_all) return;
     const uint32_t c = d.cell[s];
     const uint32_t k = atomicSub(&d.cell_fill[c], 1u) - 1u;
     d.cellorder[d.cell_start[c] + k] = s;
@@ -145,9 +143,8 @@ __global__ void k_scatter(Dev d)
 __global__ void k_cellsort(Dev d)
 {
     if (*d.rebuild == 0u) return;
-    const Params &P = *d.prm;
     const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c > P.ncells) return;
+    if (c > d.ncells_all) return;
     const uint32_t beg = d.cell_start[c], end = d.cell_start[c + 1];
     for (uint32_t i = beg + 1; i < end; ++i) {
         const uint32_t s = d.cellorder[i];
@@ -167,10 +164,10 @@ __global__ void k_cellsort(Dev d)
 __global__ void k_post_sort(Dev d, int A)
 {
     if (*d.rebuild == 0u) return;
-    const Params &P = *d.prm;
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= P.np) return;
+    if (k >= d.np_all) return;
     const uint32_t s = d.cellorder[k];
+    const Params &P = prm_of(d, s);
     d.pos[s] = k;
     const double4 x = d.xr[A][s];
     d.xs[A][k] = make_float4((float)x.x, (float)x.y, (float)x.z, (float)x.w);
@@ -190,18 +187,29 @@ __global__ void k_post_sort(Dev d, int A)
 __global__ void k_mark_dirty(Dev d)
 {
     if (*d.rebuild == 0u) return;
-    const Params &P = *d.prm;
     Verlet &V = *d.vs;
     const uint32_t n = min(V.nmovers, MOVER_CAP);
     if (blockIdx.x == 0 && threadIdx.x == 0 && V.movers_overflow) {
         V.all_rebuild = 1u;
         V.dmax_bits = 0u;
     }
-    const uint32_t nx = P.num[0], ny = P.num[1], nz = P.num[2];
     for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < 2 * n; e += gridDim.x * blockDim.x) {
         const uint2 mv = d.movers[e >> 1];
-        const uint32_t c = (e & 1u) ? mv.y : mv.x;
-        if (c >= P.ncells) continue;
+        const uint32_t cg = (e & 1u) ? mv.y : mv.x;
+        if (cg >= d.ncells_all) continue;
+        // the instance owning global cell cg (batched contexts)
+        uint32_t inst = 0;
+        if (d.inst) {
+            uint32_t lo = 0, hi = d.ninst;
+            while (hi - lo > 1) {
+                const uint32_t mid = (lo + hi) >> 1;
+                if (d.inst_cell_base[mid] <= cg) lo = mid; else hi = mid;
+            }
+            inst = lo;
+        }
+        const Params &P = d.prm[inst];
+        const uint32_t c = cg - P.cell_base;
+        const uint32_t nx = P.num[0], ny = P.num[1], nz = P.num[2];
         const int32_t cx = (int32_t)(c % nx), cy = (int32_t)((c / nx) % ny), cz = (int32_t)(c / (nx * ny));
         for (int oz = -1; oz < 2; ++oz) {
             const int32_t z = cz + oz;
@@ -218,7 +226,7 @@ __global__ void k_mark_dirty(Dev d)
                         if (P.periodic != 1 && P.periodic != 2) continue;
                         x = (x + (int32_t)nx) % (int32_t)nx;
                     }
-                    d.dirty[(uint32_t)x + (uint32_t)y * nx + (nx * ny) * (uint32_t)z] = V.step;
+                    d.dirty[P.cell_base + (uint32_t)x + (uint32_t)y * nx + (nx * ny) * (uint32_t)z] = V.step;
                 }
             }
         }
@@ -253,7 +261,7 @@ unsigned int scan_tile_count(uint32_t ncells)
 __global__ void k_relayout_inv(Dev d, uint32_t *inv)
 {
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= d.prm->np) return;
+    if (k >= d.np_all) return;
     inv[d.cellorder[k]] = k;
 }
 
@@ -287,7 +295,7 @@ __global__ void k_gather_dt(const double4 *src, double4 *dst, const uint32_t *or
 __global__ void k_relayout_finish(Dev d, int A)
 {
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= d.prm->np) return;
+    if (k >= d.np_all) return;
     d.cellorder[k] = k;
     d.pos[k] = k;
     d.sidx[d.uid[k]] = k;
@@ -335,6 +343,7 @@ void relayout(const Dev &d, uint32_t np, int a, void *scratch, cudaStream_t st)
     gather_back(d.cmask, scratch, order, np, st);
     gather_back(d.dmc, scratch, order, np, st);
     gather_back(d.wtouch, scratch, order, np, st);
+    if (d.inst) gather_back(d.inst, scratch, order, np, st);
     const unsigned int rows = div_up((unsigned long long)np * NC, CELL_BLOCK);
     {
         uint32_t *tmp = static_cast<uint32_t *>(scratch);

@@ -64,6 +64,9 @@ struct Params {
     double rmax;        // largest radius of the scene (set at upload)
     double prune_pad;   // absolute slack of the cell-level distance test (metres)
     double skin;        // Verlet-list skin (metres); 0 disables the lists
+    double reach_extra; // model 1: db, the capillary reach beyond contact (metres)
+    uint32_t cell_base; // batched contexts: first global cell id of this instance
+    uint32_t uid_base;  // batched contexts: first global particle index of this instance
 };
 
 constexpr int VL_CAP = 32;              // candidates kept per particle
@@ -97,6 +100,12 @@ struct Walls {
 // particle index and sidx[uid] its inverse.  Contact rows store partners as
 // storage indices, np marks an empty slot.
 struct Dev {
+    // sizes of the whole context: one scene, or every instance of a batch
+    uint32_t np_all, ncells_all, ninst;
+    // batched contexts: instance of each storage index and the first global
+    // cell id of each instance (ninst + 1 entries); nullptr for one scene
+    uint32_t *inst;
+    uint32_t *inst_cell_base;
     // double-buffered kinematics read by neighbours: [0]/[1]
     double4 *xr[2];       // x, y, z, radius
     double4 *vel[2];      // vx, vy, vz, fixvel
@@ -143,11 +152,30 @@ struct Dev {
     uint32_t *bond_xu;          // user index that received +f this step, or ~0u
     uint32_t *bond_ptr;         // [np + 1] CSR by uid
     uint32_t *bond_list;        // [2 nb0] (bond << 1) | role (0: x, 1: y)
+    // contact model 1: contact force xyz and pressure summed by k_topo
+    double4 *c1acc;
     // status
     uint32_t *status;
     uint32_t *rebuild;          // cell list must be rebuilt before the next step
     Params *prm;
 };
+
+// Parameters of the scene that storage index s belongs to.  Dev::prm holds
+// one Params per instance; a single-scene context has exactly one.
+__device__ __forceinline__ const Params &prm_of(const Dev &d, uint32_t s)
+{
+    return d.inst ? d.prm[d.inst[s]] : *d.prm;
+}
+
+// The same, with the kind of context fixed at compile time (the step
+// kernels are instantiated for each, so a single scene's kernels carry no
+// instance lookup).
+template <bool BATCH>
+__device__ __forceinline__ const Params &prm_at(const Dev &d, uint32_t s)
+{
+    if constexpr (BATCH) return d.prm[d.inst[s]];
+    else return *d.prm;
+}
 
 // periodic shift code: bits 0-1 x (1: +L, 2: -L), bits 2-3 y
 __device__ __forceinline__ d3 decode_dm(uint32_t code, const Params &P)

@@ -107,6 +107,130 @@ __device__ __noinline__ void contact_linear(const Params &P, d3 &F, d3 &T, doubl
     dt4 = make_double4(delta_t.x, delta_t.y, delta_t.z, 0.0f);
 }
 
+// The FP32 transcendentals of the force laws (expf in capillaryCohesion_exp,
+// powf in contactHertz), evaluated as the float nearest to the
+// double-precision result.  The reference's GPU build used its fast-math
+// intrinsics and its host build the C library's functions; neither is
+// correctly rounded, so these are the one place where this path follows
+// neither bit for bit (the oracle computes the same nearest float).
+__device__ __forceinline__ double f32_expf(double x)
+{
+    return (double)__double2float_rn(exp((double)__double2float_rn(x)));
+}
+__device__ __forceinline__ double f32_powf(double x, float y)
+{
+    return (double)__double2float_rn(pow((double)__double2float_rn(x), (double)y));
+}
+
+// contactLinearViscous, src/contactmodels.cuh:114-253 (contact model 1): no
+// tangential history, and the torque is left alone (its update is commented
+// out in the reference, :244).
+__device__ __noinline__ void contact_viscous(const Params &P, d3 &F, double &p, double4 vel_a,
+                                                double4 vel_b, d3 angvel_a, d3 angvel_b,
+                                                double ra, double rb, d3 x_ab,
+                                                double x_ab_length, double delta)
+{
+    const d3 n = divs(x_ab, x_ab_length);
+    const d3 vel_linear = mk(vel_a.x - vel_b.x, vel_a.y - vel_b.y, vel_a.z - vel_b.z);
+    const d3 vel = add(add(vel_linear, smul(ra + delta / 2.0, cross(n, angvel_a))),
+                       smul(rb + delta / 2.0, cross(n, angvel_b)));
+    const double vel_n = dot(vel_linear, n);
+    const d3 vel_t = sub(vel, muls(n, dot(vel, n)));
+    const double vel_t_length = flen(vel_t);
+    d3 f_n = smul(-P.k_n * delta - P.gamma_n * vel_n, n);
+    if (dot(f_n, n) < 0.0f) f_n = mk(0.0, 0.0, 0.0);
+    const double f_n_length = flen(f_n);
+    const d3 f_c = smul(-P.kappa * fsqrt_of(ra * rb), n);
+    d3 f_t = mk(0.0, 0.0, 0.0);
+    if (vel_t_length > 0.0) {
+        const double f_t_visc = P.gamma_t * vel_t_length;
+        double f_t_limit;
+        if (vel_t_length > 0.001f) f_t_limit = P.mu_d * flen(sub(f_n, f_c));
+        else f_t_limit = P.mu_s * flen(sub(f_n, f_c));
+        if (f_t_visc < f_t_limit) f_t = divs(smul(-f_t_visc, vel_t), vel_t_length);
+        else f_t = divs(smul(-f_t_limit, vel_t), vel_t_length);
+    }
+    F = add(F, add(add(f_n, f_t), f_c));
+    p += f_n_length / (4.0f * REF_PI * ra * ra);
+}
+
+// capillaryCohesion_exp, src/cohesion.cuh:314-350
+__device__ __noinline__ void capillary_exp(const Params &P, d3 &F, double ra, double rb,
+                                              double delta, d3 x_ab, double x_ab_length)
+{
+    const d3 n = divs(x_ab, x_ab_length);
+    double r;
+    if ((ra / rb) > (rb / ra)) r = ra / rb;
+    else r = rb / ra;
+    const double h = -fsqrt_of(r);
+    const double R_har = (2.0f * ra * rb) / (ra + rb);
+    const double R_geo = fsqrt_of(ra * rb);
+    const double lambda = 0.9f * h * fsqrt_of(P.V_b / R_har);
+    const d3 f_c = smul(-P.kappa * R_geo * f32_expf(-delta / lambda), n);
+    F = add(F, f_c);
+}
+
+// contactHertz, src/contactmodels.cuh:499-666 (contact model 3).  As in the
+// reference, delta is the (negative) overlap, so its fractional powers are
+// NaN and so are the forces of every touching pair.
+__device__ __noinline__ void contact_hertz(const Params &P, d3 &F, d3 &T, double &es_dot,
+                                              double &ev_dot, double &p, double4 vel_a,
+                                              d3 angvel_a, double4 vel_b4, double4 angvel_b4,
+                                              double ra, double rb, d3 x, double x_length,
+                                              double delta, double4 &dt4)
+{
+    const double dt = P.dt;
+    const d3 vel_b = xyz(vel_b4), angvel_b = xyz(angvel_b4);
+    const d3 dt0u = xyz(dt4);
+    const d3 n = divs(x, x_length);
+    const d3 vel_linear = mk(vel_a.x - vel_b.x, vel_a.y - vel_b.y, vel_a.z - vel_b.z);
+    const d3 vel = add(add(vel_linear, smul(ra + delta / 2.0, cross(n, angvel_a))),
+                       smul(rb + delta / 2.0, cross(n, angvel_b)));
+    const d3 angvel_ab = sub(angvel_a, angvel_b);
+    const double angvel_ab_length = flen(angvel_ab);
+    const double vel_n = dot(vel_linear, n);
+    const d3 vel_t = sub(vel, muls(n, dot(vel, n)));
+    const double vel_t_length = flen(vel_t);
+    const d3 delta_t0 = sub(dt0u, muls(n, dot(dt0u, n)));
+    const double delta_t0_length = flen(delta_t0);
+    d3 delta_t = mk(0.0, 0.0, 0.0);   // the reference leaves it unset when unused
+    d3 f_n = smul(-P.k_n * f32_powf(delta, 3.0f / 2.0f)
+                      - P.gamma_n * f32_powf(delta, 1.0f / 4.0f) * vel_n, n);
+    ev_dot += P.gamma_n * vel_n * vel_n;
+    if (dot(f_n, n) < 0.0f) f_n = mk(0.0, 0.0, 0.0);
+    const double f_n_length = flen(f_n);
+    const d3 f_c = smul(-P.kappa * fsqrt_of(ra * rb), n);
+    d3 f_t = mk(0.0, 0.0, 0.0);
+    d3 T_res = mk(0.0, 0.0, 0.0);
+    if (delta_t0_length > 0.f || vel_t_length > 0.f) {
+        const d3 f_t_elast = smul(-P.k_t * f32_powf(delta, 1.0f / 2.0f), delta_t0);
+        const d3 f_t_visc = smul(-P.gamma_t * f32_powf(delta, 1.0f / 4.0f), vel_t);
+        double f_t_limit;
+        if (vel_t_length > 0.001f) f_t_limit = P.mu_d * flen(sub(f_n, f_c));
+        else f_t_limit = P.mu_s * flen(sub(f_n, f_c));
+        f_t = add(f_t_elast, f_t_visc);
+        const double f_t_length = flen(f_t);
+        if (f_t_length > f_t_limit) {
+            f_t = muls(f_t, f_t_limit / f_t_length);
+            delta_t = divs(add(f_t, smul(P.gamma_t * f32_powf(delta, 1.0f / 4.0f), vel_t)),
+                           -P.k_t * f32_powf(delta, 1.0f / 2.0f));
+            es_dot += flen(sub(delta_t0, delta_t)) * P.k_t / dt;
+        } else {
+            delta_t = add(delta_t0, muls(vel_t, dt));
+        }
+    }
+    if (angvel_ab_length > 0.f) {
+        T_res = divs(smul(-1.0f * fmin(P.gamma_r * ra * angvel_ab_length,
+                                       P.mu_r * ra * f_n_length),
+                          angvel_ab),
+                     angvel_ab_length);
+    }
+    F = add(F, add(add(f_n, f_t), f_c));
+    T = add(T, add(smul(-(ra + delta / 2.0), cross(n, f_t)), T_res));
+    p += f_n_length / (4.0f * REF_PI * ra * ra);
+    dt4 = make_double4(delta_t.x, delta_t.y, delta_t.z, 0.0f);
+}
+
 __device__ __forceinline__ uint32_t dm_get(unsigned long long lo, unsigned long long hi, int i)
 {
     return (uint32_t)((i < 16 ? (lo >> (4 * i)) : (hi >> (4 * (i - 16)))) & 0xFull);
@@ -201,6 +325,27 @@ __device__ __forceinline__ bool overlaps(const Params &P, const double4 *xr, uin
     return delta < 0.0f;
 }
 
+// Contact model 1 processes each candidate as soon as it is found
+// (findAndProcessContactsInCell, src/contactsearch.cuh:81-175): overlap ->
+// contactLinearViscous, else a gap below db -> capillaryCohesion_exp.  Out of
+// line, with every operand loaded here, so the candidate loop stays lean.
+__device__ __noinline__ void visc_pair(const Dev &d, int A, uint32_t s, uint32_t t,
+                                       uint32_t code, d3 &F, double &p)
+{
+    const Params &P = prm_of(d, s);
+    const double4 xa = d.xr[A][s], xb = d.xr[A][t];
+    const d3 dm = decode_dm(code, P);
+    const d3 xab = add(mk(xa.x - xb.x, xa.y - xb.y, xa.z - xb.z), dm);
+    const double len = flen(xab);
+    const double delta = len - (xa.w + xb.w);
+    if (delta < 0.0f) {
+        contact_viscous(P, F, p, d.vel[A][s], d.vel[A][t], xyz(d.angvel[A][s]),
+                        xyz(d.angvel[A][t]), xa.w, xb.w, xab, len, delta);
+    } else if (delta < P.db) {
+        capillary_exp(P, F, xa.w, xb.w, delta, xab, len);
+    }
+}
+
 // k_topo: one thread per cell-list position k, particle s = cellorder[k].
 //
 // List mode: while the particle's Verlet list is valid (no epoch restart, no
@@ -212,12 +357,16 @@ __device__ __forceinline__ bool overlaps(const Params &P, const double4 *xr, uin
 //
 // Sweep mode: the 27 stencil cells are scanned as in the reference (z, y, x;
 // members by particle index) and the list is recorded on the way.
+//
+// VISC (contact model 1): no slots; every candidate within ra + rb + db is
+// processed in visiting order and the contact force and pressure sums are
+// left in Dev::c1acc for k_force.
+template <bool VISC, bool BATCH>
 __global__ void __launch_bounds__(TOPO_BLOCK, 8)
 k_topo(Dev d, int A)
 {
     __shared__ uint32_t srow[NC * TOPO_BLOCK];
-    const Params &P = *d.prm;
-    const uint32_t np = P.np;
+    const uint32_t np = d.np_all;
     const int tid = threadIdx.x;
     const uint32_t k = blockIdx.x * TOPO_BLOCK + tid;
     if (k == 0) {
@@ -227,6 +376,7 @@ k_topo(Dev d, int A)
     }
     if (k >= np) return;
     const uint32_t s = d.cellorder[k];
+    const Params &P = prm_at<BATCH>(d, s);
     const double4 xa = d.xr[A][s];
     const double ra = xa.w;
     const double4 *__restrict__ xr = d.xr[A];
@@ -243,8 +393,15 @@ k_topo(Dev d, int A)
     const uint8_t len = d.vl_len[s];
     const bool list_ok = use_lists && !V.all_rebuild && len != VL_NONE &&
                          d.dirty[d.cell[s]] != V.step;
+    d3 F1 = mk(0.0, 0.0, 0.0);   // model 1 sums
+    double p1 = 0.0f;
 
-    if (list_ok) {
+    if (VISC && list_ok) {
+        const uint32_t *vl = d.vl + (size_t)s * VL_CAP;
+        const uint16_t *vm = d.vl_meta + (size_t)s * VL_CAP;
+        for (uint32_t e = 0; e < len; ++e)
+            visc_pair(d, A, s, vl[e], (uint32_t)vm[e] >> 5, F1, p1);
+    } else if (list_ok) {
         const uint32_t *vl = d.vl + (size_t)s * VL_CAP;
         const uint16_t *vm = d.vl_meta + (size_t)s * VL_CAP;
         int skip_slot = -1;
@@ -262,6 +419,7 @@ k_topo(Dev d, int A)
         const float Lf0 = (float)P.L[0], Lf1 = (float)P.L[1];
         const float eps = P.cull_eps;
         const float skinf = (float)P.skin;
+        const float extraf = (float)P.reach_extra;
         uint32_t *vl = d.vl + (size_t)s * VL_CAP;
         uint16_t *vm = d.vl_meta + (size_t)s * VL_CAP;
         uint32_t nlist = 0;
@@ -288,8 +446,9 @@ k_topo(Dev d, int A)
                     const float fy = (xaf.y - c[j].y) + sy;
                     const float fz = xaf.z - c[j].z;
                     const float d2 = __fmaf_rn(fx, fx, __fmaf_rn(fy, fy, fz * fz));
-                    const float rr = (xaf.w + c[j].w) * 1.000004f + eps;
-                    const float rs = (xaf.w + c[j].w + skinf) * 1.000004f + eps;
+                    const float rsum = VISC ? (xaf.w + c[j].w + extraf) : (xaf.w + c[j].w);
+                    const float rr = rsum * 1.000004f + eps;
+                    const float rs = (rsum + skinf) * 1.000004f + eps;
                     const uint32_t k2 = base + (uint32_t)j;
                     const bool ok = k2 < end && k2 != k;
                     if (ok && d2 < rs * rs) near |= 1u << j;
@@ -310,7 +469,9 @@ k_topo(Dev d, int A)
                     } else {
                         list_overflow = true;
                     }
-                    if ((hit >> j) & 1u) {
+                    if (VISC) {
+                        if ((hit >> j) & 1u) visc_pair(d, A, s, t, code, F1, p1);
+                    } else if ((hit >> j) & 1u) {
                         if (overlaps(P, xr, t, code, xa) &&
                             !topo_insert(d, srow, tid, s, t, code, ts)) {
                             // nc > NC: skip the rest of this cell; the list
@@ -343,7 +504,8 @@ k_topo(Dev d, int A)
                 fhi[q] = hi > 0.0 ? (float)(hi * hi) * 0.99999f : 0.0f;
             }
         }
-        const float reach = (float)((ra + P.rmax + P.skin) * (1.0 + 1e-5) + P.prune_pad);
+        const double extra = VISC ? P.reach_extra : 0.0;
+        const float reach = (float)((ra + P.rmax + P.skin + extra) * (1.0 + 1e-5) + P.prune_pad);
         const float reach2 = prune ? reach * reach : 3.0e38f;
 
         for (int oz = -1; oz < 2; ++oz) {
@@ -368,8 +530,9 @@ k_topo(Dev d, int A)
                     // the three x cells are consecutive ids: one run of xs
                     const uint32_t cid0 = (uint32_t)c0 + rowbase;
                     if (cid0 + 2 >= P.ncells) { ts.err |= ST_OUT_OF_GRID; continue; }
-                    const uint32_t b0 = d.cell_start[cid0], b1 = d.cell_start[cid0 + 1];
-                    const uint32_t b2 = d.cell_start[cid0 + 2], b3 = d.cell_start[cid0 + 3];
+                    const uint32_t g0 = cid0 + P.cell_base;
+                    const uint32_t b0 = d.cell_start[g0], b1 = d.cell_start[g0 + 1];
+                    const uint32_t b2 = d.cell_start[g0 + 2], b3 = d.cell_start[g0 + 3];
                     const uint32_t lo = (dyz2 + flo[0] <= reach2) ? b0 : b1;
                     const uint32_t hi = (dyz2 + fhi[0] <= reach2) ? b3 : b2;
                     scan_run(lo, hi, ycode, b1, b2, slot0);
@@ -385,8 +548,9 @@ k_topo(Dev d, int A)
                         }
                         const uint32_t cid = (uint32_t)cx + rowbase;
                         if (cid >= P.ncells) { ts.err |= ST_OUT_OF_GRID; continue; }
-                        const uint32_t e = d.cell_start[cid + 1];
-                        scan_run(d.cell_start[cid], e, code, e, e, slot0 + (uint32_t)(ox + 1));
+                        const uint32_t g = cid + P.cell_base;
+                        const uint32_t e = d.cell_start[g + 1];
+                        scan_run(d.cell_start[g], e, code, e, e, slot0 + (uint32_t)(ox + 1));
                     }
                 }
             }
@@ -394,6 +558,7 @@ k_topo(Dev d, int A)
         d.vl_len[s] = (use_lists && !list_overflow) ? (uint8_t)nlist : VL_NONE;
     }
 
+    if (VISC) d.c1acc[s] = make_double4(F1.x, F1.y, F1.z, p1);
     if (ts.dirty) {
         uint4 *row = reinterpret_cast<uint4 *>(d.contacts + (size_t)s * NC);
         const uint32_t occ = ts.occ;
@@ -418,14 +583,17 @@ struct ForceArgs {
     int write_outputs;  // store force/torque/acc/angacc/edp of this step
 };
 
+// MODEL: the contact model (1, 2 or 3), a template argument so that each
+// model's kernel carries only its own force law.
+template <int MODEL, bool BATCH>
 __global__ void __launch_bounds__(FORCE_BLOCK, 6)
 k_force(ForceArgs args)
 {
     const Dev &d = args.d;
-    const Params &P = *d.prm;
-    const uint32_t np = P.np;
+    const uint32_t np = d.np_all;
     const uint32_t s = blockIdx.x * FORCE_BLOCK + threadIdx.x;
     if (s >= np) return;
+    const Params &P = prm_at<BATCH>(d, s);
     const int A = args.a, B = 1 - args.a;
     uint32_t err = 0;
     const double4 xa = d.xr[A][s];
@@ -438,7 +606,11 @@ k_force(ForceArgs args)
 
     // ---- interact: occupied slots in slot order ----------------------------
     uint32_t occ = d.cmask[s];
-    if (occ && P.contactmodel == 2) {
+    if (MODEL == 1) {
+        const double4 c = d.c1acc[s];
+        F = mk(c.x, c.y, c.z);
+        p = c.w;
+    } else if (occ) {
         const uint32_t occ0 = occ;
         const ulonglong2 dmw = d.dmc[s];
         uint32_t *crow = d.contacts + (size_t)s * NC;
@@ -454,8 +626,12 @@ k_force(ForceArgs args)
             const double delta_n = xlen - (ra + rb);
             if (delta_n < 0.0f) {
                 double4 dt4 = dtrow[i];
-                contact_linear(P, F, T, es_dot, ev_dot, p, vel_a, angvel_a, d.vel[A][t],
-                               d.angvel[A][t], ra, rb, xab, xlen, delta_n, dt4);
+                if (MODEL == 2)
+                    contact_linear(P, F, T, es_dot, ev_dot, p, vel_a, angvel_a, d.vel[A][t],
+                                   d.angvel[A][t], ra, rb, xab, xlen, delta_n, dt4);
+                else
+                    contact_hertz(P, F, T, es_dot, ev_dot, p, vel_a, angvel_a, d.vel[A][t],
+                                  d.angvel[A][t], ra, rb, xab, xlen, delta_n, dt4);
                 dtrow[i] = dt4;
             } else {
                 // separated: free the slot and zero its history
@@ -620,7 +796,8 @@ k_force(ForceArgs args)
 
     // ---- cell of the new position, for the next step's cell list -----------
     uint32_t c = cell_id(P, x.x, x.y, x.z);
-    if (c >= P.ncells) { err |= ST_OUT_OF_GRID; c = P.ncells; }
+    if (c >= P.ncells) { err |= ST_OUT_OF_GRID; c = d.ncells_all; }
+    else c += P.cell_base;
     const uint32_t c_old = d.cell[s];
     if (c != c_old) {
         d.cell[s] = c;
@@ -634,21 +811,35 @@ k_force(ForceArgs args)
     if (err) atomicOr(d.status, err);
 }
 
-void launch_topo(const Dev &d, uint32_t np, int a, cudaStream_t st)
+void launch_topo(const Dev &d, uint32_t np, bool visc, int a, cudaStream_t st)
 {
-    k_topo<<<div_up(np, TOPO_BLOCK), TOPO_BLOCK, 0, st>>>(d, a);
+    const unsigned grid = div_up(np, TOPO_BLOCK);
+    if (d.inst)   // batched contexts: contact model 2 only
+        k_topo<false, true><<<grid, TOPO_BLOCK, 0, st>>>(d, a);
+    else if (visc)
+        k_topo<true, false><<<grid, TOPO_BLOCK, 0, st>>>(d, a);
+    else
+        k_topo<false, false><<<grid, TOPO_BLOCK, 0, st>>>(d, a);
 }
 
-void launch_force(const Dev &d, uint32_t np, int a, int write_outputs, cudaStream_t st)
+void launch_force(const Dev &d, uint32_t np, int model, int a, int write_outputs, cudaStream_t st)
 {
     ForceArgs args{d, a, write_outputs};
-    k_force<<<div_up(np, FORCE_BLOCK), FORCE_BLOCK, 0, st>>>(args);
+    const unsigned grid = div_up(np, FORCE_BLOCK);
+    if (d.inst)   // batched contexts: contact model 2 only
+        k_force<2, true><<<grid, FORCE_BLOCK, 0, st>>>(args);
+    else if (model == 1)
+        k_force<1, false><<<grid, FORCE_BLOCK, 0, st>>>(args);
+    else if (model == 3)
+        k_force<3, false><<<grid, FORCE_BLOCK, 0, st>>>(args);
+    else
+        k_force<2, false><<<grid, FORCE_BLOCK, 0, st>>>(args);
 }
 
-void launch_step(const Dev &d, uint32_t np, int a, int write_outputs, cudaStream_t st)
+void launch_step(const Dev &d, uint32_t np, int model, int a, int write_outputs, cudaStream_t st)
 {
-    launch_topo(d, np, a, st);
-    launch_force(d, np, a, write_outputs, st);
+    launch_topo(d, np, model == 1, a, st);
+    launch_force(d, np, model, a, write_outputs, st);
 }
 
 }  // namespace sphk

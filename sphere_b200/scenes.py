@@ -247,3 +247,56 @@ def collision(n=2000, seed=0, periodic=0, box=(0.06, 0.06, 0.06), r=(0.8e-3, 1.6
     sb.time_total = 100 * dt
     sb.time_file_dt = sb.time_total
     return sb
+
+
+def ensemble_member(i, cell_factor=2.0, n_range=(500, 20000), sid=None) -> Spherebin:
+    """Member i of the batched settling ensemble, seeded by 1000 + i.
+
+    - particle count N = round(exp(U(ln 500, ln 20000)));
+    - radii U(0.9, 1.1) mm, density 2600 kg/m^3;
+    - mu_s = mu_d = mu_ws = mu_wd ~ U(0.2, 0.8);
+    - k_n = k_t log-uniform in [1e5, 1e7] N/m.
+
+    The layout is ``settling`` scaled to N: a jittered cubic lattice (spacing
+    2.2 r_max, jitter U(+-0.1 r), nz ~ 1.25 nx) with 3 r_max margins in a box
+    3.6 times as tall as the lattice, implicit frictional walls, gravity
+    -9.81 m/s^2.  The time step follows the reference's rule
+    0.075 sqrt(m_min / max(k_n, k_t)) (python/sphere.py:1371).  gamma_n is
+    0.48 of the critical 2 sqrt(m k_n) at the 1 mm mass, the damping ratio of
+    ``settling``, and the wall damping equals it.  Cells are at least
+    ``cell_factor`` r_max wide."""
+    rng = np.random.default_rng(1000 + i)
+    n = int(round(math.exp(rng.uniform(math.log(n_range[0]), math.log(n_range[1])))))
+    radii = rng.uniform(0.9e-3, 1.1e-3, n)
+    mu = float(rng.uniform(0.2, 0.8))
+    k = float(math.exp(rng.uniform(math.log(1e5), math.log(1e7))))
+    r_max = float(radii.max())
+    spacing = 2.2 * r_max
+    nx = max(3, int(round((n / 1.25) ** (1.0 / 3.0))))
+    nz = int(math.ceil(n / (nx * nx)))
+    idx = np.arange(n)
+    lat = np.stack([idx % nx, (idx // nx) % nx, idx // (nx * nx)], axis=1).astype(float)
+    margin = 3.0 * r_max
+    sb = Spherebin(np_=n, nw=0, sid=sid or f"ensemble{i:04d}")
+    sb.radius = radii
+    sb.x = margin + lat * spacing + rng.uniform(-0.1, 0.1, (n, 3)) * radii[:, None]
+    width = 2.0 * margin + (nx - 1) * spacing
+    height = 3.6 * (2.0 * margin + (nz - 1) * spacing)
+    sb.origo = np.zeros(3)
+    sb.L = np.array([width, width, height])
+    sb.num = np.maximum(3, np.floor(sb.L / (cell_factor * r_max))).astype(np.uint32)
+    sb.periodic = 0
+    sb.g = np.array([0.0, 0.0, -9.81])
+    m_ref = 4.0 / 3.0 * math.pi * 1e-3 ** 3 * 2600.0
+    gamma_n = 0.48 * 2.0 * math.sqrt(m_ref * k)
+    _contact_params(sb, k_n=k, k_t=k, gamma_n=gamma_n, gamma_t=0.0, mu=mu, gamma_w=gamma_n)
+    m_min = 4.0 / 3.0 * math.pi * float(radii.min()) ** 3 * sb.rho
+    sb.time_dt = 0.075 * math.sqrt(m_min / k)
+    sb.time_total = 2000 * sb.time_dt
+    sb.time_file_dt = sb.time_total
+    return sb
+
+
+def ensemble(n_inst=512, cell_factor=2.0, first=0):
+    """The batched settling ensemble: members first .. first + n_inst - 1."""
+    return [ensemble_member(first + i, cell_factor=cell_factor) for i in range(n_inst)]

@@ -95,6 +95,7 @@ def load_library(path: os.PathLike | None = None):
     sig = {
         "sph_version": ([], C.c_int),
         "sph_create": ([C.POINTER(SphConfig), C.POINTER(vp)], C.c_int),
+        "sph_batch_create": ([C.POINTER(SphConfig), C.c_uint32, C.POINTER(vp)], C.c_int),
         "sph_set_option": ([vp, C.c_int, C.c_int64], C.c_int),
         "sph_upload": ([vp, C.POINTER(SphHostState)], C.c_int),
         "sph_step": ([vp, C.c_uint64, vp], C.c_int),
@@ -263,6 +264,78 @@ class Simulation:
 
     def __exit__(self, *exc):
         self.close()
+
+
+PARTICLE_FIELDS = ("x", "xysum", "vel", "vel0", "acc", "force", "angpos", "angvel", "angvel0",
+                   "angacc", "torque", "es_dot", "es", "ev_dot", "ev", "p", "contacts",
+                   "distmod", "delta_t")
+
+
+def pack_states(states) -> HostState:
+    """Scenes end to end, as a batched context takes them: per-particle rows
+    of scene 0, then scene 1, ...; contact partners stay scene-local."""
+    first = states[0]
+    kw = {}
+    for f in PARTICLE_FIELDS:
+        parts = [getattr(st, f) for st in states]
+        kw[f] = None if any(a is None for a in parts) else np.ascontiguousarray(np.concatenate(parts))
+    kw.update(bonds=np.zeros((0, 2), np.uint32), bonds_delta=np.zeros((0, 4)),
+              bonds_omega=np.zeros((0, 4)), walls_nx=np.zeros((0, 4)), walls_mvfd=np.zeros((0, 4)),
+              walls_vel0=np.zeros(0))
+    st = HostState(**kw)
+    st.t_current = first.t_current
+    return st
+
+
+def split_state(st: HostState, nps) -> list:
+    """Inverse of pack_states."""
+    out, off = [], 0
+    for n in nps:
+        kw = {f: (None if getattr(st, f) is None else getattr(st, f)[off:off + n].copy())
+              for f in PARTICLE_FIELDS}
+        kw.update(bonds=np.zeros((0, 2), np.uint32), bonds_delta=np.zeros((0, 4)),
+                  bonds_omega=np.zeros((0, 4)), walls_nx=np.zeros((0, 4)),
+                  walls_mvfd=np.zeros((0, 4)), walls_vel0=np.zeros(0))
+        part = HostState(**kw)
+        part.t_current = st.t_current
+        out.append(part)
+        off += n
+    return out
+
+
+class BatchSimulation(Simulation):
+    """Many independent scenes stepped together by one context
+    (sph_batch_create): every kernel launch covers all of them.  Each scene
+    keeps its own grid, parameters and time step, and its results are those
+    of a Simulation of that scene alone."""
+
+    def __init__(self, cfgs, device: int = 0, graph_steps: int | None = None,
+                 relayout_every: int | None = None, verlet_skin: float | None = None):
+        self.lib = load_library()
+        self.cfgs = list(cfgs)
+        self.nps = [c.np for c in self.cfgs]
+        # the context-wide sizes (cells() reports the context-wide cell list)
+        total = SceneConfig(**{**self.cfgs[0].__dict__})
+        total.np = sum(self.nps)
+        total.num = np.array([sum(int(c.ncells) for c in self.cfgs), 1, 1], np.uint32)
+        self.cfg = total
+        self._ctx = C.c_void_p()
+        arr = (SphConfig * len(self.cfgs))(*[make_config(c, device) for c in self.cfgs])
+        self._check(self.lib.sph_batch_create(arr, len(self.cfgs), C.byref(self._ctx)))
+        if graph_steps is not None:
+            self._check(self.lib.sph_set_option(self._ctx, OPT_GRAPH_STEPS, int(graph_steps)))
+        if relayout_every is not None:
+            self._check(self.lib.sph_set_option(self._ctx, OPT_RELAYOUT_EVERY, int(relayout_every)))
+        if verlet_skin is not None:
+            self._check(self.lib.sph_set_option(self._ctx, OPT_VERLET_SKIN,
+                                                int(round(verlet_skin * 1000))))
+
+    def upload(self, states):
+        super().upload(pack_states(states))
+
+    def download_all(self) -> list:
+        """The state of every scene, in the order they were given."""
+        return split_state(self.download(), self.nps)
 
 
 def empty_state(cfg: SceneConfig) -> HostState:

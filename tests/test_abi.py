@@ -29,7 +29,8 @@ def test_version(sphk_lib):
 @pytest.mark.parametrize("patch, msg", [
     (dict(np=0), b"np must be positive"),
     (dict(nw=7), b"MAXWALLS"),
-    (dict(contactmodel=3), b"contact model"),
+    (dict(contactmodel=0), b"contact model"),
+    (dict(contactmodel=4), b"contact model"),
     (dict(dt=0.0), b"dt must be positive"),
 ])
 def test_bad_config_rejected_without_gpu(sphk_lib, patch, msg):

@@ -11,7 +11,7 @@ import numpy as np
 import pytest
 
 from helpers import (BOND_FIELDS, OUTPUT_FIELDS, STATE_FIELDS, WALL_FIELDS, active_distmod,
-                     mismatches, run_oracle)
+                     mismatches, nan_aware_mismatches, run_oracle, with_model)
 from sphere_b200 import scenes
 from sphere_b200.spherebin import readbin
 from sphere_b200.sphk import SphError, Simulation
@@ -198,3 +198,55 @@ def test_out_of_grid_is_reported():
         with pytest.raises(SphError) as e:
             sim.sync()
         assert e.value.code == -3
+
+
+MODEL_SCENES = {
+    "box": dict(periodic=0),
+    "periodic_xy": dict(periodic=1),
+    "periodic_x_wall": dict(periodic=2, nw=1),
+    "box_wall": dict(periodic=0, nw=1),
+}
+
+
+@pytest.mark.parametrize("name", sorted(MODEL_SCENES))
+@pytest.mark.parametrize("skin", [0.0, 0.1], ids=["sweep_every_step", "verlet"])
+def test_model1_with_cohesion_matches_oracle(oracle_libs, name, skin):
+    """Contact model 1 (contactLinearViscous, processed during the neighbour
+    sweep) with capillary cohesion: bit for bit over 60 steps in two calls,
+    with the Verlet lists on and off."""
+    mk = lambda: with_model(scenes.collision(n=1500, seed=61, **MODEL_SCENES[name]), 1)
+    rc, want, _ = run_oracle(oracle_libs["orc"], mk(), 60)
+    assert rc == 0
+    got, _, stats = run_gpu(mk(), (23, 37), verlet_skin=skin)
+    assert mismatches(got, want, ALL) == []
+    assert stats["active_contacts"] == 0          # no slots in model 1
+    assert np.count_nonzero(want.p) > 100
+
+
+def test_model1_cohesion_reaches_beyond_contact(oracle_libs):
+    """A pair with a gap below db attracts under model 1: the capillary term
+    is found through the neighbour search exactly as the oracle finds it."""
+    sb = with_model(scenes.collision(n=2, seed=1, periodic=0, vmax=0.0, wmax=0.0,
+                                     g=(0.0, 0.0, 0.0)), 1, kappa=0.05, V_b=1e-12, db=2e-4)
+    sb.radius[:] = 1e-3
+    sb.x[0] = (0.03, 0.03, 0.03)
+    sb.x[1] = (0.03 + 2e-3 + 1e-4, 0.03, 0.03)
+    rc, want, _ = run_oracle(oracle_libs["orc"], sb, 3)
+    assert rc == 0
+    got, _, _ = run_gpu(sb, (3,))
+    assert mismatches(got, want, ALL) == []
+    assert got.force[0, 0] > 0.0 and got.force[1, 0] < 0.0
+
+
+@pytest.mark.parametrize("name", sorted(MODEL_SCENES))
+def test_model3_reproduces_reference_step(oracle_libs, name):
+    """Contact model 3 (contactHertz) gives NaN forces to every touching
+    pair, as the reference does; the GPU reproduces the step, with NaN in the
+    same places and every other value bit for bit."""
+    mk = lambda: with_model(scenes.collision(n=1500, seed=62, **MODEL_SCENES[name]), 3)
+    rc, want, _ = run_oracle(oracle_libs["orc"], mk(), 1)
+    assert rc == 0
+    got, _, _ = run_gpu(mk(), (1,))
+    assert nan_aware_mismatches(got, want, ALL) == []
+    touching = (want.contacts != mk().np).any(axis=1)
+    assert touching.sum() > 100 and np.isnan(got.force[touching, :3]).all()
