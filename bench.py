@@ -53,6 +53,12 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0,
                     help="bound on the timed CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--batch-instances", type=int, default=512,
+                    help="members of the batched settling ensemble (0: skip that leg)")
+    ap.add_argument("--batch-steps", type=int, default=2000)
+    ap.add_argument("--batch-sample", type=int, default=16,
+                    help="members run one by one for the per-instance baseline")
+    ap.add_argument("--no-autotune", action="store_true")
     return ap.parse_args()
 
 
@@ -314,6 +320,8 @@ def gpu_arm(args, rank, world, local):
                               for k in ("cells", "bonds", "topo", "force", "walls")},
         "clocks": clocks.summary(),
     }
+    if args.batch_instances > 0:
+        out["batched"] = batched_leg(args, rank, world, local, barrier, max_over_ranks)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_reference_run(sb, 1, 1000, args.cpu_seconds)
     if world > 1:
@@ -321,6 +329,106 @@ def gpu_arm(args, rank, world, local):
         dist.barrier()
         dist.destroy_process_group()
     return out
+
+
+def binpack(nps, world):
+    """Members to ranks: largest first onto the least-loaded rank."""
+    order = sorted(range(len(nps)), key=lambda i: (-nps[i], i))
+    load = [0] * world
+    bins = [[] for _ in range(world)]
+    for i in order:
+        r = min(range(world), key=lambda k: (load[k], k))
+        bins[r].append(i)
+        load[r] += nps[i]
+    return [sorted(b) for b in bins]
+
+
+def batched_leg(args, rank, world, local, barrier, max_over_ranks):
+    """The batched settling ensemble: every member this rank holds, stepped
+    together by one context, against the same members run one by one."""
+    import torch
+    from sphere_b200 import autotune, scenes
+    from sphere_b200.sphk import BatchSimulation, Simulation
+    from sphere_b200.state import config_from_spherebin, state_from_spherebin
+
+    n_inst = args.batch_instances
+    nps = [scenes.ensemble_member(i).np for i in range(n_inst)]
+    mine = binpack(nps, world)[rank]
+    tuned = None
+    if args.no_autotune:
+        cell_factor, skin, gsteps = 2.0, 0.1, 8
+    else:
+        sub = mine[:: max(1, len(mine) // 64)][:64]
+        t0 = time.perf_counter()
+        ch = autotune.tune(lambda cf: [scenes.ensemble_member(i, cell_factor=cf) for i in sub],
+                           warmup=10, steps=40, device=local)
+        cell_factor, skin, gsteps = ch.cell_factor, ch.verlet_skin, ch.graph_steps
+        tuned = {"members": len(sub), "seconds": time.perf_counter() - t0,
+                 "trials": ch.trials}
+    members = [scenes.ensemble_member(i, cell_factor=cell_factor) for i in mine]
+    cfgs = [config_from_spherebin(sb) for sb in members]
+    states = [state_from_spherebin(sb) for sb in members]
+    stream = torch.cuda.current_stream()
+    K = args.batch_steps
+
+    # ---- batched: all members in one context, inputs resident ---------------
+    t_e2e = time.perf_counter()
+    sim = BatchSimulation(cfgs, device=local, graph_steps=gsteps, verlet_skin=skin)
+    sim.upload(states)
+    sim.step(args.warmup, stream=stream.cuda_stream)
+    sim.sync()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    start.record(stream)
+    sim.step(K, stream=stream.cuda_stream)
+    end.record(stream)
+    end.synchronize()
+    barrier()
+    sim.sync()
+    ms_batch = max_over_ranks(start.elapsed_time(end))
+    _ = sim.download_all()
+    e2e_s = max_over_ranks(time.perf_counter() - t_e2e)
+    contacts = sim.stats()["active_contacts"]
+    sim.close()
+
+    # ---- per-instance baseline: a sample of the same members, one by one -----
+    per = {}
+    if rank == 0 and args.batch_sample > 0:
+        sample = list(range(0, len(members), max(1, len(members) // args.batch_sample)))
+        sample = sample[: args.batch_sample]
+        tot_ms = 0.0
+        for j in sample:
+            one = Simulation(cfgs[j], device=local, graph_steps=gsteps, verlet_skin=skin)
+            one.upload(states[j])
+            one.step(args.warmup, stream=stream.cuda_stream)
+            one.sync()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            one.step(K, stream=stream.cuda_stream)
+            b.record(stream)
+            b.synchronize()
+            one.sync()
+            tot_ms += a.elapsed_time(b)
+            one.close()
+        est_ms = tot_ms * len(members) / len(sample)
+        per = {"sampled_members": len(sample), "sampled_ms": tot_ms,
+               "estimated_ms_all_members": est_ms,
+               "instances_per_s": len(members) / (est_ms * 1e-3),
+               "speedup_batched_vs_per_instance": est_ms / ms_batch}
+    n_part = sum(nps)
+    return {
+        "metric": "batched instances/s", "value": n_inst / (ms_batch * 1e-3), "unit": "instances/s",
+        "workload": f"{n_inst} settling members (N log-uniform 500-20000, {n_part} spheres), "
+                    f"{K} steps each, one context per GPU",
+        "particles": n_part, "steps": K, "ms": ms_batch, "scaling": "strong",
+        "particle_steps_per_s": n_part * K / (ms_batch * 1e-3),
+        "active_contacts_end": contacts,
+        "choice": {"cell_factor": cell_factor, "verlet_skin": skin, "graph_steps": gsteps},
+        "autotune": tuned,
+        "e2e": {"value": n_inst / e2e_s, "unit": "instances/s", "seconds": e2e_s,
+                "note": "create + upload + warm-up + timed steps + download"},
+        "per_instance": per,
+    }
 
 
 def reference_arm(args, rank, world):

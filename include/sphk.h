@@ -164,6 +164,34 @@ int sph_relayout(sph_ctx *ctx);
 const char *sph_last_error(const sph_ctx *ctx);
 int sph_destroy(sph_ctx *ctx);
 
+/* ---- Differentiable step ----------------------------------------------------
+ * No counterpart in the reference: gradients of a run with respect to the
+ * contact parameters, for calibration.  sph_diff_begin switches an uploaded
+ * single-scene context (contact model 2, nw = 0, nb0 = 0) to the
+ * differentiable step: contact model 2 with exact FP64 vector lengths (the
+ * reference narrows them to float) and per-particle friction mu (np values,
+ * caller order; NULL: every particle gets the configuration's mu_s), a
+ * contact using the mean of its two particles' values for mu_s and mu_d.
+ * Energy rates and pressure are not computed in this mode.  Every
+ * sph_step after it keeps a checkpoint of the state every checkpoint_every
+ * steps (about 1.4 KB per particle each) and the context holds a tape of
+ * checkpoint_every steps (about 1.3 KB per particle per step); storage is
+ * not re-ordered while the mode is on.
+ * sph_diff_backward runs the adjoint of every step taken since
+ * sph_diff_begin, seeded with x_bar and v_bar (np*3 each, caller order, the
+ * derivatives of a loss with respect to the current positions and
+ * velocities; NULL means zero): each checkpoint segment is stepped again
+ * with the tape recorded, then reversed step by step.  It returns the
+ * gradient with respect to k_n, k_t and gamma_n (grad_params[3]), per-
+ * particle friction (grad_mu[np]) and the starting positions and velocities
+ * (x0_bar, v0_bar, np*3); any output may be NULL.  The context's state after
+ * the call is the state before it.  sph_diff_end returns to the plain step
+ * and frees the checkpoints and tape. */
+int sph_diff_begin(sph_ctx *ctx, const double *mu, uint32_t checkpoint_every);
+int sph_diff_backward(sph_ctx *ctx, const double *x_bar, const double *v_bar, double *grad_params,
+                      double *grad_mu, double *x0_bar, double *v0_bar);
+int sph_diff_end(sph_ctx *ctx);
+
 /* ---- Cell list without device allocation ----------------------------------
  * No counterpart in the reference: an addition for callers that cannot
  * allocate device memory -- a plugin whose host owns the device memory pool

@@ -1,0 +1,97 @@
+"""Autotuner for the batched ensemble: picks the cell size, the neighbour-sweep
+schedule (Verlet skin) and the graph batching by timing short runs.
+
+Of the knobs, only the cell size changes the scenes themselves: it sets each
+scene's grid, which is part of the input (and decides the reference's
+contact visiting order).  The sweep schedule and graph batching never change
+results -- the parity tests hold them to the same bits -- so the tuner may
+pick any of them freely.  Block shapes are fixed at compile time from an
+offline sweep of register caps and are not tuned here.
+
+Each candidate is timed on the device with CUDA events on the context's
+stream: `warmup` untimed steps, then `steps` timed steps.
+"""
+from __future__ import annotations
+
+import itertools
+import time
+from dataclasses import dataclass, field
+
+CELL_FACTORS = (2.0, 2.5, 3.0)
+SKINS = (0.0, 0.05, 0.1, 0.2)
+GRAPH_STEPS = (8, 16)
+
+
+@dataclass
+class Choice:
+    cell_factor: float
+    verlet_skin: float
+    graph_steps: int
+    ms_per_step: float
+    trials: list = field(default_factory=list)
+
+
+def _time_batch(scenes_list, verlet_skin, graph_steps, warmup, steps, device=0):
+    import torch
+
+    from .sphk import BatchSimulation
+    from .state import config_from_spherebin, state_from_spherebin
+    with BatchSimulation([config_from_spherebin(sb) for sb in scenes_list], device=device,
+                         graph_steps=graph_steps, verlet_skin=verlet_skin) as sim:
+        sim.upload([state_from_spherebin(sb) for sb in scenes_list])
+        cur = torch.cuda.current_stream()
+        sim.step(warmup, stream=cur.cuda_stream)
+        sim.sync()
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record(cur)
+        sim.step(steps, stream=cur.cuda_stream)
+        t1.record(cur)
+        t1.synchronize()
+        sim.sync()
+        return t0.elapsed_time(t1) / steps
+
+
+def tune(build_scenes, warmup=20, steps=60, cell_factors=CELL_FACTORS, skins=SKINS,
+         graph_steps=GRAPH_STEPS, device=0, log=None) -> Choice:
+    """Time every combination and return the fastest.
+
+    ``build_scenes(cell_factor)`` returns the list of scenes (Spherebin) for
+    that cell size.  The sweep schedule and graph batching are tuned for the
+    cell size that is best with the default schedule, so the number of runs
+    is len(cell_factors) + len(skins) * len(graph_steps)."""
+    trials = []
+    best_cf, best_ms = None, float("inf")
+    for cf in cell_factors:
+        sc = build_scenes(cf)
+        ms = _time_batch(sc, 0.1, 8, warmup, steps, device)
+        trials.append(dict(cell_factor=cf, verlet_skin=0.1, graph_steps=8, ms_per_step=ms))
+        if log:
+            log(f"autotune cell_factor={cf}: {ms:.4f} ms/step")
+        if ms < best_ms:
+            best_cf, best_ms = cf, ms
+    sc = build_scenes(best_cf)
+    best = Choice(best_cf, 0.1, 8, best_ms)
+    for skin, gs in itertools.product(skins, graph_steps):
+        if skin == 0.1 and gs == 8:
+            continue
+        ms = _time_batch(sc, skin, gs, warmup, steps, device)
+        trials.append(dict(cell_factor=best_cf, verlet_skin=skin, graph_steps=gs, ms_per_step=ms))
+        if log:
+            log(f"autotune skin={skin} graph_steps={gs}: {ms:.4f} ms/step")
+        if ms < best.ms_per_step:
+            best = Choice(best_cf, skin, gs, ms)
+    best.trials = trials
+    return best
+
+
+if __name__ == "__main__":
+    import json
+    import sys
+
+    from . import scenes
+    n = int(sys.argv[1]) if len(sys.argv) > 1 else 64
+    t = time.perf_counter()
+    c = tune(lambda cf: scenes.ensemble(n, cell_factor=cf), log=print)
+    print(json.dumps({"choice": {k: v for k, v in c.__dict__.items() if k != "trials"},
+                      "seconds": time.perf_counter() - t}))

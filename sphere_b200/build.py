@@ -28,7 +28,8 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC = os.environ.get("NVCC", shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc")
 CUDA_HOME = Path(NVCC).resolve().parent.parent
 
-KERNEL_SOURCES = ["api.cu", "step.cu", "cells.cu", "walls.cu", "bonds.cu", "noalloc.cu"]
+KERNEL_SOURCES = ["api.cu", "step.cu", "cells.cu", "walls.cu", "bonds.cu", "noalloc.cu",
+                  "adjoint.cu"]
 HOST_SOURCES = ["host/sphere.cpp", "host/file_io.cpp", "host/main.cpp"]
 
 
@@ -51,7 +52,8 @@ def _stale(target: Path, sources) -> bool:
 
 def build_lib(force=False, verbose_ptxas=False) -> Path:
     srcs = [CSRC / s for s in KERNEL_SOURCES]
-    deps = srcs + [CSRC / "sphk_internal.cuh", ROOT / "include" / "sphk.h"]
+    deps = srcs + [CSRC / "sphk_internal.cuh", CSRC / "diff_law.h", CSRC / "diff_step.cuh",
+                   ROOT / "include" / "sphk.h"]
     if not force and not _stale(LIB, deps):
         return LIB
     LIB.parent.mkdir(parents=True, exist_ok=True)

@@ -1,8 +1,9 @@
 // api.cu -- the C ABI of libsphk (include/sphk.h): contexts, host<->device
 // transfer in the reference's host layout, and stepping through CUDA graphs.
-#include "sphk_internal.cuh"
+#include "diff_step.cuh"
 #include "../../include/sphk.h"
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -19,6 +20,16 @@ void launch_cell_init(const Dev &d, uint32_t np, int a, cudaStream_t st);
 void launch_rebuild(const Dev &d, uint32_t np, uint32_t ncells, int a, cudaStream_t st);
 unsigned int scan_tile_count(uint32_t ncells);
 void relayout(const Dev &d, uint32_t np, int a, void *scratch, cudaStream_t st);
+void launch_force_tape(const Dev &d, uint32_t np, int a, int tape_step, cudaStream_t st);
+void launch_rev_step(const Dev &d, const AdjDev &a, uint32_t np, int j, cudaStream_t st);
+void launch_user_to_storage3(const double *src, double4 *dst, const uint32_t *uid, uint32_t n,
+                             cudaStream_t st);
+void launch_user_to_storage1(const double *src, double *dst, const uint32_t *uid, double dflt,
+                             uint32_t n, cudaStream_t st);
+void launch_storage_to_user3(const double4 *a, const double4 *b, double *dst, const uint32_t *sidx,
+                             uint32_t n, cudaStream_t st);
+void launch_storage_to_user1(const double *src, double *dst, const uint32_t *sidx, uint32_t n,
+                             cudaStream_t st);
 }  // namespace sphk
 
 using namespace sphk;
@@ -52,6 +63,21 @@ struct sph_ctx {
     std::vector<cudaEvent_t> ev;          // 5 events per profiled step
     double prof_ms[SPH_NPHASES] = {};
     uint64_t prof_steps = 0;
+    // differentiable mode: checkpoints every ckpt_every steps since
+    // sph_diff_begin, the tape of one segment and the adjoint arrays
+    bool diff = false;
+    uint32_t ckpt_every = 0;
+    uint64_t diff_steps = 0;
+    int64_t relayout_saved = 0;
+    struct Ckpt {
+        int a;
+        double t_host;
+        char *buf;
+    };
+    std::vector<Ckpt> ckpts;
+    std::vector<void *> diff_allocs;
+    size_t diff_bytes = 0;
+    AdjDev adj{};
 };
 
 namespace {
@@ -73,7 +99,7 @@ int fail(sph_ctx *c, int code, const std::string &msg)
     } while (0)
 
 template <typename T>
-int dalloc(sph_ctx *c, T **p, size_t count)
+int dalloc(sph_ctx *c, T **p, size_t count, std::vector<void *> *owner = nullptr)
 {
     const size_t bytes = sizeof(T) * (count ? count : 1);
     void *q = nullptr;
@@ -81,8 +107,8 @@ int dalloc(sph_ctx *c, T **p, size_t count)
     if (e != cudaSuccess) return fail(c, SPH_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
     e = cudaMemset(q, 0, bytes);
     if (e != cudaSuccess) return fail(c, SPH_ERR_CUDA, std::string("cudaMemset: ") + cudaGetErrorString(e));
-    c->allocs.push_back(q);
-    c->device_bytes += bytes;
+    (owner ? owner : &c->allocs)->push_back(q);
+    (owner ? c->diff_bytes : c->device_bytes) += bytes;
     *p = static_cast<T *>(q);
     return SPH_OK;
 }
@@ -640,9 +666,37 @@ int sph_upload(sph_ctx *c, const sph_host_state *h)
     return sync_status(c);
 }
 
+static int step_plain(sph_ctx *c, uint64_t nsteps, void *stream);
+static int save_ckpt(sph_ctx *c, sph_ctx::Ckpt &k);
+
 int sph_step(sph_ctx *c, uint64_t nsteps, void *stream)
 {
     if (!c || !c->uploaded) return fail(c, SPH_ERR_BAD_INPUT, "sph_step before sph_upload");
+    if (!c->diff) return step_plain(c, nsteps, stream);
+    // differentiable mode: a checkpoint at every multiple of ckpt_every steps
+    if (c->sticky != SPH_OK) return c->sticky;
+    CK(cudaSetDevice(c->device));
+    const uint64_t K = c->ckpt_every;
+    uint64_t left = nsteps;
+    while (left > 0) {
+        if (c->diff_steps % K == 0 && c->diff_steps / K == c->ckpts.size()) {
+            if (stream) CK(cudaStreamSynchronize(static_cast<cudaStream_t>(stream)));
+            sph_ctx::Ckpt k{};
+            const int rc = save_ckpt(c, k);
+            if (rc != SPH_OK) return rc;
+            c->ckpts.push_back(k);
+        }
+        const uint64_t chunk = std::min<uint64_t>(left, K - c->diff_steps % K);
+        const int rc = step_plain(c, chunk, stream);
+        if (rc != SPH_OK) return rc;
+        left -= chunk;
+        c->diff_steps += chunk;
+    }
+    return SPH_OK;
+}
+
+static int step_plain(sph_ctx *c, uint64_t nsteps, void *stream)
+{
     if (c->sticky != SPH_OK) return c->sticky;
     if (nsteps == 0) return SPH_OK;
     CK(cudaSetDevice(c->device));
@@ -841,7 +895,7 @@ int sph_get_stats(sph_ctx *c, sph_stats *out)
     }
     out->steps = c->steps;
     out->relayouts = c->relayouts;
-    out->device_bytes = c->device_bytes;
+    out->device_bytes = c->device_bytes + c->diff_bytes;
     return SPH_OK;
 }
 
@@ -866,6 +920,207 @@ int sph_relayout(sph_ctx *c)
     return sync_status(c);
 }
 
+// ---- differentiable mode ---------------------------------------------------
+
+// The arrays a checkpoint holds, in order: the state a step reads and
+// carries (buffer `a` of the double-buffered kinematics) and the contact
+// slots with their history.  Cell lists and Verlet lists are rebuilt on
+// restore; results do not depend on them.
+static std::vector<std::pair<void *, size_t>> ckpt_fields(sph_ctx *c, int a)
+{
+    Dev &d = c->d;
+    const size_t np = c->np_all;
+    return {{d.xr[a], np * 32},       {d.vel[a], np * 32},  {d.angvel[a], np * 32},
+            {d.vel0, np * 32},        {d.angvel0, np * 32}, {d.angpos, np * 32},
+            {d.xysum, np * 16},       {d.esv, np * 16},     {d.contacts, np * NC * 4},
+            {d.dmc, np * 16},         {d.cmask, np * 4},    {d.delta_t, np * NC * 32}};
+}
+
+static int save_ckpt(sph_ctx *c, sph_ctx::Ckpt &k)
+{
+    k.a = c->a;
+    k.t_host = c->t_host;
+    size_t bytes = 0;
+    for (auto &f : ckpt_fields(c, c->a)) bytes += f.second;
+    k.buf = nullptr;
+    int rc = dalloc(c, &k.buf, bytes, &c->diff_allocs);
+    if (rc != SPH_OK) return rc;
+    size_t off = 0;
+    for (auto &f : ckpt_fields(c, c->a)) {
+        CK(cudaMemcpyAsync(k.buf + off, f.first, f.second, cudaMemcpyDeviceToDevice, c->stream));
+        off += f.second;
+    }
+    CK(cudaStreamSynchronize(c->stream));
+    return SPH_OK;
+}
+
+static int restore_ckpt(sph_ctx *c, const sph_ctx::Ckpt &k)
+{
+    c->a = k.a;
+    c->t_host = k.t_host;
+    size_t off = 0;
+    for (auto &f : ckpt_fields(c, k.a)) {
+        CK(cudaMemcpyAsync(f.first, k.buf + off, f.second, cudaMemcpyDeviceToDevice, c->stream));
+        off += f.second;
+    }
+    Dev &d = c->d;
+    launch_cell_init(d, c->np_all, k.a, c->stream);
+    CK(cudaMemsetAsync(d.dirty, 0, ((size_t)c->ncells_all + 1) * sizeof(uint32_t), c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    const uint32_t one = 1;
+    CK(cudaMemcpy(d.rebuild, &one, 4, cudaMemcpyHostToDevice));
+    Verlet V{};
+    V.step = 1;
+    V.all_rebuild = 1;
+    CK(cudaMemcpy(d.vs, &V, sizeof(V), cudaMemcpyHostToDevice));
+    return SPH_OK;
+}
+
+static void free_diff(sph_ctx *c)
+{
+    for (void *p : c->diff_allocs) cudaFree(p);
+    c->diff_allocs.clear();
+    c->diff_bytes = 0;
+    c->ckpts.clear();
+    c->adj = AdjDev{};
+    Dev &d = c->d;
+    d.mu_p = nullptr;
+    d.tp_x = d.tp_v = d.tp_w = d.tp_dt0 = nullptr;
+    d.tp_mask = d.tp_partner = nullptr;
+    d.tp_dmc = nullptr;
+}
+
+int sph_diff_begin(sph_ctx *c, const double *mu, uint32_t checkpoint_every)
+{
+    if (!c || !c->uploaded) return fail(c, SPH_ERR_BAD_INPUT, "sph_diff_begin before sph_upload");
+    if (c->diff) return fail(c, SPH_ERR_BAD_INPUT, "sph_diff_begin: already in differentiable mode");
+    const Params &P = c->hp;
+    if (c->batched || P.contactmodel != 2 || P.nw != 0 || P.nb0 != 0)
+        return fail(c, SPH_ERR_BAD_INPUT,
+                    "the differentiable step takes one scene with contact model 2, no dynamic "
+                    "walls and no bonds");
+    if (checkpoint_every == 0) return fail(c, SPH_ERR_BAD_INPUT, "checkpoint_every must be >= 1");
+    CK(cudaSetDevice(c->device));
+    CK(cudaDeviceSynchronize());
+    const size_t np = c->np_all, K = checkpoint_every;
+    Dev &d = c->d;
+    AdjDev &A = c->adj;
+    std::vector<void *> *own = &c->diff_allocs;
+    int rc = SPH_OK;
+#define ALD(ptr, n) if ((rc = dalloc(c, &(ptr), (n), own)) != SPH_OK) { free_diff(c); return rc; }
+    ALD(d.mu_p, np);
+    ALD(d.tp_x, K * np); ALD(d.tp_v, K * np); ALD(d.tp_w, K * np);
+    ALD(d.tp_mask, K * np); ALD(d.tp_dmc, K * np);
+    ALD(d.tp_partner, K * np * NC); ALD(d.tp_dt0, K * np * NC);
+    ALD(A.xb, np); ALD(A.vb, np); ALD(A.wb, np); ALD(A.v0b, np); ALD(A.w0b, np);
+    ALD(A.Fb, np); ALD(A.Tb, np); ALD(A.dtb, np * NC); ALD(A.mub, np); ALD(A.theta_b, 3);
+    double *tmp = nullptr;
+    ALD(tmp, np);
+#undef ALD
+    if (mu) CK(cudaMemcpy(tmp, mu, np * 8, cudaMemcpyHostToDevice));
+    launch_user_to_storage1(mu ? tmp : nullptr, d.mu_p, d.uid, P.mu_s, (uint32_t)np, c->stream);
+    CK(cudaStreamSynchronize(c->stream));
+    // kernels and graphs take Dev by value: capture again with the new arrays
+    drop_graphs(c);
+    c->relayout_saved = c->relayout_every;
+    c->relayout_every = 0;   // the tape and checkpoints are storage-indexed
+    c->diff = true;
+    c->ckpt_every = checkpoint_every;
+    c->diff_steps = 0;
+    sph_ctx::Ckpt k{};
+    if ((rc = save_ckpt(c, k)) != SPH_OK) return rc;
+    c->ckpts.push_back(k);
+    return SPH_OK;
+}
+
+int sph_diff_backward(sph_ctx *c, const double *x_bar, const double *v_bar, double *grad_params,
+                      double *grad_mu, double *x0_bar, double *v0_bar)
+{
+    if (!c || !c->diff) return fail(c, SPH_ERR_BAD_INPUT, "sph_diff_backward outside differentiable mode");
+    if (c->sticky != SPH_OK) return c->sticky;
+    CK(cudaSetDevice(c->device));
+    CK(cudaDeviceSynchronize());
+    const uint32_t np = c->np_all;
+    const uint64_t N = c->diff_steps, K = c->ckpt_every;
+    Dev &d = c->d;
+    AdjDev &A = c->adj;
+    cudaStream_t st = c->stream;
+    // the state after the forward, put back at the end
+    sph_ctx::Ckpt fin{};
+    int rc = save_ckpt(c, fin);
+    if (rc != SPH_OK) return rc;
+    // seeds: dL/dx and dL/dv of the current state
+    double *hx = nullptr;
+    {
+        rc = dalloc(c, &hx, 6 * (size_t)np, &c->diff_allocs);
+        if (rc != SPH_OK) return rc;
+        if (x_bar) CK(cudaMemcpy(hx, x_bar, (size_t)np * 24, cudaMemcpyHostToDevice));
+        if (v_bar) CK(cudaMemcpy(hx + 3 * (size_t)np, v_bar, (size_t)np * 24, cudaMemcpyHostToDevice));
+        launch_user_to_storage3(x_bar ? hx : nullptr, A.xb, d.uid, np, st);
+        launch_user_to_storage3(v_bar ? hx + 3 * (size_t)np : nullptr, A.vb, d.uid, np, st);
+    }
+    for (double4 *p : {A.wb, A.v0b, A.w0b}) CK(cudaMemsetAsync(p, 0, (size_t)np * 32, st));
+    CK(cudaMemsetAsync(A.dtb, 0, (size_t)np * NC * 32, st));
+    CK(cudaMemsetAsync(A.mub, 0, (size_t)np * 8, st));
+    CK(cudaMemsetAsync(A.theta_b, 0, 24, st));
+    const uint64_t nseg = (N + K - 1) / K;
+    for (uint64_t seg = nseg; seg-- > 0;) {
+        // adjoints survive the restore: they live apart from the state
+        if ((rc = restore_ckpt(c, c->ckpts[seg])) != SPH_OK) return rc;
+        const int len = (int)std::min<uint64_t>(K, N - seg * K);
+        int aa = c->a;
+        for (int j = 0; j < len; ++j) {
+            launch_rebuild(d, np, c->ncells_all, aa, st);
+            launch_topo(d, np, false, aa, st);
+            launch_force_tape(d, np, aa, j, st);
+            launch_walls(d, np, 0, st);
+            aa ^= 1;
+        }
+        for (int j = len - 1; j >= 0; --j) launch_rev_step(d, A, np, j, st);
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(st));
+    }
+    if ((rc = restore_ckpt(c, fin)) != SPH_OK) return rc;
+    if ((rc = sync_status(c)) != SPH_OK) return rc;
+    // results in the caller's order
+    double *out = nullptr;
+    rc = dalloc(c, &out, 7 * (size_t)np, &c->diff_allocs);
+    if (rc != SPH_OK) return rc;
+    launch_storage_to_user1(A.mub, out, d.sidx, np, st);
+    launch_storage_to_user3(A.xb, nullptr, out + np, d.sidx, np, st);
+    launch_storage_to_user3(A.vb, A.v0b, out + 4 * (size_t)np, d.sidx, np, st);
+    CK(cudaStreamSynchronize(st));
+    if (grad_params) CK(cudaMemcpy(grad_params, A.theta_b, 24, cudaMemcpyDeviceToHost));
+    if (grad_mu) CK(cudaMemcpy(grad_mu, out, (size_t)np * 8, cudaMemcpyDeviceToHost));
+    if (x0_bar) CK(cudaMemcpy(x0_bar, out + np, (size_t)np * 24, cudaMemcpyDeviceToHost));
+    if (v0_bar) CK(cudaMemcpy(v0_bar, out + 4 * (size_t)np, (size_t)np * 24, cudaMemcpyDeviceToHost));
+    // scratch of this call and the final-state copy
+    size_t fin_bytes = 0;
+    for (auto &f : ckpt_fields(c, c->a)) fin_bytes += f.second;
+    const std::pair<void *, size_t> scratch[] = {
+        {out, 7 * (size_t)np * 8}, {hx, 6 * (size_t)np * 8}, {fin.buf, fin_bytes}};
+    for (const auto &p : scratch) {
+        cudaFree(p.first);
+        auto &v = c->diff_allocs;
+        v.erase(std::remove(v.begin(), v.end(), p.first), v.end());
+        c->diff_bytes -= p.second;
+    }
+    return SPH_OK;
+}
+
+int sph_diff_end(sph_ctx *c)
+{
+    if (!c) return SPH_ERR_BAD_INPUT;
+    if (!c->diff) return SPH_OK;
+    CK(cudaSetDevice(c->device));
+    CK(cudaDeviceSynchronize());
+    free_diff(c);
+    drop_graphs(c);
+    c->diff = false;
+    c->relayout_every = c->relayout_saved;
+    return SPH_OK;
+}
+
 int sph_destroy(sph_ctx *c)
 {
     if (!c) return SPH_OK;
@@ -873,6 +1128,7 @@ int sph_destroy(sph_ctx *c)
     if (c->stream) cudaStreamSynchronize(c->stream);
     drop_graphs(c);
     for (auto e : c->ev) cudaEventDestroy(e);
+    free_diff(c);
     for (void *p : c->allocs) cudaFree(p);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;

@@ -154,6 +154,13 @@ struct Dev {
     uint32_t *bond_list;        // [2 nb0] (bond << 1) | role (0: x, 1: y)
     // contact model 1: contact force xyz and pressure summed by k_topo
     double4 *c1acc;
+    // differentiable step: per-particle friction and the tape of one segment
+    // ([step][np] rows; partner and history rows [step][np][NC], written for
+    // evaluated slots only)
+    double *mu_p;
+    double4 *tp_x, *tp_v, *tp_w, *tp_dt0;
+    uint32_t *tp_mask, *tp_partner;
+    ulonglong2 *tp_dmc;
     // status
     uint32_t *status;
     uint32_t *rebuild;          // cell list must be rebuilt before the next step

@@ -23,6 +23,7 @@
 // visiting order is the reference's: stencil cells z, y, x, members of a cell
 // by particle index.
 #include "sphk_internal.cuh"
+#include "diff_step.cuh"
 
 namespace sphk {
 
@@ -581,11 +582,16 @@ struct ForceArgs {
     Dev d;
     int a;              // read buffer (start of step); the kernel writes buffer 1-a
     int write_outputs;  // store force/torque/acc/angacc/edp of this step
+    int tape_step;      // differentiable step: tape row to record, or -1
 };
 
 // MODEL: the contact model (1, 2 or 3), a template argument so that each
 // model's kernel carries only its own force law.
-template <int MODEL, bool BATCH>
+// DIFF: the differentiable step (contact model 2 in exact FP64 with
+// per-particle friction, implicit walls only, no bonds), recording the tape
+// row args.tape_step when it is >= 0.  Energy rates and pressure are not
+// computed in this variant.
+template <int MODEL, bool BATCH, bool DIFF>
 __global__ void __launch_bounds__(FORCE_BLOCK, 6)
 k_force(ForceArgs args)
 {
@@ -606,7 +612,57 @@ k_force(ForceArgs args)
 
     // ---- interact: occupied slots in slot order ----------------------------
     uint32_t occ = d.cmask[s];
-    if (MODEL == 1) {
+    if constexpr (DIFF) {
+        const int j = args.tape_step;
+        const size_t row = (j >= 0) ? ((size_t)j * np + s) : 0;
+        uint32_t lawmask = 0;
+        const ulonglong2 dmw = d.dmc[s];
+        uint32_t *crow = d.contacts + (size_t)s * NC;
+        double4 *dtrow = d.delta_t + (size_t)s * NC;
+        const uint32_t occ0 = occ;
+        for (uint32_t m = occ0; m; m &= m - 1) {
+            const int i = __ffs(m) - 1;
+            const uint32_t t = crow[i];
+            const d3 dm = decode_dm(dm_get(dmw.x, dmw.y, i), P);
+            const double4 xb = d.xr[A][t];
+            dl::PairIn in;
+            in.xab = dl::v3(xa.x - xb.x + dm.x, xa.y - xb.y + dm.y, xa.z - xb.z + dm.z);
+            in.ra = ra;
+            in.rb = xb.w;
+            if (dl::len(in.xab) - (ra + xb.w) < 0.0) {
+                const double4 vb = d.vel[A][t], wb = d.angvel[A][t], d0 = dtrow[i];
+                in.va = dl::v3(vel_a.x, vel_a.y, vel_a.z);
+                in.vb = dl::v3(vb.x, vb.y, vb.z);
+                in.wa = dl::v3(angvel_a4.x, angvel_a4.y, angvel_a4.z);
+                in.wb = dl::v3(wb.x, wb.y, wb.z);
+                in.d0u = dl::v3(d0.x, d0.y, d0.z);
+                const dl::Law law{P.k_n, P.k_t, P.gamma_n, P.gamma_t,
+                                  0.5 * (d.mu_p[s] + d.mu_p[t]), P.kappa, P.dt};
+                dl::PairOut o;
+                dl::pair_fwd(law, in, o);
+                F = add(F, mk(o.F.x, o.F.y, o.F.z));
+                T = add(T, mk(o.T.x, o.T.y, o.T.z));
+                dtrow[i] = make_double4(o.dtn.x, o.dtn.y, o.dtn.z, 0.0);
+                lawmask |= 1u << i;
+                if (j >= 0) {
+                    d.tp_partner[row * NC + i] = t;
+                    d.tp_dt0[row * NC + i] = d0;
+                }
+            } else {
+                occ &= ~(1u << i);
+                crow[i] = np;
+                dtrow[i] = make_double4(0.0, 0.0, 0.0, 0.0);
+            }
+        }
+        if (occ != occ0) d.cmask[s] = occ;
+        if (j >= 0) {
+            d.tp_x[row] = xa;
+            d.tp_v[row] = vel_a;
+            d.tp_w[row] = angvel_a4;
+            d.tp_mask[row] = lawmask;
+            d.tp_dmc[row] = dmw;
+        }
+    } else if (MODEL == 1) {
         const double4 c = d.c1acc[s];
         F = mk(c.x, c.y, c.z);
         p = c.w;
@@ -645,7 +701,19 @@ k_force(ForceArgs args)
 
     // ---- walls, src/contactsearch.cuh:578-663 (defaults :416-427) ----------
     double w0f = 0.0;
-    {
+    if constexpr (DIFF) {
+        WallHits wh;
+        implicit_walls(P, xa, wh);
+        const dl::WallLaw wl{P.k_n, P.gamma_wn, P.gamma_wt, P.mu_ws, P.mu_wd};
+        for (int k = 0; k < wh.count; ++k) {
+            dl::V3 fw, tw;
+            dl::wall_fwd(wl, ra, dl::v3(vel_a.x, vel_a.y, vel_a.z),
+                         dl::v3(angvel_a4.x, angvel_a4.y, angvel_a4.z), wh.n[k], wh.delta[k], 0.0,
+                         fw, tw);
+            F = add(F, mk(fw.x, fw.y, fw.z));
+            T = add(T, mk(tw.x, tw.y, tw.z));
+        }
+    } else {
         const Walls &W = *d.walls;
         double4 wnx[5] = {make_double4(0.0f, 0.0f, -1.0f, P.L[2]), make_double4(-1.0f, 0.0f, 0.0f, P.L[0]),
                           make_double4(1.0f, 0.0f, 0.0f, 0.0f), make_double4(0.0f, -1.0f, 0.0f, P.L[1]),
@@ -795,8 +863,10 @@ k_force(ForceArgs args)
     }
 
     // ---- cell of the new position, for the next step's cell list -----------
+    // a position that is not finite (NaN forces, contact model 3) is
+    // outside the grid whatever its float-to-integer conversion gives
     uint32_t c = cell_id(P, x.x, x.y, x.z);
-    if (c >= P.ncells) { err |= ST_OUT_OF_GRID; c = d.ncells_all; }
+    if (c >= P.ncells || !isfinite(x.x + x.y + x.z)) { err |= ST_OUT_OF_GRID; c = d.ncells_all; }
     else c += P.cell_base;
     const uint32_t c_old = d.cell[s];
     if (c != c_old) {
@@ -824,16 +894,25 @@ void launch_topo(const Dev &d, uint32_t np, bool visc, int a, cudaStream_t st)
 
 void launch_force(const Dev &d, uint32_t np, int model, int a, int write_outputs, cudaStream_t st)
 {
-    ForceArgs args{d, a, write_outputs};
+    ForceArgs args{d, a, write_outputs, -1};
     const unsigned grid = div_up(np, FORCE_BLOCK);
     if (d.inst)   // batched contexts: contact model 2 only
-        k_force<2, true><<<grid, FORCE_BLOCK, 0, st>>>(args);
+        k_force<2, true, false><<<grid, FORCE_BLOCK, 0, st>>>(args);
+    else if (d.mu_p)   // the differentiable step
+        k_force<2, false, true><<<grid, FORCE_BLOCK, 0, st>>>(args);
     else if (model == 1)
-        k_force<1, false><<<grid, FORCE_BLOCK, 0, st>>>(args);
+        k_force<1, false, false><<<grid, FORCE_BLOCK, 0, st>>>(args);
     else if (model == 3)
-        k_force<3, false><<<grid, FORCE_BLOCK, 0, st>>>(args);
+        k_force<3, false, false><<<grid, FORCE_BLOCK, 0, st>>>(args);
     else
-        k_force<2, false><<<grid, FORCE_BLOCK, 0, st>>>(args);
+        k_force<2, false, false><<<grid, FORCE_BLOCK, 0, st>>>(args);
+}
+
+// The differentiable step, recording tape row `tape_step`.
+void launch_force_tape(const Dev &d, uint32_t np, int a, int tape_step, cudaStream_t st)
+{
+    ForceArgs args{d, a, 0, tape_step};
+    k_force<2, false, true><<<div_up(np, FORCE_BLOCK), FORCE_BLOCK, 0, st>>>(args);
 }
 
 void launch_step(const Dev &d, uint32_t np, int model, int a, int write_outputs, cudaStream_t st)

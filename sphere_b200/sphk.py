@@ -110,6 +110,9 @@ def load_library(path: os.PathLike | None = None):
         "sph_last_error": ([vp], C.c_char_p),
         "sph_destroy": ([vp], C.c_int),
         "sph_cell_list_noalloc": ([C.POINTER(SphConfig), vp, vp, vp, vp, vp, vp], C.c_int),
+        "sph_diff_begin": ([vp, _dp, C.c_uint32], C.c_int),
+        "sph_diff_backward": ([vp, _dp, _dp, _dp, _dp, _dp, _dp], C.c_int),
+        "sph_diff_end": ([vp], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)
@@ -247,6 +250,34 @@ class Simulation:
 
     def relayout(self):
         self._check(self.lib.sph_relayout(self._ctx))
+
+    # ---- differentiable step (sph_diff_*) ----------------------------------
+    def diff_begin(self, mu=None, checkpoint_every: int = 100):
+        """Switch to the differentiable step: exact FP64 lengths, per-particle
+        friction ``mu`` (np values; None: the configuration's mu_s)."""
+        m = None if mu is None else np.ascontiguousarray(mu, dtype=np.float64)
+        self._diff_keep = m
+        ptr = None if m is None else m.ctypes.data_as(_dp)
+        self._check(self.lib.sph_diff_begin(self._ctx, ptr, int(checkpoint_every)))
+
+    def diff_backward(self, x_bar=None, v_bar=None) -> dict:
+        """Adjoint of every step since diff_begin, seeded with dL/dx and dL/dv
+        of the current state ((np, 3) each).  Returns the gradients with
+        respect to k_n, k_t, gamma_n, per-particle friction and the starting
+        positions and velocities."""
+        n = self.cfg.np
+        xb = None if x_bar is None else np.ascontiguousarray(x_bar, dtype=np.float64).reshape(n, 3)
+        vb = None if v_bar is None else np.ascontiguousarray(v_bar, dtype=np.float64).reshape(n, 3)
+        gp = np.zeros(3)
+        gmu = np.zeros(n)
+        x0 = np.zeros((n, 3))
+        v0 = np.zeros((n, 3))
+        P = lambda a: None if a is None else a.ctypes.data_as(_dp)
+        self._check(self.lib.sph_diff_backward(self._ctx, P(xb), P(vb), P(gp), P(gmu), P(x0), P(v0)))
+        return {"k_n": gp[0], "k_t": gp[1], "gamma_n": gp[2], "mu": gmu, "x0": x0, "v0": v0}
+
+    def diff_end(self):
+        self._check(self.lib.sph_diff_end(self._ctx))
 
     def close(self):
         if self._ctx:
