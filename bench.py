@@ -59,6 +59,10 @@ def parse():
     ap.add_argument("--batch-sample", type=int, default=16,
                     help="members run one by one for the per-instance baseline")
     ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--adjoint-n", type=int, default=100_000,
+                    help="spheres of the calibration column (0: skip the adjoint leg)")
+    ap.add_argument("--adjoint-steps", type=int, default=4000)
+    ap.add_argument("--adjoint-checkpoint", type=int, default=100)
     return ap.parse_args()
 
 
@@ -78,6 +82,17 @@ def dist_env():
     world = int(os.environ.get("WORLD_SIZE", 1))
     local = int(os.environ.get("LOCAL_RANK", rank))
     return rank, world, local
+
+
+def reduce_max(x, world, device="cuda"):
+    """The largest of every rank's x (the timing rule: max over ranks)."""
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
 
 
 class ClockSampler:
@@ -216,12 +231,7 @@ def gpu_arm(args, rank, world, local):
         torch.cuda.synchronize()
 
     def max_over_ranks(x):
-        if world == 1:
-            return x
-        import torch.distributed as dist
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return reduce_max(x, world, "cuda")
 
     stream = torch.cuda.Stream()
     sim = Simulation(cfg, device=local)
@@ -322,6 +332,8 @@ def gpu_arm(args, rank, world, local):
     }
     if args.batch_instances > 0:
         out["batched"] = batched_leg(args, rank, world, local, barrier, max_over_ranks)
+    if args.adjoint_n > 0 and rank == 0:
+        out["adjoint"] = adjoint_leg(args, local)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_reference_run(sb, 1, 1000, args.cpu_seconds)
     if world > 1:
@@ -428,6 +440,110 @@ def batched_leg(args, rank, world, local, barrier, max_over_ranks):
         "e2e": {"value": n_inst / e2e_s, "unit": "instances/s", "seconds": e2e_s,
                 "note": "create + upload + warm-up + timed steps + download"},
         "per_instance": per,
+    }
+
+
+def height_profile_loss(x, r, lo, hi, target):
+    """Mean squared deviation of the 64-bin height profile (highest sphere
+    top per x-bin, 0 when empty) from `target`, and dLoss/dx."""
+    import numpy as np
+    bins = len(target)
+    top = x[:, 2] + r
+    b = np.clip(((x[:, 0] - lo) / (hi - lo) * bins).astype(np.int64), 0, bins - 1)
+    h = np.zeros(bins)
+    arg = np.full(bins, -1)
+    order = np.lexsort((top, b))           # by bin, then by height
+    last = np.r_[b[order][1:] != b[order][:-1], True]
+    for i in order[last]:
+        h[b[i]] = top[i]
+        arg[b[i]] = i
+    loss = float(np.mean((h - target) ** 2))
+    xbar = np.zeros_like(x)
+    for k in range(bins):
+        if arg[k] >= 0:
+            xbar[arg[k], 2] = 2.0 * (h[k] - target[k]) / bins
+    return loss, xbar
+
+
+def adjoint_leg(args, local):
+    """The calibration column: time of the checkpointed adjoint against the
+    differentiable forward, gradients of the height-profile loss, and a
+    finite-difference check of the k_n gradient on a contact-rich scene."""
+    import numpy as np
+    import torch
+    from sphere_b200 import adjoint, scenes
+    from sphere_b200.sphk import Simulation
+    from sphere_b200.state import config_from_spherebin, state_from_spherebin
+
+    sb = scenes.column(args.adjoint_n, seed=args.seed)
+    steps, K = args.adjoint_steps, args.adjoint_checkpoint
+    cfg = config_from_spherebin(sb)
+    st0 = state_from_spherebin(sb)
+    stream = torch.cuda.current_stream()
+    # the plain step (the reference's arithmetic) for scale
+    plain = Simulation(cfg, device=local)
+    plain.upload(st0)
+    plain.step(args.warmup, stream=stream.cuda_stream)
+    plain.sync()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    plain.step(steps, stream=stream.cuda_stream)
+    b.record(stream)
+    b.synchronize()
+    plain.sync()
+    ms_plain = a.elapsed_time(b)
+    plain.close()
+    # differentiable forward with checkpoints, then the adjoint
+    sim = Simulation(cfg, device=local)
+    sim.upload(st0)
+    sim.diff_begin(mu=None, checkpoint_every=K)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    sim.step(steps)
+    sim.sync()
+    t_fwd = time.perf_counter() - t0
+    st = sim.download()
+    target = np.random.default_rng(args.seed + 7).uniform(0.2, 0.32, 64)
+    loss, xbar = height_profile_loss(st.x[:, :3], st.x[:, 3], 0.0, float(sb.L[0]), target)
+    t0 = time.perf_counter()
+    g = sim.diff_backward(xbar)
+    t_bwd = time.perf_counter() - t0
+    stats = sim.stats()
+    sim.close()
+
+    # finite-difference check of dL/dk_n, h = 1e-6 relative, on a dense scene
+    fsb = scenes.collision(n=2000, seed=args.seed + 3, periodic=0, vmax=0.2, wmax=50.0)
+    w = np.random.default_rng(args.seed + 4).normal(size=(fsb.np, 3))
+    fsteps = 60
+
+    def floss(kn):
+        s_, st_ = adjoint.run_forward(fsb, fsteps, kn, fsb.k_t, fsb.gamma_n, None,
+                                      checkpoint_every=20, device=local)
+        return s_, float(np.sum(w * (st_.x[:, :3] - fsb.x)))
+    s_, _ = floss(fsb.k_n)
+    gk = s_.diff_backward(w)["k_n"]
+    s_.close()
+    h = 1e-6 * fsb.k_n
+    sp, lp = floss(fsb.k_n + h)
+    sp.close()
+    sm, lm = floss(fsb.k_n - h)
+    sm.close()
+    fd = (lp - lm) / (2 * h)
+    return {
+        "metric": "adjoint/forward time ratio", "value": t_bwd / t_fwd, "unit": "ratio",
+        "higher_is_better": False,
+        "workload": f"calibration column: {sb.np} spheres (radii as the 1M workload), RSA in "
+                    f"0.1x0.1x0.3 m on the floor of a 0.6x0.6x0.35 m box, FP64, dt 5e-7 s, "
+                    f"{steps} steps, checkpoints every {K}",
+        "forward_s": t_fwd, "backward_s": t_bwd,
+        "plain_step_ms": ms_plain / steps, "diff_forward_step_ms": 1e3 * t_fwd / steps,
+        "loss": loss, "grad": {"k_n": g["k_n"], "k_t": g["k_t"], "gamma_n": g["gamma_n"],
+                               "mu_global": float(g["mu"].sum()),
+                               "mu_particles_nonzero": int(np.count_nonzero(g["mu"]))},
+        "device_bytes": stats["device_bytes"],
+        "fd_check": {"scene": f"collision, {fsb.np} spheres, {fsteps} steps",
+                     "param": "k_n", "adjoint": gk, "central_difference": fd,
+                     "rel_error": abs(gk - fd) / abs(fd) if fd else None},
     }
 
 

@@ -300,3 +300,38 @@ def ensemble_member(i, cell_factor=2.0, n_range=(500, 20000), sid=None) -> Spher
 def ensemble(n_inst=512, cell_factor=2.0, first=0):
     """The batched settling ensemble: members first .. first + n_inst - 1."""
     return [ensemble_member(first + i, cell_factor=cell_factor) for i in range(n_inst)]
+
+
+def column(n=100_000, seed=0, col=(0.1, 0.1, 0.3), box=(0.6, 0.6, 0.35), k=1e6, mu=0.5,
+           dt=5e-7, sid="column") -> Spherebin:
+    """The calibration column: n spheres with the radii of ``polydisperse``
+    (log-normal, median 1 mm, sigma 0.2, clipped 0.5-2 mm), placed by random
+    sequential placement in a col[0] x col[1] x col[2] column standing on the
+    floor at the centre of a non-periodic box with the implicit frictional
+    walls; gravity -9.81 m/s^2, k_n = k_t = k, mu_s = mu_d = mu (walls too),
+    dt = 5e-7 s.  gamma_n (and the wall damping) is 0.48 of the critical
+    2 sqrt(m k_n) at the 1 mm mass, the damping ratio of ``settling``: the
+    settling scene's 100 N s/m would damp a millimetre grain by a factor
+    gamma dt / m of about 5 per step, which the explicit step cannot
+    integrate.  Cells are 2 r_max wide."""
+    rng = np.random.default_rng(seed)
+    radii = _lognormal_radii(rng, n)
+    pos = rsa_place(rng, radii, col, periodic_xy=False)
+    box = np.asarray(box, float)
+    pos[:, 0] += 0.5 * (box[0] - col[0])
+    pos[:, 1] += 0.5 * (box[1] - col[1])
+    sb = Spherebin(np_=n, nw=0, sid=sid)
+    sb.radius = radii
+    sb.x = pos
+    sb.origo = np.zeros(3)
+    sb.L = box
+    sb.num = np.floor(box / (2.0 * float(radii.max()))).astype(np.uint32)
+    sb.periodic = 0
+    sb.g = np.array([0.0, 0.0, -9.81])
+    m_ref = 4.0 / 3.0 * math.pi * 1e-3 ** 3 * 2600.0
+    gamma_n = 0.48 * 2.0 * math.sqrt(m_ref * k)
+    _contact_params(sb, k_n=k, k_t=k, gamma_n=gamma_n, gamma_t=0.0, mu=mu, gamma_w=gamma_n)
+    sb.time_dt = dt
+    sb.time_total = 4000 * dt
+    sb.time_file_dt = sb.time_total
+    return sb
