@@ -20,6 +20,7 @@ void launch_cell_init(const Dev &d, uint32_t np, int a, cudaStream_t st);
 void launch_rebuild(const Dev &d, uint32_t np, uint32_t ncells, int a, cudaStream_t st);
 unsigned int scan_tile_count(uint32_t ncells);
 void relayout(const Dev &d, uint32_t np, int a, void *scratch, cudaStream_t st);
+void launch_rebuild_gate(cudaGraphConditionalHandle h, const uint32_t *rebuild, cudaStream_t st);
 void launch_force_tape(const Dev &d, uint32_t np, int a, int tape_step, cudaStream_t st);
 void launch_rev_step(const Dev &d, const AdjDev &a, uint32_t np, int j, cudaStream_t st);
 void launch_user_to_storage3(const double *src, double4 *dst, const uint32_t *uid, uint32_t n,
@@ -42,6 +43,8 @@ struct sph_ctx {
     bool batched = false;
     int device = 0;
     cudaStream_t stream = nullptr;
+    cudaStream_t side = nullptr;     // captures the bodies of conditional graph nodes
+    bool cond_rebuild = true;        // graphs skip the rebuild kernels when no cell changed
     int a = 0;                       // buffer holding the current state
     uint64_t steps = 0, relayouts = 0, since_relayout = 0;
     double t_host = 0.0;
@@ -202,12 +205,47 @@ int sync_status(sph_ctx *c)
     return SPH_OK;
 }
 
-void enqueue_one_step(sph_ctx *c, int a, int write_outputs, cudaStream_t st)
+// Inside a stream capture: the rebuild as a conditional node whose body the
+// side stream captures, gated by k_rebuild_gate.
+int capture_rebuild_conditional(sph_ctx *c, int a, cudaStream_t st)
 {
-    launch_rebuild(c->d, c->np_all, c->ncells_all, a, st);
+    cudaStreamCaptureStatus cs;
+    unsigned long long id;
+    cudaGraph_t g;
+    const cudaGraphNode_t *deps;
+    size_t nd;
+    CK(cudaStreamGetCaptureInfo(st, &cs, &id, &g, &deps, &nd));
+    cudaGraphConditionalHandle h;
+    CK(cudaGraphConditionalHandleCreate(&h, g, 0, 0));
+    launch_rebuild_gate(h, c->d.rebuild, st);
+    CK(cudaStreamGetCaptureInfo(st, &cs, &id, &g, &deps, &nd));
+    cudaGraphNodeParams np{};
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = h;
+    np.conditional.type = cudaGraphCondTypeIf;
+    np.conditional.size = 1;
+    cudaGraphNode_t node;
+    CK(cudaGraphAddNode(&node, g, deps, nd, &np));
+    cudaGraph_t body = np.conditional.phGraph_out[0];
+    CK(cudaStreamBeginCaptureToGraph(c->side, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+    launch_rebuild(c->d, c->np_all, c->ncells_all, a, c->side);
+    CK(cudaStreamEndCapture(c->side, &body));
+    CK(cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies));
+    return SPH_OK;
+}
+
+int enqueue_one_step(sph_ctx *c, int a, int write_outputs, cudaStream_t st, bool capturing = false)
+{
+    if (capturing && c->cond_rebuild) {
+        const int rc = capture_rebuild_conditional(c, a, st);
+        if (rc != SPH_OK) return rc;
+    } else {
+        launch_rebuild(c->d, c->np_all, c->ncells_all, a, st);
+    }
     launch_bonds(c->d, c->hp.nb0, a, st);
     launch_step(c->d, c->np_all, (int)c->hp.contactmodel, a, write_outputs, st);
     launch_walls(c->d, c->np_all, c->hp.nw, st);
+    return SPH_OK;
 }
 
 int capture(sph_ctx *c, cudaGraphExec_t *out, int a, int nsteps, int write_last)
@@ -215,9 +253,23 @@ int capture(sph_ctx *c, cudaGraphExec_t *out, int a, int nsteps, int write_last)
     cudaGraph_t g = nullptr;
     CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
     int aa = a;
-    for (int i = 0; i < nsteps; ++i) {
-        enqueue_one_step(c, aa, (write_last && i == nsteps - 1) ? 1 : 0, c->stream);
+    int rc = SPH_OK;
+    for (int i = 0; i < nsteps && rc == SPH_OK; ++i) {
+        rc = enqueue_one_step(c, aa, (write_last && i == nsteps - 1) ? 1 : 0, c->stream, true);
         aa ^= 1;
+    }
+    if (rc != SPH_OK) {
+        // conditional nodes unavailable: end the broken capture and capture
+        // the plain rebuild instead
+        cudaStreamEndCapture(c->stream, &g);
+        if (g) cudaGraphDestroy(g);
+        if (c->side) cudaStreamEndCapture(c->side, &g);
+        cudaGetLastError();
+        if (!c->cond_rebuild) return rc;
+        c->cond_rebuild = false;
+        c->sticky = SPH_OK;
+        c->err.clear();
+        return capture(c, out, a, nsteps, write_last);
     }
     CK(cudaStreamEndCapture(c->stream, &g));
     cudaError_t e = cudaGraphInstantiate(out, g, 0);
@@ -399,6 +451,7 @@ int create_impl(const sph_config *cfgs, uint32_t ninst, bool batched, sph_ctx **
     c->device = cfgs[0].device;
     CK(cudaSetDevice(c->device));
     CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking));
 
     const size_t np = c->np_all;
     const size_t ncells = c->ncells_all;
@@ -1131,6 +1184,7 @@ int sph_destroy(sph_ctx *c)
     free_diff(c);
     for (void *p : c->allocs) cudaFree(p);
     if (c->stream) cudaStreamDestroy(c->stream);
+    if (c->side) cudaStreamDestroy(c->side);
     delete c;
     return SPH_OK;
 }

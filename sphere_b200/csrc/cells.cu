@@ -33,7 +33,7 @@ __global__ void k_cell_init(Dev d, int A)
     const Params &P = prm_of(d, s);
     const double4 x = d.xr[A][s];
     uint32_t c = cell_id(P, x.x, x.y, x.z);
-    if (c >= P.ncells) {
+    if (c >= P.ncells || !isfinite(x.x + x.y + x.z)) {
         atomicOr(d.status, ST_OUT_OF_GRID);
         c = d.ncells_all;
     } else {
@@ -231,6 +231,19 @@ __global__ void k_mark_dirty(Dev d)
             }
         }
     }
+}
+
+// Graph gate of the rebuild: the six rebuild kernels and the flag reset form
+// the body of a conditional graph node that runs only when the step before
+// moved a particle to another cell; this kernel sets the node's condition.
+__global__ void k_rebuild_gate(cudaGraphConditionalHandle h, const uint32_t *rebuild)
+{
+    cudaGraphSetConditional(h, *rebuild ? 1u : 0u);
+}
+
+void launch_rebuild_gate(cudaGraphConditionalHandle h, const uint32_t *rebuild, cudaStream_t st)
+{
+    k_rebuild_gate<<<1, 1, 0, st>>>(h, rebuild);
 }
 
 void launch_cell_init(const Dev &d, uint32_t np, int a, cudaStream_t st)
