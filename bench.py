@@ -380,7 +380,7 @@ def batched_leg(args, rank, world, local, barrier, max_over_ranks):
     members = [scenes.ensemble_member(i, cell_factor=cell_factor) for i in mine]
     cfgs = [config_from_spherebin(sb) for sb in members]
     states = [state_from_spherebin(sb) for sb in members]
-    stream = torch.cuda.current_stream()
+    stream = torch.cuda.Stream()   # not the default stream (handle 0)
     K = args.batch_steps
 
     # ---- batched: all members in one context, inputs resident ---------------
@@ -479,7 +479,7 @@ def adjoint_leg(args, local):
     steps, K = args.adjoint_steps, args.adjoint_checkpoint
     cfg = config_from_spherebin(sb)
     st0 = state_from_spherebin(sb)
-    stream = torch.cuda.current_stream()
+    stream = torch.cuda.Stream()   # not the default stream (handle 0)
     # the plain step (the reference's arithmetic) for scale
     plain = Simulation(cfg, device=local)
     plain.upload(st0)

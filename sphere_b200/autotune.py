@@ -39,7 +39,10 @@ def _time_batch(scenes_list, verlet_skin, graph_steps, warmup, steps, device=0):
     with BatchSimulation([config_from_spherebin(sb) for sb in scenes_list], device=device,
                          graph_steps=graph_steps, verlet_skin=verlet_skin) as sim:
         sim.upload([state_from_spherebin(sb) for sb in scenes_list])
-        cur = torch.cuda.current_stream()
+        # a stream of its own: the default stream's handle is 0, which the
+        # binding reads as "the context's stream", and events recorded on the
+        # default stream would not bracket that work
+        cur = torch.cuda.Stream()
         sim.step(warmup, stream=cur.cuda_stream)
         sim.sync()
         t0 = torch.cuda.Event(enable_timing=True)
