@@ -147,8 +147,10 @@ static int build_cells(orc_scene *s, work_t *w)
     const uint32_t np = s->np, nc = w->ncells;
     int err = 0;
     for (uint32_t i = 0; i < np; ++i) {
-        uint32_t c = cell_id(s, &s->x[4 * (size_t)i]);
-        if (c >= nc) { err |= ORC_ERR_OUT_OF_GRID; c = nc; }
+        const double *xi = &s->x[4 * (size_t)i];
+        uint32_t c = cell_id(s, xi);
+        /* a position that is not finite lies outside the grid */
+        if (c >= nc || !isfinite(xi[0] + xi[1] + xi[2])) { err |= ORC_ERR_OUT_OF_GRID; c = nc; }
         w->cellid[i] = c;
     }
     memset(w->count, 0, sizeof(uint32_t) * ((size_t)nc + 1));

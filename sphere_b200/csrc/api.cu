@@ -472,6 +472,7 @@ int create_impl(const sph_config *cfgs, uint32_t ninst, bool batched, sph_ctx **
     AL(d.scan_tiles, scan_tile_count(c->ncells_all));
     AL(d.alias_any, 1);
     AL(d.vl, np * VL_CAP); AL(d.vl_meta, np * VL_CAP); AL(d.vl_len, np); AL(d.disp, np);
+    AL(d.vl_gap, np);
     AL(d.movers, MOVER_CAP); AL(d.dirty, ncells + 1); AL(d.vs, 1);
     AL(d.wf_pp, np); AL(d.wtouch, np); AL(d.wf_partial, div_up(np, 256));
     AL(d.walls, 1);

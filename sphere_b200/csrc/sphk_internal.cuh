@@ -136,6 +136,7 @@ struct Dev {
     uint32_t *vl;         // [np][VL_CAP] candidate storage indices, in visiting order
     uint16_t *vl_meta;    // [np][VL_CAP] stencil cell (0..26) | shift code << 5
     uint8_t *vl_len;      // [np] list length or VL_NONE
+    float *vl_gap;        // [np] lower bound of the smallest gap to a listed candidate
     float *disp;          // [np] displacement bound since the epoch started
     uint2 *movers;        // [MOVER_CAP] (old cell, new cell) of the last step
     uint32_t *dirty;      // [ncells + 1] step stamp: a neighbour cell changed members

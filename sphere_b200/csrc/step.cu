@@ -347,6 +347,15 @@ __device__ __noinline__ void visc_pair(const Dev &d, int A, uint32_t s, uint32_t
     }
 }
 
+// How far particle s and any partner can have closed their gap since s's list
+// was recorded: its own displacement bound plus the largest of any particle,
+// rounded up.  While that stays below the list's smallest gap (Dev::vl_gap)
+// no listed candidate can overlap, and the list need not be tested.
+__device__ __forceinline__ float moved_bound(const Dev &d, uint32_t s, const Verlet &V)
+{
+    return __fadd_ru(d.disp[s], __uint_as_float(V.dmax_bits));
+}
+
 // k_topo: one thread per cell-list position k, particle s = cellorder[k].
 //
 // List mode: while the particle's Verlet list is valid (no epoch restart, no
@@ -400,13 +409,15 @@ k_topo(Dev d, int A)
     if (VISC && list_ok) {
         const uint32_t *vl = d.vl + (size_t)s * VL_CAP;
         const uint16_t *vm = d.vl_meta + (size_t)s * VL_CAP;
-        for (uint32_t e = 0; e < len; ++e)
+        const uint32_t n = (d.vl_gap[s] <= moved_bound(d, s, V)) ? len : 0u;
+        for (uint32_t e = 0; e < n; ++e)
             visc_pair(d, A, s, vl[e], (uint32_t)vm[e] >> 5, F1, p1);
     } else if (list_ok) {
         const uint32_t *vl = d.vl + (size_t)s * VL_CAP;
         const uint16_t *vm = d.vl_meta + (size_t)s * VL_CAP;
         int skip_slot = -1;
-        for (uint32_t e = 0; e < len; ++e) {
+        const uint32_t n = (d.vl_gap[s] <= moved_bound(d, s, V)) ? len : 0u;
+        for (uint32_t e = 0; e < n; ++e) {
             const uint32_t meta = vm[e];
             const int slot = (int)(meta & 31u);
             if (slot == skip_slot) continue;   // nc > NC: rest of that cell
@@ -425,6 +436,7 @@ k_topo(Dev d, int A)
         uint16_t *vm = d.vl_meta + (size_t)s * VL_CAP;
         uint32_t nlist = 0;
         bool list_overflow = false;
+        float gmin = 3.0e38f;   // smallest gap to a listed candidate, bounded below
 
         // A run [beg, end) of cell-list positions (one cell, or the three
         // cells of an x-row whose inner boundaries are bnd1 <= bnd2, stencil
@@ -452,7 +464,13 @@ k_topo(Dev d, int A)
                     const float rs = (rsum + skinf) * 1.000004f + eps;
                     const uint32_t k2 = base + (uint32_t)j;
                     const bool ok = k2 < end && k2 != k;
-                    if (ok && d2 < rs * rs) near |= 1u << j;
+                    if (ok && d2 < rs * rs) {
+                        near |= 1u << j;
+                        // the gap, with the cull's float slack taken against
+                        // it (over every near candidate: at least the listed)
+                        gmin = fminf(gmin, __fsub_rd(__fmul_rd(__fsqrt_rd(d2), 0.999996f),
+                                                     rr));
+                    }
                     if (ok && d2 < rr * rr) hit |= 1u << j;
                 }
                 uint32_t next = base + 4;
@@ -557,6 +575,7 @@ k_topo(Dev d, int A)
             }
         }
         d.vl_len[s] = (use_lists && !list_overflow) ? (uint8_t)nlist : VL_NONE;
+        if (use_lists) d.vl_gap[s] = gmin;
     }
 
     if (VISC) d.c1acc[s] = make_double4(F1.x, F1.y, F1.z, p1);
