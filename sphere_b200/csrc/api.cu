@@ -145,6 +145,16 @@ __global__ void k_to_user(const T *src, T *dst, const uint32_t *sidx, uint32_t n
     if (u < n) dst[u] = src[sidx[u]];
 }
 
+// a three-double row and its kept fourth lane, as the host's four-double row
+__global__ void k_p3_to_user(const P3 *src, const double *w, int lane, double4 *dst,
+                             const uint32_t *sidx, uint32_t n)
+{
+    const uint32_t u = blockIdx.x * blockDim.x + threadIdx.x;
+    if (u >= n) return;
+    const P3 v = src[sidx[u]];
+    dst[u] = make_double4(v.x, v.y, v.z, w[3 * (size_t)u + lane]);
+}
+
 __global__ void k_rows_to_user(Dev d, uint32_t *contacts, double4 *distmod, double4 *delta_t,
                                int A)
 {
@@ -465,6 +475,7 @@ int create_impl(const sph_config *cfgs, uint32_t ninst, bool batched, sph_ctx **
         AL(d.xr[b], np); AL(d.vel[b], np); AL(d.angvel[b], np); AL(d.xs[b], np);
     }
     AL(d.vel0, np); AL(d.angvel0, np); AL(d.angpos, np); AL(d.xysum, np); AL(d.esv, np);
+    AL(d.w_user, 3 * np);
     AL(d.force, np); AL(d.torque, np); AL(d.acc, np); AL(d.angacc, np); AL(d.edp, np);
     AL(d.uid, np); AL(d.sidx, np); AL(d.cell, np);
     AL(d.contacts, np * NC); AL(d.dmc, np); AL(d.delta_t, np * NC); AL(d.cmask, np);
@@ -572,6 +583,12 @@ int sph_upload(sph_ctx *c, const sph_host_state *h)
             rmax_all = std::fmax(rmax_all, rmax);
         }
         for (auto &Q : c->hps) Q.skin = c->skin_rel * rmax_all;
+        // a zero energy rate may skip the es/ev update only if no sum is -0.0
+        bool negzero = false;
+        for (size_t i = 0; i < np && !negzero; ++i)
+            negzero = (h->es[i] == 0.0 && std::signbit(h->es[i])) ||
+                      (h->ev[i] == 0.0 && std::signbit(h->ev[i]));
+        for (auto &Q : c->hps) Q.esv_skip = negzero ? 0u : 1u;
         c->hp = c->hps[0];
         CK(cudaMemcpy(d.prm, c->hps.data(), sizeof(Params) * c->ninst, cudaMemcpyHostToDevice));
         Verlet V{};
@@ -582,10 +599,23 @@ int sph_upload(sph_ctx *c, const sph_host_state *h)
         CK(cudaMemset(d.vl_len, VL_NONE, np));
     }
     CK(cudaMemcpy(d.vel[A], h->vel, np * 32, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(d.vel0, h->vel0 ? h->vel0 : h->vel, np * 32, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(d.angvel[A], h->angvel, np * 32, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(d.angvel0, h->angvel0 ? h->angvel0 : h->angvel, np * 32, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(d.angpos, h->angpos, np * 32, cudaMemcpyHostToDevice));
+    {
+        // vel0, angvel0, angpos: three doubles on the device, the fourth lane
+        // kept by caller index for the download
+        std::vector<double> p3(np * 3), w(np * 3);
+        const double *src[3] = {h->vel0 ? h->vel0 : h->vel, h->angvel0 ? h->angvel0 : h->angvel,
+                                h->angpos};
+        P3 *dst[3] = {d.vel0, d.angvel0, d.angpos};
+        for (int f = 0; f < 3; ++f) {
+            for (size_t i = 0; i < np; ++i) {
+                for (int k = 0; k < 3; ++k) p3[3 * i + k] = src[f][4 * i + k];
+                w[3 * i + f] = src[f][4 * i + 3];
+            }
+            CK(cudaMemcpy(dst[f], p3.data(), np * 24, cudaMemcpyHostToDevice));
+        }
+        CK(cudaMemcpy(d.w_user, w.data(), np * 24, cudaMemcpyHostToDevice));
+    }
     CK(cudaMemcpy(d.force, h->force, np * 32, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(d.torque, h->torque, np * 32, cudaMemcpyHostToDevice));
     if (h->acc) {
@@ -828,9 +858,16 @@ int sph_download(sph_ctx *c, sph_host_state *h)
         return SPH_OK;
     };
     int rc;
-    if ((rc = get4(d.xr[A], h->x)) || (rc = get4(d.vel[A], h->vel)) || (rc = get4(d.vel0, h->vel0)) ||
-        (rc = get4(d.acc, h->acc)) || (rc = get4(d.force, h->force)) || (rc = get4(d.angpos, h->angpos)) ||
-        (rc = get4(d.angvel[A], h->angvel)) || (rc = get4(d.angvel0, h->angvel0)) ||
+    auto get3 = [&](const P3 *src, int lane, double *dst) -> int {
+        if (!dst) return SPH_OK;
+        k_p3_to_user<<<grid, 256, 0, c->stream>>>(src, d.w_user, lane, t4, d.sidx, np);
+        CK(cudaMemcpyAsync(dst, t4, (size_t)np * 32, cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        return SPH_OK;
+    };
+    if ((rc = get4(d.xr[A], h->x)) || (rc = get4(d.vel[A], h->vel)) || (rc = get3(d.vel0, 0, h->vel0)) ||
+        (rc = get4(d.acc, h->acc)) || (rc = get4(d.force, h->force)) || (rc = get3(d.angpos, 2, h->angpos)) ||
+        (rc = get4(d.angvel[A], h->angvel)) || (rc = get3(d.angvel0, 1, h->angvel0)) ||
         (rc = get4(d.angacc, h->angacc)) || (rc = get4(d.torque, h->torque)))
         return rc;
     {
@@ -985,7 +1022,7 @@ static std::vector<std::pair<void *, size_t>> ckpt_fields(sph_ctx *c, int a)
     Dev &d = c->d;
     const size_t np = c->np_all;
     return {{d.xr[a], np * 32},       {d.vel[a], np * 32},  {d.angvel[a], np * 32},
-            {d.vel0, np * 32},        {d.angvel0, np * 32}, {d.angpos, np * 32},
+            {d.vel0, np * 24},        {d.angvel0, np * 24}, {d.angpos, np * 24},
             {d.xysum, np * 16},       {d.esv, np * 16},     {d.contacts, np * NC * 4},
             {d.dmc, np * 16},         {d.cmask, np * 4},    {d.delta_t, np * NC * 32}};
 }

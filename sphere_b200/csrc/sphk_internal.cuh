@@ -65,6 +65,7 @@ struct Params {
     double prune_pad;   // absolute slack of the cell-level distance test (metres)
     double skin;        // Verlet-list skin (metres); 0 disables the lists
     double reach_extra; // model 1: db, the capillary reach beyond contact (metres)
+    uint32_t esv_skip;  // no es/ev is -0.0: adding a zero rate may be skipped exactly
     uint32_t cell_base; // batched contexts: first global cell id of this instance
     uint32_t uid_base;  // batched contexts: first global particle index of this instance
 };
@@ -95,6 +96,11 @@ struct Walls {
     uint32_t pad;
 };
 
+// Three doubles (24 bytes): rows whose fourth lane a step never reads.
+struct P3 {
+    double x, y, z;
+};
+
 // Device pointers of one simulation.  Per-particle arrays are indexed by the
 // storage index s (particles are kept in cell order); uid[s] is the caller's
 // particle index and sidx[uid] its inverse.  Contact rows store partners as
@@ -111,8 +117,11 @@ struct Dev {
     double4 *vel[2];      // vx, vy, vz, fixvel
     double4 *angvel[2];   // wx, wy, wz, (w lane carried)
     float4 *xs[2];        // float copy of xr in cell-list order, for the neighbour cull
-    // private per-particle state (updated in place)
-    double4 *vel0, *angvel0, *angpos;
+    // private per-particle state (updated in place); three doubles each, the
+    // fourth lane of the host rows (never changed by a step) is kept apart in
+    // w_user
+    P3 *vel0, *angvel0, *angpos;
+    double *w_user;       // [np][3] fourth lanes of vel0, angvel0, angpos, by caller index
     double2 *xysum;
     double2 *esv;         // es, ev
     // per-step outputs

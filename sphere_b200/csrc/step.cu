@@ -784,7 +784,9 @@ k_force(ForceArgs args)
     }
 
     const double dt = P.dt;
-    {
+    // es += es_dot dt, ev += ev_dot dt; a zero rate adds +0.0, which leaves
+    // the sums unchanged unless one is -0.0 (esv_skip clear)
+    if (es_dot != 0.0 || ev_dot != 0.0 || !P.esv_skip) {
         const double2 e = d.esv[s];
         d.esv[s] = make_double2(e.x + es_dot * dt, e.y + ev_dot * dt);
     }
@@ -798,7 +800,7 @@ k_force(ForceArgs args)
 
     // ---- integrate, src/integration.cuh:9-187 -------------------------------
     double4 x = xa, vel = vel_a, angvel = angvel_a4;
-    double4 angpos = d.angpos[s], vel0 = d.vel0[s], angvel0 = d.angvel0[s];
+    P3 angpos = d.angpos[s], vel0 = d.vel0[s], angvel0 = d.angvel0[s];
     const double radius = x.w;
     const double m = 4.0 / 3.0 * REF_PI * radius * radius * radius * P.rho;
     double4 acc, angacc;
