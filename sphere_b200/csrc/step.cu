@@ -29,6 +29,14 @@ namespace sphk {
 
 constexpr int TOPO_BLOCK = 128;
 constexpr int FORCE_BLOCK = 128;
+// Resident blocks per SM that the register allocation must allow (the
+// __launch_bounds__ minimum), from a sweep of caps at 1M spheres.
+#ifndef SPHK_TOPO_MIN_BLOCKS
+#define SPHK_TOPO_MIN_BLOCKS 8
+#endif
+#ifndef SPHK_FORCE_MIN_BLOCKS
+#define SPHK_FORCE_MIN_BLOCKS 6
+#endif
 
 // contactLinear_wall, src/contactmodels.cuh:10-109.  Out of line: six call
 // sites, taken only by particles touching a wall.
@@ -356,7 +364,8 @@ __device__ __forceinline__ float moved_bound(const Dev &d, uint32_t s, const Ver
     return __fadd_ru(d.disp[s], __uint_as_float(V.dmax_bits));
 }
 
-// k_topo: one thread per cell-list position k, particle s = cellorder[k].
+// k_topo: one thread per particle s (storage order, which relayout keeps close
+// to cell order); its cell-list position k = pos[s] locates it in the runs.
 //
 // List mode: while the particle's Verlet list is valid (no epoch restart, no
 // cell of its neighbourhood changed members this step) only the listed
@@ -372,20 +381,19 @@ __device__ __forceinline__ float moved_bound(const Dev &d, uint32_t s, const Ver
 // processed in visiting order and the contact force and pressure sums are
 // left in Dev::c1acc for k_force.
 template <bool VISC, bool BATCH>
-__global__ void __launch_bounds__(TOPO_BLOCK, 8)
+__global__ void __launch_bounds__(TOPO_BLOCK, SPHK_TOPO_MIN_BLOCKS)
 k_topo(Dev d, int A)
 {
     __shared__ uint32_t srow[NC * TOPO_BLOCK];
     const uint32_t np = d.np_all;
     const int tid = threadIdx.x;
-    const uint32_t k = blockIdx.x * TOPO_BLOCK + tid;
-    if (k == 0) {
+    const uint32_t s = blockIdx.x * TOPO_BLOCK + tid;
+    if (s == 0) {
         // the movers of the last step have been consumed by the rebuild
         d.vs->nmovers = 0u;
         d.vs->movers_overflow = 0u;
     }
-    if (k >= np) return;
-    const uint32_t s = d.cellorder[k];
+    if (s >= np) return;
     const Params &P = prm_at<BATCH>(d, s);
     const double4 xa = d.xr[A][s];
     const double ra = xa.w;
@@ -427,6 +435,7 @@ k_topo(Dev d, int A)
         }
     } else {
         const float4 *__restrict__ xs = d.xs[A];
+        const uint32_t k = d.pos[s];
         const float4 xaf = xs[k];
         const float Lf0 = (float)P.L[0], Lf1 = (float)P.L[1];
         const float eps = P.cull_eps;
@@ -611,7 +620,7 @@ struct ForceArgs {
 // row args.tape_step when it is >= 0.  Energy rates and pressure are not
 // computed in this variant.
 template <int MODEL, bool BATCH, bool DIFF>
-__global__ void __launch_bounds__(FORCE_BLOCK, 6)
+__global__ void __launch_bounds__(FORCE_BLOCK, SPHK_FORCE_MIN_BLOCKS)
 k_force(ForceArgs args)
 {
     const Dev &d = args.d;
@@ -760,10 +769,10 @@ k_force(ForceArgs args)
         }
     }
 
-    const uint32_t u = d.uid[s];
     // ---- bonds: per-bond contributions in bond order (bondsLinear's serial
     // scatter order, cohesion.cuh:220-226) ------------------------------------
     if (P.nb0 > 0) {
+        const uint32_t u = d.uid[s];
         const uint32_t e0 = d.bond_ptr[u], e1 = d.bond_ptr[u + 1];
         for (uint32_t e = e0; e < e1; ++e) {
             const uint32_t ent = d.bond_list[e];
@@ -793,7 +802,7 @@ k_force(ForceArgs args)
     if (P.nw > 0) {
         const uint8_t touched = d.wtouch[s];
         if (w0f != 0.0 || touched) {
-            d.wf_pp[u] = w0f;
+            d.wf_pp[d.uid[s]] = w0f;
             d.wtouch[s] = (w0f != 0.0) ? 1 : 0;
         }
     }
