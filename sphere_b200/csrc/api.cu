@@ -477,7 +477,7 @@ int create_impl(const sph_config *cfgs, uint32_t ninst, bool batched, sph_ctx **
     AL(d.vel0, np); AL(d.angvel0, np); AL(d.angpos, np); AL(d.xysum, np); AL(d.esv, np);
     AL(d.w_user, 3 * np);
     AL(d.force, np); AL(d.torque, np); AL(d.acc, np); AL(d.angacc, np); AL(d.edp, np);
-    AL(d.uid, np); AL(d.sidx, np); AL(d.cell, np);
+    AL(d.uid, np); AL(d.sidx, np); AL(d.cell, np); AL(d.outside, np);
     AL(d.contacts, np * NC); AL(d.dmc, np); AL(d.delta_t, np * NC); AL(d.cmask, np);
     AL(d.cell_start, ncells + 2); AL(d.cellorder, np); AL(d.pos, np); AL(d.cell_fill, ncells + 1);
     AL(d.scan_tiles, scan_tile_count(c->ncells_all));

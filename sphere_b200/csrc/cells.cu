@@ -32,6 +32,7 @@ __global__ void k_cell_init(Dev d, int A)
     if (s >= d.np_all) return;
     const Params &P = prm_of(d, s);
     const double4 x = d.xr[A][s];
+    d.outside[s] = cell_outside(P, x.x, x.y, x.z) ? 1 : 0;
     uint32_t c = cell_id(P, x.x, x.y, x.z);
     if (c >= P.ncells || !isfinite(x.x + x.y + x.z)) {
         atomicOr(d.status, ST_OUT_OF_GRID);
@@ -227,6 +228,7 @@ __global__ void k_mark_dirty(Dev d)
                         x = (x + (int32_t)nx) % (int32_t)nx;
                     }
                     d.dirty[P.cell_base + (uint32_t)x + (uint32_t)y * nx + (nx * ny) * (uint32_t)z] = V.step;
+                    V.dirty_step = V.step;
                 }
             }
         }
@@ -353,6 +355,7 @@ void relayout(const Dev &d, uint32_t np, int a, void *scratch, cudaStream_t st)
     gather_back(d.edp, scratch, order, np, st);
     gather_back(d.uid, scratch, order, np, st);
     gather_back(d.cell, scratch, order, np, st);
+    gather_back(d.outside, scratch, order, np, st);
     gather_back(d.cmask, scratch, order, np, st);
     gather_back(d.dmc, scratch, order, np, st);
     gather_back(d.wtouch, scratch, order, np, st);

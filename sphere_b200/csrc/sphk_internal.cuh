@@ -83,7 +83,8 @@ struct Verlet {
     uint32_t dmax_bits;     // float bits of the displacement bound (atomicMax)
     uint32_t nmovers;       // particles that changed cell in the last step
     uint32_t movers_overflow;
-    uint32_t pad[3];
+    uint32_t dirty_step;    // the last step in which any cell was stamped dirty
+    uint32_t pad[2];
 };
 
 // Wall state (src/datatypes.h:95-100), device resident.
@@ -129,6 +130,7 @@ struct Dev {
     double4 *edp;         // es_dot, ev_dot, p, 0
     uint32_t *uid, *sidx;
     uint32_t *cell;       // cell id (calcCellID semantics) of the current positions
+    uint8_t *outside;     // the position's floored cell coordinates leave the grid
     // contacts
     uint32_t *contacts;   // [np][NC]
     ulonglong2 *dmc;      // [np] 4-bit periodic shift code of each of the NC slots
@@ -219,6 +221,16 @@ __device__ __forceinline__ uint32_t cell_id(const Params &P, double x, double y,
     uint32_t iy = __double2uint_rz(cell_floor(P, 1, y));
     uint32_t iz = __double2uint_rz(cell_floor(P, 2, z));
     return (iz * P.num[1]) * P.num[0] + iy * P.num[0] + ix;
+}
+
+// Whether some floored cell coordinate of the position lies outside
+// [0, num): the particle is not inside its own cell's box (contact search
+// takes the reference's stencil from the floored coordinates, not the id).
+__device__ __forceinline__ bool cell_outside(const Params &P, double x, double y, double z)
+{
+    const double f0 = cell_floor(P, 0, x), f1 = cell_floor(P, 1, y), f2 = cell_floor(P, 2, z);
+    return !(f0 >= 0.0 && f0 < (double)P.num[0] && f1 >= 0.0 && f1 < (double)P.num[1] &&
+             f2 >= 0.0 && f2 < (double)P.num[2]);
 }
 
 inline unsigned int div_up(unsigned long long a, unsigned int b)

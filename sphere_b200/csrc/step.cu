@@ -32,7 +32,7 @@ constexpr int FORCE_BLOCK = 128;
 // Resident blocks per SM that the register allocation must allow (the
 // __launch_bounds__ minimum), from a sweep of caps at 1M spheres.
 #ifndef SPHK_TOPO_MIN_BLOCKS
-#define SPHK_TOPO_MIN_BLOCKS 8
+#define SPHK_TOPO_MIN_BLOCKS 10
 #endif
 #ifndef SPHK_FORCE_MIN_BLOCKS
 #define SPHK_FORCE_MIN_BLOCKS 6
@@ -395,11 +395,20 @@ k_topo(Dev d, int A)
     }
     if (s >= np) return;
     const Params &P = prm_at<BATCH>(d, s);
+    const Verlet &V = *d.vs;
+    // The list decision first, from a few bytes: a valid list whose gap
+    // bound rules out every contact ends the particle's work here.
+    const uint8_t len = d.vl_len[s];
+    bool list_ok = P.skin > 0.0 && !V.all_rebuild && len != VL_NONE && d.outside[s] == 0;
+    if (list_ok && V.dirty_step == V.step) list_ok = d.dirty[d.cell[s]] != V.step;
+    if (list_ok && d.vl_gap[s] > moved_bound(d, s, V)) {
+        if (VISC) d.c1acc[s] = make_double4(0.0, 0.0, 0.0, 0.0);
+        return;
+    }
     const double4 xa = d.xr[A][s];
     const double ra = xa.w;
     const double4 *__restrict__ xr = d.xr[A];
     TopoSlots ts{d.cmask[s], 0u, 0ull, 0ull, 0, false, false};
-    const Verlet &V = *d.vs;
     const uint32_t nx = P.num[0], ny = P.num[1], nz = P.num[2];
     int32_t gp[3];
     gp[0] = __double2int_rz(cell_floor(P, 0, xa.x));
@@ -408,24 +417,19 @@ k_topo(Dev d, int A)
     const bool gp_in = gp[0] >= 0 && (uint32_t)gp[0] < nx && gp[1] >= 0 && (uint32_t)gp[1] < ny &&
                        gp[2] >= 0 && (uint32_t)gp[2] < nz;
     const bool use_lists = P.skin > 0.0 && gp_in;
-    const uint8_t len = d.vl_len[s];
-    const bool list_ok = use_lists && !V.all_rebuild && len != VL_NONE &&
-                         d.dirty[d.cell[s]] != V.step;
     d3 F1 = mk(0.0, 0.0, 0.0);   // model 1 sums
     double p1 = 0.0f;
 
     if (VISC && list_ok) {
         const uint32_t *vl = d.vl + (size_t)s * VL_CAP;
         const uint16_t *vm = d.vl_meta + (size_t)s * VL_CAP;
-        const uint32_t n = (d.vl_gap[s] <= moved_bound(d, s, V)) ? len : 0u;
-        for (uint32_t e = 0; e < n; ++e)
+        for (uint32_t e = 0; e < len; ++e)
             visc_pair(d, A, s, vl[e], (uint32_t)vm[e] >> 5, F1, p1);
     } else if (list_ok) {
         const uint32_t *vl = d.vl + (size_t)s * VL_CAP;
         const uint16_t *vm = d.vl_meta + (size_t)s * VL_CAP;
         int skip_slot = -1;
-        const uint32_t n = (d.vl_gap[s] <= moved_bound(d, s, V)) ? len : 0u;
-        for (uint32_t e = 0; e < n; ++e) {
+        for (uint32_t e = 0; e < len; ++e) {
             const uint32_t meta = vm[e];
             const int slot = (int)(meta & 31u);
             if (slot == skip_slot) continue;   // nc > NC: rest of that cell
@@ -898,6 +902,7 @@ k_force(ForceArgs args)
     uint32_t c = cell_id(P, x.x, x.y, x.z);
     if (c >= P.ncells || !isfinite(x.x + x.y + x.z)) { err |= ST_OUT_OF_GRID; c = d.ncells_all; }
     else c += P.cell_base;
+    d.outside[s] = cell_outside(P, x.x, x.y, x.z) ? 1 : 0;
     const uint32_t c_old = d.cell[s];
     if (c != c_old) {
         d.cell[s] = c;
