@@ -242,6 +242,7 @@ def gpu_arm(args, rank, world, local):
 
     # ---- device-resident throughput: exactly K steps between events -------
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    rebuilds0 = sim.stats()["cell_rebuilds"]
     barrier()
     with ClockSampler(local) as clocks:
         start.record(stream)
@@ -306,7 +307,11 @@ def gpu_arm(args, rank, world, local):
     b_step, b_whole = algorithmic_bytes(cfg.np, cfg.ncells, C, cfg.nb0)
     peak, peak_kind = measured_peak_hbm()
     achieved = b_step / (step_ms * 1e-3) / 1e9
-    kernels_per_step = 6 + (1 if cfg.nb0 else 0) + 2 + (1 if cfg.nw else 0)
+    # per step: the rebuild gate, k_bonds (with bonds), k_topo, k_force and
+    # the wall kernel (k_walls, or k_tail without walls); the 7 cell-list
+    # kernels only in steps whose cell list changed (a conditional graph node)
+    rebuilt = stats["cell_rebuilds"] - rebuilds0
+    launches = args.steps * (4 + (1 if cfg.nb0 else 0)) + 7 * rebuilt
     out = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
@@ -318,7 +323,7 @@ def gpu_arm(args, rank, world, local):
         "e2e": {"value": e2e_value, "unit": UNIT,
                 "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
                 "seconds": e2e_s},
-        "gpu_launches": kernels_per_step * args.steps,
+        "gpu_launches": launches, "cell_rebuilds_timed": rebuilt,
         "roofline": {"bound": "hbm", "kernel": "k_topo+k_force", "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
                      "traffic": ncu_traffic(cfg.np),

@@ -34,7 +34,7 @@
 extern "C" {
 #endif
 
-#define SPHK_VERSION 1
+#define SPHK_VERSION 2
 #define SPHK_NC 32        /* contact slots per particle (src/constants.h:24) */
 #define SPHK_MAXWALLS 6   /* src/constants.h:11 */
 
@@ -100,6 +100,7 @@ typedef struct sph_stats {
     uint64_t steps;             /* steps taken since upload */
     uint64_t relayouts;         /* storage re-orderings performed */
     uint64_t device_bytes;      /* device memory held by the context */
+    uint64_t cell_rebuilds;     /* steps whose cell list was rebuilt (a particle changed cell) */
 } sph_stats;
 
 /* Options for sph_set_option. */

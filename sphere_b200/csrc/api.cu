@@ -984,6 +984,11 @@ int sph_get_stats(sph_ctx *c, sph_stats *out)
         CK(cudaStreamSynchronize(c->stream));
         out->active_contacts = v;
     }
+    if (c->uploaded) {
+        Verlet V{};
+        CK(cudaMemcpy(&V, c->d.vs, sizeof(V), cudaMemcpyDeviceToHost));
+        out->cell_rebuilds = V.rebuilds;
+    }
     out->steps = c->steps;
     out->relayouts = c->relayouts;
     out->device_bytes = c->device_bytes + c->diff_bytes;

@@ -190,6 +190,7 @@ __global__ void k_mark_dirty(Dev d)
     if (*d.rebuild == 0u) return;
     Verlet &V = *d.vs;
     const uint32_t n = min(V.nmovers, MOVER_CAP);
+    if (blockIdx.x == 0 && threadIdx.x == 0) V.rebuilds += 1u;
     if (blockIdx.x == 0 && threadIdx.x == 0 && V.movers_overflow) {
         V.all_rebuild = 1u;
         V.dmax_bits = 0u;

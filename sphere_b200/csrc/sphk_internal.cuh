@@ -84,7 +84,8 @@ struct Verlet {
     uint32_t nmovers;       // particles that changed cell in the last step
     uint32_t movers_overflow;
     uint32_t dirty_step;    // the last step in which any cell was stamped dirty
-    uint32_t pad[2];
+    uint32_t rebuilds;      // cell-list rebuilds performed since upload
+    uint32_t pad;
 };
 
 // Wall state (src/datatypes.h:95-100), device resident.

@@ -65,7 +65,8 @@ class SphHostState(C.Structure):
 
 class SphStats(C.Structure):
     _fields_ = [("active_contacts", C.c_uint64), ("steps", C.c_uint64),
-                ("relayouts", C.c_uint64), ("device_bytes", C.c_uint64)]
+                ("relayouts", C.c_uint64), ("device_bytes", C.c_uint64),
+                ("cell_rebuilds", C.c_uint64)]
 
 
 class SphError(RuntimeError):
