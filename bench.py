@@ -162,7 +162,7 @@ def measured_peak_hbm():
 def ncu_traffic(np_):
     """DRAM bytes per launch of the step kernel from the committed ncu summary
     (profiles/), scaled to this particle count; None when absent."""
-    p = ROOT / "profiles" / "k_step_polydisperse.md"
+    p = ROOT / "profiles" / "k_force_polydisperse_1m_dram.md"
     if not p.exists():
         return None
     for ln in p.read_text().splitlines():

@@ -103,15 +103,17 @@ k_rev_contacts(Dev d, AdjDev a, int j)
             knb += kb;
         }
 
-        // contact slots the law was evaluated on
+        // contact slots the law was evaluated on; a slot outside them starts
+        // the step with constant (zero) history, so its adjoint is cleared
+        // -- only where an earlier (later-in-time) step left one
         const uint32_t mask = d.tp_mask[row];
         const ulonglong2 dmw = d.tp_dmc[row];
         double4 *dtb = a.dtb + (size_t)s * NC;
-        for (int i = 0; i < NC; ++i) {
-            if (!((mask >> i) & 1u)) {
-                dtb[i] = make_double4(0.0, 0.0, 0.0, 0.0);
-                continue;
-            }
+        for (uint32_t m = a.dtb_mask[s] & ~mask; m; m &= m - 1)
+            dtb[__ffs(m) - 1] = make_double4(0.0, 0.0, 0.0, 0.0);
+        if (a.dtb_mask[s] != mask) a.dtb_mask[s] = mask;
+        for (uint32_t m = mask; m; m &= m - 1) {
+            const int i = __ffs(m) - 1;
             const uint32_t t = d.tp_partner[row * NC + i];
             const size_t rt = (size_t)j * np + t;
             const double4 xb = d.tp_x[rt];
@@ -144,9 +146,11 @@ k_rev_contacts(Dev d, AdjDev a, int j)
             atomicAdd(&a.mub[s], 0.5 * lb.mu);
             atomicAdd(&a.mub[t], 0.5 * lb.mu);
         }
-        atomic_add3(&a.xb[s], xbs);
-        atomic_add3(&a.vb[s], vbs);
-        atomic_add3(&a.wb[s], wbs);
+        if (mask != 0u || wh.count > 0) {   // nothing to add otherwise
+            atomic_add3(&a.xb[s], xbs);
+            atomic_add3(&a.vb[s], vbs);
+            atomic_add3(&a.wb[s], wbs);
+        }
     }
     // parameter adjoints: warp sums, one atomic per warp
 #pragma unroll

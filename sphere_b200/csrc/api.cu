@@ -8,6 +8,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <map>
 #include <vector>
 
 namespace sphk {
@@ -81,6 +82,9 @@ struct sph_ctx {
     std::vector<void *> diff_allocs;
     size_t diff_bytes = 0;
     AdjDev adj{};
+    // graphs of one segment's re-run with the tape and of its reverse, by
+    // (segment length, starting buffer)
+    std::map<std::pair<int, int>, cudaGraphExec_t> diff_graphs;
 };
 
 namespace {
@@ -1072,8 +1076,45 @@ static int restore_ckpt(sph_ctx *c, const sph_ctx::Ckpt &k)
     return SPH_OK;
 }
 
+// One segment of the backward pass as a graph: the `len` steps re-run from
+// the restored checkpoint (buffer a) recording tape rows 0 .. len-1, then the
+// reverse of each step, last first.
+static int capture_segment(sph_ctx *c, int len, int a, cudaGraphExec_t *out)
+{
+    Dev &d = c->d;
+    const uint32_t np = c->np_all;
+    cudaStream_t st = c->stream;
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    int rc = SPH_OK;
+    int aa = a;
+    for (int j = 0; j < len && rc == SPH_OK; ++j) {
+        if (c->cond_rebuild) rc = capture_rebuild_conditional(c, aa, st);
+        else launch_rebuild(d, np, c->ncells_all, aa, st);
+        launch_topo(d, np, false, aa, st);
+        launch_force_tape(d, np, aa, j, st);
+        launch_walls(d, np, 0, st);
+        aa ^= 1;
+    }
+    for (int j = len - 1; j >= 0 && rc == SPH_OK; --j) launch_rev_step(d, c->adj, np, j, st);
+    cudaError_t e = cudaStreamEndCapture(st, &g);
+    if (rc != SPH_OK) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+    }
+    if (e != cudaSuccess) return fail(c, SPH_ERR_CUDA, std::string("segment capture: ") + cudaGetErrorString(e));
+    e = cudaGraphInstantiate(out, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess)
+        return fail(c, SPH_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+    return SPH_OK;
+}
+
 static void free_diff(sph_ctx *c)
 {
+    for (auto &kv : c->diff_graphs)
+        if (kv.second) cudaGraphExecDestroy(kv.second);
+    c->diff_graphs.clear();
     for (void *p : c->diff_allocs) cudaFree(p);
     c->diff_allocs.clear();
     c->diff_bytes = 0;
@@ -1110,6 +1151,7 @@ int sph_diff_begin(sph_ctx *c, const double *mu, uint32_t checkpoint_every)
     ALD(d.tp_partner, K * np * NC); ALD(d.tp_dt0, K * np * NC);
     ALD(A.xb, np); ALD(A.vb, np); ALD(A.wb, np); ALD(A.v0b, np); ALD(A.w0b, np);
     ALD(A.Fb, np); ALD(A.Tb, np); ALD(A.dtb, np * NC); ALD(A.mub, np); ALD(A.theta_b, 3);
+    ALD(A.dtb_mask, np);
     double *tmp = nullptr;
     ALD(tmp, np);
 #undef ALD
@@ -1157,6 +1199,7 @@ int sph_diff_backward(sph_ctx *c, const double *x_bar, const double *v_bar, doub
     }
     for (double4 *p : {A.wb, A.v0b, A.w0b}) CK(cudaMemsetAsync(p, 0, (size_t)np * 32, st));
     CK(cudaMemsetAsync(A.dtb, 0, (size_t)np * NC * 32, st));
+    CK(cudaMemsetAsync(A.dtb_mask, 0, (size_t)np * 4, st));
     CK(cudaMemsetAsync(A.mub, 0, (size_t)np * 8, st));
     CK(cudaMemsetAsync(A.theta_b, 0, 24, st));
     const uint64_t nseg = (N + K - 1) / K;
@@ -1164,16 +1207,9 @@ int sph_diff_backward(sph_ctx *c, const double *x_bar, const double *v_bar, doub
         // adjoints survive the restore: they live apart from the state
         if ((rc = restore_ckpt(c, c->ckpts[seg])) != SPH_OK) return rc;
         const int len = (int)std::min<uint64_t>(K, N - seg * K);
-        int aa = c->a;
-        for (int j = 0; j < len; ++j) {
-            launch_rebuild(d, np, c->ncells_all, aa, st);
-            launch_topo(d, np, false, aa, st);
-            launch_force_tape(d, np, aa, j, st);
-            launch_walls(d, np, 0, st);
-            aa ^= 1;
-        }
-        for (int j = len - 1; j >= 0; --j) launch_rev_step(d, A, np, j, st);
-        CK(cudaGetLastError());
+        cudaGraphExec_t &gx = c->diff_graphs[{len, c->a}];
+        if (!gx && (rc = capture_segment(c, len, c->a, &gx)) != SPH_OK) return rc;
+        CK(cudaGraphLaunch(gx, st));
         CK(cudaStreamSynchronize(st));
     }
     if ((rc = restore_ckpt(c, fin)) != SPH_OK) return rc;

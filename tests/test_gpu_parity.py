@@ -271,3 +271,40 @@ def test_sparse_scene_forms_contacts_exactly(oracle_libs, periodic):
     got, _, stats = run_gpu(sb, (120, 180))
     assert mismatches(got, want, ALL) == []
     assert stats["active_contacts"] > 0
+
+
+def test_bonded_tension_breaks_bonds_exactly(oracle_libs):
+    """The bonded-tension workload at small size: both ends pulled apart
+    (fixvel) at 2 m/s with finite bond strengths, so bonds stretch and break
+    (marker nb0, nb0 >= np); bit for bit over 500 steps, bond history and
+    breaks included."""
+    sb = scenes.bonded(nx=5, ny=3, nz=3, sigma_b=2e3, tau_b=2e3, pull=2.0)
+    assert sb.nb0 >= sb.np
+    rc, want, _ = run_oracle(oracle_libs["orc"], sb, 500)
+    assert rc == 0
+    got, _, _ = run_gpu(sb, (200, 300))
+    assert mismatches(got, want, ALL + BOND_FIELDS) == []
+    broken = int((got.bonds[:, 0] == sb.nb0).sum())
+    assert 0 < broken < sb.nb0
+
+
+def _ensemble_stats(sb, st):
+    m = 4.0 / 3.0 * np.pi * st.x[:, 3] ** 3 * sb.rho
+    ke = float(np.sum(0.5 * m * np.sum(st.vel[:, :3] ** 2, axis=1)))
+    v_solid = float(np.sum(4.0 / 3.0 * np.pi * st.x[:, 3] ** 3))
+    phi = v_solid / float(np.prod(sb.L))
+    coordination = float((st.contacts != sb.np).sum()) / sb.np
+    return dict(kinetic=ke, packing_fraction=phi, coordination=coordination,
+                shear_energy=float(st.es.sum()), viscous_energy=float(st.ev.sum()))
+
+
+def test_ensemble_statistics_after_ten_thousand_steps(oracle_libs):
+    """10^4 steps of a colliding scene: the trajectories stay bit-identical,
+    so packing fraction, coordination number and energies agree exactly."""
+    sb = scenes.collision(n=600, seed=77, periodic=0)
+    rc, want, _ = run_oracle(oracle_libs["orc"], sb, 10_000)
+    assert rc == 0
+    got, _, _ = run_gpu(sb, (3000, 7000))
+    assert mismatches(got, want, ALL) == []
+    assert _ensemble_stats(sb, got) == _ensemble_stats(sb, want)
+    assert _ensemble_stats(sb, got)["viscous_energy"] > 0.0
