@@ -156,7 +156,7 @@ __global__ void k_p3_to_user(const P3 *src, const double *w, int lane, double4 *
     const uint32_t u = blockIdx.x * blockDim.x + threadIdx.x;
     if (u >= n) return;
     const P3 v = src[sidx[u]];
-    dst[u] = make_double4(v.x, v.y, v.z, w[3 * (size_t)u + lane]);
+    dst[u] = make_double4(v.x, v.y, v.z, w[WLANES * (size_t)u + lane]);
 }
 
 __global__ void k_rows_to_user(Dev d, uint32_t *contacts, double4 *distmod, double4 *delta_t,
@@ -479,7 +479,7 @@ int create_impl(const sph_config *cfgs, uint32_t ninst, bool batched, sph_ctx **
         AL(d.xr[b], np); AL(d.vel[b], np); AL(d.angvel[b], np); AL(d.xs[b], np);
     }
     AL(d.vel0, np); AL(d.angvel0, np); AL(d.angpos, np); AL(d.xysum, np); AL(d.esv, np);
-    AL(d.w_user, 3 * np);
+    AL(d.w_user, WLANES * np); AL(d.fixed, np);
     AL(d.force, np); AL(d.torque, np); AL(d.acc, np); AL(d.angacc, np); AL(d.edp, np);
     AL(d.uid, np); AL(d.sidx, np); AL(d.cell, np); AL(d.outside, np);
     AL(d.contacts, np * NC); AL(d.dmc, np); AL(d.delta_t, np * NC); AL(d.cmask, np);
@@ -602,23 +602,34 @@ int sph_upload(sph_ctx *c, const sph_host_state *h)
         CK(cudaMemset(d.dirty, 0, ((size_t)c->ncells_all + 1) * sizeof(uint32_t)));
         CK(cudaMemset(d.vl_len, VL_NONE, np));
     }
-    CK(cudaMemcpy(d.vel[A], h->vel, np * 32, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(d.angvel[A], h->angvel, np * 32, cudaMemcpyHostToDevice));
     {
-        // vel0, angvel0, angpos: three doubles on the device, the fourth lane
-        // kept by caller index for the download
-        std::vector<double> p3(np * 3), w(np * 3);
-        const double *src[3] = {h->vel0 ? h->vel0 : h->vel, h->angvel0 ? h->angvel0 : h->angvel,
-                                h->angpos};
-        P3 *dst[3] = {d.vel0, d.angvel0, d.angpos};
-        for (int f = 0; f < 3; ++f) {
+        // vel, angvel, vel0, angvel0, angpos: three doubles on the device, the
+        // fourth lane kept by caller index for the download; fixvel > 0 as a
+        // flag for the integration
+        std::vector<double> p3(np * 3), w(np * WLANES);
+        const double *src[WLANES];
+        P3 *dst[WLANES];
+        src[W_VEL0] = h->vel0 ? h->vel0 : h->vel;
+        src[W_ANGVEL0] = h->angvel0 ? h->angvel0 : h->angvel;
+        src[W_ANGPOS] = h->angpos;
+        src[W_ANGVEL] = h->angvel;
+        src[W_VEL] = h->vel;
+        dst[W_VEL0] = d.vel0;
+        dst[W_ANGVEL0] = d.angvel0;
+        dst[W_ANGPOS] = d.angpos;
+        dst[W_ANGVEL] = d.angvel[A];
+        dst[W_VEL] = d.vel[A];
+        for (int f = 0; f < WLANES; ++f) {
             for (size_t i = 0; i < np; ++i) {
                 for (int k = 0; k < 3; ++k) p3[3 * i + k] = src[f][4 * i + k];
-                w[3 * i + f] = src[f][4 * i + 3];
+                w[WLANES * i + f] = src[f][4 * i + 3];
             }
             CK(cudaMemcpy(dst[f], p3.data(), np * 24, cudaMemcpyHostToDevice));
         }
-        CK(cudaMemcpy(d.w_user, w.data(), np * 24, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(d.w_user, w.data(), np * 8 * WLANES, cudaMemcpyHostToDevice));
+        std::vector<uint8_t> fx(np);
+        for (size_t i = 0; i < np; ++i) fx[i] = h->vel[4 * i + 3] > 0.0f ? 1 : 0;
+        CK(cudaMemcpy(d.fixed, fx.data(), np, cudaMemcpyHostToDevice));
     }
     CK(cudaMemcpy(d.force, h->force, np * 32, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(d.torque, h->torque, np * 32, cudaMemcpyHostToDevice));
@@ -869,9 +880,10 @@ int sph_download(sph_ctx *c, sph_host_state *h)
         CK(cudaStreamSynchronize(c->stream));
         return SPH_OK;
     };
-    if ((rc = get4(d.xr[A], h->x)) || (rc = get4(d.vel[A], h->vel)) || (rc = get3(d.vel0, 0, h->vel0)) ||
-        (rc = get4(d.acc, h->acc)) || (rc = get4(d.force, h->force)) || (rc = get3(d.angpos, 2, h->angpos)) ||
-        (rc = get4(d.angvel[A], h->angvel)) || (rc = get3(d.angvel0, 1, h->angvel0)) ||
+    if ((rc = get4(d.xr[A], h->x)) || (rc = get3(d.vel[A], W_VEL, h->vel)) ||
+        (rc = get3(d.vel0, W_VEL0, h->vel0)) || (rc = get4(d.acc, h->acc)) ||
+        (rc = get4(d.force, h->force)) || (rc = get3(d.angpos, W_ANGPOS, h->angpos)) ||
+        (rc = get3(d.angvel[A], W_ANGVEL, h->angvel)) || (rc = get3(d.angvel0, W_ANGVEL0, h->angvel0)) ||
         (rc = get4(d.angacc, h->angacc)) || (rc = get4(d.torque, h->torque)))
         return rc;
     {
@@ -1030,7 +1042,7 @@ static std::vector<std::pair<void *, size_t>> ckpt_fields(sph_ctx *c, int a)
 {
     Dev &d = c->d;
     const size_t np = c->np_all;
-    return {{d.xr[a], np * 32},       {d.vel[a], np * 32},  {d.angvel[a], np * 32},
+    return {{d.xr[a], np * 32},       {d.vel[a], np * 24},  {d.angvel[a], np * 24},
             {d.vel0, np * 24},        {d.angvel0, np * 24}, {d.angpos, np * 24},
             {d.xysum, np * 16},       {d.esv, np * 16},     {d.contacts, np * NC * 4},
             {d.dmc, np * 16},         {d.cmask, np * 4},    {d.delta_t, np * NC * 32}};

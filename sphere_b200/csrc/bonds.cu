@@ -29,8 +29,8 @@ k_bonds(Dev d, int A)
     d3 omega0_t = xyz(o0);
     const double omega0_n = o0.w;
     const double4 xi = d.xr[A][si], xj = d.xr[A][sj];
-    const double4 vi = d.vel[A][si], vj = d.vel[A][sj];
-    const d3 wi = xyz(d.angvel[A][si]), wj = xyz(d.angvel[A][sj]);
+    const double4 vi = ld4(d.vel[A], si), vj = ld4(d.vel[A], sj);
+    const d3 wi = xyz(ld4(d.angvel[A], si)), wj = xyz(ld4(d.angvel[A], sj));
     const double R_bar = P.lambda_bar * fmin(xi.w, xj.w);
     const double Ab = REF_PI * R_bar * R_bar;
     const double I = 0.25 * REF_PI * R_bar * R_bar * R_bar * R_bar;

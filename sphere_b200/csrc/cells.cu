@@ -356,6 +356,7 @@ void relayout(const Dev &d, uint32_t np, int a, void *scratch, cudaStream_t st)
     gather_back(d.edp, scratch, order, np, st);
     gather_back(d.uid, scratch, order, np, st);
     gather_back(d.cell, scratch, order, np, st);
+    gather_back(d.fixed, scratch, order, np, st);
     gather_back(d.outside, scratch, order, np, st);
     gather_back(d.cmask, scratch, order, np, st);
     gather_back(d.dmc, scratch, order, np, st);

@@ -103,6 +103,18 @@ struct P3 {
     double x, y, z;
 };
 
+// The fourth lanes of the host's four-double rows that the device keeps as
+// three doubles; a step never changes them.
+constexpr int W_VEL0 = 0, W_ANGVEL0 = 1, W_ANGPOS = 2, W_ANGVEL = 3, W_VEL = 4, WLANES = 5;
+
+// A P3 row as a double4 with a zero fourth lane.
+__device__ __forceinline__ double4 ld4(const P3 *a, uint32_t i)
+{
+    const P3 v = a[i];
+    return make_double4(v.x, v.y, v.z, 0.0);
+}
+__device__ __forceinline__ P3 p3of(double4 v) { return P3{v.x, v.y, v.z}; }
+
 // Device pointers of one simulation.  Per-particle arrays are indexed by the
 // storage index s (particles are kept in cell order); uid[s] is the caller's
 // particle index and sidx[uid] its inverse.  Contact rows store partners as
@@ -116,14 +128,15 @@ struct Dev {
     uint32_t *inst_cell_base;
     // double-buffered kinematics read by neighbours: [0]/[1]
     double4 *xr[2];       // x, y, z, radius
-    double4 *vel[2];      // vx, vy, vz, fixvel
-    double4 *angvel[2];   // wx, wy, wz, (w lane carried)
+    P3 *vel[2];           // vx, vy, vz (fixvel in `fixed`, the host lane in w_user)
+    P3 *angvel[2];        // wx, wy, wz (the host lane in w_user)
     float4 *xs[2];        // float copy of xr in cell-list order, for the neighbour cull
     // private per-particle state (updated in place); three doubles each, the
     // fourth lane of the host rows (never changed by a step) is kept apart in
     // w_user
     P3 *vel0, *angvel0, *angpos;
-    double *w_user;       // [np][3] fourth lanes of vel0, angvel0, angpos, by caller index
+    double *w_user;       // [np][WLANES] fourth host lanes, by caller index (W_* below)
+    uint8_t *fixed;       // fixvel > 0: x/y acceleration and spin held (integration.cuh:65-77)
     double2 *xysum;
     double2 *esv;         // es, ev
     // per-step outputs

@@ -35,7 +35,7 @@ constexpr int FORCE_BLOCK = 128;
 #define SPHK_TOPO_MIN_BLOCKS 10
 #endif
 #ifndef SPHK_FORCE_MIN_BLOCKS
-#define SPHK_FORCE_MIN_BLOCKS 6
+#define SPHK_FORCE_MIN_BLOCKS 8
 #endif
 
 // contactLinear_wall, src/contactmodels.cuh:10-109.  Out of line: six call
@@ -348,8 +348,8 @@ __device__ __noinline__ void visc_pair(const Dev &d, int A, uint32_t s, uint32_t
     const double len = flen(xab);
     const double delta = len - (xa.w + xb.w);
     if (delta < 0.0f) {
-        contact_viscous(P, F, p, d.vel[A][s], d.vel[A][t], xyz(d.angvel[A][s]),
-                        xyz(d.angvel[A][t]), xa.w, xb.w, xab, len, delta);
+        contact_viscous(P, F, p, ld4(d.vel[A], s), ld4(d.vel[A], t), xyz(ld4(d.angvel[A], s)),
+                        xyz(ld4(d.angvel[A], t)), xa.w, xb.w, xab, len, delta);
     } else if (delta < P.db) {
         capillary_exp(P, F, xa.w, xb.w, delta, xab, len);
     }
@@ -636,8 +636,8 @@ k_force(ForceArgs args)
     uint32_t err = 0;
     const double4 xa = d.xr[A][s];
     const double ra = xa.w;
-    const double4 vel_a = d.vel[A][s];
-    const double4 angvel_a4 = d.angvel[A][s];
+    const double4 vel_a = ld4(d.vel[A], s);
+    const double4 angvel_a4 = ld4(d.angvel[A], s);
     const d3 angvel_a = xyz(angvel_a4);
     d3 F = mk(0.0, 0.0, 0.0), T = mk(0.0, 0.0, 0.0);
     double es_dot = 0.0f, ev_dot = 0.0f, p = 0.0f;
@@ -662,7 +662,7 @@ k_force(ForceArgs args)
             in.ra = ra;
             in.rb = xb.w;
             if (dl::len(in.xab) - (ra + xb.w) < 0.0) {
-                const double4 vb = d.vel[A][t], wb = d.angvel[A][t], d0 = dtrow[i];
+                const double4 vb = ld4(d.vel[A], t), wb = ld4(d.angvel[A], t), d0 = dtrow[i];
                 in.va = dl::v3(vel_a.x, vel_a.y, vel_a.z);
                 in.vb = dl::v3(vb.x, vb.y, vb.z);
                 in.wa = dl::v3(angvel_a4.x, angvel_a4.y, angvel_a4.z);
@@ -689,7 +689,7 @@ k_force(ForceArgs args)
         if (occ != occ0) d.cmask[s] = occ;
         if (j >= 0) {
             d.tp_x[row] = xa;
-            d.tp_v[row] = vel_a;
+            d.tp_v[row] = make_double4(vel_a.x, vel_a.y, vel_a.z, d.fixed[s] ? 1.0 : 0.0);
             d.tp_w[row] = angvel_a4;
             d.tp_mask[row] = lawmask;
             d.tp_dmc[row] = dmw;
@@ -715,11 +715,11 @@ k_force(ForceArgs args)
             if (delta_n < 0.0f) {
                 double4 dt4 = dtrow[i];
                 if (MODEL == 2)
-                    contact_linear(P, F, T, es_dot, ev_dot, p, vel_a, angvel_a, d.vel[A][t],
-                                   d.angvel[A][t], ra, rb, xab, xlen, delta_n, dt4);
+                    contact_linear(P, F, T, es_dot, ev_dot, p, vel_a, angvel_a, ld4(d.vel[A], t),
+                                   ld4(d.angvel[A], t), ra, rb, xab, xlen, delta_n, dt4);
                 else
-                    contact_hertz(P, F, T, es_dot, ev_dot, p, vel_a, angvel_a, d.vel[A][t],
-                                  d.angvel[A][t], ra, rb, xab, xlen, delta_n, dt4);
+                    contact_hertz(P, F, T, es_dot, ev_dot, p, vel_a, angvel_a, ld4(d.vel[A], t),
+                                  ld4(d.angvel[A], t), ra, rb, xab, xlen, delta_n, dt4);
                 dtrow[i] = dt4;
             } else {
                 // separated: free the slot and zero its history
@@ -812,27 +812,52 @@ k_force(ForceArgs args)
     }
 
     // ---- integrate, src/integration.cuh:9-187 -------------------------------
-    double4 x = xa, vel = vel_a, angvel = angvel_a4;
-    P3 angpos = d.angpos[s], vel0 = d.vel0[s], angvel0 = d.angvel0[s];
-    const double radius = x.w;
+    // The rotation and the translation are independent; each is finished and
+    // stored before the other starts, so fewer values are live at once.
+    // Every expression keeps the reference's operands and order.
+    const double radius = xa.w;
     const double m = 4.0 / 3.0 * REF_PI * radius * radius * radius * P.rho;
-    double4 acc, angacc;
+    const bool fixed = d.fixed[s] != 0;   // fixvel > 0
+    {
+        P3 angpos = d.angpos[s], angvel0 = d.angvel0[s];
+        double4 angacc;
+        angacc.x = T.x * 1.0 / (2.0 / 5.0 * m * radius * radius);
+        angacc.y = T.y * 1.0 / (2.0 / 5.0 * m * radius * radius);
+        angacc.z = T.z * 1.0 / (2.0 / 5.0 * m * radius * radius);
+        angacc.w = 0.0;
+        if (fixed) angacc = make_double4(0.0f, 0.0f, 0.0f, 0.0f);
+        angvel0.x += angacc.x * dt;
+        angvel0.y += angacc.y * dt;
+        angvel0.z += angacc.z * dt;
+        angpos.x += angvel0.x * dt;
+        angpos.y += angvel0.y * dt;
+        angpos.z += angvel0.z * dt;
+        P3 angvel;
+        angvel.x = angvel0.x + 0.5 * angacc.x * dt;
+        angvel.y = angvel0.y + 0.5 * angacc.y * dt;
+        angvel.z = angvel0.z + 0.5 * angacc.z * dt;
+        d.angvel[B][s] = angvel;
+        d.angvel0[s] = angvel0;
+        d.angpos[s] = angpos;
+        if (args.write_outputs) {
+            d.torque[s] = make_double4(T.x, T.y, T.z, 0.0f);
+            d.angacc[s] = angacc;
+        }
+    }
+    double4 x = xa, vel = vel_a;
+    P3 vel0 = d.vel0[s];
+    double4 acc;
     acc.x = F.x / m;
     acc.y = F.y / m;
     acc.z = F.z / m;
     acc.w = 0.0;
-    angacc.x = T.x * 1.0 / (2.0 / 5.0 * m * radius * radius);
-    angacc.y = T.y * 1.0 / (2.0 / 5.0 * m * radius * radius);
-    angacc.z = T.z * 1.0 / (2.0 / 5.0 * m * radius * radius);
-    angacc.w = 0.0;
     acc.x += P.g[0];
     acc.y += P.g[1];
     acc.z += P.g[2];
-    if (vel.w > 0.0f) {
+    if (fixed) {
         acc.x = 0.0;
         acc.y = 0.0;
         acc.z -= P.g[2];
-        angacc = make_double4(0.0f, 0.0f, 0.0f, 0.0f);
     }
     if (P.periodic == 1) {
         if (x.x < P.origo[0]) x.x += P.L[0];
@@ -846,21 +871,12 @@ k_force(ForceArgs args)
     vel0.x += acc.x * dt;
     vel0.y += acc.y * dt;
     vel0.z += acc.z * dt;
-    angvel0.x += angacc.x * dt;
-    angvel0.y += angacc.y * dt;
-    angvel0.z += angacc.z * dt;
     x.x += vel0.x * dt;
     x.y += vel0.y * dt;
     x.z += vel0.z * dt;
-    angpos.x += angvel0.x * dt;
-    angpos.y += angvel0.y * dt;
-    angpos.z += angvel0.z * dt;
     vel.x = vel0.x + 0.5 * acc.x * dt;
     vel.y = vel0.y + 0.5 * acc.y * dt;
     vel.z = vel0.z + 0.5 * acc.z * dt;
-    angvel.x = angvel0.x + 0.5 * angacc.x * dt;
-    angvel.y = angvel0.y + 0.5 * angacc.y * dt;
-    angvel.z = angvel0.z + 0.5 * angacc.z * dt;
     double2 xys = make_double2(0.0f, 0.0f);
     xys.x += vel.x * dt;
     xys.y += vel.y * dt;
@@ -869,19 +885,14 @@ k_force(ForceArgs args)
         d.xysum[s] = make_double2(o.x + xys.x, o.y + xys.y);
     }
     d.xr[B][s] = x;
-    d.vel[B][s] = vel;
-    d.angvel[B][s] = angvel;
+    d.vel[B][s] = p3of(vel);
     d.vel0[s] = vel0;
-    d.angvel0[s] = angvel0;
-    d.angpos[s] = angpos;
     // float copy for the next step's contact search, at this particle's
     // cell-list position (rewritten by the rebuild when the order changes)
     d.xs[B][d.pos[s]] = make_float4((float)x.x, (float)x.y, (float)x.z, (float)x.w);
     if (args.write_outputs) {
         d.force[s] = make_double4(F.x, F.y, F.z, 0.0f);
-        d.torque[s] = make_double4(T.x, T.y, T.z, 0.0f);
         d.acc[s] = acc;
-        d.angacc[s] = angacc;
         d.edp[s] = make_double4(es_dot, ev_dot, p, 0.0);
     }
 
