@@ -172,10 +172,17 @@ def ncu_traffic(np_):
 
 
 def algorithmic_bytes(np_, ncells, contacts, nbonds=0):
-    """Compulsory HBM bytes of one step: 368 B of particle state per particle,
-    16 B of sort key/permutation, 16 B per cell of start/end, 52 B per active
-    directed contact (partner 4 + history read 24 + write 24), 136 B per bond."""
-    step_kernel = 368 * np_ + 52 * contacts
+    """Compulsory HBM bytes of one step.
+
+    Per particle 329 B of state: a read of x,r 32, v 24, the fixvel flag 1,
+    vel0 24, angvel 24, angvel0 24, angpos 24, xysum 16, and a write of the
+    same less r and the flag.  The es/ev sums (read 16 + write 16) move only
+    for a particle whose energy rates are nonzero, which needs a contact;
+    min(np, contacts) bounds the number of such particles from above.  Then
+    52 B per active directed contact (partner 4 + history read 24 + write
+    24).  The whole step adds 16 B of sort key/permutation per particle, 16 B
+    of start/end per cell and 136 B per bond."""
+    step_kernel = 329 * np_ + 32 * min(np_, contacts) + 52 * contacts
     whole = step_kernel + 16 * np_ + 16 * ncells + 136 * nbonds
     return step_kernel, whole
 

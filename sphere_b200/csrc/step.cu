@@ -746,30 +746,34 @@ k_force(ForceArgs args)
             T = add(T, mk(tw.x, tw.y, tw.z));
         }
     } else {
+        // a wall's position only for its test, its normal and velocity only
+        // on contact; dynamic walls replace the defaults (contactsearch.cuh:
+        // 416-427) in order
         const Walls &W = *d.walls;
-        double4 wnx[5] = {make_double4(0.0f, 0.0f, -1.0f, P.L[2]), make_double4(-1.0f, 0.0f, 0.0f, P.L[0]),
-                          make_double4(1.0f, 0.0f, 0.0f, 0.0f), make_double4(0.0f, -1.0f, 0.0f, P.L[1]),
-                          make_double4(0.0f, 1.0f, 0.0f, 0.0f)};
-        double wv[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-#pragma unroll
-        for (int k = 0; k < 5; ++k)
-            if ((uint32_t)k < P.nw) { wnx[k] = W.nx[k]; wv[k] = W.mvfd[k].y; }
+        auto wpos = [&](int k, double dflt) { return ((uint32_t)k < P.nw) ? W.nx[k].w : dflt; };
+        auto wnrm = [&](int k, d3 dflt) { return ((uint32_t)k < P.nw) ? xyz(W.nx[k]) : dflt; };
+        auto wvel = [&](int k) { return ((uint32_t)k < P.nw) ? W.mvfd[k].y : 0.0; };
         double dw;
-        dw = wnx[0].w - (xa.z + ra);
-        if (dw < 0.0f) w0f = contact_wall(P, F, T, p, ra, vel_a, angvel_a4, xyz(wnx[0]), dw, wv[0]);
+        dw = wpos(0, P.L[2]) - (xa.z + ra);
+        if (dw < 0.0f)
+            w0f = contact_wall(P, F, T, p, ra, vel_a, angvel_a4, wnrm(0, mk(0.0, 0.0, -1.0)), dw, wvel(0));
         dw = xa.z - ra - P.origo[2];
         if (dw < 0.0f) (void)contact_wall(P, F, T, p, ra, vel_a, angvel_a4, mk(0.0, 0.0, 1.0), dw, 0.0f);
         if (P.periodic == 0) {
-            dw = wnx[1].w - (xa.x + ra);
-            if (dw < 0.0f) (void)contact_wall(P, F, T, p, ra, vel_a, angvel_a4, xyz(wnx[1]), dw, wv[1]);
-            dw = xa.x - ra - wnx[2].w;
-            if (dw < 0.0f) (void)contact_wall(P, F, T, p, ra, vel_a, angvel_a4, xyz(wnx[2]), dw, wv[2]);
+            dw = wpos(1, P.L[0]) - (xa.x + ra);
+            if (dw < 0.0f)
+                (void)contact_wall(P, F, T, p, ra, vel_a, angvel_a4, wnrm(1, mk(-1.0, 0.0, 0.0)), dw, wvel(1));
+            dw = xa.x - ra - wpos(2, 0.0);
+            if (dw < 0.0f)
+                (void)contact_wall(P, F, T, p, ra, vel_a, angvel_a4, wnrm(2, mk(1.0, 0.0, 0.0)), dw, wvel(2));
         }
         if (P.periodic == 0 || P.periodic == 2) {
-            dw = wnx[3].w - (xa.y + ra);
-            if (dw < 0.0f) (void)contact_wall(P, F, T, p, ra, vel_a, angvel_a4, xyz(wnx[3]), dw, wv[3]);
-            dw = xa.y - ra - wnx[4].w;
-            if (dw < 0.0f) (void)contact_wall(P, F, T, p, ra, vel_a, angvel_a4, xyz(wnx[4]), dw, wv[4]);
+            dw = wpos(3, P.L[1]) - (xa.y + ra);
+            if (dw < 0.0f)
+                (void)contact_wall(P, F, T, p, ra, vel_a, angvel_a4, wnrm(3, mk(0.0, -1.0, 0.0)), dw, wvel(3));
+            dw = xa.y - ra - wpos(4, 0.0);
+            if (dw < 0.0f)
+                (void)contact_wall(P, F, T, p, ra, vel_a, angvel_a4, wnrm(4, mk(0.0, 1.0, 0.0)), dw, wvel(4));
         }
     }
 
