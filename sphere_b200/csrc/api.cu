@@ -79,6 +79,11 @@ struct sph_ctx {
         char *buf;
     };
     std::vector<Ckpt> ckpts;
+    // checkpoint buffers handed back by sph_diff_end and the backward, kept
+    // for the next forward of a calibration loop; freed by sph_destroy
+    std::vector<char *> ckpt_pool;
+    size_t ckpt_bytes = 0;                // size of one pooled buffer
+    cudaEvent_t ckpt_ev = nullptr;        // orders a checkpoint copy against the caller's stream
     std::vector<void *> diff_allocs;
     size_t diff_bytes = 0;
     AdjDev adj{};
@@ -779,11 +784,22 @@ int sph_step(sph_ctx *c, uint64_t nsteps, void *stream)
     uint64_t left = nsteps;
     while (left > 0) {
         if (c->diff_steps % K == 0 && c->diff_steps / K == c->ckpts.size()) {
-            if (stream) CK(cudaStreamSynchronize(static_cast<cudaStream_t>(stream)));
+            // the copy runs on the context's stream: after the caller's
+            // steps so far, and before the caller's next ones
+            cudaStream_t us = stream ? static_cast<cudaStream_t>(stream) : c->stream;
+            if (!c->ckpt_ev) CK(cudaEventCreateWithFlags(&c->ckpt_ev, cudaEventDisableTiming));
+            if (us != c->stream) {
+                CK(cudaEventRecord(c->ckpt_ev, us));
+                CK(cudaStreamWaitEvent(c->stream, c->ckpt_ev, 0));
+            }
             sph_ctx::Ckpt k{};
             const int rc = save_ckpt(c, k);
             if (rc != SPH_OK) return rc;
             c->ckpts.push_back(k);
+            if (us != c->stream) {
+                CK(cudaEventRecord(c->ckpt_ev, c->stream));
+                CK(cudaStreamWaitEvent(us, c->ckpt_ev, 0));
+            }
         }
         const uint64_t chunk = std::min<uint64_t>(left, K - c->diff_steps % K);
         const int rc = step_plain(c, chunk, stream);
@@ -1007,7 +1023,8 @@ int sph_get_stats(sph_ctx *c, sph_stats *out)
     }
     out->steps = c->steps;
     out->relayouts = c->relayouts;
-    out->device_bytes = c->device_bytes + c->diff_bytes;
+    out->device_bytes = c->device_bytes + c->diff_bytes +
+                        (c->ckpts.size() + c->ckpt_pool.size()) * c->ckpt_bytes;
     return SPH_OK;
 }
 
@@ -1055,15 +1072,29 @@ static int save_ckpt(sph_ctx *c, sph_ctx::Ckpt &k)
     size_t bytes = 0;
     for (auto &f : ckpt_fields(c, c->a)) bytes += f.second;
     k.buf = nullptr;
-    int rc = dalloc(c, &k.buf, bytes, &c->diff_allocs);
-    if (rc != SPH_OK) return rc;
+    if (c->ckpt_bytes != bytes) {
+        for (char *b : c->ckpt_pool) cudaFree(b);
+        c->ckpt_pool.clear();
+        c->ckpt_bytes = bytes;
+    }
+    if (!c->ckpt_pool.empty()) {
+        k.buf = c->ckpt_pool.back();
+        c->ckpt_pool.pop_back();
+    } else {
+        // fully overwritten below, so no clearing
+        CK(cudaMalloc(&k.buf, bytes));
+    }
     size_t off = 0;
     for (auto &f : ckpt_fields(c, c->a)) {
         CK(cudaMemcpyAsync(k.buf + off, f.first, f.second, cudaMemcpyDeviceToDevice, c->stream));
         off += f.second;
     }
-    CK(cudaStreamSynchronize(c->stream));
     return SPH_OK;
+}
+
+static void ckpt_release(sph_ctx *c, char *buf)
+{
+    if (buf) c->ckpt_pool.push_back(buf);
 }
 
 static int restore_ckpt(sph_ctx *c, const sph_ctx::Ckpt &k)
@@ -1130,6 +1161,7 @@ static void free_diff(sph_ctx *c)
     for (void *p : c->diff_allocs) cudaFree(p);
     c->diff_allocs.clear();
     c->diff_bytes = 0;
+    for (auto &k : c->ckpts) ckpt_release(c, k.buf);
     c->ckpts.clear();
     c->adj = AdjDev{};
     Dev &d = c->d;
@@ -1239,10 +1271,9 @@ int sph_diff_backward(sph_ctx *c, const double *x_bar, const double *v_bar, doub
     if (x0_bar) CK(cudaMemcpy(x0_bar, out + np, (size_t)np * 24, cudaMemcpyDeviceToHost));
     if (v0_bar) CK(cudaMemcpy(v0_bar, out + 4 * (size_t)np, (size_t)np * 24, cudaMemcpyDeviceToHost));
     // scratch of this call and the final-state copy
-    size_t fin_bytes = 0;
-    for (auto &f : ckpt_fields(c, c->a)) fin_bytes += f.second;
+    ckpt_release(c, fin.buf);
     const std::pair<void *, size_t> scratch[] = {
-        {out, 7 * (size_t)np * 8}, {hx, 6 * (size_t)np * 8}, {fin.buf, fin_bytes}};
+        {out, 7 * (size_t)np * 8}, {hx, 6 * (size_t)np * 8}};
     for (const auto &p : scratch) {
         cudaFree(p.first);
         auto &v = c->diff_allocs;
@@ -1273,6 +1304,8 @@ int sph_destroy(sph_ctx *c)
     drop_graphs(c);
     for (auto e : c->ev) cudaEventDestroy(e);
     free_diff(c);
+    for (char *b : c->ckpt_pool) cudaFree(b);
+    if (c->ckpt_ev) cudaEventDestroy(c->ckpt_ev);
     for (void *p : c->allocs) cudaFree(p);
     if (c->stream) cudaStreamDestroy(c->stream);
     if (c->side) cudaStreamDestroy(c->side);

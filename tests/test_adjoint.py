@@ -108,6 +108,35 @@ def test_checkpoint_interval_does_not_change_gradients(grads):
     assert np.allclose(g["mu"], grads["g"]["mu"], rtol=1e-10, atol=1e-12 * np.abs(g["mu"]).max())
 
 
+def test_repeated_iterations_on_a_callers_stream_give_the_same_gradients(grads):
+    """A calibration loop in one context: the second forward reuses the
+    checkpoint buffers of the first, and both run on a stream of the
+    caller's, in pieces that do not line up with the checkpoint interval."""
+    sb, wx, wv = grads["sb"], grads["wx"], grads["wv"]
+    sim = Simulation(adjoint._scene_config(sb, sb.k_n, sb.k_t, sb.gamma_n))
+    s = torch.cuda.Stream()
+    try:
+        for _ in range(2):
+            sim.upload(state_from_spherebin(sb))
+            sim.diff_begin(mu=grads["mu_p"], checkpoint_every=K)
+            for n in (7, 9, STEPS - 16):
+                sim.step(n, stream=s.cuda_stream)
+            s.synchronize()
+            sim.sync()
+            st = sim.download()
+            assert np.array_equal(st.x, grads["st"].x)
+            g = sim.diff_backward(wx, wv)
+            sim.diff_end()
+            # the reverse pass adds partners' adjoints atomically, so only
+            # the order of those additions may differ
+            for k in ("k_n", "k_t", "gamma_n"):
+                assert abs(g[k] - grads["g"][k]) <= 1e-12 * abs(g[k]), k
+            assert np.allclose(g["mu"], grads["g"]["mu"], rtol=1e-10,
+                               atol=1e-12 * np.abs(g["mu"]).max())
+    finally:
+        sim.close()
+
+
 def test_autograd_function_gives_the_same_gradients(grads):
     sb, wx, wv = grads["sb"], grads["wx"], grads["wv"]
     kn = torch.tensor(sb.k_n, dtype=torch.float64, requires_grad=True)
