@@ -610,6 +610,13 @@ k_topo(Dev d, int A)
     if (ts.err) atomicOr(d.status, ts.err);
 }
 
+// Asks the copy engine to bring `bytes` at `p` into L2 (a hint: nothing is
+// waited for, no register is held).  `p` and `bytes` are multiples of 16.
+__device__ __forceinline__ void bulk_prefetch_l2(const void *p, uint32_t bytes)
+{
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
 struct ForceArgs {
     Dev d;
     int a;              // read buffer (start of step); the kernel writes buffer 1-a
@@ -631,6 +638,23 @@ k_force(ForceArgs args)
     const uint32_t np = d.np_all;
     const uint32_t s = blockIdx.x * FORCE_BLOCK + threadIdx.x;
     if (s >= np) return;
+#ifndef SPHK_NO_PREFETCH
+    // The state the integration reads comes after the contact work and
+    // after stores the compiler may not move loads across, so each of its
+    // loads would wait out a full DRAM latency in turn.  Lane 0 of every
+    // warp whose 32 rows all exist asks for the warp's rows of it up front.
+    if ((threadIdx.x & 31u) == 0 && s + 32 <= np) {
+        bulk_prefetch_l2(d.angpos + s, 32 * sizeof(P3));
+        bulk_prefetch_l2(d.angvel0 + s, 32 * sizeof(P3));
+        bulk_prefetch_l2(d.vel0 + s, 32 * sizeof(P3));
+        bulk_prefetch_l2(d.xysum + s, 32 * sizeof(double2));
+        bulk_prefetch_l2(d.pos + s, 32 * sizeof(uint32_t));
+        bulk_prefetch_l2(d.disp + s, 32 * sizeof(float));
+        bulk_prefetch_l2(d.cell + s, 32 * sizeof(uint32_t));
+        bulk_prefetch_l2(d.fixed + s, 32);
+        if (d.wtouch) bulk_prefetch_l2(d.wtouch + s, 32);
+    }
+#endif
     const Params &P = prm_at<BATCH>(d, s);
     const int A = args.a, B = 1 - args.a;
     uint32_t err = 0;
