@@ -397,11 +397,16 @@ k_topo(Dev d, int A)
     const Params &P = prm_at<BATCH>(d, s);
     const Verlet &V = *d.vs;
     // The list decision first, from a few bytes: a valid list whose gap
-    // bound rules out every contact ends the particle's work here.
+    // bound rules out every contact ends the particle's work here.  Its four
+    // per-particle loads are unconditional so that they are in flight
+    // together, one memory latency instead of a chain of them.
     const uint8_t len = d.vl_len[s];
-    bool list_ok = P.skin > 0.0 && !V.all_rebuild && len != VL_NONE && d.outside[s] == 0;
+    const uint8_t outs = d.outside[s];
+    const float gap = d.vl_gap[s];
+    const float bound = moved_bound(d, s, V);
+    bool list_ok = P.skin > 0.0 && !V.all_rebuild && len != VL_NONE && outs == 0;
     if (list_ok && V.dirty_step == V.step) list_ok = d.dirty[d.cell[s]] != V.step;
-    if (list_ok && d.vl_gap[s] > moved_bound(d, s, V)) {
+    if (list_ok && gap > bound) {
         if (VISC) d.c1acc[s] = make_double4(0.0, 0.0, 0.0, 0.0);
         return;
     }
