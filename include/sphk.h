@@ -17,6 +17,9 @@
  *   sph_get_contacts the CONTACTINFO dump of slots (src/device.cu:1148-1176)
  *   sph_get_cells    the sorted arrays of the last step (src/device.cu:747-800)
  *   sph_destroy      DEM::freeGlobalDeviceMemory (src/device.cu:326-391)
+ *   sph_darcy_init   DEM::initDarcy (src/darcy.cpp:760-798)
+ *   sph_darcy_upload, sph_darcy_download
+ *                    DEM::transferDarcy{To,From}GlobalDeviceMemory (src/darcy.cuh:60-121)
  *
  * Conventions: plain C types only; every entry point returns an int status,
  * SPH_OK (0) or a negative SPH_ERR_* code; the message of the last failure
@@ -34,7 +37,7 @@
 extern "C" {
 #endif
 
-#define SPHK_VERSION 2
+#define SPHK_VERSION 3
 #define SPHK_NC 32        /* contact slots per particle (src/constants.h:24) */
 #define SPHK_MAXWALLS 6   /* src/constants.h:11 */
 
@@ -47,6 +50,7 @@ extern "C" {
 #define SPH_ERR_BOND_ALIAS (-6)   /* a broken bond's marker (nb0 < np) aliases a particle */
 #define SPH_ERR_NOMEM (-7)        /* device allocation failed */
 #define SPH_ERR_TOO_LARGE (-8)    /* input exceeds the fixed scratch of sph_cell_list_noalloc */
+#define SPH_ERR_UNSTABLE (-9)     /* sph_darcy_init: the explicit Darcy step would be unstable */
 
 typedef struct sph_ctx sph_ctx;
 
@@ -120,7 +124,8 @@ typedef struct sph_stats {
 #define SPH_PHASE_TOPO 2    /* contact detection into the slots */
 #define SPH_PHASE_FORCE 3   /* contact and wall forces + integration */
 #define SPH_PHASE_WALLS 4   /* wall force reduction + wall integration */
-#define SPH_NPHASES 5
+#define SPH_PHASE_DARCY 5   /* Darcy flow (zero without sph_darcy_upload) */
+#define SPH_NPHASES 6
 
 int sph_version(void);
 int sph_create(const sph_config *cfg, sph_ctx **out);
@@ -164,6 +169,49 @@ int sph_get_profile(sph_ctx *ctx, double *ms, uint64_t *steps, int reset);
 int sph_relayout(sph_ctx *ctx);
 const char *sph_last_error(const sph_ctx *ctx);
 int sph_destroy(sph_ctx *ctx);
+
+/* ---- Darcy flow -------------------------------------------------------------
+ * The reference's fluid coupling for darcy == 1 and nu > 0 (src/darcy.cuh,
+ * src/darcy.cpp; DEM's darcyflow argument, src/sphere.h:254): each step,
+ * between the contact forces and the integration, the porosity of every
+ * cell from the step's start positions, the cell conductivities and an
+ * explicit step of the pore pressure (src/device.cu:913-1021).  The flow
+ * does not act on the particles.
+ *
+ * The fluid grid is the cell grid with one ghost node on every side:
+ * (num[0]+2)(num[1]+2)(num[2]+2) nodes, x fastest; node (x, y, z), with
+ * -1 <= x <= num[0] and so on, at (x+1) + (num[0]+2)(y+1) +
+ * (num[0]+2)(num[1]+2)(z+1).  These are the reference's host arrays of
+ * DEM::d (src/darcy.cpp:17-38): one double per node, three for V, dH, T. */
+typedef struct sph_darcy_state {
+    double *H, *H_new;   /* hydraulic pressure: current and spare buffer */
+    double *V;           /* 3 per node: pore velocity */
+    double *dH;          /* 3 per node: pressure gradient */
+    double *K;           /* hydraulic conductivity */
+    double *T;           /* 3 per node: transmissivity */
+    double *Ss, *W;      /* specific storativity, recharge */
+    double *phi, *dphi;  /* porosity and its change in the last step */
+} sph_darcy_state;
+
+/* DEM::initDarcy (src/darcy.cpp:760-798), on the host: Ss := 1 and W := 0
+ * on every node; the porosity of every cell from the particles whose centres
+ * it holds (x: np*4, the reference's host rows) into phi; K and T from it;
+ * dphi := 0.  H, H_new, V and dH are left as they are (the input file gives
+ * V and H; the reference leaves the rest unset, read here as zero by
+ * convention of the caller).  *stability (may be NULL) receives the
+ * criterion of checkDarcyTimestep (src/darcy.cpp:733-758); above 0.5 the
+ * call returns SPH_ERR_UNSTABLE, where the reference exits. */
+int sph_darcy_init(const sph_config *cfg, double nu, const double *x, sph_darcy_state *st,
+                   double *stability);
+/* transferDarcyToGlobalDeviceMemory (src/darcy.cuh:60-92) plus the
+ * Kozeny-Carman factor of DEM::startTime (src/device.cu:673-678, from the
+ * mean radius of the uploaded particles): after sph_upload, switches the
+ * context to run the Darcy flow in every step, with dynamic viscosity nu.
+ * The first step after this call leaves dphi zero (src/darcy.cuh:463-466).
+ * Not for batched or differentiable contexts.  Every array is required. */
+int sph_darcy_upload(sph_ctx *ctx, double nu, const sph_darcy_state *st);
+/* transferDarcyFromGlobalDeviceMemory (src/darcy.cuh:95-121). */
+int sph_darcy_download(sph_ctx *ctx, sph_darcy_state *st);
 
 /* ---- Differentiable step ----------------------------------------------------
  * No counterpart in the reference: gradients of a run with respect to the

@@ -748,6 +748,187 @@ static void integrate_walls(orc_scene *s, const work_t *w, double t_current)
     }
 }
 
+/* ---- Darcy flow: src/darcy.cuh ------------------------------------------
+ * The six kernels the time loop runs between bondsLinear and integrate when
+ * darcy == 1 and nu > 0 (src/device.cu:913-1021), each over the interior
+ * nodes, in that order.  The fluid grid is the cell grid plus one ghost node
+ * on every side. */
+static const double D_PI = 3.14159265358979323846;   /* M_PI */
+
+/* node (x, y, z) with ghosts at -1 and num; src/darcy.cuh:125-135 */
+static inline size_t d_idx(const orc_scene *s, int x, int y, int z)
+{
+    const size_t nx2 = (size_t)s->num[0] + 2, ny2 = (size_t)s->num[1] + 2;
+    return (size_t)(x + 1) + nx2 * (size_t)(y + 1) + nx2 * ny2 * (size_t)(z + 1);
+}
+
+/* findPorositiesSphericalDev, src/darcy.cuh:338-477: the void fraction of a
+ * sphere of radius min(dx,dy,dz)/2 at the cell centre (measured from the
+ * origin, not from origo), from the lens-shaped overlaps of the particles of
+ * the 27 neighbour cells, visited z, y, x outermost to innermost and in
+ * sorted order within a cell; clamped to [0.1, 0.9].  The change is zero in
+ * the run's first step. */
+static void darcy_porosity(orc_scene *s, const work_t *w, uint32_t x, uint32_t y, uint32_t z)
+{
+    const uint32_t nx = s->num[0], ny = s->num[1], nz = s->num[2];
+    const double dx = s->L[0] / nx, dy = s->L[1] / ny, dz = s->L[2] / nz;
+    const double R = fmin(dx, fmin(dy, dz)) * 0.5;
+    const double cell_volume = 4.0 / 3.0 * D_PI * R * R * R;
+    double void_volume = cell_volume;
+    const v3 X = mk(x * dx + 0.5 * dx, y * dy + 0.5 * dy, z * dz + 0.5 * dz);
+    const size_t me = d_idx(s, (int)x, (int)y, (int)z);
+    const double phi_0 = s->d_phi[me];
+    for (int oz = -1; oz < 2; ++oz)
+        for (int oy = -1; oy < 2; ++oy)
+            for (int ox = -1; ox < 2; ++ox) {
+                int32_t c[3] = {(int32_t)x + ox, (int32_t)y + oy, (int32_t)z + oz};
+                v3 dm = mk(0.0, 0.0, 0.0);
+                if (dist_mod(s, c, &dm) == -1) continue;
+                const uint32_t cid = (uint32_t)c[0] + (uint32_t)c[1] * nx + (nx * ny) * (uint32_t)c[2];
+                const uint32_t beg = s->cell_start[cid];
+                if (beg == 0xffffffffu) continue;
+                const uint32_t end = s->cell_end[cid];
+                for (uint32_t i = beg; i < end; ++i) {
+                    const double *xr = &w->x_s[4 * (size_t)i];
+                    const double r = xr[3];
+                    const v3 dist = add(mk(X.x - xr[0], X.y - xr[1], X.z - xr[2]), dm);
+                    const double d = vlen(dist);
+                    if ((R - r) < d && d < (R + r))
+                        void_volume -= 1.0 / (12.0 * d) *
+                                       (D_PI * (R + r - d) * (R + r - d) *
+                                        (d * d + 2.0 * d * r - 3.0 * r * r + 2.0 * d * R +
+                                         6.0 * r * R - 3.0 * R * R));
+                    if (d <= R - r) void_volume -= 4.0 / 3.0 * D_PI * r * r * r;
+                }
+            }
+    const double phi = fmin(0.9, fmax(0.1, void_volume / cell_volume));
+    s->d_phi[me] = phi;
+    s->d_dphi[me] = (s->iteration == 0) ? 0.0 : phi - phi_0;
+}
+
+/* findDarcyTransmissivitiesDev, src/darcy.cuh:480-538: Kozeny-Carman
+ * conductivity from the porosity, and the transmissivity K * (dx, dy, dz). */
+static void darcy_transmissivity(orc_scene *s, uint32_t x, uint32_t y, uint32_t z)
+{
+    const double dx = s->L[0] / s->num[0], dy = s->L[1] / s->num[1], dz = s->L[2] / s->num[2];
+    const double rho = 1000.0;
+    const size_t me = d_idx(s, (int)x, (int)y, (int)z);
+    const double phi = s->d_phi[me];
+    const double k = phi * phi * phi / ((1.0 - phi) * (1.0 - phi)) * s->d_factor;
+    const double K = k * rho * -s->g[2] / s->nu;
+    s->d_K[me] = K;
+    s->d_T[3 * me + 0] = K * dx;
+    s->d_T[3 * me + 1] = K * dy;
+    s->d_T[3 * me + 2] = K * dz;
+}
+
+/* copyDarcyValsDev, src/darcy.cuh:137-166: every field of node `from`
+ * onto node `to` */
+static void darcy_copy_node(orc_scene *s, size_t from, size_t to)
+{
+    double *H = s->d_Hbuf[s->d_hsel], *Hn = s->d_Hbuf[1 - s->d_hsel];
+    H[to] = H[from];
+    Hn[to] = Hn[from];
+    for (int c = 0; c < 3; ++c) {
+        s->d_V[3 * to + c] = s->d_V[3 * from + c];
+        s->d_dH[3 * to + c] = s->d_dH[3 * from + c];
+        s->d_T[3 * to + c] = s->d_T[3 * from + c];
+    }
+    s->d_K[to] = s->d_K[from];
+    s->d_Ss[to] = s->d_Ss[from];
+    s->d_W[to] = s->d_W[from];
+    s->d_phi[to] = s->d_phi[from];
+    s->d_dphi[to] = s->d_dphi[from];
+}
+
+/* setDarcyGhostNodesDev, src/darcy.cuh:169-261: a boundary node is copied
+ * onto the ghost node on the opposite side of the grid (faces only) */
+static void darcy_ghosts(orc_scene *s, uint32_t x, uint32_t y, uint32_t z)
+{
+    const int nx = (int)s->num[0], ny = (int)s->num[1], nz = (int)s->num[2];
+    const int X = (int)x, Y = (int)y, Z = (int)z;
+    const size_t me = d_idx(s, X, Y, Z);
+    if (X == 0) darcy_copy_node(s, me, d_idx(s, nx, Y, Z));
+    if (X == nx - 1) darcy_copy_node(s, me, d_idx(s, -1, Y, Z));
+    if (Y == 0) darcy_copy_node(s, me, d_idx(s, X, ny, Z));
+    if (Y == ny - 1) darcy_copy_node(s, me, d_idx(s, X, -1, Z));
+    if (Z == 0) darcy_copy_node(s, me, d_idx(s, X, Y, nz));
+    if (Z == nz - 1) darcy_copy_node(s, me, d_idx(s, X, Y, -1));
+}
+
+static inline double d_hmean(double a, double b) { return (2.0 * a * b) / (a + b); }
+
+/* explDarcyStepDev, src/darcy.cuh:604-725: explicit finite-difference step
+ * of the pressure into H_new, with zero flux through the z faces */
+static void darcy_explicit(orc_scene *s, uint32_t x, uint32_t y, uint32_t z)
+{
+    const uint32_t nz = s->num[2];
+    const double dx = s->L[0] / s->num[0], dy = s->L[1] / s->num[1], dz = s->L[2] / s->num[2];
+    const int X = (int)x, Y = (int)y, Z = (int)z;
+    const double *H = s->d_Hbuf[s->d_hsel];
+    double *Hn = s->d_Hbuf[1 - s->d_hsel];
+    const double *T = s->d_T;
+    const size_t me = d_idx(s, X, Y, Z);
+    const size_t xn = d_idx(s, X - 1, Y, Z), xp = d_idx(s, X + 1, Y, Z);
+    const size_t yn = d_idx(s, X, Y - 1, Z), yp = d_idx(s, X, Y + 1, Z);
+    const size_t zn = d_idx(s, X, Y, Z - 1), zp = d_idx(s, X, Y, Z + 1);
+    const double Ss = s->d_Ss[me], Q = s->d_W[me], dphi = s->d_dphi[me], Hc = H[me];
+    const double TdH_xn = d_hmean(T[3 * me + 0], T[3 * xn + 0]) * (H[xn] - Hc) / (dx * dx);
+    const double TdH_xp = d_hmean(T[3 * me + 0], T[3 * xp + 0]) * (H[xp] - Hc) / (dx * dx);
+    const double TdH_yn = d_hmean(T[3 * me + 1], T[3 * yn + 1]) * (H[yn] - Hc) / (dy * dy);
+    const double TdH_yp = d_hmean(T[3 * me + 1], T[3 * yp + 1]) * (H[yp] - Hc) / (dy * dy);
+    double TdH_zn = d_hmean(T[3 * me + 2], T[3 * zn + 2]) * (H[zn] - Hc) / (dz * dz);
+    double TdH_zp = d_hmean(T[3 * me + 2], T[3 * zp + 2]) * (H[zp] - Hc) / (dz * dz);
+    const double dx_bar = (dx + dy + dz) / 3.0;
+    if (z == 0) TdH_zn = 0.0;
+    if (z == nz - 1) TdH_zp = 0.0;
+    const double laplacianH = TdH_xn + TdH_xp + TdH_yn + TdH_yp + TdH_zn + TdH_zp;
+    const double porevol = -dx_bar * dphi / s->dt;
+    const double deltaH = s->dt / (Ss * dx * dy * dz) * (laplacianH + Q + porevol);
+    Hn[me] = fmax(0.0, Hc + deltaH);
+}
+
+/* findDarcyGradientsDev + findDarcyVelocitiesDev, src/darcy.cuh:541-598 and
+ * 728-776: central-difference pressure gradient (after the swap, so from the
+ * new pressure and the ghost values set before the step), flux -K/nu dH and
+ * the pore velocity flux / phi */
+static void darcy_grad_vel(orc_scene *s, uint32_t x, uint32_t y, uint32_t z)
+{
+    const double dx = s->L[0] / s->num[0], dy = s->L[1] / s->num[1], dz = s->L[2] / s->num[2];
+    const int X = (int)x, Y = (int)y, Z = (int)z;
+    const double *H = s->d_Hbuf[s->d_hsel];
+    const size_t me = d_idx(s, X, Y, Z);
+    const double gx = (H[d_idx(s, X + 1, Y, Z)] - H[d_idx(s, X - 1, Y, Z)]) / (2.0 * dx);
+    const double gy = (H[d_idx(s, X, Y + 1, Z)] - H[d_idx(s, X, Y - 1, Z)]) / (2.0 * dy);
+    const double gz = (H[d_idx(s, X, Y, Z + 1)] - H[d_idx(s, X, Y, Z - 1)]) / (2.0 * dz);
+    s->d_dH[3 * me + 0] = gx;
+    s->d_dH[3 * me + 1] = gy;
+    s->d_dH[3 * me + 2] = gz;
+    const double nu = s->nu, K = s->d_K[me], phi = s->d_phi[me];
+    const double qx = -K / nu * gx, qy = -K / nu * gy, qz = -K / nu * gz;
+    s->d_V[3 * me + 0] = qx / phi;
+    s->d_V[3 * me + 1] = qy / phi;
+    s->d_V[3 * me + 2] = qz / phi;
+}
+
+/* the Darcy block of one step, src/device.cu:913-1021 */
+static void darcy_step(orc_scene *s, const work_t *w, int nt)
+{
+    const int64_t nx = s->num[0], ny = s->num[1], nz = s->num[2], n = nx * ny * nz;
+#pragma omp parallel for num_threads(nt) schedule(dynamic, 64)
+    for (int64_t i = 0; i < n; ++i)
+        darcy_porosity(s, w, (uint32_t)(i % nx), (uint32_t)(i / nx % ny), (uint32_t)(i / (nx * ny)));
+    for (int64_t i = 0; i < n; ++i)
+        darcy_transmissivity(s, (uint32_t)(i % nx), (uint32_t)(i / nx % ny), (uint32_t)(i / (nx * ny)));
+    for (int64_t i = 0; i < n; ++i)
+        darcy_ghosts(s, (uint32_t)(i % nx), (uint32_t)(i / nx % ny), (uint32_t)(i / (nx * ny)));
+    for (int64_t i = 0; i < n; ++i)
+        darcy_explicit(s, (uint32_t)(i % nx), (uint32_t)(i / nx % ny), (uint32_t)(i / (nx * ny)));
+    s->d_hsel ^= 1u;
+    for (int64_t i = 0; i < n; ++i)
+        darcy_grad_vel(s, (uint32_t)(i % nx), (uint32_t)(i / nx % ny), (uint32_t)(i / (nx * ny)));
+}
+
 int orc_kind(void) { return 1; }
 
 int orc_threads(int nthreads)
@@ -784,10 +965,12 @@ int orc_step(orc_scene *s, uint64_t nsteps, int nthreads)
         for (int64_t a = 0; a < (int64_t)s->np; ++a) e_int |= interact_one(s, &w, (uint32_t)a);
         err |= e_int;
         for (uint32_t b = 0; b < s->nb0; ++b) bond_one(s, b);
+        if (s->darcy == 1 && s->nu > 0.0) darcy_step(s, &w, nt);
 #pragma omp parallel for num_threads(nt) schedule(static)
         for (int64_t k = 0; k < (int64_t)s->np; ++k) integrate_one(s, &w, (uint32_t)k);
         integrate_walls(s, &w, s->t_current);
         s->t_current += s->dt;
+        s->iteration++;
     }
     if (s->wall0_force) memcpy(s->wall0_force, w.wf_pp, sizeof(double) * s->np);
     work_free(&w);

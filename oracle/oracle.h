@@ -63,6 +63,21 @@ typedef struct orc_scene {
     uint32_t *cell_sorted, *perm, *cell_start, *cell_end;
     /* wall-0 force of every particle in the most recent step (np) */
     double *wall0_force;
+    /* Darcy flow (src/darcy.cuh:169-779, launched at src/device.cu:913-1021
+     * between bondsLinear and integrate), run when darcy == 1 and nu > 0.
+     * The fluid grid is the cell grid with one ghost node on every side:
+     * (num[0]+2)(num[1]+2)(num[2]+2) nodes, x fastest, node (x,y,z) at
+     * (x+1) + (num[0]+2)(y+1) + (num[0]+2)(num[1]+2)(z+1).  The pressure
+     * has two buffers, H = d_Hbuf[d_hsel] and H_new = d_Hbuf[1 - d_hsel];
+     * each step swaps them (d_hsel ^= 1), as the reference swaps pointers. */
+    double nu;
+    int32_t darcy;
+    uint32_t iteration;     /* steps since the run started: at 0 the porosity change is zero */
+    double d_factor;        /* grain-size factor of the Kozeny-Carman relation */
+    double *d_Hbuf[2];
+    uint32_t d_hsel;
+    double *d_V, *d_dH, *d_T;                 /* 3 doubles per node */
+    double *d_K, *d_Ss, *d_W, *d_phi, *d_dphi;
 } orc_scene;
 
 /* Advance the scene by nsteps time steps.  nthreads <= 0 uses the OpenMP

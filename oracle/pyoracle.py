@@ -48,6 +48,10 @@ class OrcScene(C.Structure):
         ("walls_nx", _dp), ("walls_mvfd", _dp), ("walls_vel0", _dp),
         ("cell_sorted", _up), ("perm", _up), ("cell_start", _up), ("cell_end", _up),
         ("wall0_force", _dp),
+        ("nu", C.c_double), ("darcy", C.c_int32), ("iteration", C.c_uint32),
+        ("d_factor", C.c_double), ("d_Hbuf", _dp * 2), ("d_hsel", C.c_uint32),
+        ("d_V", _dp), ("d_dH", _dp), ("d_T", _dp),
+        ("d_K", _dp), ("d_Ss", _dp), ("d_W", _dp), ("d_phi", _dp), ("d_dphi", _dp),
     ]
 
 
@@ -73,9 +77,13 @@ def load(kind: str = "orc"):
 
 
 class OracleRun:
-    """Owns the scratch/output arrays of one oracle scene."""
+    """Owns the scratch/output arrays of one oracle scene.  With ``darcy`` (a
+    ``sphere_b200.darcy.DarcyState``), each step also runs the Darcy flow
+    block with dynamic viscosity ``nu`` and grain-size factor ``d_factor``;
+    the state's arrays are updated in place (``H``/``H_new`` swap roles as
+    the reference swaps its pointers)."""
 
-    def __init__(self, lib, cfg, st):
+    def __init__(self, lib, cfg, st, darcy=None, nu=0.0, d_factor=0.0):
         self.lib, self.cfg, self.st = lib, cfg, st
         n = cfg.np
         self.cell_sorted = np.zeros(n, np.uint32)
@@ -106,7 +114,19 @@ class OracleRun:
         s.cell_start = self._ptr(self.cell_start, np.uint32)
         s.cell_end = self._ptr(self.cell_end, np.uint32)
         s.wall0_force = self._ptr(self.wall0_force, np.float64)
+        self.darcy = darcy
+        if darcy is not None:
+            s.darcy, s.nu, s.d_factor, s.iteration = 1, float(nu), float(d_factor), 0
+            for name in ("V", "dH", "T", "K", "Ss", "W", "phi", "dphi"):
+                setattr(s, "d_" + name, self._ptr(getattr(darcy, name), np.float64))
+            self._bind_pressure(s)
         self.scene = s
+
+    def _bind_pressure(self, s=None):
+        s = s if s is not None else self.scene
+        s.d_Hbuf[0] = self._ptr(self.darcy.H, np.float64)
+        s.d_Hbuf[1] = self._ptr(self.darcy.H_new, np.float64)
+        s.d_hsel = 0
 
     def _ptr(self, a, dtype):
         assert a.dtype == dtype and a.flags.c_contiguous, (a.dtype, a.flags)
@@ -119,4 +139,7 @@ class OracleRun:
         self.scene.t_current = self.st.t_current
         rc = self.lib.orc_step(C.byref(self.scene), nsteps, nthreads)
         self.st.t_current = self.scene.t_current
+        if self.darcy is not None and self.scene.d_hsel == 1:
+            self.darcy.H, self.darcy.H_new = self.darcy.H_new, self.darcy.H
+            self._bind_pressure()
         return rc

@@ -22,6 +22,7 @@
 #include "contactmodels.cuh"
 #include "cohesion.cuh"
 #include "contactsearch.cuh"
+#include "darcy.cuh"
 
 #include "oracle.h"
 
@@ -74,6 +75,18 @@ static void summation_same_order(const Float *in, Float *out, unsigned int np,
     }
 }
 
+/* src/darcy.cuh also holds DEM's Darcy memory-transfer methods, which the
+ * harness never calls; these stand-ins resolve the CUDA runtime and utility
+ * symbols they name, and stay private to this library. */
+#define REF_HIDDEN __attribute__((visibility("hidden")))
+extern "C" REF_HIDDEN cudaError_t cudaMalloc(void **, size_t) { return cudaErrorNotSupported; }
+extern "C" REF_HIDDEN cudaError_t cudaFree(void *) { return cudaErrorNotSupported; }
+extern "C" REF_HIDDEN cudaError_t cudaMemcpy(void *, const void *, size_t, cudaMemcpyKind)
+{
+    return cudaErrorNotSupported;
+}
+REF_HIDDEN void checkForCudaErrors(const char *) {}
+
 extern "C" int orc_kind(void) { return 2; }
 
 extern "C" int orc_threads(int nthreads)
@@ -90,6 +103,13 @@ static inline void launch1(unsigned int i)
 {
     blockIdx.x = i;
     threadIdx.x = 0;
+}
+
+/* one-thread block (x, y, z) of a 3-D launch */
+static inline void launch3(unsigned int x, unsigned int y, unsigned int z)
+{
+    blockIdx.x = x; blockIdx.y = y; blockIdx.z = z;
+    threadIdx.x = 0; threadIdx.y = 0; threadIdx.z = 0;
 }
 
 extern "C" int orc_step(orc_scene *s, uint64_t nsteps, int nthreads)
@@ -125,7 +145,7 @@ extern "C" int orc_step(orc_scene *s, uint64_t nsteps, int nthreads)
     P.kappa = s->kappa; P.db = s->db; P.V_b = s->V_b;
     P.lambda_bar = s->lambda_bar; P.nb0 = s->nb0;
     P.sigma_b = s->sigma_b; P.tau_b = s->tau_b;
-    P.devs_A = s->devs_A; P.devs_f = s->devs_f; P.nu = 0.0;
+    P.devs_A = s->devs_A; P.devs_f = s->devs_f; P.nu = s->nu;
 
     /* The host build cannot reproduce the device's saturating conversion of
      * floor(negative) (src/sorting.cuh:12-14), and a cell id past the grid
@@ -206,6 +226,49 @@ extern "C" int orc_step(orc_scene *s, uint64_t nsteps, int nthreads)
             }
             gridDim = dim3(np, 1, 1);
         }
+        if (s->darcy == 1 && s->nu > 0.0) {
+            /* src/device.cu:913-1021: one-thread blocks over the fluid grid */
+            const unsigned int fx = s->num[0], fy = s->num[1], fz = s->num[2];
+            const long nfl = (long)fx * fy * fz;
+            blockDim = dim3(1, 1, 1);
+            gridDim = dim3(fx, fy, fz);
+            Float *H = s->d_Hbuf[s->d_hsel], *Hn = s->d_Hbuf[1 - s->d_hsel];
+            Float3 *V = (Float3 *)s->d_V, *dH = (Float3 *)s->d_dH, *T = (Float3 *)s->d_T;
+            auto at = [&](long i) {
+                launch3((unsigned int)(i % fx), (unsigned int)(i / fx % fy),
+                        (unsigned int)(i / ((long)fx * fy)));
+            };
+#pragma omp parallel for num_threads(nt) schedule(dynamic, 64)
+            for (long i = 0; i < nfl; ++i) {
+                at(i);
+                findPorositiesSphericalDev(s->cell_start, s->cell_end, x_sorted.data(), s->d_phi,
+                                           s->d_dphi, s->iteration);
+            }
+            for (long i = 0; i < nfl; ++i) {
+                at(i);
+                findDarcyTransmissivitiesDev(s->d_K, T, s->d_phi, s->d_factor);
+            }
+            for (long i = 0; i < nfl; ++i) {
+                at(i);
+                setDarcyGhostNodesDev(H, Hn, V, dH, s->d_K, T, s->d_Ss, s->d_W, s->d_phi,
+                                      s->d_dphi);
+            }
+            for (long i = 0; i < nfl; ++i) {
+                at(i);
+                explDarcyStepDev(H, Hn, T, s->d_Ss, s->d_W, s->d_dphi);
+            }
+            s->d_hsel ^= 1u;   /* the pointer swap of src/device.cu:991-994 */
+            std::swap(H, Hn);
+            for (long i = 0; i < nfl; ++i) {
+                at(i);
+                findDarcyGradientsDev(H, dH);
+            }
+            for (long i = 0; i < nfl; ++i) {
+                at(i);
+                findDarcyVelocitiesDev(H, dH, V, s->d_phi, s->d_K);
+            }
+            gridDim = dim3(np, 1, 1);
+        }
 #pragma omp parallel for num_threads(nt) schedule(static)
         for (long i = 0; i < (long)np; ++i)
             ref_integrate_one(x_sorted.data(), vel_sorted.data(), angvel_sorted.data(), x, vel,
@@ -220,6 +283,7 @@ extern "C" int orc_step(orc_scene *s, uint64_t nsteps, int nthreads)
                                 s->walls_vel0, nblocks, s->t_current, s->nw);
         }
         s->t_current += s->dt;
+        s->iteration++;
     }
     for (unsigned int i = 0; i < np; ++i) { s->cell_sorted[i] = cellid[i]; s->perm[i] = index[i]; }
     if (s->wall0_force) memcpy(s->wall0_force, walls_force_pp.data(), sizeof(double) * np);

@@ -22,6 +22,7 @@ void launch_rebuild(const Dev &d, uint32_t np, uint32_t ncells, int a, cudaStrea
 unsigned int scan_tile_count(uint32_t ncells);
 void relayout(const Dev &d, uint32_t np, int a, void *scratch, cudaStream_t st);
 void launch_rebuild_gate(cudaGraphConditionalHandle h, const uint32_t *rebuild, cudaStream_t st);
+void launch_darcy(const Dev &d, const DarcyDev &f, const Params &hp, int a, int hs, cudaStream_t st);
 void launch_force_tape(const Dev &d, uint32_t np, int a, int tape_step, cudaStream_t st);
 void launch_rev_step(const Dev &d, const AdjDev &a, uint32_t np, int j, cudaStream_t st);
 void launch_user_to_storage3(const double *src, double4 *dst, const uint32_t *uid, uint32_t n,
@@ -64,7 +65,7 @@ struct sph_ctx {
     int sticky = SPH_OK;
     // profile mode: events bracket each phase of each step
     bool profile = false;
-    std::vector<cudaEvent_t> ev;          // 5 events per profiled step
+    std::vector<cudaEvent_t> ev;          // SPH_NPHASES + 1 events per profiled step
     double prof_ms[SPH_NPHASES] = {};
     uint64_t prof_steps = 0;
     // differentiable mode: checkpoints every ckpt_every steps since
@@ -82,6 +83,12 @@ struct sph_ctx {
     // checkpoint buffers handed back by sph_diff_end and the backward, kept
     // for the next forward of a calibration loop; freed by sph_destroy
     std::vector<char *> ckpt_pool;
+    // Darcy flow, on after sph_darcy_upload; the current pressure buffer is
+    // darcy.H[a ^ dflip] (both flip once per step)
+    bool darcy_on = false;
+    DarcyDev darcy{};
+    int dflip = 0;
+    double mean_radius = 0.0;        // of the uploaded particles, summed in caller order
     size_t ckpt_bytes = 0;                // size of one pooled buffer
     cudaEvent_t ckpt_ev = nullptr;        // orders a checkpoint copy against the caller's stream
     std::vector<void *> diff_allocs;
@@ -263,6 +270,9 @@ int enqueue_one_step(sph_ctx *c, int a, int write_outputs, cudaStream_t st, bool
     }
     launch_bonds(c->d, c->hp.nb0, a, st);
     launch_step(c->d, c->np_all, (int)c->hp.contactmodel, a, write_outputs, st);
+    // the Darcy block reads the step's start positions (buffer a) and its
+    // cell list, neither of which the force kernel changes
+    if (c->darcy_on) launch_darcy(c->d, c->darcy, c->hp, a, a ^ c->dflip, st);
     launch_walls(c->d, c->np_all, c->hp.nw, st);
     return SPH_OK;
 }
@@ -340,8 +350,10 @@ int profiled_step(sph_ctx *c, int a, int write_outputs, cudaStream_t st)
     CK(cudaEventRecord(c->ev[4], st));
     launch_walls(c->d, c->np_all, c->hp.nw, st);
     CK(cudaEventRecord(c->ev[5], st));
+    if (c->darcy_on) launch_darcy(c->d, c->darcy, c->hp, a, a ^ c->dflip, st);
+    CK(cudaEventRecord(c->ev[6], st));
     CK(cudaGetLastError());
-    CK(cudaEventSynchronize(c->ev[5]));
+    CK(cudaEventSynchronize(c->ev[6]));
     for (int k = 0; k < SPH_NPHASES; ++k) {
         float ms = 0.f;
         CK(cudaEventElapsedTime(&ms, c->ev[k], c->ev[k + 1]));
@@ -569,7 +581,17 @@ int sph_upload(sph_ctx *c, const sph_host_state *h)
     const size_t np = c->np_all, nb0 = P.nb0;
     Dev &d = c->d;
     const int A = 0;
+    // the Darcy pressure buffers keep their roles across the parity reset;
+    // graphs hold the buffer of each step, so they are captured again
+    if (c->darcy_on && c->a != A) drop_graphs(c);
+    c->dflip ^= c->a ^ A;
     c->a = A;
+    {
+        // meanRadius (src/darcy.cpp:646-653) for the Darcy grain-size factor
+        double r_sum = 0.0;
+        for (size_t i = 0; i < np; ++i) r_sum += h->x[4 * i + 3];
+        c->mean_radius = r_sum / (double)np;
+    }
     // scene of every particle (particles of scene i follow those of scene i-1)
     std::vector<uint32_t> inst_of(np, 0u);
     for (uint32_t i = 0; i < c->ninst; ++i)
@@ -1176,10 +1198,10 @@ int sph_diff_begin(sph_ctx *c, const double *mu, uint32_t checkpoint_every)
     if (!c || !c->uploaded) return fail(c, SPH_ERR_BAD_INPUT, "sph_diff_begin before sph_upload");
     if (c->diff) return fail(c, SPH_ERR_BAD_INPUT, "sph_diff_begin: already in differentiable mode");
     const Params &P = c->hp;
-    if (c->batched || P.contactmodel != 2 || P.nw != 0 || P.nb0 != 0)
+    if (c->batched || P.contactmodel != 2 || P.nw != 0 || P.nb0 != 0 || c->darcy_on)
         return fail(c, SPH_ERR_BAD_INPUT,
                     "the differentiable step takes one scene with contact model 2, no dynamic "
-                    "walls and no bonds");
+                    "walls, no bonds and no Darcy flow");
     if (checkpoint_every == 0) return fail(c, SPH_ERR_BAD_INPUT, "checkpoint_every must be >= 1");
     CK(cudaSetDevice(c->device));
     CK(cudaDeviceSynchronize());
@@ -1293,6 +1315,68 @@ int sph_diff_end(sph_ctx *c)
     drop_graphs(c);
     c->diff = false;
     c->relayout_every = c->relayout_saved;
+    return SPH_OK;
+}
+
+int sph_darcy_upload(sph_ctx *c, double nu, const sph_darcy_state *h)
+{
+    if (!c || !c->uploaded) return fail(c, SPH_ERR_BAD_INPUT, "sph_darcy_upload before sph_upload");
+    if (c->batched || c->diff)
+        return fail(c, SPH_ERR_BAD_INPUT, "Darcy flow needs a plain (not batched or differentiable) context");
+    if (!(nu > 0.0)) return fail(c, SPH_ERR_BAD_INPUT, "Darcy flow needs a dynamic viscosity nu > 0");
+    if (!h || !h->H || !h->H_new || !h->V || !h->dH || !h->K || !h->T || !h->Ss || !h->W || !h->phi ||
+        !h->dphi)
+        return fail(c, SPH_ERR_BAD_INPUT, "sph_darcy_upload: missing array");
+    CK(cudaSetDevice(c->device));
+    CK(cudaStreamSynchronize(c->stream));
+    const size_t n = (size_t)(c->hp.num[0] + 2) * (c->hp.num[1] + 2) * (c->hp.num[2] + 2);
+    DarcyDev &f = c->darcy;
+    int rc;
+    if (!f.first) {
+        if ((rc = dalloc(c, &f.H[0], n)) || (rc = dalloc(c, &f.H[1], n)) ||
+            (rc = dalloc(c, &f.V, 3 * n)) || (rc = dalloc(c, &f.dH, 3 * n)) ||
+            (rc = dalloc(c, &f.K, n)) || (rc = dalloc(c, &f.T, 3 * n)) ||
+            (rc = dalloc(c, &f.Ss, n)) || (rc = dalloc(c, &f.W, n)) ||
+            (rc = dalloc(c, &f.phi, n)) || (rc = dalloc(c, &f.dphi, n)) ||
+            (rc = dalloc(c, &f.first, 1)))
+            return rc;
+    }
+    // the uploaded pressure is the current one for the context's parity
+    c->dflip = c->a;
+    const std::pair<double *, const double *> one[] = {
+        {f.H[0], h->H}, {f.H[1], h->H_new}, {f.K, h->K}, {f.Ss, h->Ss},
+        {f.W, h->W},    {f.phi, h->phi},    {f.dphi, h->dphi}};
+    for (const auto &p : one) CK(cudaMemcpy(p.first, p.second, n * 8, cudaMemcpyHostToDevice));
+    const std::pair<double *, const double *> three[] = {{f.V, h->V}, {f.dH, h->dH}, {f.T, h->T}};
+    for (const auto &p : three) CK(cudaMemcpy(p.first, p.second, 3 * n * 8, cudaMemcpyHostToDevice));
+    const uint32_t one_u = 1u;
+    CK(cudaMemcpy(f.first, &one_u, 4, cudaMemcpyHostToDevice));
+    f.nu = nu;
+    // src/device.cu:673-678
+    const double r_bar2 = c->mean_radius * 2.0;
+    f.d_factor = r_bar2 * r_bar2 / 180.0 * 1.0e-6;
+    c->darcy_on = true;
+    drop_graphs(c);   // the step graphs gain the Darcy kernels
+    return SPH_OK;
+}
+
+int sph_darcy_download(sph_ctx *c, sph_darcy_state *h)
+{
+    if (!c || !c->darcy_on) return fail(c, SPH_ERR_BAD_INPUT, "sph_darcy_download without sph_darcy_upload");
+    if (!h) return fail(c, SPH_ERR_BAD_INPUT, "sph_darcy_download: null state");
+    CK(cudaSetDevice(c->device));
+    CK(cudaStreamSynchronize(c->stream));
+    const size_t n = (size_t)(c->hp.num[0] + 2) * (c->hp.num[1] + 2) * (c->hp.num[2] + 2);
+    const DarcyDev &f = c->darcy;
+    const int hs = c->a ^ c->dflip;
+    const std::pair<double *, const double *> one[] = {
+        {h->H, f.H[hs]}, {h->H_new, f.H[hs ^ 1]}, {h->K, f.K},      {h->Ss, f.Ss},
+        {h->W, f.W},     {h->phi, f.phi},         {h->dphi, f.dphi}};
+    for (const auto &p : one)
+        if (p.first) CK(cudaMemcpy(p.first, p.second, n * 8, cudaMemcpyDeviceToHost));
+    const std::pair<double *, const double *> three[] = {{h->V, f.V}, {h->dH, f.dH}, {h->T, f.T}};
+    for (const auto &p : three)
+        if (p.first) CK(cudaMemcpy(p.first, p.second, 3 * n * 8, cudaMemcpyDeviceToHost));
     return SPH_OK;
 }
 

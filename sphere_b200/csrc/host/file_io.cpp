@@ -11,7 +11,9 @@
 //   (m, vel, force, devs) per wall, devs_A, devs_f f64;
 //   lambda_bar f64, nb0 u32, sigma_b, tau_b f64, bonds (u32,u32)*nb0,
 //   delta_n[nb0], delta_t[nb0][3], omega_n[nb0], omega_t[nb0][3] f64; nu f64;
-//   fluid cells when nu > 0 (kept as opaque bytes here).
+//   fluid cells when nu > 0: with Darcy flow, per cell (x fastest, then y,
+//   then z) V[3], H, phi, K f64 (src/file_io.cpp:270-292, 466-479); without
+//   it, kept as opaque bytes.
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -139,7 +141,21 @@ void DEM::readbin(const char *target)
     for (size_t b = 0; b < nb; ++b)
         for (int k = 0; k < 3; ++k) bonds_omega_[4 * b + k] = in.get<double>();
     nu_ = in.get<double>();
-    fluid_trailer_.assign(in.buf.begin() + (std::ptrdiff_t)in.off, in.buf.end());
+    fluid_trailer_.clear();
+    if (darcyOn()) {
+        initDarcyMem();
+        for (uint32_t z = 0; z < cfg_.num[2]; ++z)
+            for (uint32_t y = 0; y < cfg_.num[1]; ++y)
+                for (uint32_t x = 0; x < cfg_.num[0]; ++x) {
+                    const size_t i = darcyNode((int)x, (int)y, (int)z);
+                    for (int k = 0; k < 3; ++k) d_V_[3 * i + k] = in.get<double>();
+                    d_H_[i] = in.get<double>();
+                    d_phi_[i] = in.get<double>();
+                    d_K_[i] = in.get<double>();
+                }
+    } else {
+        fluid_trailer_.assign(in.buf.begin() + (std::ptrdiff_t)in.off, in.buf.end());
+    }
 }
 
 void DEM::writebin(const char *target)
@@ -198,5 +214,17 @@ void DEM::writebin(const char *target)
     for (size_t b = 0; b < nb; ++b)
         for (int k = 0; k < 3; ++k) o.put(bonds_omega_[4 * b + k]);
     o.put(nu_);
-    if (!fluid_trailer_.empty()) ofs.write(fluid_trailer_.data(), (std::streamsize)fluid_trailer_.size());
+    if (darcyOn()) {
+        for (uint32_t z = 0; z < cfg_.num[2]; ++z)
+            for (uint32_t y = 0; y < cfg_.num[1]; ++y)
+                for (uint32_t x = 0; x < cfg_.num[0]; ++x) {
+                    const size_t i = darcyNode((int)x, (int)y, (int)z);
+                    for (int k = 0; k < 3; ++k) o.put(d_V_[3 * i + k]);
+                    o.put(d_H_[i]);
+                    o.put(d_phi_[i]);
+                    o.put(d_K_[i]);
+                }
+    } else if (!fluid_trailer_.empty()) {
+        ofs.write(fluid_trailer_.data(), (std::streamsize)fluid_trailer_.size());
+    }
 }

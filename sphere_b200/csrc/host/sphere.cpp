@@ -37,7 +37,91 @@ DEM::DEM(std::string inputbin, const int verbosity, const int checkVals, const i
         reportValues();
         exit(0);
     }
+    if (darcyOn()) initDarcy();   // src/sphere.cpp:52-54
     if (initCuda == 1) initDevice();
+}
+
+// ---- Darcy flow: the host side of src/darcy.cpp -----------------------------
+
+size_t DEM::darcyNode(int x, int y, int z) const
+{
+    const size_t nx2 = (size_t)cfg_.num[0] + 2, ny2 = (size_t)cfg_.num[1] + 2;
+    return (size_t)(x + 1) + nx2 * (size_t)(y + 1) + nx2 * ny2 * (size_t)(z + 1);
+}
+
+// initDarcyMem (src/darcy.cpp:17-38) with the cell grid; the values the
+// reference leaves unset are zero here
+void DEM::initDarcyMem()
+{
+    const size_t n = (size_t)(cfg_.num[0] + 2) * (cfg_.num[1] + 2) * (cfg_.num[2] + 2);
+    for (auto *v : {&d_H_, &d_H_new_, &d_K_, &d_Ss_, &d_W_, &d_phi_, &d_dphi_}) v->assign(n, 0.0);
+    for (auto *v : {&d_V_, &d_dH_, &d_T_}) v->assign(3 * n, 0.0);
+}
+
+sph_darcy_state DEM::darcyState()
+{
+    sph_darcy_state s{};
+    s.H = d_H_.data();
+    s.H_new = d_H_new_.data();
+    s.V = d_V_.data();
+    s.dH = d_dH_.data();
+    s.K = d_K_.data();
+    s.T = d_T_.data();
+    s.Ss = d_Ss_.data();
+    s.W = d_W_.data();
+    s.phi = d_phi_.data();
+    s.dphi = d_dphi_.data();
+    return s;
+}
+
+// initDarcy (src/darcy.cpp:760-798)
+void DEM::initDarcy()
+{
+    const double dx = cfg_.L[0] / cfg_.num[0], dy = cfg_.L[1] / cfg_.num[1],
+                 dz = cfg_.L[2] / cfg_.num[2];
+    if (verbose_ == 1) {
+        std::cout << "  - Fluid grid dimensions: " << cfg_.num[0] << "*" << cfg_.num[1] << "*"
+                  << cfg_.num[2] << std::endl;
+        std::cout << "  - Fluid grid cell size: " << dx << "*" << dy << "*" << dz << std::endl;
+    }
+    sph_darcy_state s = darcyState();
+    double value = 0.0;
+    const int rc = sph_darcy_init(&cfg_, nu_, x_.data(), &s, &value);
+    if (rc == SPH_ERR_UNSTABLE) {
+        std::cerr << "Error! The explicit Darcy solution will be unstable.\n"
+                  << " Reason: (" << value << " > 0.5)" << std::endl;
+        exit(1);
+    }
+    if (rc != SPH_OK) {
+        std::cerr << "Error in initDarcy. The dynamic viscosity (params.nu) should be larger "
+                     "than 0.0, but is "
+                  << nu_ << std::endl;
+        exit(1);
+    }
+}
+
+// endDarcy (src/darcy.cpp:826-836): porosity and conductivity of every cell
+// as text, as printDarcyArray lays them out (src/darcy.cpp:483-495)
+void DEM::endDarcy()
+{
+    const std::pair<const char *, const std::vector<double> *> out[] = {{"d_phi.txt", &d_phi_},
+                                                                       {"d_K.txt", &d_K_}};
+    for (const auto &o : out) {
+        FILE *f = fopen(o.first, "w");
+        if (!f) {
+            fprintf(stderr, "Error, could not open %s.\n", o.first);
+            continue;
+        }
+        for (uint32_t z = 0; z < cfg_.num[2]; ++z) {
+            for (uint32_t y = 0; y < cfg_.num[1]; ++y) {
+                for (uint32_t x = 0; x < cfg_.num[0]; ++x)
+                    fprintf(f, "%f\t", (*o.second)[darcyNode((int)x, (int)y, (int)z)]);
+                fprintf(f, "\n");
+            }
+            fprintf(f, "\n");
+        }
+        fclose(f);
+    }
 }
 
 DEM::~DEM()
@@ -84,10 +168,9 @@ sph_host_state DEM::hostState()
 
 void DEM::initDevice()
 {
-    if (nu_ > 0.0) {
-        std::cerr << "Error: fluid coupling (nu > 0, "
-                  << (darcy_ ? "Darcy" : "lattice-Boltzmann")
-                  << ") is not part of this DEM step implementation." << std::endl;
+    if (nu_ > 0.0 && !darcyOn()) {
+        std::cerr << "Error: the lattice-Boltzmann fluid coupling (nu > 0 without Darcy flow) "
+                     "is not part of this DEM step implementation." << std::endl;
         exit(1);
     }
     cfg_.device = 0;
@@ -100,16 +183,26 @@ void DEM::initDevice()
 void DEM::upload()
 {
     sph_host_state h = hostState();
-    const int rc = sph_upload(ctx_, &h);
+    int rc = sph_upload(ctx_, &h);
     if (rc != SPH_OK) fail(rc, "sph_upload");
+    if (darcyOn()) {
+        sph_darcy_state s = darcyState();
+        rc = sph_darcy_upload(ctx_, nu_, &s);
+        if (rc != SPH_OK) fail(rc, "sph_darcy_upload");
+    }
     if (verbose_ == 1) std::cout << "  Transfering data to the device:                 Done\n";
 }
 
 void DEM::download()
 {
     sph_host_state h = hostState();
-    const int rc = sph_download(ctx_, &h);
+    int rc = sph_download(ctx_, &h);
     if (rc != SPH_OK) fail(rc, "sph_download");
+    if (darcyOn()) {
+        sph_darcy_state s = darcyState();
+        rc = sph_darcy_download(ctx_, &s);
+        if (rc != SPH_OK) fail(rc, "sph_darcy_download");
+    }
 }
 
 void DEM::checkValues()
@@ -286,6 +379,7 @@ void DEM::startTime()
                   << "  - Mean duration of iteration:\n"
                   << "      " << (iter ? secs / (double)iter : 0.0) << " s" << std::endl;
     }
+    if (darcyOn()) endDarcy();   // src/device.cu:1292-1297
 }
 
 void DEM::render(const int, const float, const float, const float, const unsigned int,

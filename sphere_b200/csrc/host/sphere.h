@@ -6,9 +6,12 @@
 // transferConstMem, darcyflow), readbin, writebin, checkValues,
 // reportValues, startTime, and the destructor.  The state is held in the
 // reference's host layout (Float4 rows, src/datatypes.h:17-33) and moved to
-// and from the device with sph_upload / sph_download.  The renderer, porosity,
-// force-chain and fluid (Darcy/LBM) members of the reference are not part of
-// this DEM step; render(), porosity() and forcechains() report that and exit.
+// and from the device with sph_upload / sph_download.  With darcyflow = 1 and
+// nu > 0 the Darcy flow runs with the step (src/darcy.cpp, src/darcy.cuh):
+// its grid is read from and written to the files' fluid section, set up by
+// sph_darcy_init and stepped on the device.  The lattice-Boltzmann coupling
+// (nu > 0 without darcyflow) and the porosity and force-chain tools are not
+// part of this build: they report that and exit.
 #ifndef SPHERE_B200_SPHERE_H_
 #define SPHERE_B200_SPHERE_H_
 
@@ -61,7 +64,16 @@ class DEM {
     std::vector<uint32_t> bonds_;
     std::vector<double> bonds_delta_, bonds_omega_;
     double nu_ = 0.0;
-    std::vector<char> fluid_trailer_;   // carried unchanged when nu > 0
+    std::vector<char> fluid_trailer_;   // carried unchanged when nu > 0 without Darcy flow
+
+    // Darcy grid (DEM::d, src/darcy.cpp:17-38): (num+2)^3 nodes with ghosts
+    std::vector<double> d_H_, d_H_new_, d_V_, d_dH_, d_K_, d_T_, d_Ss_, d_W_, d_phi_, d_dphi_;
+    bool darcyOn() const { return nu_ > 0.0 && darcy_ == 1; }
+    size_t darcyNode(int x, int y, int z) const;
+    void initDarcyMem();
+    void initDarcy();
+    void endDarcy();
+    sph_darcy_state darcyState();
 
     sph_ctx *ctx_ = nullptr;
 

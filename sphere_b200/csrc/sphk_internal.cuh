@@ -252,4 +252,17 @@ inline unsigned int div_up(unsigned long long a, unsigned int b)
     return (unsigned int)((a + b - 1) / b);
 }
 
+// Darcy flow state (src/darcy.cuh): the fluid grid is the cell grid with one
+// ghost node on every side, (num[0]+2)(num[1]+2)(num[2]+2) nodes, x fastest,
+// laid out as the reference's host arrays so that upload and download are
+// plain copies.  V, dH and T hold three doubles per node.
+struct DarcyDev {
+    double *H[2];          // pressure buffers; a step reads H[hs], writes H[hs ^ 1]
+    double *V, *dH, *T;
+    double *K, *Ss, *W, *phi, *dphi;
+    uint32_t *first;       // 1 until the first step after upload has run
+    double nu;             // dynamic viscosity
+    double d_factor;       // grain-size factor of the Kozeny-Carman relation
+};
+
 }  // namespace sphk

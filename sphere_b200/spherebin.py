@@ -17,8 +17,11 @@ Differences, all deliberate:
   * every random draw goes through a ``numpy.random.Generator`` passed in (or
     seeded) so scenes are reproducible;
   * ``__eq__`` replaces the Python-2 ``__cmp__`` (``python/sphere.py:142-215``);
-  * a fluid trailer (``nu > 0``) is kept as opaque bytes: fluid coupling is
-    outside this implementation.
+  * the fluid section (``nu > 0``) is read into ``f_v``, ``f_rho``, ``f_phi``
+    and ``f_K`` (per cell, shaped as ``python/sphere.py:388-410`` makes them)
+    when it holds the six values per cell that the Darcy flow writes
+    (``src/file_io.cpp:466-479``); any other fluid section (the
+    lattice-Boltzmann one) is kept as opaque bytes.
 """
 from __future__ import annotations
 
@@ -132,6 +135,7 @@ class Spherebin:
         self.bonds_omega_t = np.zeros((0, 3))
         self.nu = 0.0
         self.fluid_trailer = b""
+        self.f_v = self.f_rho = self.f_phi = self.f_K = None
 
     @property
     def nb0(self) -> int:
@@ -172,7 +176,19 @@ class Spherebin:
             np.asarray(self.bonds_omega_n, _F64), np.asarray(self.bonds_omega_t, _F64),
             np.array([self.nu], _F64),
         ]
-        return b"".join(np.ascontiguousarray(p).tobytes() for p in parts) + self.fluid_trailer
+        return b"".join(np.ascontiguousarray(p).tobytes() for p in parts) + self._fluid_bytes()
+
+    def _fluid_bytes(self) -> bytes:
+        """The fluid section: per cell, z outermost and x innermost, V[3], H
+        (``f_rho``), phi, K (``python/sphere.py:516-527``)."""
+        if self.nu > 0.0 and self.f_v is not None:
+            cells = np.concatenate([
+                np.asarray(self.f_v, _F64),
+                np.asarray(self.f_rho, _F64)[..., None],
+                np.asarray(self.f_phi, _F64)[..., None],
+                np.asarray(self.f_K, _F64)[..., None]], axis=3)        # (nx, ny, nz, 6)
+            return np.ascontiguousarray(cells.transpose(2, 1, 0, 3)).tobytes()
+        return self.fluid_trailer
 
     def writebin(self, folder="../input/", verbose=True, path=None):
         """Write ``<folder>/<sid>.bin`` (``python/sphere.py:416``)."""
@@ -233,6 +249,15 @@ class Spherebin:
         sb.bonds_omega_t = r.take(_F64, 3 * nb0).reshape(nb0, 3)
         sb.nu = float(r.take(_F64, 1)[0])
         sb.fluid_trailer = buf[r.off:]
+        nx, ny, nz = (int(v) for v in sb.num)
+        if sb.nu > 0.0 and len(sb.fluid_trailer) == 6 * 8 * nx * ny * nz:
+            cells = np.frombuffer(sb.fluid_trailer, _F64).reshape(nz, ny, nx, 6)
+            cells = cells.transpose(2, 1, 0, 3).copy()                 # [x, y, z, k]
+            sb.f_v = cells[..., 0:3].copy()
+            sb.f_rho = cells[..., 3].copy()
+            sb.f_phi = cells[..., 4].copy()
+            sb.f_K = cells[..., 5].copy()
+            sb.fluid_trailer = b""
         return sb
 
     def readbin(self, targetbin, verbose=True, **_ignored):

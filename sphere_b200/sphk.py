@@ -26,13 +26,13 @@ SPH_OK = 0
 ERRORS = {
     -1: "SPH_ERR_CUDA", -2: "SPH_ERR_NC_OVERFLOW", -3: "SPH_ERR_OUT_OF_GRID",
     -4: "SPH_ERR_TIMEOUT", -5: "SPH_ERR_BAD_INPUT", -6: "SPH_ERR_BOND_ALIAS", -7: "SPH_ERR_NOMEM",
-    -8: "SPH_ERR_TOO_LARGE",
+    -8: "SPH_ERR_TOO_LARGE", -9: "SPH_ERR_UNSTABLE",
 }
 OPT_RELAYOUT_EVERY = 1
 OPT_GRAPH_STEPS = 2
 OPT_PROFILE = 3
 OPT_VERLET_SKIN = 4
-PHASES = ("cells", "bonds", "topo", "force", "walls")
+PHASES = ("cells", "bonds", "topo", "force", "walls", "darcy")
 
 _dp = C.POINTER(C.c_double)
 _up = C.POINTER(C.c_uint32)
@@ -61,6 +61,10 @@ class SphHostState(C.Structure):
     _fields_ += [("contacts", _up), ("distmod", _dp), ("delta_t", _dp), ("bonds", _up),
                  ("bonds_delta", _dp), ("bonds_omega", _dp), ("walls_nx", _dp), ("walls_mvfd", _dp),
                  ("walls_vel0", _dp), ("t_current", C.c_double)]
+
+
+class SphDarcyState(C.Structure):
+    _fields_ = [(n, _dp) for n in ("H", "H_new", "V", "dH", "K", "T", "Ss", "W", "phi", "dphi")]
 
 
 class SphStats(C.Structure):
@@ -114,6 +118,10 @@ def load_library(path: os.PathLike | None = None):
         "sph_diff_begin": ([vp, _dp, C.c_uint32], C.c_int),
         "sph_diff_backward": ([vp, _dp, _dp, _dp, _dp, _dp, _dp], C.c_int),
         "sph_diff_end": ([vp], C.c_int),
+        "sph_darcy_init": ([C.POINTER(SphConfig), C.c_double, _dp, C.POINTER(SphDarcyState), _dp],
+                           C.c_int),
+        "sph_darcy_upload": ([vp, C.c_double, C.POINTER(SphDarcyState)], C.c_int),
+        "sph_darcy_download": ([vp, C.POINTER(SphDarcyState)], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)
@@ -160,6 +168,31 @@ def _host_struct(st: HostState, keep) -> SphHostState:
     h.bonds = _ptr(st.bonds, np.uint32, keep)
     h.t_current = float(st.t_current)
     return h
+
+
+def _darcy_struct(state, keep) -> SphDarcyState:
+    d = SphDarcyState()
+    for name, _ in SphDarcyState._fields_:
+        setattr(d, name, _ptr(getattr(state, name), np.float64, keep))
+    return d
+
+
+def darcy_init(cfg: SceneConfig, nu: float, x, state, device: int = 0) -> float:
+    """The reference's host-side Darcy initialisation (DEM::initDarcy) into
+    `state`: storativity, recharge, porosity from the particle rows `x`
+    (np x 4), conductivity and transmissivity.  Returns the stability
+    criterion; raises SphError(SPH_ERR_UNSTABLE) above 0.5, where the
+    reference exits."""
+    lib = load_library()
+    keep = []
+    c = make_config(cfg, device)
+    xa = np.ascontiguousarray(x, dtype=np.float64)
+    value = C.c_double(0.0)
+    rc = lib.sph_darcy_init(C.byref(c), float(nu), xa.ctypes.data_as(_dp),
+                            C.byref(_darcy_struct(state, keep)), C.byref(value))
+    if rc != SPH_OK:
+        raise SphError(rc, f"Darcy initialisation (stability criterion {value.value:.6g})")
+    return float(value.value)
 
 
 class Simulation:
@@ -251,6 +284,21 @@ class Simulation:
 
     def relayout(self):
         self._check(self.lib.sph_relayout(self._ctx))
+
+    # ---- Darcy flow (sph_darcy_*) ------------------------------------------
+    def darcy_upload(self, state, nu: float):
+        """Run the Darcy flow in every following step, starting from `state`
+        (a ``sphere_b200.darcy.DarcyState``), with dynamic viscosity `nu`."""
+        keep = []
+        self._check(self.lib.sph_darcy_upload(self._ctx, float(nu), C.byref(_darcy_struct(state, keep))))
+
+    def darcy_download(self, state=None):
+        """The Darcy grid after the last step (into `state` when given)."""
+        from .darcy import DarcyState
+        st = state if state is not None else DarcyState.zeros(self.cfg.num)
+        keep = []
+        self._check(self.lib.sph_darcy_download(self._ctx, C.byref(_darcy_struct(st, keep))))
+        return st
 
     # ---- differentiable step (sph_diff_*) ----------------------------------
     def diff_begin(self, mu=None, checkpoint_every: int = 100):

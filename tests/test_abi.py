@@ -23,7 +23,7 @@ def test_library_exports_every_declared_symbol(sphk_lib):
 
 
 def test_version(sphk_lib):
-    assert sphk_lib.sph_version() == 2
+    assert sphk_lib.sph_version() == 3
 
 
 @pytest.mark.parametrize("patch, msg", [
