@@ -63,6 +63,12 @@ def parse():
                     help="spheres of the calibration column (0: skip the adjoint leg)")
     ap.add_argument("--adjoint-steps", type=int, default=4000)
     ap.add_argument("--adjoint-checkpoint", type=int, default=100)
+    ap.add_argument("--no-darcy", action="store_true",
+                    help="skip the Darcy-flow leg (the 1M workload with the fluid grid on)")
+    ap.add_argument("--darcy-steps", type=int, default=400)
+    ap.add_argument("--no-render", action="store_true",
+                    help="skip the ray-tracer leg (one 800 x 800 image of the 1M workload)")
+    ap.add_argument("--render-frames", type=int, default=10)
     return ap.parse_args()
 
 
@@ -358,6 +364,10 @@ def gpu_arm(args, rank, world, local):
         out["batched"] = batched_leg(args, rank, world, local, barrier, max_over_ranks)
     if args.adjoint_n > 0 and rank == 0:
         out["adjoint"] = adjoint_leg(args, local)
+    if not args.no_darcy and rank == 0:
+        out["darcy"] = darcy_leg(args, local, sb)
+    if not args.no_render and rank == 0:
+        out["render"] = render_leg(args, local, sb)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_reference_run(sb, 1, 1000, args.cpu_seconds)
     if world > 1:
@@ -577,6 +587,129 @@ def adjoint_leg(args, local):
         "fd_check": {"scene": f"collision, {fsb.np} spheres, {fsteps} steps",
                      "param": "k_n", "adjoint": gk, "central_difference": fd,
                      "rel_error": abs(gk - fd) / abs(fd) if fd else None},
+    }
+
+
+def darcy_leg(args, local, sb):
+    """The Darcy flow (src/darcy.cuh) on the headline workload: the fluid
+    grid is the 50 x 50 x 100 cell grid, initialised as DEM::initDarcy does
+    from a uniform pressure.  Reports the per-step time of the Darcy kernels
+    (profile mode), the whole step with and without them (graphs), and the
+    kernels' algorithmic bytes against the measured HBM bandwidth."""
+    import numpy as np
+    import torch
+    from sphere_b200.darcy import DarcyState
+    from sphere_b200.sphk import Simulation, darcy_init
+    from sphere_b200.state import config_from_spherebin, state_from_spherebin
+
+    nu = 8.9e-4
+    cfg = config_from_spherebin(sb)
+    st0 = state_from_spherebin(sb)
+    ds = DarcyState.zeros(cfg.num)
+    shape = tuple(int(v) for v in cfg.num)
+    ds.set_cells(H=np.full(shape, 1.0e4))
+    stability = darcy_init(cfg, nu, st0.x, ds)
+    stream = torch.cuda.Stream()
+    K = args.darcy_steps
+
+    def timed(with_flow):
+        sim = Simulation(cfg, device=local)
+        sim.upload(st0)
+        if with_flow:
+            sim.darcy_upload(ds, nu)
+        sim.step(args.warmup, stream=stream.cuda_stream)
+        sim.sync()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        sim.step(K, stream=stream.cuda_stream)
+        b.record(stream)
+        b.synchronize()
+        sim.sync()
+        ms = a.elapsed_time(b) / K
+        prof = None
+        if with_flow:
+            sim.set_profile(True)
+            sim.profile(reset=True)
+            sim.step(min(K, 100))
+            sim.sync()
+            prof = sim.profile()
+        sim.close()
+        return ms, prof
+
+    ms_plain, _ = timed(False)
+    ms_flow, prof = timed(True)
+    darcy_ms = prof["darcy"] / max(1, prof["steps"])
+    ncell = int(np.prod(shape))
+    # compulsory bytes: the particles' positions once (32 B) and their
+    # cell-list entries (4 B); per cell the porosity's start/end words (8),
+    # the old porosity (8) and the new porosity, change, conductivity and
+    # transmissivity (56); the explicit step's T, Ss, W, dphi, H (56) and new
+    # H (8); the gradient's H, K, phi (24) and dH, V (48)
+    b_step = 36 * cfg.np + (8 + 8 + 56 + 56 + 8 + 24 + 48) * ncell
+    peak, peak_kind = measured_peak_hbm()
+    achieved = b_step / (darcy_ms * 1e-3) / 1e9
+    return {
+        "metric": "Darcy flow time per step", "value": darcy_ms, "unit": "ms",
+        "higher_is_better": False,
+        "workload": f"{WORKLOAD}; Darcy flow on the {shape[0]}x{shape[1]}x{shape[2]} cell grid, "
+                    f"nu {nu} Pa s, uniform starting pressure",
+        "cells": ncell, "steps": K, "stability_criterion": stability,
+        "cells_per_s": ncell / (darcy_ms * 1e-3),
+        "step_ms_without_flow": ms_plain, "step_ms_with_flow": ms_flow,
+        "roofline": {"bound": "hbm", "kernel": "k_darcy_*", "achieved": achieved, "peak": peak,
+                     "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
+                     "algorithmic_bytes_per_step": b_step},
+    }
+
+
+def render_leg(args, local, sb):
+    """The ray tracer (DEM::render) on the headline workload: 800 x 800
+    images of the 1M spheres, plain and through the velocity colour map, each
+    call including the image's copy to the host.  The CPU baseline runs the
+    reference's own kernels (oracle/_ref; the plain-C restatement where that
+    is not built) on a band of rows on all host cores and scales to a frame:
+    the reference tests every sphere for every pixel."""
+    import numpy as np
+    from sphere_b200.sphk import Simulation
+    from sphere_b200.state import config_from_spherebin, state_from_spherebin
+
+    cfg = config_from_spherebin(sb)
+    st0 = state_from_spherebin(sb)
+    W = H = 800
+    sim = Simulation(cfg, device=local)
+    sim.upload(st0)
+    out = {}
+    for name, method, maxval in (("normal", 0, 0.0), ("vel", 2, 0.05)):
+        img = sim.render(method, maxval, 0.0, W, H)   # warm-up: scratch allocation
+        t0 = time.perf_counter()
+        for _ in range(args.render_frames):
+            img = sim.render(method, maxval, 0.0, W, H)
+        out[name] = (time.perf_counter() - t0) / args.render_frames * 1e3
+    covered = int(((img[..., :3] != 255).any(axis=2)).sum())
+    sim.close()
+    cpu = None
+    if not args.no_cpu_baseline:
+        sys.path.insert(0, str(ROOT / "oracle"))
+        import pyoracle
+        kind = "reference" if pyoracle.LIB_REF.exists() else "port"
+        lib_orc = pyoracle.load("orc")
+        lib = pyoracle.load("ref") if kind == "reference" else lib_orc
+        rows = 2
+        t0 = time.perf_counter()
+        pyoracle.render(lib, lib_orc, st0, sb.L, 0, 0.0, 0.0, W, H, rows=(H // 2, rows))
+        secs = time.perf_counter() - t0
+        frame_s = secs * H / rows
+        cpu = {"value": 1.0 / frame_s, "unit": "frames/s", "cores": os.cpu_count(), "kind": kind,
+               "sample": f"{rows} of {H} rows of the plain 800 x 800 image ({secs:.1f} s), "
+                         f"scaled to a frame"}
+    ms = out["normal"]
+    return {
+        "metric": "ray-traced frames/s at 1M spheres, 800 x 800", "value": 1e3 / ms,
+        "unit": "frames/s", "higher_is_better": True,
+        "workload": f"{WORKLOAD}; DEM::render's camera and shading",
+        "ms_per_frame": out, "pixels_covered": covered,
+        "sphere_pixel_tests_per_s_equivalent": cfg.np * W * H / (ms * 1e-3),
+        "cpu_baseline": cpu,
     }
 
 

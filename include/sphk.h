@@ -20,6 +20,7 @@
  *   sph_darcy_init   DEM::initDarcy (src/darcy.cpp:760-798)
  *   sph_darcy_upload, sph_darcy_download
  *                    DEM::transferDarcy{To,From}GlobalDeviceMemory (src/darcy.cuh:60-121)
+ *   sph_render       DEM::render (src/raytracer.cuh:303-553)
  *
  * Conventions: plain C types only; every entry point returns an int status,
  * SPH_OK (0) or a negative SPH_ERR_* code; the message of the last failure
@@ -212,6 +213,27 @@ int sph_darcy_init(const sph_config *cfg, double nu, const double *x, sph_darcy_
 int sph_darcy_upload(sph_ctx *ctx, double nu, const sph_darcy_state *st);
 /* transferDarcyFromGlobalDeviceMemory (src/darcy.cuh:95-121). */
 int sph_darcy_download(sph_ctx *ctx, sph_darcy_state *st);
+
+/* ---- Ray tracer -------------------------------------------------------------
+ * DEM::render (src/raytracer.cuh:303-553, the kernels at :14-263): one image
+ * of the context's current state, from the reference's camera (eye at
+ * (2.3, -5, 1.3) x L, looking at half the largest coordinates, an image
+ * plane 1.35 L[0] wide), white background, Lambertian shading, plain or
+ * through the blue-white-red colour map.  The pixels are those of the
+ * reference's brute-force search, bit for bit, with IEEE single-precision
+ * arithmetic (the reference's GPU build used fast-math approximations). */
+typedef struct sph_render_opts {
+    int32_t method;        /* 0 plain; colour map of 1 pressure, 2 |velocity|,
+                              3 |angular velocity|, 4 x displacement, 5 |rotation| */
+    float maxval;          /* value at the top of the colour map */
+    float lower_cutoff;    /* > 0 (methods 1-5): draw only spheres whose value exceeds
+                              it and whose fixvel is zero */
+    uint32_t width, height;   /* pixels, width * height < 2^24 (else SPH_ERR_TOO_LARGE) */
+} sph_render_opts;
+/* rgba: width * height * 4 bytes, rows top to bottom as the reference's
+ * image buffer (pixel m = row * width + column); alpha is 0.  Not for
+ * batched contexts. */
+int sph_render(sph_ctx *ctx, const sph_render_opts *opts, uint8_t *rgba);
 
 /* ---- Differentiable step ----------------------------------------------------
  * No counterpart in the reference: gradients of a run with respect to the

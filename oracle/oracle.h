@@ -80,6 +80,39 @@ typedef struct orc_scene {
     double *d_K, *d_Ss, *d_W, *d_phi, *d_dphi;
 } orc_scene;
 
+/* ---- ray tracer (src/raytracer.cuh:14-553, DEM::render) ------------------ */
+typedef struct orc_render {
+    uint32_t np;
+    const double *x;        /* np*4: positions and radii, particle order */
+    const double *vel;      /* np*4: the fourth lane is fixvel */
+    const double *values;   /* np colour-map values (methods 1-5), else NULL */
+    double L[3];            /* grid.L */
+    int32_t method;         /* 0 plain, 1 pressure, 2 |v|, 3 |omega|, 4 x displacement, 5 |rotation| */
+    float maxval, lower_cutoff;
+    uint32_t width, height;
+} orc_render;
+
+/* the camera that DEM::render and DEM::cameraInit set up
+ * (src/raytracer.cuh:269-300, 351-367), the raytracer's __constant__ values */
+typedef struct orc_camera {
+    float u[3], v[3], w[3], eye[3], light[3];
+    float imgplane[4];
+    float d;
+} orc_camera;
+
+/* Fill *cam for the scene and image size of *r (plain-C restatement only). */
+void orc_render_camera(const orc_render *r, orc_camera *cam);
+/* DEM::render's colour-map array for `method` (plain-C restatement only). */
+void orc_render_values(int method, uint32_t np, const double *vel, const double *angvel,
+                       const double *angpos, const double *xysum, const double *p, double *out);
+/* Render one image into rgba (width*height*4 bytes; alpha 0).  Both
+ * oracles provide it: the restatement and the reference kernels. */
+int orc_render_image(const orc_render *r, const orc_camera *cam, uint8_t *rgba, int nthreads);
+/* The same for the pixel rows [row0, row0 + nrows) only (the rest of rgba
+ * is left alone): a bounded sample for timing. */
+int orc_render_rows(const orc_render *r, const orc_camera *cam, uint8_t *rgba, uint32_t row0,
+                    uint32_t nrows, int nthreads);
+
 /* Advance the scene by nsteps time steps.  nthreads <= 0 uses the OpenMP
  * default.  Returns the OR of the ORC_ERR_* flags raised (0 when clean). */
 int orc_step(orc_scene *s, uint64_t nsteps, int nthreads);

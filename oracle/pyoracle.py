@@ -143,3 +143,59 @@ class OracleRun:
             self.darcy.H, self.darcy.H_new = self.darcy.H_new, self.darcy.H
             self._bind_pressure()
         return rc
+
+
+# ---- ray tracer ---------------------------------------------------------------
+
+class OrcRender(C.Structure):
+    _fields_ = [("np", C.c_uint32), ("x", _dp), ("vel", _dp), ("values", _dp),
+                ("L", C.c_double * 3), ("method", C.c_int32), ("maxval", C.c_float),
+                ("lower_cutoff", C.c_float), ("width", C.c_uint32), ("height", C.c_uint32)]
+
+
+class OrcCamera(C.Structure):
+    _fields_ = [("u", C.c_float * 3), ("v", C.c_float * 3), ("w", C.c_float * 3),
+                ("eye", C.c_float * 3), ("light", C.c_float * 3), ("imgplane", C.c_float * 4),
+                ("d", C.c_float)]
+
+
+def render_values(lib_orc, method, st):
+    """DEM::render's colour-map values of a HostState (restatement)."""
+    n = st.x.shape[0]
+    out = np.zeros(n)
+    f = lib_orc.orc_render_values
+    f.argtypes = [C.c_int, C.c_uint32, _dp, _dp, _dp, _dp, _dp, _dp]
+    f(int(method), n, *(np.ascontiguousarray(a).ctypes.data_as(_dp)
+                         for a in (st.vel, st.angvel, st.angpos, st.xysum, st.p)),
+      out.ctypes.data_as(_dp))
+    return out
+
+
+def render(lib, lib_orc, st, L, method=0, maxval=1.0e3, lower_cutoff=0.0, width=800,
+           height=800, nthreads=0, values=None, rows=None):
+    """One image (height, width, 4) uint8 of HostState `st` through `lib`'s
+    kernels, with the camera of the restatement `lib_orc`."""
+    r = OrcRender()
+    x = np.ascontiguousarray(st.x, np.float64)
+    vel = np.ascontiguousarray(st.vel, np.float64)
+    r.np = x.shape[0]
+    r.x, r.vel = x.ctypes.data_as(_dp), vel.ctypes.data_as(_dp)
+    if method > 0 and values is None:
+        values = render_values(lib_orc, method, st)
+    vals = None if values is None else np.ascontiguousarray(values, np.float64)
+    r.values = vals.ctypes.data_as(_dp) if vals is not None else None
+    r.L[:] = [float(v) for v in L]
+    r.method, r.maxval, r.lower_cutoff = int(method), float(maxval), float(lower_cutoff)
+    r.width, r.height = int(width), int(height)
+    cam = OrcCamera()
+    lib_orc.orc_render_camera.argtypes = [C.POINTER(OrcRender), C.POINTER(OrcCamera)]
+    lib_orc.orc_render_camera(C.byref(r), C.byref(cam))
+    img = np.zeros((height, width, 4), np.uint8)
+    row0, nrows = (0, height) if rows is None else rows
+    lib.orc_render_rows.argtypes = [C.POINTER(OrcRender), C.POINTER(OrcCamera),
+                                    C.POINTER(C.c_uint8), C.c_uint32, C.c_uint32, C.c_int]
+    rc = lib.orc_render_rows(C.byref(r), C.byref(cam), img.ctypes.data_as(C.POINTER(C.c_uint8)),
+                             int(row0), int(nrows), int(nthreads))
+    if rc != 0:
+        raise RuntimeError(f"orc_render_image failed ({rc})")
+    return img, cam

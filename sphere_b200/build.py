@@ -29,7 +29,7 @@ NVCC = os.environ.get("NVCC", shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
 CUDA_HOME = Path(NVCC).resolve().parent.parent
 
 KERNEL_SOURCES = ["api.cu", "step.cu", "cells.cu", "walls.cu", "bonds.cu", "noalloc.cu",
-                  "adjoint.cu", "darcy.cu"]
+                  "adjoint.cu", "darcy.cu", "render.cu"]
 HOST_SOURCES = ["host/sphere.cpp", "host/file_io.cpp", "host/main.cpp"]
 
 

@@ -23,6 +23,11 @@ unsigned int scan_tile_count(uint32_t ncells);
 void relayout(const Dev &d, uint32_t np, int a, void *scratch, cudaStream_t st);
 void launch_rebuild_gate(cudaGraphConditionalHandle h, const uint32_t *rebuild, cudaStream_t st);
 void launch_darcy(const Dev &d, const DarcyDev &f, const Params &hp, int a, int hs, cudaStream_t st);
+struct RenderArgs;
+void launch_maxpos(const Dev &d, uint32_t np, int a, unsigned long long *mx, cudaStream_t st);
+int render_image(const Dev &d, uint32_t np, int a, const double L[3], const double maxpos[3],
+                 const sph_render_opts &o, double *values, unsigned long long *keys, uchar4 *img,
+                 cudaStream_t st);
 void launch_force_tape(const Dev &d, uint32_t np, int a, int tape_step, cudaStream_t st);
 void launch_rev_step(const Dev &d, const AdjDev &a, uint32_t np, int j, cudaStream_t st);
 void launch_user_to_storage3(const double *src, double4 *dst, const uint32_t *uid, uint32_t n,
@@ -89,6 +94,9 @@ struct sph_ctx {
     DarcyDev darcy{};
     int dflip = 0;
     double mean_radius = 0.0;        // of the uploaded particles, summed in caller order
+    // ray tracer scratch: per-pixel keys and image, per-particle values
+    void *rt_buf = nullptr;
+    size_t rt_bytes = 0;
     size_t ckpt_bytes = 0;                // size of one pooled buffer
     cudaEvent_t ckpt_ev = nullptr;        // orders a checkpoint copy against the caller's stream
     std::vector<void *> diff_allocs;
@@ -1380,6 +1388,47 @@ int sph_darcy_download(sph_ctx *c, sph_darcy_state *h)
     return SPH_OK;
 }
 
+int sph_render(sph_ctx *c, const sph_render_opts *o, uint8_t *rgba)
+{
+    if (!c || !c->uploaded) return fail(c, SPH_ERR_BAD_INPUT, "sph_render before sph_upload");
+    if (c->batched) return fail(c, SPH_ERR_BAD_INPUT, "sph_render takes a single-scene context");
+    if (!o || !rgba || o->method < 0 || o->method > 5 || o->width == 0 || o->height == 0)
+        return fail(c, SPH_ERR_BAD_INPUT, "sph_render: bad options");
+    const uint64_t pixels = (uint64_t)o->width * o->height;
+    if (pixels >= (1ull << 24))
+        return fail(c, SPH_ERR_TOO_LARGE, "sph_render: width * height must stay below 2^24");
+    CK(cudaSetDevice(c->device));
+    const size_t np = c->np_all;
+    const size_t need = 32 + pixels * 8 + pixels * 4 + np * 8;
+    if (c->rt_bytes < need) {
+        if (c->rt_buf) cudaFree(c->rt_buf);
+        c->rt_buf = nullptr;
+        c->rt_bytes = 0;
+        CK(cudaMalloc(&c->rt_buf, need));
+        c->rt_bytes = need;
+    }
+    char *base = static_cast<char *>(c->rt_buf);
+    auto *mx = reinterpret_cast<unsigned long long *>(base);
+    auto *keys = reinterpret_cast<unsigned long long *>(base + 32);
+    auto *img = reinterpret_cast<uchar4 *>(base + 32 + pixels * 8);
+    auto *values = reinterpret_cast<double *>(base + 32 + pixels * 12);
+    cudaStream_t st = c->stream;
+    // DEM::maxPos on the device, then the camera on the host
+    CK(cudaMemsetAsync(mx, 0, 24, st));
+    launch_maxpos(c->d, c->np_all, c->a, mx, st);
+    unsigned long long mxh[3];
+    CK(cudaMemcpyAsync(mxh, mx, 24, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    double maxpos[3];
+    for (int k = 0; k < 3; ++k) memcpy(&maxpos[k], &mxh[k], 8);
+    CK(cudaMemsetAsync(keys, 0xff, pixels * 8, st));
+    render_image(c->d, c->np_all, c->a, c->hp.L, maxpos, *o, values, keys, img, st);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(rgba, img, pixels * 4, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    return SPH_OK;
+}
+
 int sph_destroy(sph_ctx *c)
 {
     if (!c) return SPH_OK;
@@ -1389,6 +1438,7 @@ int sph_destroy(sph_ctx *c)
     for (auto e : c->ev) cudaEventDestroy(e);
     free_diff(c);
     for (char *b : c->ckpt_pool) cudaFree(b);
+    if (c->rt_buf) cudaFree(c->rt_buf);
     if (c->ckpt_ev) cudaEventDestroy(c->ckpt_ev);
     for (void *p : c->allocs) cudaFree(p);
     if (c->stream) cudaStreamDestroy(c->stream);

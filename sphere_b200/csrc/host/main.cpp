@@ -4,8 +4,9 @@
 // output/<sid>.outputNNNNN.bin and output/<sid>.status.dat.
 //
 // Flags: -h/--help, -V/--version, -q/--quiet, -n/--dry, -dc/--dont-check,
-// and -r/--render, -m/--method, which name the reference's ray tracer; the
-// renderer is not part of this DEM step, so those report that and exit 1.
+// -r/--render (render the input files to img_out/<sid>.ppm instead of
+// simulating) and -m/--method <method> [<maxval> [-l <cutoff>]] (the colour
+// map: normal, pres, vel, angvel, xdisp, angpos).
 #include <cstdlib>
 #include <iostream>
 #include <string>
@@ -14,7 +15,8 @@
 
 int main(const int argc, const char *argv[])
 {
-    int verbose = 1, checkVals = 1, dry = 0, render = 0, nfiles = 0;
+    int verbose = 1, checkVals = 1, dry = 0, render = 0, nfiles = 0, method = 0;
+    float max_val = 0.0f, lower_cutoff = 0.0f;
     for (int i = 1; i < argc; ++i) {
         const std::string a(argv[i]);
         if (a == "-h" || a == "--help") {
@@ -24,8 +26,14 @@ int main(const int argc, const char *argv[])
                       << "-V, --version\t\tprint version information and exit\n"
                       << "-q, --quiet\t\tsuppress status messages to stdout\n"
                       << "-n, --dry\t\tshow key experiment parameters and quit\n"
-                      << "-r, --render\t\t(renderer not part of this build)\n"
+                      << "-r, --render\t\trender input files instead of simulating temporal evolution\n"
                       << "-dc, --dont-check\tdon't check values before running\n"
+                      << "\nRaytracer (-r) specific options:\n"
+                      << "-m <method> <maxval> [-l <lower cutoff val>], or\n"
+                      << "--method <method> <maxval> [-l <lower cutoff val>]\n"
+                      << "\tcolor visualization method, possible values:\n"
+                      << "\tnormal, pres, vel, angvel, xdisp, angpos\n"
+                      << "\tif -l is appended, don't render particles with value below\n"
                       << std::endl;
             return 0;
         } else if (a == "-V" || a == "--version") {
@@ -38,19 +46,44 @@ int main(const int argc, const char *argv[])
             dry = 1;
         } else if (a == "-dc" || a == "--dont-check") {
             checkVals = 0;
-        } else if (a == "-r" || a == "--render" || a == "-m" || a == "--method") {
+        } else if (a == "-r" || a == "--render") {
             render = 1;
-            break;
+            checkVals = 0;
+        } else if (a == "-m" || a == "--method") {
+            // src/main.cpp:97-134
+            render = 1;
+            const std::string m = (i + 1 < argc) ? argv[i + 1] : "";
+            if (m == "normal") method = 0;
+            else if (m == "pres") method = 1;
+            else if (m == "vel") method = 2;
+            else if (m == "angvel") method = 3;
+            else if (m == "xdisp") method = 4;
+            else if (m == "angpos") method = 5;
+            else {
+                std::cerr << "Visualization method not understood. See `" << argv[0]
+                          << " --help` for more information." << std::endl;
+                return 1;
+            }
+            if (method != 0) {
+                max_val = (i + 2 < argc) ? (float)std::atof(argv[i + 2]) : 0.0f;
+                if (i + 4 < argc && std::string(argv[i + 3]) == "-l") {
+                    lower_cutoff = (float)std::atof(argv[i + 4]);
+                    i += 4;
+                } else {
+                    i += 2;
+                }
+            } else {
+                i += 1;
+            }
         } else {
             ++nfiles;
             if (verbose == 1) std::cout << argv[0] << ": processing input file: " << a << std::endl;
             DEM dem(a, verbose, checkVals, dry, 1, nfiles == 1 ? 1 : 0);
-            dem.startTime();
+            if (render == 1)
+                dem.render(method, max_val, lower_cutoff);
+            else
+                dem.startTime();
         }
-    }
-    if (render) {
-        std::cerr << argv[0] << ": the ray-traced renderer is not part of this build" << std::endl;
-        return 1;
     }
     if (argc == 1 || nfiles == 0) {
         std::cerr << argv[0] << ": missing input binary file\n"

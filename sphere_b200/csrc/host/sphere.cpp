@@ -11,6 +11,7 @@
 #include "sphere.h"
 
 #include <chrono>
+#include <fstream>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -382,12 +383,39 @@ void DEM::startTime()
     if (darcyOn()) endDarcy();   // src/device.cu:1292-1297
 }
 
-void DEM::render(const int, const float, const float, const float, const unsigned int,
-                 const unsigned int)
+// DEM::render (src/raytracer.cuh:303-553) through sph_render, then
+// writePPM (src/file_io.cpp:493-516).  focalLength is unused there too.
+void DEM::render(const int method, const float maxval, const float lower_cutoff, const float,
+                 const unsigned int img_width, const unsigned int img_height)
 {
-    std::cerr << "Error: the ray-traced renderer is not part of this DEM step implementation."
-              << std::endl;
-    exit(1);
+    if (!ctx_) initDevice();
+    if (verbose_ == 1 && method != 0) {
+        static const char *desc[] = {"", "Pressure", "Linear velocity", "Angular velocity",
+                                     "X-axis displacement", "Angular positions"};
+        static const char *unit[] = {"", "Pa", "m/s", "rad/s", "m", "rad"};
+        if (method > 0 && method < 6)
+            std::cout << "  " << desc[method] << " color map range: [0, " << maxval << "] "
+                      << unit[method] << std::endl;
+    }
+    sph_render_opts o{};
+    o.method = method;
+    o.maxval = maxval;
+    o.lower_cutoff = lower_cutoff;
+    o.width = img_width;
+    o.height = img_height;
+    std::vector<unsigned char> img((size_t)img_width * img_height * 4);
+    const int rc = sph_render(ctx_, &o, img.data());
+    if (rc != SPH_OK) fail(rc, "sph_render");
+    const std::string target = "img_out/" + sid_ + ".ppm";
+    std::ofstream ofs(target, std::ios_base::binary);
+    if (!ofs) {
+        std::cerr << "Could not create output PPM file '" << target << std::endl;
+        exit(1);
+    }
+    if (verbose_ == 1) std::cout << "  Saving image: " << target << std::endl;
+    ofs << "P6 " << img_width << " " << img_height << " 255\n";
+    for (size_t i = 0; i < (size_t)img_width * img_height; ++i)
+        ofs << img[4 * i] << img[4 * i + 1] << img[4 * i + 2];
 }
 
 void DEM::porosity(const int)

@@ -9,9 +9,11 @@
 // and from the device with sph_upload / sph_download.  With darcyflow = 1 and
 // nu > 0 the Darcy flow runs with the step (src/darcy.cpp, src/darcy.cuh):
 // its grid is read from and written to the files' fluid section, set up by
-// sph_darcy_init and stepped on the device.  The lattice-Boltzmann coupling
-// (nu > 0 without darcyflow) and the porosity and force-chain tools are not
-// part of this build: they report that and exit.
+// sph_darcy_init and stepped on the device.  render() draws the current
+// state with the reference's ray tracer (sph_render) into img_out/<sid>.ppm.
+// The lattice-Boltzmann coupling (nu > 0 without darcyflow) and the
+// porosity and force-chain tools are not part of this build: they report
+// that and exit.
 #ifndef SPHERE_B200_SPHERE_H_
 #define SPHERE_B200_SPHERE_H_
 

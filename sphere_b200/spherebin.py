@@ -502,6 +502,23 @@ class Spherebin:
             print(f"Warning: the sphere run returned with status {status_}")
         return status_
 
+    def render(self, method="pres", max_val=1e3, lower_cutoff=0.0, graphicsformat="png",
+               verbose=True, root="..", binary=None):
+        """Render every output file of this simulation with the ray tracer
+        into ``<root>/img_out/<file>.ppm`` (``python/sphere.py:1698-1725``).
+        The PPM images are kept as they are: the reference's conversion to
+        ``graphicsformat`` calls ImageMagick, which is not part of this build."""
+        exe = binary or str(Path(__file__).resolve().parent / "bin" / "sphere")
+        (Path(root) / "img_out").mkdir(exist_ok=True)
+        status_ = 0
+        for f in sorted((Path(root) / "output").glob(f"{self.sid}*.bin")):
+            args = [exe] + ([] if verbose else ["-q"])
+            if method != "normal":
+                args += ["--method", method, f"{max_val}", "-l", f"{lower_cutoff}"]
+            args += ["--render", str(f.relative_to(root))]
+            status_ |= subprocess.call(args, cwd=root)
+        return status_
+
 
 def status(project, root=".."):
     """Last output-file number of a run (``python/sphere.py:2892-2907``)."""

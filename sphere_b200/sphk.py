@@ -67,6 +67,15 @@ class SphDarcyState(C.Structure):
     _fields_ = [(n, _dp) for n in ("H", "H_new", "V", "dH", "K", "T", "Ss", "W", "phi", "dphi")]
 
 
+class SphRenderOpts(C.Structure):
+    _fields_ = [("method", C.c_int32), ("maxval", C.c_float), ("lower_cutoff", C.c_float),
+                ("width", C.c_uint32), ("height", C.c_uint32)]
+
+
+# colour-map methods of the reference's command line (src/main.cpp:97-118)
+RENDER_METHODS = {"normal": 0, "pres": 1, "vel": 2, "angvel": 3, "xdisp": 4, "angpos": 5}
+
+
 class SphStats(C.Structure):
     _fields_ = [("active_contacts", C.c_uint64), ("steps", C.c_uint64),
                 ("relayouts", C.c_uint64), ("device_bytes", C.c_uint64),
@@ -122,6 +131,7 @@ def load_library(path: os.PathLike | None = None):
                            C.c_int),
         "sph_darcy_upload": ([vp, C.c_double, C.POINTER(SphDarcyState)], C.c_int),
         "sph_darcy_download": ([vp, C.POINTER(SphDarcyState)], C.c_int),
+        "sph_render": ([vp, C.POINTER(SphRenderOpts), C.POINTER(C.c_uint8)], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)
@@ -284,6 +294,18 @@ class Simulation:
 
     def relayout(self):
         self._check(self.lib.sph_relayout(self._ctx))
+
+    # ---- ray tracer (sph_render) -----------------------------------------------
+    def render(self, method=0, maxval=1.0e3, lower_cutoff=0.0, width=800, height=800):
+        """DEM::render of the current state: a (height, width, 4) uint8 image
+        (alpha 0).  `method` is 0-5 or one of RENDER_METHODS' names."""
+        if isinstance(method, str):
+            method = RENDER_METHODS[method]
+        o = SphRenderOpts(int(method), float(maxval), float(lower_cutoff), int(width), int(height))
+        img = np.zeros((int(height), int(width), 4), np.uint8)
+        self._check(self.lib.sph_render(self._ctx, C.byref(o),
+                                        img.ctypes.data_as(C.POINTER(C.c_uint8))))
+        return img
 
     # ---- Darcy flow (sph_darcy_*) ------------------------------------------
     def darcy_upload(self, state, nu: float):

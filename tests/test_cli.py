@@ -54,9 +54,11 @@ def test_unreadable_input_file(cli, tmp_path):
     assert r.returncode == 1 and "Could not read input binary file" in r.stderr
 
 
-def test_renderer_is_reported_as_absent(cli, tmp_path):
+def test_render_flags_need_an_input_file(cli, tmp_path):
     r = _run(cli, ["--render"], tmp_path)
-    assert r.returncode == 1 and "renderer" in r.stderr
+    assert r.returncode == 1 and "missing input binary file" in r.stderr
+    r = _run(cli, ["--method", "colour", "--render"], tmp_path)
+    assert r.returncode == 1 and "Visualization method not understood" in r.stderr
 
 
 def test_dry_run_reports_parameters(cli, tmp_path):
@@ -139,3 +141,24 @@ def test_cli_run_writes_the_oracles_files(cli, oracle_libs, tmp_path, kw):
     assert (tmp_path / "output" / "cli.output00000.bin").read_bytes() == path.read_bytes()
     for name in want:
         assert (tmp_path / "output" / name).read_bytes() == (want_dir / name).read_bytes(), name
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("flags,method,maxval,cut", [
+    (["--render"], 0, 0.0, 0.0),
+    (["--method", "vel", "0.4", "-l", "0.1", "--render"], 2, 0.4, 0.1),
+], ids=["normal", "vel_cutoff"])
+def test_cli_render_writes_the_oracles_image(cli, oracle_libs, tmp_path, flags, method, maxval,
+                                             cut):
+    """sphere [-m ...] --render <file>: img_out/<sid>.ppm, 800 x 800 P6, byte
+    for byte against the oracle's image of the file's state."""
+    import pyoracle
+    sb, path = _scene(tmp_path, sid="rt", n=900, seed=53)
+    (tmp_path / "img_out").mkdir()
+    r = _run(cli, ["-q"] + flags + [path.name], tmp_path)
+    assert r.returncode == 0, r.stderr
+    st = state_from_spherebin(readbin(path))
+    img, _ = pyoracle.render(oracle_libs["orc"], oracle_libs["orc"], st, sb.L, method, maxval, cut,
+                             800, 800)
+    want = b"P6 800 800 255\n" + np.ascontiguousarray(img[..., :3]).tobytes()
+    assert (tmp_path / "img_out" / "rt.ppm").read_bytes() == want

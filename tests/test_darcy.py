@@ -197,3 +197,85 @@ def test_host_init_rejects_nonpositive_viscosity(sphk_lib):
     with pytest.raises(SphError) as e:
         darcy_init(cfg, 0.0, state_from_spherebin(sb).x, DarcyState.zeros(cfg.num))
     assert e.value.code == -5
+
+
+# ---- file format and the DEM class ---------------------------------------------
+
+def darcy_scene(tmp_path=None, sid="darcy", nu=NU, n=500, seed=44, steps=23):
+    """A settling scene with a fluid section: uniform pressure, zero velocity,
+    porosity and conductivity to be set up by DEM::initDarcy."""
+    sb = scenes.collision(n=n, seed=seed, periodic=1, vmax=0.3)
+    sb.sid = sid
+    sb.nu = nu
+    sb.time_current = 0.0
+    sb.time_total = steps * sb.time_dt
+    sb.time_file_dt = 5.0 * sb.time_dt
+    sb.time_step_count = 0
+    ds = DarcyState.zeros(sb.num)
+    shape = tuple(int(v) for v in sb.num)
+    ds.set_cells(H=np.full(shape, 1.0e4), phi=np.full(shape, 0.5), K=np.full(shape, 1e-9))
+    ds.to_spherebin(sb)
+    path = None
+    if tmp_path is not None:
+        (tmp_path / "output").mkdir(exist_ok=True)
+        path = sb.writebin(path=tmp_path / f"{sid}.bin", verbose=False)
+    return sb, path
+
+
+def test_fluid_section_round_trips_in_the_reference_layout():
+    from sphere_b200.spherebin import Spherebin
+    sb, _ = darcy_scene()
+    rng = np.random.default_rng(3)
+    shape = tuple(int(v) for v in sb.num)
+    sb.f_v = rng.normal(size=shape + (3,))
+    sb.f_rho, sb.f_phi, sb.f_K = (rng.normal(size=shape) for _ in range(3))
+    raw = sb.to_bytes()
+    back = Spherebin.from_bytes(raw)
+    for f in ("f_v", "f_rho", "f_phi", "f_K"):
+        assert np.array_equal(getattr(back, f), getattr(sb, f)), f
+    # python/sphere.py:516-527: per cell, z outermost, V[3], H, phi, K
+    want = []
+    for z in range(shape[2]):
+        for y in range(shape[1]):
+            for x in range(shape[0]):
+                want += list(sb.f_v[x, y, z]) + [sb.f_rho[x, y, z], sb.f_phi[x, y, z],
+                                                  sb.f_K[x, y, z]]
+    tail = np.frombuffer(raw[-8 * len(want):], np.float64)
+    assert np.array_equal(tail, np.array(want))
+    assert back == sb
+
+
+@pytest.fixture(scope="module")
+def darcy_driver(sphk_lib, tmp_path_factory):
+    """tests/darcy_driver.cpp linked with the DEM class and libsphk."""
+    import subprocess
+    from pathlib import Path
+    from sphere_b200 import build
+    root = Path(__file__).resolve().parent.parent
+    host = root / "sphere_b200" / "csrc" / "host"
+    out = tmp_path_factory.mktemp("driver") / "darcy_driver"
+    cmd = ["g++", "-O2", "-std=c++17", "-I", str(root / "include"), "-I", str(host),
+           str(host / "sphere.cpp"), str(host / "file_io.cpp"),
+           str(Path(__file__).resolve().parent / "darcy_driver.cpp"), "-o", str(out),
+           "-L", str(build.LIB.parent), "-lsphk", f"-Wl,-rpath,{build.LIB.parent}"]
+    subprocess.run(cmd, check=True, capture_output=True, text=True)
+    return out
+
+
+def test_dem_class_refuses_an_unstable_darcy_step(darcy_driver, tmp_path):
+    import subprocess
+    sb, _ = darcy_scene()
+    sb.time_dt = 1.0e6
+    sb.time_total = 2.0e6
+    path = sb.writebin(path=tmp_path / "unstable.bin", verbose=False)
+    r = subprocess.run([str(darcy_driver), str(path), "0"], cwd=tmp_path, capture_output=True,
+                       text=True, timeout=120)
+    assert r.returncode == 1 and "explicit Darcy solution will be unstable" in r.stderr
+
+
+def test_dem_class_sets_up_darcy_flow_without_a_device(darcy_driver, tmp_path):
+    import subprocess
+    _, path = darcy_scene(tmp_path)
+    r = subprocess.run([str(darcy_driver), str(path), "0"], cwd=tmp_path, capture_output=True,
+                       text=True, timeout=120)
+    assert r.returncode == 0, r.stderr

@@ -6,7 +6,8 @@ from helpers import STATE_FIELDS, mismatches
 from sphere_b200.darcy import DarcyState
 from sphere_b200.sphk import SphError, Simulation, darcy_init
 from sphere_b200.state import config_from_spherebin, state_from_spherebin
-from test_darcy import (NU, SCENES, darcy_mismatches, run_darcy_oracle, seeded_grid)
+from test_darcy import (NU, SCENES, darcy_driver, darcy_mismatches, run_darcy_oracle,  # noqa: F401
+                         seeded_grid)
 
 pytestmark = pytest.mark.gpu
 
@@ -74,3 +75,66 @@ def test_gpu_darcy_is_refused_in_differentiable_mode():
         sim.diff_begin(checkpoint_every=10)
         with pytest.raises(SphError):
             sim.darcy_upload(seeded_grid(sb.num, 1), NU)
+
+
+class _DarcyOracleStepper:
+    """The oracle with the Darcy block, for sphere_b200.driver.run."""
+
+    def __init__(self, lib, sb, ds):
+        import pyoracle
+        from test_darcy import d_factor_of
+        self.sb, self.ds = sb, ds
+        self.st = state_from_spherebin(sb)
+        self.run = pyoracle.OracleRun(lib, config_from_spherebin(sb), self.st, darcy=ds, nu=NU,
+                                      d_factor=d_factor_of(sb))
+
+    def __call__(self, n):
+        assert self.run.step(n, 0) == 0
+
+    def snapshot(self):
+        from sphere_b200.state import to_spherebin
+        out = to_spherebin(self.sb, self.st)
+        self.ds.to_spherebin(out)
+        return out
+
+
+def _darcy_text(ds, name):
+    nx, ny, nz = ds.num
+    cells = ds.cells(name)
+    out = []
+    for z in range(nz):
+        for y in range(ny):
+            out.append("".join("%f\t" % cells[x, y, z] for x in range(nx)) + "\n")
+        out.append("\n")
+    return "".join(out)
+
+
+def test_dem_class_runs_the_darcy_flow(oracle_libs, darcy_driver, tmp_path):
+    """DEM(..., darcyflow = 1): every output file (particles and fluid
+    section) and the closing d_phi.txt / d_K.txt, byte for byte against the
+    same schedule through the oracle."""
+    import subprocess
+    from sphere_b200 import driver
+    from sphere_b200.spherebin import readbin
+    from test_darcy import darcy_scene
+    _, path = darcy_scene(tmp_path)
+    r = subprocess.run([str(darcy_driver), str(path), "1"], cwd=tmp_path, capture_output=True,
+                       text=True, timeout=600)
+    assert r.returncode == 0, r.stderr
+    # the reference writes output00000 after DEM::initDarcy
+    sb0 = readbin(path)
+    ds = DarcyState.from_spherebin(sb0)
+    darcy_init(config_from_spherebin(sb0), NU, state_from_spherebin(sb0).x, ds)
+    ds.to_spherebin(sb0)
+    stepper = _DarcyOracleStepper(oracle_libs["orc"], sb0, ds)
+    want_dir = tmp_path / "want"
+    driver.run(sb0, stepper, outdir=want_dir)
+    want = sorted(p.name for p in want_dir.iterdir())
+    got = sorted(p.name for p in (tmp_path / "output").iterdir())
+    assert got == want and len(got) >= 5
+    for name in want:
+        assert (tmp_path / "output" / name).read_bytes() == (want_dir / name).read_bytes(), name
+    assert (tmp_path / "d_phi.txt").read_text() == _darcy_text(stepper.ds, "phi")
+    assert (tmp_path / "d_K.txt").read_text() == _darcy_text(stepper.ds, "K")
+    last = readbin(want_dir / [n for n in want if n.endswith(".bin")][-1])
+    assert np.count_nonzero(last.f_v) > 0
