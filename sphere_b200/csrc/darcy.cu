@@ -29,7 +29,6 @@
 namespace sphk {
 
 constexpr int DARCY_BLOCK = 128;
-constexpr int GATHER = 8;   // particle loads in flight per porosity thread
 constexpr double D_PI = 3.14159265358979323846;   // M_PI, which src/darcy.cuh uses
 
 // node (x, y, z) with ghost nodes at -1 and num (src/darcy.cuh:125-135)
@@ -92,27 +91,17 @@ k_darcy_porosity(Dev d, DarcyDev f, int A)
                 if (!neighbour_cell(P, cx, cy, cz, dm)) continue;
                 const uint32_t c = (uint32_t)cx + (uint32_t)cy * nx + (nx * ny) * (uint32_t)cz;
                 const uint32_t beg = d.cell_start[c], end = d.cell_start[c + 1];
-                // the cell's particles GATHER at a time: their loads are in
-                // flight together, their subtractions stay in list order
-                for (uint32_t k0 = beg; k0 < end; k0 += GATHER) {
-                    double4 q[GATHER];
-#pragma unroll
-                    for (int j = 0; j < GATHER; ++j)
-                        if (k0 + j < end) q[j] = xr[__ldg(&d.cellorder[k0 + j])];
-#pragma unroll
-                    for (int j = 0; j < GATHER; ++j) {
-                        if (k0 + j >= end) break;
-                        const double4 p = q[j];
-                        const double r = p.w;
-                        const d3 dist = add(mk(X.x - p.x, X.y - p.y, X.z - p.z), dm);
-                        const double dd = flen(dist);
-                        if ((R - r) < dd && dd < (R + r))
-                            void_volume -= 1.0 / (12.0 * dd) *
-                                           (D_PI * (R + r - dd) * (R + r - dd) *
-                                            (dd * dd + 2.0 * dd * r - 3.0 * r * r + 2.0 * dd * R +
-                                             6.0 * r * R - 3.0 * R * R));
-                        if (dd <= R - r) void_volume -= 4.0 / 3.0 * D_PI * r * r * r;
-                    }
+                for (uint32_t k = beg; k < end; ++k) {
+                    const double4 p = xr[d.cellorder[k]];
+                    const double r = p.w;
+                    const d3 dist = add(mk(X.x - p.x, X.y - p.y, X.z - p.z), dm);
+                    const double dd = flen(dist);
+                    if ((R - r) < dd && dd < (R + r))
+                        void_volume -= 1.0 / (12.0 * dd) *
+                                       (D_PI * (R + r - dd) * (R + r - dd) *
+                                        (dd * dd + 2.0 * dd * r - 3.0 * r * r + 2.0 * dd * R +
+                                         6.0 * r * R - 3.0 * R * R));
+                    if (dd <= R - r) void_volume -= 4.0 / 3.0 * D_PI * r * r * r;
                 }
             }
     const double phi = fmin(0.9, fmax(0.1, void_volume / cell_volume));
