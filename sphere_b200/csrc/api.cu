@@ -101,6 +101,7 @@ struct sph_ctx {
     cudaEvent_t ckpt_ev = nullptr;        // orders a checkpoint copy against the caller's stream
     std::vector<void *> diff_allocs;
     size_t diff_bytes = 0;
+    double *bwd_scratch = nullptr;        // the backward's seeds and results, 13 np doubles
     AdjDev adj{};
     // graphs of one segment's re-run with the tape and of its reverse, by
     // (segment length, starting buffer)
@@ -1190,6 +1191,7 @@ static void free_diff(sph_ctx *c)
     c->diff_graphs.clear();
     for (void *p : c->diff_allocs) cudaFree(p);
     c->diff_allocs.clear();
+    c->bwd_scratch = nullptr;
     c->diff_bytes = 0;
     for (auto &k : c->ckpts) ckpt_release(c, k.buf);
     c->ckpts.clear();
@@ -1261,11 +1263,13 @@ int sph_diff_backward(sph_ctx *c, const double *x_bar, const double *v_bar, doub
     sph_ctx::Ckpt fin{};
     int rc = save_ckpt(c, fin);
     if (rc != SPH_OK) return rc;
-    // seeds: dL/dx and dL/dv of the current state
-    double *hx = nullptr;
+    // seeds: dL/dx and dL/dv of the current state; the scratch stays for the
+    // rest of the differentiable session
+    if (!c->bwd_scratch && (rc = dalloc(c, &c->bwd_scratch, 13 * (size_t)np, &c->diff_allocs)))
+        return rc;
+    double *hx = c->bwd_scratch;
+    double *out = c->bwd_scratch + 6 * (size_t)np;
     {
-        rc = dalloc(c, &hx, 6 * (size_t)np, &c->diff_allocs);
-        if (rc != SPH_OK) return rc;
         if (x_bar) CK(cudaMemcpy(hx, x_bar, (size_t)np * 24, cudaMemcpyHostToDevice));
         if (v_bar) CK(cudaMemcpy(hx + 3 * (size_t)np, v_bar, (size_t)np * 24, cudaMemcpyHostToDevice));
         launch_user_to_storage3(x_bar ? hx : nullptr, A.xb, d.uid, np, st);
@@ -1289,9 +1293,6 @@ int sph_diff_backward(sph_ctx *c, const double *x_bar, const double *v_bar, doub
     if ((rc = restore_ckpt(c, fin)) != SPH_OK) return rc;
     if ((rc = sync_status(c)) != SPH_OK) return rc;
     // results in the caller's order
-    double *out = nullptr;
-    rc = dalloc(c, &out, 7 * (size_t)np, &c->diff_allocs);
-    if (rc != SPH_OK) return rc;
     launch_storage_to_user1(A.mub, out, d.sidx, np, st);
     launch_storage_to_user3(A.xb, nullptr, out + np, d.sidx, np, st);
     launch_storage_to_user3(A.vb, A.v0b, out + 4 * (size_t)np, d.sidx, np, st);
@@ -1300,16 +1301,7 @@ int sph_diff_backward(sph_ctx *c, const double *x_bar, const double *v_bar, doub
     if (grad_mu) CK(cudaMemcpy(grad_mu, out, (size_t)np * 8, cudaMemcpyDeviceToHost));
     if (x0_bar) CK(cudaMemcpy(x0_bar, out + np, (size_t)np * 24, cudaMemcpyDeviceToHost));
     if (v0_bar) CK(cudaMemcpy(v0_bar, out + 4 * (size_t)np, (size_t)np * 24, cudaMemcpyDeviceToHost));
-    // scratch of this call and the final-state copy
-    ckpt_release(c, fin.buf);
-    const std::pair<void *, size_t> scratch[] = {
-        {out, 7 * (size_t)np * 8}, {hx, 6 * (size_t)np * 8}};
-    for (const auto &p : scratch) {
-        cudaFree(p.first);
-        auto &v = c->diff_allocs;
-        v.erase(std::remove(v.begin(), v.end(), p.first), v.end());
-        c->diff_bytes -= p.second;
-    }
+    ckpt_release(c, fin.buf);   // the final-state copy goes back to the pool
     return SPH_OK;
 }
 
