@@ -92,6 +92,10 @@ struct sph_ctx {
     // darcy.H[a ^ dflip] (both flip once per step)
     bool darcy_on = false;
     DarcyDev darcy{};
+    // in the step graphs the Darcy kernels run on a branch beside the force
+    // and wall kernels: forked after the cell list, joined at the step's end
+    cudaStream_t darcy_stream = nullptr;
+    cudaEvent_t darcy_fork = nullptr, darcy_join = nullptr;
     int dflip = 0;
     double mean_radius = 0.0;        // of the uploaded particles, summed in caller order
     // ray tracer scratch: per-pixel keys and image, per-particle values
@@ -278,11 +282,21 @@ int enqueue_one_step(sph_ctx *c, int a, int write_outputs, cudaStream_t st, bool
         launch_rebuild(c->d, c->np_all, c->ncells_all, a, st);
     }
     launch_bonds(c->d, c->hp.nb0, a, st);
+    // The Darcy block reads the step's start positions (buffer a) and its
+    // cell list, which nothing changes before the next step's rebuild, and
+    // writes only the fluid grid: in a graph it runs beside the force and
+    // wall kernels and joins before the step ends.
+    const bool branch = capturing && c->darcy_on && c->darcy_stream;
+    if (branch) {
+        CK(cudaEventRecord(c->darcy_fork, st));
+        CK(cudaStreamWaitEvent(c->darcy_stream, c->darcy_fork, 0));
+        launch_darcy(c->d, c->darcy, c->hp, a, a ^ c->dflip, c->darcy_stream);
+        CK(cudaEventRecord(c->darcy_join, c->darcy_stream));
+    }
     launch_step(c->d, c->np_all, (int)c->hp.contactmodel, a, write_outputs, st);
-    // the Darcy block reads the step's start positions (buffer a) and its
-    // cell list, neither of which the force kernel changes
-    if (c->darcy_on) launch_darcy(c->d, c->darcy, c->hp, a, a ^ c->dflip, st);
+    if (c->darcy_on && !branch) launch_darcy(c->d, c->darcy, c->hp, a, a ^ c->dflip, st);
     launch_walls(c->d, c->np_all, c->hp.nw, st);
+    if (branch) CK(cudaStreamWaitEvent(st, c->darcy_join, 0));
     return SPH_OK;
 }
 
@@ -1355,6 +1369,11 @@ int sph_darcy_upload(sph_ctx *c, double nu, const sph_darcy_state *h)
     // src/device.cu:673-678
     const double r_bar2 = c->mean_radius * 2.0;
     f.d_factor = r_bar2 * r_bar2 / 180.0 * 1.0e-6;
+    if (!c->darcy_stream) {
+        CK(cudaStreamCreateWithFlags(&c->darcy_stream, cudaStreamNonBlocking));
+        CK(cudaEventCreateWithFlags(&c->darcy_fork, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&c->darcy_join, cudaEventDisableTiming));
+    }
     c->darcy_on = true;
     drop_graphs(c);   // the step graphs gain the Darcy kernels
     return SPH_OK;
@@ -1432,6 +1451,9 @@ int sph_destroy(sph_ctx *c)
     for (char *b : c->ckpt_pool) cudaFree(b);
     if (c->rt_buf) cudaFree(c->rt_buf);
     if (c->ckpt_ev) cudaEventDestroy(c->ckpt_ev);
+    if (c->darcy_fork) cudaEventDestroy(c->darcy_fork);
+    if (c->darcy_join) cudaEventDestroy(c->darcy_join);
+    if (c->darcy_stream) cudaStreamDestroy(c->darcy_stream);
     for (void *p : c->allocs) cudaFree(p);
     if (c->stream) cudaStreamDestroy(c->stream);
     if (c->side) cudaStreamDestroy(c->side);

@@ -20,6 +20,8 @@ SCENES = {
     # shifts positions by +-L
     "periodic_xy": lambda: scenes.collision(n=900, seed=42, periodic=1, straddle=True),
     "periodic_x": lambda: scenes.collision(n=900, seed=43, periodic=2, straddle=True),
+    # a dynamic top wall beside the flow (the wall kernel runs in the same step)
+    "box_wall": lambda: scenes.collision(n=900, seed=45, periodic=0, nw=1),
 }
 
 
