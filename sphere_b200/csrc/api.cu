@@ -27,7 +27,7 @@ struct RenderArgs;
 void launch_maxpos(const Dev &d, uint32_t np, int a, unsigned long long *mx, cudaStream_t st);
 int render_image(const Dev &d, uint32_t np, int a, const double L[3], const double maxpos[3],
                  const sph_render_opts &o, double *values, unsigned long long *keys, uchar4 *img,
-                 cudaStream_t st);
+                 float *rays, cudaStream_t st);
 void launch_force_tape(const Dev &d, uint32_t np, int a, int tape_step, cudaStream_t st);
 void launch_rev_step(const Dev &d, const AdjDev &a, uint32_t np, int j, cudaStream_t st);
 void launch_user_to_storage3(const double *src, double4 *dst, const uint32_t *uid, uint32_t n,
@@ -1410,7 +1410,7 @@ int sph_render(sph_ctx *c, const sph_render_opts *o, uint8_t *rgba)
         return fail(c, SPH_ERR_TOO_LARGE, "sph_render: width * height must stay below 2^24");
     CK(cudaSetDevice(c->device));
     const size_t np = c->np_all;
-    const size_t need = 32 + pixels * 8 + pixels * 4 + np * 8;
+    const size_t need = 32 + pixels * 8 + pixels * 4 + np * 8 + (size_t)o->width * 24;
     if (c->rt_bytes < need) {
         if (c->rt_buf) cudaFree(c->rt_buf);
         c->rt_buf = nullptr;
@@ -1423,6 +1423,7 @@ int sph_render(sph_ctx *c, const sph_render_opts *o, uint8_t *rgba)
     auto *keys = reinterpret_cast<unsigned long long *>(base + 32);
     auto *img = reinterpret_cast<uchar4 *>(base + 32 + pixels * 8);
     auto *values = reinterpret_cast<double *>(base + 32 + pixels * 12);
+    auto *rays = reinterpret_cast<float *>(base + 32 + pixels * 12 + np * 8);
     cudaStream_t st = c->stream;
     // DEM::maxPos on the device, then the camera on the host
     CK(cudaMemsetAsync(mx, 0, 24, st));
@@ -1433,7 +1434,7 @@ int sph_render(sph_ctx *c, const sph_render_opts *o, uint8_t *rgba)
     double maxpos[3];
     for (int k = 0; k < 3; ++k) memcpy(&maxpos[k], &mxh[k], 8);
     CK(cudaMemsetAsync(keys, 0xff, pixels * 8, st));
-    render_image(c->d, c->np_all, c->a, c->hp.L, maxpos, *o, values, keys, img, st);
+    render_image(c->d, c->np_all, c->a, c->hp.L, maxpos, *o, values, keys, img, rays, st);
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(rgba, img, pixels * 4, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));

@@ -86,6 +86,24 @@ __device__ __forceinline__ fl3 ray_dir(const RenderArgs &g, uint32_t m)
     return (-g.cam.d * Wv + p_u * U) + p_v * V;
 }
 
+// The reference's direction is ((-D w) + p_u u) + p_v v (rayInitPerspective,
+// in that order): the first sum depends on the column only, the last term on
+// the (wrapped) row only.  They are tabulated once per image with the same
+// float operations, so a pixel's direction is A[column] + B[row], exactly.
+__global__ void __launch_bounds__(RT_BLOCK) k_rt_rays(RenderArgs g, fl3 *A, fl3 *B)
+{
+    const uint32_t t = blockIdx.x * RT_BLOCK + threadIdx.x;
+    if (t >= g.W) return;
+    const float *ip = g.cam.imgplane;
+    const fl3 U = f3(g.cam.u[0], g.cam.u[1], g.cam.u[2]);
+    const fl3 V = f3(g.cam.v[0], g.cam.v[1], g.cam.v[2]);
+    const fl3 Wv = f3(g.cam.w[0], g.cam.w[1], g.cam.w[2]);
+    const float p_u = ip[0] + (ip[1] - ip[0]) * (t + 0.5f) / g.W;
+    A[t] = -g.cam.d * Wv + p_u * U;
+    const float p_v = ip[2] + (ip[3] - ip[2]) * (t + 0.5f) / g.H;
+    B[t] = p_v * V;
+}
+
 // the reference's intersection (src/raytracer.cuh:84-108): true when the
 // discriminant is positive and |t_minus| < 1e10, with |t_minus| in *t
 __device__ __forceinline__ bool intersect(fl3 d, fl3 ec, float R, float *t)
@@ -141,7 +159,8 @@ __global__ void __launch_bounds__(RT_BLOCK) k_rt_maxpos(Dev d, int A, unsigned l
 }
 
 __global__ void __launch_bounds__(RT_BLOCK)
-k_rt_splat(Dev d, int A, RenderArgs g, const double *values, unsigned long long *keys)
+k_rt_splat(Dev d, int A, RenderArgs g, const double *values, const fl3 *__restrict__ colA,
+           const fl3 *__restrict__ rowB, unsigned long long *keys)
 {
     const uint32_t s = blockIdx.x * RT_BLOCK + threadIdx.x;
     if (s >= d.np_all) return;
@@ -213,14 +232,28 @@ k_rt_splat(Dev d, int A, RenderArgs g, const double *values, unsigned long long 
     const uint32_t H = g.H;
     for (uint32_t base = 0; base < H; base += (uint32_t)W) {
         const int ylo = (int)base + max(j0 - 1, 0), yhi = (int)base + min(j1 + 1, W - 1);
-        for (int y = ylo; y <= yhi && y < (int)H; ++y)
+        for (int y = ylo; y <= yhi && y < (int)H; ++y) {
+            // the row index floor((float)m / W) mod W does not decrease with
+            // m: equal at both ends of the box's row, it is the row's own
+            const uint32_t mrow = (uint32_t)y * g.W;
+            const uint32_t ja = (uint32_t)((int)floorf((float)(mrow + i0) / g.W) % (int)g.W);
+            const uint32_t jb = (uint32_t)((int)floorf((float)(mrow + i1) / g.W) % (int)g.W);
+            const fl3 Bj = rowB[ja];
             for (int xi = i0; xi <= i1; ++xi) {
-                const uint32_t m = (uint32_t)y * g.W + (uint32_t)xi;
+                const uint32_t m = mrow + (uint32_t)xi;
+                fl3 dir;
+                if (ja == jb) {
+                    dir = colA[xi] + Bj;
+                } else {
+                    const uint32_t j = (uint32_t)((int)floorf((float)m / g.W) % (int)g.W);
+                    dir = colA[xi] + rowB[j];
+                }
                 float t;
-                if (!intersect(ray_dir(g, m), ec, R, &t)) continue;
+                if (!intersect(dir, ec, R, &t)) continue;
                 const unsigned long long key = ((unsigned long long)__float_as_uint(t) << 32) | idx;
                 atomicMin(&keys[m], key);
             }
+        }
     }
 }
 
@@ -323,11 +356,12 @@ Camera make_camera(const double L[3], const double maxpos[3], uint32_t W, uint32
     return c;
 }
 
-// One image: the colour-map values, the splat and the resolve.  `keys`
-// must hold all ones (no hit) for every pixel.
+// One image: the colour-map values, the direction tables, the splat and
+// the resolve.  `keys` must hold all ones (no hit) for every pixel; `rays`
+// holds 2 * width directions.
 int render_image(const Dev &d, uint32_t np, int a, const double L[3], const double maxpos[3],
                  const sph_render_opts &o, double *values, unsigned long long *keys, uchar4 *img,
-                 cudaStream_t st)
+                 float *rays, cudaStream_t st)
 {
     RenderArgs g{};
     g.cam = make_camera(L, maxpos, o.width, o.height);
@@ -337,8 +371,10 @@ int render_image(const Dev &d, uint32_t np, int a, const double L[3], const doub
     g.maxval = o.maxval;
     g.lower_cutoff = o.lower_cutoff;
     const unsigned gp = div_up(np, RT_BLOCK);
+    fl3 *colA = reinterpret_cast<fl3 *>(rays), *rowB = colA + g.W;
     if (g.method > 0) k_rt_values<<<gp, RT_BLOCK, 0, st>>>(d, a, g.method, values);
-    k_rt_splat<<<gp, RT_BLOCK, 0, st>>>(d, a, g, values, keys);
+    k_rt_rays<<<div_up(g.W, RT_BLOCK), RT_BLOCK, 0, st>>>(g, colA, rowB);
+    k_rt_splat<<<gp, RT_BLOCK, 0, st>>>(d, a, g, values, colA, rowB, keys);
     k_rt_resolve<<<div_up((uint64_t)g.W * g.H, RT_BLOCK), RT_BLOCK, 0, st>>>(d, a, g, values, keys, img);
     return 0;
 }
