@@ -166,6 +166,62 @@ const char *status_msg(int code)
     }
 }
 
+// ---- host -> device conversion kernels -------------------------------------
+// The caller's rows are copied as they are into device staging and repacked
+// here, so a pinned host buffer goes over the bus at full speed and the host
+// runs no per-particle loop.  At upload, storage order is the caller's order.
+
+// four-double host rows: the first three into `dst`, the fourth into lane
+// `lane` of w_user
+__global__ void k_user_to_p3(const double4 *src, P3 *dst, double *w, int lane, uint32_t n)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double4 v = src[i];
+    dst[i] = P3{v.x, v.y, v.z};
+    w[WLANES * (size_t)i + lane] = v.w;
+}
+
+// the fixvel flag of the integration (vel.w > 0)
+__global__ void k_fixed_flags(const double4 *vel, uint8_t *fixed, uint32_t n)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) fixed[i] = vel[i].w > 0.0f ? 1 : 0;
+}
+
+// acc / angacc rows with their unused fourth lane cleared
+__global__ void k_rows_zero_w(const double4 *src, double4 *dst, uint32_t n)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double4 v = src[i];
+    dst[i] = make_double4(v.x, v.y, v.z, 0.0);
+}
+
+// planar es, ev into the interleaved esv rows
+__global__ void k_pack2(const double *a, const double *b, double2 *dst, uint32_t n)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) dst[i] = make_double2(a[i], b[i]);
+}
+
+// planar es_dot, ev_dot, p into the edp rows
+__global__ void k_pack3(const double *a, const double *b, const double *c, double4 *dst, uint32_t n)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) dst[i] = make_double4(a[i], b[i], c[i], 0.0);
+}
+
+// the identity storage order of an upload
+__global__ void k_iota3(uint32_t *a, uint32_t *b, uint32_t *c, uint32_t n)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    a[i] = i;
+    b[i] = i;
+    c[i] = i;
+}
+
 // ---- device -> host conversion kernels ------------------------------------
 template <typename T>
 __global__ void k_to_user(const T *src, T *dst, const uint32_t *sidx, uint32_t n)
@@ -182,6 +238,16 @@ __global__ void k_p3_to_user(const P3 *src, const double *w, int lane, double4 *
     if (u >= n) return;
     const P3 v = src[sidx[u]];
     dst[u] = make_double4(v.x, v.y, v.z, w[WLANES * (size_t)u + lane]);
+}
+
+// one lane of interleaved rows (esv, edp) in caller order, planar
+template <typename T, int K>
+__global__ void k_lane_to_user(const T *src, double *dst, const uint32_t *sidx, uint32_t n)
+{
+    const uint32_t u = blockIdx.x * blockDim.x + threadIdx.x;
+    if (u >= n) return;
+    const T v = src[sidx[u]];
+    dst[u] = reinterpret_cast<const double *>(&v)[K];
 }
 
 __global__ void k_rows_to_user(Dev d, uint32_t *contacts, double4 *distmod, double4 *delta_t,
@@ -615,13 +681,16 @@ int sph_upload(sph_ctx *c, const sph_host_state *h)
         for (size_t i = 0; i < np; ++i) r_sum += h->x[4 * i + 3];
         c->mean_radius = r_sum / (double)np;
     }
-    // scene of every particle (particles of scene i follow those of scene i-1)
-    std::vector<uint32_t> inst_of(np, 0u);
-    for (uint32_t i = 0; i < c->ninst; ++i)
-        for (uint32_t u = 0; u < c->hps[i].np; ++u) inst_of[c->hps[i].uid_base + u] = i;
+    // scene of every particle (particles of scene i follow those of scene i-1),
+    // for batched contexts and for contact rows given by the caller
+    std::vector<uint32_t> inst_of;
+    if (c->batched || h->contacts) {
+        inst_of.assign(np, 0u);
+        for (uint32_t i = 0; i < c->ninst; ++i)
+            for (uint32_t u = 0; u < c->hps[i].np; ++u) inst_of[c->hps[i].uid_base + u] = i;
+    }
     if (c->batched) CK(cudaMemcpy(d.inst, inst_of.data(), np * 4, cudaMemcpyHostToDevice));
     // kinematics (identity storage order for now)
-    std::vector<double> buf(np * 4);
     CK(cudaMemcpy(d.xr[A], h->x, np * 32, cudaMemcpyHostToDevice));
     {
         // largest radius of each scene, for the cell-level distance test of
@@ -656,7 +725,11 @@ int sph_upload(sph_ctx *c, const sph_host_state *h)
         // vel, angvel, vel0, angvel0, angpos: three doubles on the device, the
         // fourth lane kept by caller index for the download; fixvel > 0 as a
         // flag for the integration
-        std::vector<double> p3(np * 3), w(np * WLANES);
+        // the caller's rows go to device staging as they are and are
+        // repacked there (stream order serialises the reuse of the staging)
+        cudaStream_t st = c->stream;
+        const unsigned g = div_up(np, 256);
+        double4 *stage = static_cast<double4 *>(c->scratch);
         const double *src[WLANES];
         P3 *dst[WLANES];
         src[W_VEL0] = h->vel0 ? h->vel0 : h->vel;
@@ -670,57 +743,33 @@ int sph_upload(sph_ctx *c, const sph_host_state *h)
         dst[W_ANGVEL] = d.angvel[A];
         dst[W_VEL] = d.vel[A];
         for (int f = 0; f < WLANES; ++f) {
-            for (size_t i = 0; i < np; ++i) {
-                for (int k = 0; k < 3; ++k) p3[3 * i + k] = src[f][4 * i + k];
-                w[WLANES * i + f] = src[f][4 * i + 3];
+            CK(cudaMemcpyAsync(stage, src[f], np * 32, cudaMemcpyHostToDevice, st));
+            k_user_to_p3<<<g, 256, 0, st>>>(stage, dst[f], d.w_user, f, (uint32_t)np);
+            if (f == W_VEL) k_fixed_flags<<<g, 256, 0, st>>>(stage, d.fixed, (uint32_t)np);
+        }
+        CK(cudaMemcpyAsync(d.force, h->force, np * 32, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(d.torque, h->torque, np * 32, cudaMemcpyHostToDevice, st));
+        const std::pair<const double *, double4 *> accs[] = {{h->acc, d.acc}, {h->angacc, d.angacc}};
+        for (const auto &a : accs) {
+            if (a.first) {
+                CK(cudaMemcpyAsync(stage, a.first, np * 32, cudaMemcpyHostToDevice, st));
+                k_rows_zero_w<<<g, 256, 0, st>>>(stage, a.second, (uint32_t)np);
+            } else {
+                CK(cudaMemsetAsync(a.second, 0, np * 32, st));
             }
-            CK(cudaMemcpy(dst[f], p3.data(), np * 24, cudaMemcpyHostToDevice));
         }
-        CK(cudaMemcpy(d.w_user, w.data(), np * 8 * WLANES, cudaMemcpyHostToDevice));
-        std::vector<uint8_t> fx(np);
-        for (size_t i = 0; i < np; ++i) fx[i] = h->vel[4 * i + 3] > 0.0f ? 1 : 0;
-        CK(cudaMemcpy(d.fixed, fx.data(), np, cudaMemcpyHostToDevice));
-    }
-    CK(cudaMemcpy(d.force, h->force, np * 32, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(d.torque, h->torque, np * 32, cudaMemcpyHostToDevice));
-    if (h->acc) {
-        for (size_t i = 0; i < np; ++i) {
-            for (int k = 0; k < 3; ++k) buf[4 * i + k] = h->acc[4 * i + k];
-            buf[4 * i + 3] = 0.0;
-        }
-        CK(cudaMemcpy(d.acc, buf.data(), np * 32, cudaMemcpyHostToDevice));
-    } else {
-        CK(cudaMemset(d.acc, 0, np * 32));
-    }
-    if (h->angacc) {
-        for (size_t i = 0; i < np; ++i) {
-            for (int k = 0; k < 3; ++k) buf[4 * i + k] = h->angacc[4 * i + k];
-            buf[4 * i + 3] = 0.0;
-        }
-        CK(cudaMemcpy(d.angacc, buf.data(), np * 32, cudaMemcpyHostToDevice));
-    } else {
-        CK(cudaMemset(d.angacc, 0, np * 32));
-    }
-    CK(cudaMemcpy(d.xysum, h->xysum, np * 16, cudaMemcpyHostToDevice));
-    {
-        std::vector<double> esv(np * 2), edp(np * 4);
-        for (size_t i = 0; i < np; ++i) {
-            esv[2 * i] = h->es[i];
-            esv[2 * i + 1] = h->ev[i];
-            edp[4 * i] = h->es_dot[i];
-            edp[4 * i + 1] = h->ev_dot[i];
-            edp[4 * i + 2] = h->p[i];
-            edp[4 * i + 3] = 0.0;
-        }
-        CK(cudaMemcpy(d.esv, esv.data(), np * 16, cudaMemcpyHostToDevice));
-        CK(cudaMemcpy(d.edp, edp.data(), np * 32, cudaMemcpyHostToDevice));
-    }
-    {
-        std::vector<uint32_t> ident(np);
-        for (size_t i = 0; i < np; ++i) ident[i] = (uint32_t)i;
-        CK(cudaMemcpy(d.uid, ident.data(), np * 4, cudaMemcpyHostToDevice));
-        CK(cudaMemcpy(d.sidx, ident.data(), np * 4, cudaMemcpyHostToDevice));
-        CK(cudaMemcpy(d.cellorder, ident.data(), np * 4, cudaMemcpyHostToDevice));
+        CK(cudaMemcpyAsync(d.xysum, h->xysum, np * 16, cudaMemcpyHostToDevice, st));
+        double *planar = reinterpret_cast<double *>(stage);
+        CK(cudaMemcpyAsync(planar, h->es, np * 8, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(planar + np, h->ev, np * 8, cudaMemcpyHostToDevice, st));
+        k_pack2<<<g, 256, 0, st>>>(planar, planar + np, d.esv, (uint32_t)np);
+        CK(cudaMemcpyAsync(planar, h->es_dot, np * 8, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(planar + np, h->ev_dot, np * 8, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(planar + 2 * np, h->p, np * 8, cudaMemcpyHostToDevice, st));
+        k_pack3<<<g, 256, 0, st>>>(planar, planar + np, planar + 2 * np, d.edp, (uint32_t)np);
+        k_iota3<<<g, 256, 0, st>>>(d.uid, d.sidx, d.cellorder, (uint32_t)np);
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(st));
     }
     // contact slots: partners, periodic-shift codes, occupancy, history
     if (!h->contacts) {
@@ -930,7 +979,6 @@ int sph_download(sph_ctx *c, sph_host_state *h)
         if (!dst) return SPH_OK;
         k_to_user<double4><<<grid, 256, 0, c->stream>>>(src, t4, d.sidx, np);
         CK(cudaMemcpyAsync(dst, t4, (size_t)np * 32, cudaMemcpyDeviceToHost, c->stream));
-        CK(cudaStreamSynchronize(c->stream));
         return SPH_OK;
     };
     int rc;
@@ -938,7 +986,6 @@ int sph_download(sph_ctx *c, sph_host_state *h)
         if (!dst) return SPH_OK;
         k_p3_to_user<<<grid, 256, 0, c->stream>>>(src, d.w_user, lane, t4, d.sidx, np);
         CK(cudaMemcpyAsync(dst, t4, (size_t)np * 32, cudaMemcpyDeviceToHost, c->stream));
-        CK(cudaStreamSynchronize(c->stream));
         return SPH_OK;
     };
     if ((rc = get4(d.xr[A], h->x)) || (rc = get3(d.vel[A], W_VEL, h->vel)) ||
@@ -948,28 +995,30 @@ int sph_download(sph_ctx *c, sph_host_state *h)
         (rc = get4(d.angacc, h->angacc)) || (rc = get4(d.torque, h->torque)))
         return rc;
     {
+        // xysum, and the lanes of esv / edp as the caller's planar arrays,
+        // copied straight into them
         double2 *t2 = static_cast<double2 *>(c->scratch);
-        std::vector<double> tmp((size_t)np * 2);
-        k_to_user<double2><<<grid, 256, 0, c->stream>>>(d.xysum, t2, d.sidx, np);
-        CK(cudaMemcpyAsync(tmp.data(), t2, (size_t)np * 16, cudaMemcpyDeviceToHost, c->stream));
-        CK(cudaStreamSynchronize(c->stream));
-        if (h->xysum) memcpy(h->xysum, tmp.data(), (size_t)np * 16);
-        k_to_user<double2><<<grid, 256, 0, c->stream>>>(d.esv, t2, d.sidx, np);
-        CK(cudaMemcpyAsync(tmp.data(), t2, (size_t)np * 16, cudaMemcpyDeviceToHost, c->stream));
-        CK(cudaStreamSynchronize(c->stream));
-        for (uint32_t i = 0; i < np; ++i) {
-            if (h->es) h->es[i] = tmp[2 * i];
-            if (h->ev) h->ev[i] = tmp[2 * i + 1];
+        double *t1 = static_cast<double *>(c->scratch);
+        cudaStream_t st = c->stream;
+        if (h->xysum) {
+            k_to_user<double2><<<grid, 256, 0, st>>>(d.xysum, t2, d.sidx, np);
+            CK(cudaMemcpyAsync(h->xysum, t2, (size_t)np * 16, cudaMemcpyDeviceToHost, st));
         }
-        std::vector<double> e4((size_t)np * 4);
-        k_to_user<double4><<<grid, 256, 0, c->stream>>>(d.edp, t4, d.sidx, np);
-        CK(cudaMemcpyAsync(e4.data(), t4, (size_t)np * 32, cudaMemcpyDeviceToHost, c->stream));
-        CK(cudaStreamSynchronize(c->stream));
-        for (uint32_t i = 0; i < np; ++i) {
-            if (h->es_dot) h->es_dot[i] = e4[4 * i];
-            if (h->ev_dot) h->ev_dot[i] = e4[4 * i + 1];
-            if (h->p) h->p[i] = e4[4 * i + 2];
+        const struct { double *dst; int src; } lanes[] = {
+            {h->es, 0}, {h->ev, 1}, {h->es_dot, 2}, {h->ev_dot, 3}, {h->p, 4}};
+        for (const auto &l : lanes) {
+            if (!l.dst) continue;
+            switch (l.src) {
+            case 0: k_lane_to_user<double2, 0><<<grid, 256, 0, st>>>(d.esv, t1, d.sidx, np); break;
+            case 1: k_lane_to_user<double2, 1><<<grid, 256, 0, st>>>(d.esv, t1, d.sidx, np); break;
+            case 2: k_lane_to_user<double4, 0><<<grid, 256, 0, st>>>(d.edp, t1, d.sidx, np); break;
+            case 3: k_lane_to_user<double4, 1><<<grid, 256, 0, st>>>(d.edp, t1, d.sidx, np); break;
+            default: k_lane_to_user<double4, 2><<<grid, 256, 0, st>>>(d.edp, t1, d.sidx, np); break;
+            }
+            CK(cudaMemcpyAsync(l.dst, t1, (size_t)np * 8, cudaMemcpyDeviceToHost, st));
         }
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(st));
     }
     if (h->contacts || h->distmod || h->delta_t) {
         rc = sph_get_contacts(c, h->contacts, h->distmod, h->delta_t);
