@@ -38,11 +38,28 @@ constexpr int FORCE_BLOCK = 128;
 #define SPHK_FORCE_MIN_BLOCKS 8
 #endif
 
+// What one law adds to a particle's sums.  The laws are out of line and
+// return their terms by value, so the caller's sums stay in registers (a
+// reference into them would put them in local memory for the whole
+// kernel).  Each reference update `s += term` is the caller's `s + term`,
+// the same operation.
+struct WallOut {
+    d3 f, t;       // F += f, T += t
+    double pr;     // p += pr
+    double fn;     // the normal force along n (walls_force_pp)
+};
+struct LawOut {
+    d3 f, t;           // F += f, T += t
+    double pr, ev;     // p += pr, ev_dot += ev
+    double es;         // es_dot += es, where es_set
+    bool es_set;
+    double4 dt4;       // the slot's new tangential history
+};
+
 // contactLinear_wall, src/contactmodels.cuh:10-109.  Out of line: six call
 // sites, taken only by particles touching a wall.
-__device__ __noinline__ double contact_wall(const Params &P, d3 &F, d3 &T, double &p,
-                                               double ra, double4 vel_a, double4 angvel_a,
-                                               d3 n, double delta, double wvel)
+__device__ __noinline__ WallOut contact_wall(const Params &P, double ra, double4 vel_a,
+                                             double4 angvel_a, d3 n, double delta, double wvel)
 {
     const d3 linvel = xyz(vel_a), angvel = xyz(angvel_a);
     const d3 vel = adds(add(linvel, smul(ra, cross(n, angvel))), wvel);
@@ -62,20 +79,24 @@ __device__ __noinline__ double contact_wall(const Params &P, d3 &F, d3 &T, doubl
         if (f_t_visc < f_t_limit) f_t = divs(smul(-1.0f * f_t_visc, vel_t), vel_t_length);
         else f_t = divs(smul(-1.0f * f_t_limit, vel_t), vel_t_length);
     }
-    F = add(F, add(f_n, f_t));
-    T = add(T, add(smul(-ra, cross(n, f_t)), T_res));
-    p += f_n_length / (4.0f * REF_PI * ra * ra);
-    return dot(f_n, n);
+    WallOut o;
+    o.f = add(f_n, f_t);
+    o.t = add(smul(-ra, cross(n, f_t)), T_res);
+    o.pr = f_n_length / (4.0f * REF_PI * ra * ra);
+    o.fn = dot(f_n, n);
+    return o;
 }
 
 // contactLinear, src/contactmodels.cuh:283-493 (contact model 2).  Out of
 // line so that particles without contacts run a lean kernel.
-__device__ __noinline__ void contact_linear(const Params &P, d3 &F, d3 &T, double &es_dot,
-                                               double &ev_dot, double &p, double4 vel_a,
-                                               d3 angvel_a, double4 vel_b4, double4 angvel_b4,
-                                               double ra, double rb, d3 x, double x_length,
-                                               double delta, double4 &dt4)
+__device__ __noinline__ LawOut contact_linear(const Params &P, double4 vel_a, d3 angvel_a,
+                                              double4 vel_b4, double4 angvel_b4, double ra,
+                                              double rb, d3 x, double x_length, double delta,
+                                              double4 dt4)
 {
+    LawOut o;
+    o.es = 0.0;
+    o.es_set = false;
     const double dt = P.dt;
     const d3 vel_b = xyz(vel_b4), angvel_b = xyz(angvel_b4);
     const d3 dt0u = xyz(dt4);
@@ -90,7 +111,7 @@ __device__ __noinline__ void contact_linear(const Params &P, d3 &F, d3 &T, doubl
     const double delta_t0_length = flen(delta_t0);
     d3 delta_t = mk(0.0, 0.0, 0.0);   // the reference leaves it unset when unused
     d3 f_n = smul(-P.k_n * delta - P.gamma_n * vel_n, n);
-    ev_dot += P.gamma_n * vel_n * vel_n;
+    o.ev = P.gamma_n * vel_n * vel_n;
     if (dot(f_n, n) < 0.0f) f_n = mk(0.0, 0.0, 0.0);
     const double f_n_length = flen(f_n);
     const d3 f_c = smul(-P.kappa * fsqrt_of(ra * rb), n);
@@ -107,13 +128,15 @@ __device__ __noinline__ void contact_linear(const Params &P, d3 &F, d3 &T, doubl
             f_t = smul(f_t_limit, t);
             delta_t = smul(-1.0 / P.k_t,
                            add(smul(P.mu_d * flen(sub(f_n, f_c)), t), smul(P.gamma_t, vel_t)));
-            es_dot += flen(muls(smul(flen(f_t), vel_t), dt)) / dt;
+            o.es = flen(muls(smul(flen(f_t), vel_t), dt)) / dt;
+            o.es_set = true;
         }
     }
-    F = add(F, add(add(f_n, f_t), f_c));
-    T = add(T, cross(smul(-(ra + delta * 0.5), n), f_t));
-    p += f_n_length / (4.0f * REF_PI * ra * ra);
-    dt4 = make_double4(delta_t.x, delta_t.y, delta_t.z, 0.0f);
+    o.f = add(add(f_n, f_t), f_c);
+    o.t = cross(smul(-(ra + delta * 0.5), n), f_t);
+    o.pr = f_n_length / (4.0f * REF_PI * ra * ra);
+    o.dt4 = make_double4(delta_t.x, delta_t.y, delta_t.z, 0.0f);
+    return o;
 }
 
 // The FP32 transcendentals of the force laws (expf in capillaryCohesion_exp,
@@ -182,12 +205,14 @@ __device__ __noinline__ void capillary_exp(const Params &P, d3 &F, double ra, do
 // contactHertz, src/contactmodels.cuh:499-666 (contact model 3).  As in the
 // reference, delta is the (negative) overlap, so its fractional powers are
 // NaN and so are the forces of every touching pair.
-__device__ __noinline__ void contact_hertz(const Params &P, d3 &F, d3 &T, double &es_dot,
-                                              double &ev_dot, double &p, double4 vel_a,
-                                              d3 angvel_a, double4 vel_b4, double4 angvel_b4,
-                                              double ra, double rb, d3 x, double x_length,
-                                              double delta, double4 &dt4)
+__device__ __noinline__ LawOut contact_hertz(const Params &P, double4 vel_a, d3 angvel_a,
+                                             double4 vel_b4, double4 angvel_b4, double ra,
+                                             double rb, d3 x, double x_length, double delta,
+                                             double4 dt4)
 {
+    LawOut o;
+    o.es = 0.0;
+    o.es_set = false;
     const double dt = P.dt;
     const d3 vel_b = xyz(vel_b4), angvel_b = xyz(angvel_b4);
     const d3 dt0u = xyz(dt4);
@@ -205,7 +230,7 @@ __device__ __noinline__ void contact_hertz(const Params &P, d3 &F, d3 &T, double
     d3 delta_t = mk(0.0, 0.0, 0.0);   // the reference leaves it unset when unused
     d3 f_n = smul(-P.k_n * f32_powf(delta, 3.0f / 2.0f)
                       - P.gamma_n * f32_powf(delta, 1.0f / 4.0f) * vel_n, n);
-    ev_dot += P.gamma_n * vel_n * vel_n;
+    o.ev = P.gamma_n * vel_n * vel_n;
     if (dot(f_n, n) < 0.0f) f_n = mk(0.0, 0.0, 0.0);
     const double f_n_length = flen(f_n);
     const d3 f_c = smul(-P.kappa * fsqrt_of(ra * rb), n);
@@ -223,7 +248,8 @@ __device__ __noinline__ void contact_hertz(const Params &P, d3 &F, d3 &T, double
             f_t = muls(f_t, f_t_limit / f_t_length);
             delta_t = divs(add(f_t, smul(P.gamma_t * f32_powf(delta, 1.0f / 4.0f), vel_t)),
                            -P.k_t * f32_powf(delta, 1.0f / 2.0f));
-            es_dot += flen(sub(delta_t0, delta_t)) * P.k_t / dt;
+            o.es = flen(sub(delta_t0, delta_t)) * P.k_t / dt;
+            o.es_set = true;
         } else {
             delta_t = add(delta_t0, muls(vel_t, dt));
         }
@@ -234,10 +260,11 @@ __device__ __noinline__ void contact_hertz(const Params &P, d3 &F, d3 &T, double
                           angvel_ab),
                      angvel_ab_length);
     }
-    F = add(F, add(add(f_n, f_t), f_c));
-    T = add(T, add(smul(-(ra + delta / 2.0), cross(n, f_t)), T_res));
-    p += f_n_length / (4.0f * REF_PI * ra * ra);
-    dt4 = make_double4(delta_t.x, delta_t.y, delta_t.z, 0.0f);
+    o.f = add(add(f_n, f_t), f_c);
+    o.t = add(smul(-(ra + delta / 2.0), cross(n, f_t)), T_res);
+    o.pr = f_n_length / (4.0f * REF_PI * ra * ra);
+    o.dt4 = make_double4(delta_t.x, delta_t.y, delta_t.z, 0.0f);
+    return o;
 }
 
 __device__ __forceinline__ uint32_t dm_get(unsigned long long lo, unsigned long long hi, int i)
@@ -742,14 +769,17 @@ k_force(ForceArgs args)
             const double xlen = flen(xab);
             const double delta_n = xlen - (ra + rb);
             if (delta_n < 0.0f) {
-                double4 dt4 = dtrow[i];
-                if (MODEL == 2)
-                    contact_linear(P, F, T, es_dot, ev_dot, p, vel_a, angvel_a, ld4(d.vel[A], t),
-                                   ld4(d.angvel[A], t), ra, rb, xab, xlen, delta_n, dt4);
-                else
-                    contact_hertz(P, F, T, es_dot, ev_dot, p, vel_a, angvel_a, ld4(d.vel[A], t),
-                                  ld4(d.angvel[A], t), ra, rb, xab, xlen, delta_n, dt4);
-                dtrow[i] = dt4;
+                const LawOut o = (MODEL == 2)
+                    ? contact_linear(P, vel_a, angvel_a, ld4(d.vel[A], t), ld4(d.angvel[A], t), ra,
+                                     rb, xab, xlen, delta_n, dtrow[i])
+                    : contact_hertz(P, vel_a, angvel_a, ld4(d.vel[A], t), ld4(d.angvel[A], t), ra,
+                                    rb, xab, xlen, delta_n, dtrow[i]);
+                F = add(F, o.f);
+                T = add(T, o.t);
+                p += o.pr;
+                ev_dot += o.ev;
+                if (o.es_set) es_dot += o.es;
+                dtrow[i] = o.dt4;
             } else {
                 // separated: free the slot and zero its history
                 occ &= ~(1u << i);
@@ -782,27 +812,29 @@ k_force(ForceArgs args)
         auto wpos = [&](int k, double dflt) { return ((uint32_t)k < P.nw) ? W.nx[k].w : dflt; };
         auto wnrm = [&](int k, d3 dflt) { return ((uint32_t)k < P.nw) ? xyz(W.nx[k]) : dflt; };
         auto wvel = [&](int k) { return ((uint32_t)k < P.nw) ? W.mvfd[k].y : 0.0; };
+        auto wall = [&](d3 n, double dw, double wv) {
+            const WallOut o = contact_wall(P, ra, vel_a, angvel_a4, n, dw, wv);
+            F = add(F, o.f);
+            T = add(T, o.t);
+            p += o.pr;
+            return o.fn;
+        };
         double dw;
         dw = wpos(0, P.L[2]) - (xa.z + ra);
-        if (dw < 0.0f)
-            w0f = contact_wall(P, F, T, p, ra, vel_a, angvel_a4, wnrm(0, mk(0.0, 0.0, -1.0)), dw, wvel(0));
+        if (dw < 0.0f) w0f = wall(wnrm(0, mk(0.0, 0.0, -1.0)), dw, wvel(0));
         dw = xa.z - ra - P.origo[2];
-        if (dw < 0.0f) (void)contact_wall(P, F, T, p, ra, vel_a, angvel_a4, mk(0.0, 0.0, 1.0), dw, 0.0f);
+        if (dw < 0.0f) (void)wall(mk(0.0, 0.0, 1.0), dw, 0.0f);
         if (P.periodic == 0) {
             dw = wpos(1, P.L[0]) - (xa.x + ra);
-            if (dw < 0.0f)
-                (void)contact_wall(P, F, T, p, ra, vel_a, angvel_a4, wnrm(1, mk(-1.0, 0.0, 0.0)), dw, wvel(1));
+            if (dw < 0.0f) (void)wall(wnrm(1, mk(-1.0, 0.0, 0.0)), dw, wvel(1));
             dw = xa.x - ra - wpos(2, 0.0);
-            if (dw < 0.0f)
-                (void)contact_wall(P, F, T, p, ra, vel_a, angvel_a4, wnrm(2, mk(1.0, 0.0, 0.0)), dw, wvel(2));
+            if (dw < 0.0f) (void)wall(wnrm(2, mk(1.0, 0.0, 0.0)), dw, wvel(2));
         }
         if (P.periodic == 0 || P.periodic == 2) {
             dw = wpos(3, P.L[1]) - (xa.y + ra);
-            if (dw < 0.0f)
-                (void)contact_wall(P, F, T, p, ra, vel_a, angvel_a4, wnrm(3, mk(0.0, -1.0, 0.0)), dw, wvel(3));
+            if (dw < 0.0f) (void)wall(wnrm(3, mk(0.0, -1.0, 0.0)), dw, wvel(3));
             dw = xa.y - ra - wpos(4, 0.0);
-            if (dw < 0.0f)
-                (void)contact_wall(P, F, T, p, ra, vel_a, angvel_a4, wnrm(4, mk(0.0, 1.0, 0.0)), dw, wvel(4));
+            if (dw < 0.0f) (void)wall(wnrm(4, mk(0.0, 1.0, 0.0)), dw, wvel(4));
         }
     }
 
