@@ -27,12 +27,19 @@
 
 namespace sphk {
 
-constexpr int TOPO_BLOCK = 128;
-constexpr int FORCE_BLOCK = 128;
-// Resident blocks per SM that the register allocation must allow (the
-// __launch_bounds__ minimum), from a sweep of caps at 1M spheres.
+// Threads per block, and resident blocks per SM that the register
+// allocation must allow (the __launch_bounds__ minimum), from sweeps of
+// block shapes and caps at 1M spheres.
+#ifndef SPHK_TOPO_BLOCK
+#define SPHK_TOPO_BLOCK 64
+#endif
+#ifndef SPHK_FORCE_BLOCK
+#define SPHK_FORCE_BLOCK 128
+#endif
+constexpr int TOPO_BLOCK = SPHK_TOPO_BLOCK;
+constexpr int FORCE_BLOCK = SPHK_FORCE_BLOCK;
 #ifndef SPHK_TOPO_MIN_BLOCKS
-#define SPHK_TOPO_MIN_BLOCKS 10
+#define SPHK_TOPO_MIN_BLOCKS 20
 #endif
 #ifndef SPHK_FORCE_MIN_BLOCKS
 #define SPHK_FORCE_MIN_BLOCKS 8
