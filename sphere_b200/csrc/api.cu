@@ -596,6 +596,7 @@ int create_impl(const sph_config *cfgs, uint32_t ninst, bool batched, sph_ctx **
     AL(d.vl_gap, np);
     AL(d.movers, MOVER_CAP); AL(d.dirty, ncells + 1); AL(d.vs, 1);
     AL(d.wf_pp, np); AL(d.wtouch, np); AL(d.wf_partial, div_up(np, 256));
+    AL(d.wf_flag, div_up(np, 256));
     AL(d.walls, 1);
     AL(d.bonds, nb0); AL(d.bonds_delta, nb0); AL(d.bonds_omega, nb0);
     AL(d.bond_f, nb0); AL(d.bond_t, nb0); AL(d.bond_xu, nb0);
@@ -824,6 +825,7 @@ int sph_upload(sph_ctx *c, const sph_host_state *h)
     }
     CK(cudaMemset(d.wf_pp, 0, np * sizeof(double)));
     CK(cudaMemset(d.wtouch, 0, np));
+    CK(cudaMemset(d.wf_flag, 0, div_up(np, 256)));
     // bonds and their per-particle lists (by user index, in bond order)
     if (nb0 > 0) {
         std::vector<uint32_t> ptr(np + 1, 0), list;

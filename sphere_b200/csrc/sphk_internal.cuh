@@ -170,6 +170,7 @@ struct Dev {
     double *wf_pp;        // [np] wall-0 force by uid
     uint8_t *wtouch;      // [np] by storage index: wall-0 force was nonzero
     double *wf_partial;   // [ceil(np/256)]
+    uint8_t *wf_flag;     // [ceil(np/256)] a wall-0 force of the 256-block was written
     Walls *walls;
     // bonds (user indices, as the reference stores them)
     uint2 *bonds;

@@ -428,6 +428,12 @@ k_topo(Dev d, int A)
         d.vs->movers_overflow = 0u;
     }
     if (s >= np) return;
+    // After a position left the grid (the step reports SPH_ERR_OUT_OF_GRID)
+    // the scene has come apart: saturated cell ids pile its particles into
+    // the edge cells, where the stencil sweep grows with the square of their
+    // count.  The search stops for the rest of the call; an upload clears
+    // the status.  A batch goes on, since its other scenes are still sound.
+    if (!BATCH && (*(volatile const uint32_t *)d.status & ST_OUT_OF_GRID)) return;
     const Params &P = prm_at<BATCH>(d, s);
     const Verlet &V = *d.vs;
     // The list decision first, from a few bytes: a valid list whose gap
@@ -878,7 +884,9 @@ k_force(ForceArgs args)
     if (P.nw > 0) {
         const uint8_t touched = d.wtouch[s];
         if (w0f != 0.0 || touched) {
-            d.wf_pp[d.uid[s]] = w0f;
+            const uint32_t u = d.uid[s];
+            d.wf_pp[u] = w0f;
+            d.wf_flag[u / 256u] = 1;
             d.wtouch[s] = (w0f != 0.0) ? 1 : 0;
         }
     }

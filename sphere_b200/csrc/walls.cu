@@ -8,6 +8,13 @@
 // (atomic ticket, no waiting) adds the partials and moves the walls.  Partials
 // equal to +0.0 are skipped in that serial fold: the running sum starts at
 // +0.0 and is never -0.0, so adding +0.0 leaves it unchanged bit for bit.
+//
+// Only the 256-blocks that the force kernel wrote a wall-0 force into this
+// step (wf_flag) are read.  Every other block holds zeros only (+0.0, or a
+// -0.0 that the reference's `temp = 0; temp += f` turns into +0.0), whose
+// tree sum is +0.0: its partial is written as +0.0 without reading it.  An
+// entry changes only when it is written, and a write flags its block, so a
+// block that turned nonzero, changed or went back to zero is always read.
 #include "sphk_internal.cuh"
 
 namespace sphk {
@@ -46,7 +53,9 @@ k_walls(Dev d)
     // pairing order: lane l holds c[l + 32 m], m = 0..7; levels 128, 64 and
     // 32 pair registers of a lane, levels 16..1 pair lanes (shfl_down).
     const uint32_t rb = blockIdx.x * WARPS + warp;
-    if (rb < nref) {
+    if (rb < nref && d.wf_flag[rb] == 0) {
+        if (lane == 0) d.wf_partial[rb] = 0.0;
+    } else if (rb < nref) {
         double c[8];
 #pragma unroll
         for (int m = 0; m < 8; ++m) {
@@ -60,7 +69,10 @@ k_walls(Dev d)
         double e = b0 + b1;
 #pragma unroll
         for (int i = 16; i != 0; i /= 2) e += __shfl_down_sync(0xffffffffu, e, i);
-        if (lane == 0) d.wf_partial[rb] = e;
+        if (lane == 0) {
+            d.wf_partial[rb] = e;
+            d.wf_flag[rb] = 0;
+        }
     }
     __syncthreads();
     if (t == 0) {

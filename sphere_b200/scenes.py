@@ -131,6 +131,67 @@ def polydisperse(n=1_000_000, seed=0, L=(0.2, 0.2, 0.4), num=(50, 50, 100),
     return sb
 
 
+def packed(nx=100, ny=100, nz=100, r=1e-3, sigma=20e3, seed=0, height=0.4,
+           sid="packed") -> Spherebin:
+    """A jammed simple-cubic column: every sphere presses on its six lattice
+    neighbours, so each holds six contacts through the whole run
+    (C ~ 6 N directed contacts, the packed-bed coordination number).
+
+    - nx x ny x nz spheres of radius r (1 mm), density 2600 kg/m^3;
+    - lattice spacing 2 r - delta, delta = sigma s^2 / k_n, the overlap at
+      which the contact force carries the wall's normal stress sigma over
+      one lattice site (8e-8 m at 20 kPa and k_n = 1e6 N/m);
+    - x and y periodic with the period equal to the lattice, so contacts
+      cross the periodic faces too; the floor at z = 0 and a stress-
+      controlled top wall (20 kPa) each overlap their layer by delta;
+    - contact parameters of ``polydisperse`` and its dt (2e-7 s), except the
+      viscosities.  gamma_n is 0: contact model 2's normal viscosity
+      (src/contactmodels.cuh, f_n = (-k_n delta - gamma_n vel_n) n with
+      vel_n = -dv.n) lowers the push between approaching spheres and raises
+      it between separating ones, so in a lattice that vibrates it feeds
+      energy in at a rate of about gamma_n / m, and any gamma_n above zero
+      blows the column up within a few hundred steps.  The wall viscosities
+      are 0.48 of critical for one contact (the damping ratio of
+      ``settling``): at 100 N s/m, the value of the other scenes, the wall's
+      tangential damping of a 1 mm sphere's spin (gamma r^2 dt / I = 4.6) is
+      past the explicit step's stability limit;
+    - a seeded jitter of delta / 100 breaks the lattice's exact symmetry.
+
+    The grid is two lattice sites per cell in x and y and 4 mm cells in z."""
+    rng = np.random.default_rng(seed)
+    n = nx * ny * nz
+    k_n = 1e6
+    m = 2600.0 * float(V_sphere(r))
+    gamma_w = 0.48 * 2.0 * math.sqrt(k_n * m)
+    s0 = 2.0 * r
+    delta = sigma * s0 * s0 / k_n
+    s = s0 - delta
+    sb = Spherebin(np_=n, nw=1, sid=sid)
+    i = np.arange(n)
+    lat = np.stack([i % nx, (i // nx) % ny, i // (nx * ny)], axis=1).astype(float)
+    sb.x = lat * s + np.array([0.5 * s, 0.5 * s, r - delta])
+    sb.x += rng.uniform(-0.01 * delta, 0.01 * delta, size=(n, 3))
+    sb.radius = np.full(n, r)
+    sb.origo = np.zeros(3)
+    sb.L = np.array([nx * s, ny * s, float(height)])
+    sb.num = np.array([nx // 2, ny // 2, int(height / (4.0 * r))], dtype=np.uint32)
+    sb.periodic = 1
+    sb.g = np.array([0.0, 0.0, -9.81])
+    _contact_params(sb, gamma_n=0.0, gamma_w=gamma_w, mu_r=0.01)
+    sb.nw = 1
+    sb.wmode = np.array([1], dtype=np.int32)
+    sb.w_n = np.array([[0.0, 0.0, -1.0]])
+    sb.w_x = np.array([float(np.max(sb.x[:, 2])) + r - delta])
+    sb.w_m = np.array([m * nx * ny])
+    sb.w_vel = np.zeros(1)
+    sb.w_force = np.zeros(1)
+    sb.w_devs = np.array([float(sigma)])
+    sb.time_dt = 2e-7
+    sb.time_total = 1e4 * sb.time_dt
+    sb.time_file_dt = sb.time_total
+    return sb
+
+
 def bonded(seed=0, nx=40, ny=20, nz=20, r_lo=0.9e-3, r_hi=1.1e-3, pull=0.01,
            sigma_b=2e7, tau_b=2e7, sid="bonded") -> Spherebin:
     """FCC lattice with the nearest-neighbour distance equal to the mean

@@ -32,6 +32,8 @@ SCENES = {
     # and alias while particles cross, which turns the cell-level pruning off
     "periodic_crossing": lambda: _crossing(),
     "polydisperse_small": lambda: _small_polydisperse(),
+    # jammed lattice: six contacts per sphere, across the periodic faces too
+    "packed": lambda: scenes.packed(nx=12, ny=12, nz=10),
 }
 
 

@@ -153,3 +153,33 @@ def test_model3_matches_reference_kernels(oracle_libs, name):
     assert touching.sum() > 100
     assert np.isnan(a.force[touching, :3]).all()
     assert not np.isnan(a.force[~touching, :3]).any()
+
+
+def test_packed_column_matches_reference_kernels(oracle_libs):
+    """The jammed column: six contacts per sphere, across the periodic faces
+    and against the floor and the stress-controlled top wall."""
+    _need_ref(oracle_libs)
+    sb = scenes.packed(nx=12, ny=12, nz=10)
+    rc1, a, ra = run_oracle(oracle_libs["orc"], sb, 40, nthreads=4)
+    rc2, b, rb = run_oracle(oracle_libs["ref"], sb, 40, nthreads=4)
+    assert rc1 == 0 and rc2 == 0
+    assert mismatches(a, b, ALL) == []
+    assert np.array_equal(ra.perm, rb.perm)
+    assert (a.contacts != sb.np).sum() == 6 * sb.np - 2 * 144
+    assert np.count_nonzero(a.delta_t) > 0
+
+
+def test_packed_column_stays_jammed(oracle_libs):
+    """The contact-heavy bench scene holds its six contacts per sphere: over
+    600 steps the lattice only vibrates (speeds under 1 cm/s) and no contact
+    opens.  With the reference's model-2 normal viscosity on, the same column
+    flies apart within a few hundred steps, which is why it is off there."""
+    sb = scenes.packed(nx=10, ny=10, nz=10)
+    rc, st, _ = run_oracle(oracle_libs["orc"], sb, 600, nthreads=4)
+    assert rc == 0
+    assert np.abs(st.vel[:, :3]).max() < 1e-2
+    # 6 per sphere less one for each sphere of the top and bottom layers
+    assert (st.contacts != sb.np).sum() == 6 * sb.np - 2 * 100
+    sb.gamma_n = 3.0
+    rc, st, _ = run_oracle(oracle_libs["orc"], sb, 600, nthreads=4)
+    assert rc != 0 or np.abs(st.vel[:, :3]).max() > 1.0
