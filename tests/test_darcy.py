@@ -22,7 +22,16 @@ SCENES = {
     "periodic_x": lambda: scenes.collision(n=900, seed=43, periodic=2, straddle=True),
     # a dynamic top wall beside the flow (the wall kernel runs in the same step)
     "box_wall": lambda: scenes.collision(n=900, seed=45, periodic=0, nw=1),
+    # 1 cm cells: about 2500 particles in the 6 x 6 x 6 cells around a
+    # porosity tile, more than its shared-memory stage holds, so the GPU walks
+    # them in global memory; the second tile of each axis is partial
+    "dense_cells": lambda: _coarse(scenes.collision(n=2500, seed=46, periodic=1), 6),
 }
+
+
+def _coarse(sb, cells):
+    sb.num = np.full(3, cells, dtype=np.uint32)
+    return sb
 
 
 def seeded_grid(num, seed):
