@@ -431,8 +431,8 @@ k_topo(Dev d, int A)
     // After a position left the grid (the step reports SPH_ERR_OUT_OF_GRID)
     // the scene has come apart: saturated cell ids pile its particles into
     // the edge cells, where the stencil sweep grows with the square of their
-    // count.  The search stops for the rest of the call; an upload clears
-    // the status.  A batch goes on, since its other scenes are still sound.
+    // count.  The search stays off until an upload clears the status.  A
+    // batch goes on, since its other scenes are still sound.
     if (!BATCH && (*(volatile const uint32_t *)d.status & ST_OUT_OF_GRID)) return;
     const Params &P = prm_at<BATCH>(d, s);
     const Verlet &V = *d.vs;
