@@ -428,12 +428,6 @@ k_topo(Dev d, int A)
         d.vs->movers_overflow = 0u;
     }
     if (s >= np) return;
-    // After a position left the grid (the step reports SPH_ERR_OUT_OF_GRID)
-    // the scene has come apart: saturated cell ids pile its particles into
-    // the edge cells, where the stencil sweep grows with the square of their
-    // count.  The search stays off until an upload clears the status.  A
-    // batch goes on, since its other scenes are still sound.
-    if (!BATCH && (*(volatile const uint32_t *)d.status & ST_OUT_OF_GRID)) return;
     const Params &P = prm_at<BATCH>(d, s);
     const Verlet &V = *d.vs;
     // The list decision first, from a few bytes: a valid list whose gap
@@ -450,6 +444,14 @@ k_topo(Dev d, int A)
         if (VISC) d.c1acc[s] = make_double4(0.0, 0.0, 0.0, 0.0);
         return;
     }
+    // After a position left the grid (the step reports SPH_ERR_OUT_OF_GRID)
+    // the scene has come apart: saturated cell ids pile its particles into
+    // the edge cells, where the stencil sweep grows with the square of their
+    // count.  The search stays off until an upload clears the status.  A
+    // batch goes on, since its other scenes are still sound.  Tested only
+    // here, past the list decision, so that the particles the decision
+    // settles do not wait for the status word.
+    if (!BATCH && (*(volatile const uint32_t *)d.status & ST_OUT_OF_GRID)) return;
     const double4 xa = d.xr[A][s];
     const double ra = xa.w;
     const double4 *__restrict__ xr = d.xr[A];
