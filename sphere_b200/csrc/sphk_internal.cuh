@@ -158,8 +158,8 @@ struct Dev {
     uint32_t *scan_tiles; // scratch for the scan
     uint32_t *alias_any;  // some particle sits outside its cell's box (set by the rebuild)
     // Verlet lists
-    uint32_t *vl;         // [VL_CAP][np] candidate storage indices, in visiting order
-    uint16_t *vl_meta;    // [VL_CAP][np] stencil cell (0..26) | shift code << 5
+    uint32_t *vl;         // [np][VL_CAP] candidate storage indices, in visiting order
+    uint16_t *vl_meta;    // [np][VL_CAP] stencil cell (0..26) | shift code << 5
     uint8_t *vl_len;      // [np] list length or VL_NONE
     float *vl_gap;        // [np] lower bound of the smallest gap to a listed candidate
     float *disp;          // [np] displacement bound since the epoch started

@@ -467,25 +467,33 @@ k_topo(Dev d, int A)
     d3 F1 = mk(0.0, 0.0, 0.0);   // model 1 sums
     double p1 = 0.0f;
 
-    // Entry e of particle s's list sits at e * np + s (entry-major), so a
-    // warp reading entry e of its 32 particles touches 128 contiguous bytes
-    // of d.vl and 64 of d.vl_meta instead of 32 scattered sectors each.
     if (VISC && list_ok) {
-        const uint32_t *vl = d.vl + s;
-        const uint16_t *vm = d.vl_meta + s;
+        const uint32_t *vl = d.vl + (size_t)s * VL_CAP;
+        const uint16_t *vm = d.vl_meta + (size_t)s * VL_CAP;
         for (uint32_t e = 0; e < len; ++e)
-            visc_pair(d, A, s, vl[(size_t)e * np], (uint32_t)vm[(size_t)e * np] >> 5, F1, p1);
+            visc_pair(d, A, s, vl[e], (uint32_t)vm[e] >> 5, F1, p1);
     } else if (list_ok) {
-        const uint32_t *vl = d.vl + s;
-        const uint16_t *vm = d.vl_meta + s;
+        // the list row is read four entries at a time (16 B of candidates,
+        // 8 B of their codes), a quarter of the load instructions and of
+        // the sectors requested of one entry a load
+        const uint4 *vl4 = reinterpret_cast<const uint4 *>(d.vl + (size_t)s * VL_CAP);
+        const uint2 *vm4 = reinterpret_cast<const uint2 *>(d.vl_meta + (size_t)s * VL_CAP);
         int skip_slot = -1;
-        for (uint32_t e = 0; e < len; ++e) {
-            const uint32_t meta = vm[(size_t)e * np];
-            const int slot = (int)(meta & 31u);
-            if (slot == skip_slot) continue;   // nc > NC: rest of that cell
-            const uint32_t t = vl[(size_t)e * np], code = meta >> 5;
-            if (overlaps(P, xr, t, code, xa) && !topo_insert(d, srow, tid, s, t, code, ts))
-                skip_slot = slot;
+        for (uint32_t e0 = 0; e0 < len; e0 += 4) {
+            const uint4 tq = vl4[e0 >> 2];
+            const uint2 mq = vm4[e0 >> 2];
+            const uint32_t tv[4] = {tq.x, tq.y, tq.z, tq.w};
+            const uint32_t mv[4] = {mq.x & 0xffffu, mq.x >> 16, mq.y & 0xffffu, mq.y >> 16};
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                if (e0 + (uint32_t)j >= len) break;
+                const uint32_t meta = mv[j];
+                const int slot = (int)(meta & 31u);
+                if (slot == skip_slot) continue;   // nc > NC: rest of that cell
+                const uint32_t t = tv[j], code = meta >> 5;
+                if (overlaps(P, xr, t, code, xa) && !topo_insert(d, srow, tid, s, t, code, ts))
+                    skip_slot = slot;
+            }
         }
     } else {
         const float4 *__restrict__ xs = d.xs[A];
@@ -495,8 +503,8 @@ k_topo(Dev d, int A)
         const float eps = P.cull_eps;
         const float skinf = (float)P.skin;
         const float extraf = (float)P.reach_extra;
-        uint32_t *vl = d.vl + s;
-        uint16_t *vm = d.vl_meta + s;
+        uint32_t *vl = d.vl + (size_t)s * VL_CAP;
+        uint16_t *vm = d.vl_meta + (size_t)s * VL_CAP;
         uint32_t nlist = 0;
         bool list_overflow = false;
         float gmin = 3.0e38f;   // smallest gap to a listed candidate, bounded below
@@ -545,8 +553,8 @@ k_topo(Dev d, int A)
                     const uint32_t slot = slot0 + ((k2 < bnd1) ? 0u : ((k2 < bnd2) ? 1u : 2u));
                     if (!use_lists) {
                     } else if (nlist < VL_CAP) {
-                        vl[(size_t)nlist * np] = t;
-                        vm[(size_t)nlist * np] = (uint16_t)(slot | (code << 5));
+                        vl[nlist] = t;
+                        vm[nlist] = (uint16_t)(slot | (code << 5));
                         ++nlist;
                     } else {
                         list_overflow = true;
