@@ -615,6 +615,12 @@ int create_impl(const sph_config *cfgs, uint32_t ninst, bool batched, sph_ctx **
     c->scratch = sc;
 #undef AL
     CK(cudaMemcpy(d.prm, c->hps.data(), sizeof(Params) * ninst, cudaMemcpyHostToDevice));
+    // The step graphs depend only on what is fixed here (sizes, device
+    // pointers, contact model, walls, bonds); every value an upload changes
+    // is read from device memory.  Capturing them now puts their cost in
+    // context creation rather than in the first sph_step.  A later change of
+    // SPH_OPT_GRAPH_STEPS, or the Darcy flow, captures them again.
+    if (!batched) return ensure_graphs(c);
     return SPH_OK;
 }
 
