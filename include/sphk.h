@@ -9,7 +9,8 @@
  * (sphere_b200/csrc/host/sphere.cpp) and any FFI can sit on top:
  *
  *   sph_create       DEM::initializeGPU + transferToConstantDeviceMemory +
- *                    allocateGlobalDeviceMemory   (src/device.cu:34-84,201-324)
+ *                    allocateGlobalDeviceMemory   (src/device.cu:34-84,201-324);
+ *                    also captures the step's CUDA graphs
  *   sph_upload       DEM::transferToGlobalDeviceMemory (src/device.cu:394-488)
  *   sph_step         n iterations of the time loop body (src/device.cu:731-1109)
  *   sph_sync         the checkForCudaErrors after each kernel (src/utility.cu:9-28)
