@@ -330,7 +330,7 @@ def gpu_arm(args, rank, world, local):
     n_total = cfg.np * world
     value = n_total * args.steps / (ms * 1e-3)
     e2e_value = n_total * args.steps / e2e_s
-    step_ms = (prof["topo"] + prof["force"]) / max(1, prof["steps"])
+    step_ms = (prof["topo"] + prof["contact"] + prof["force"]) / max(1, prof["steps"])
     C = stats["active_contacts"]
     b_step, b_whole, b_tight = algorithmic_bytes(cfg.np, cfg.ncells, C, cfg.nb0)
     peak, peak_kind = measured_peak_hbm()
@@ -352,7 +352,7 @@ def gpu_arm(args, rank, world, local):
                 "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
                 "seconds": e2e_s},
         "gpu_launches": launches, "cell_rebuilds_timed": rebuilt,
-        "roofline": {"bound": "hbm", "kernel": "k_topo+k_force", "achieved": achieved, "peak": peak,
+        "roofline": {"bound": "hbm", "kernel": "k_topo+k_contact+k_force", "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
                      "traffic": ncu_traffic(cfg.np),
                      "algorithmic_bytes_per_launch": b_step,
@@ -362,7 +362,7 @@ def gpu_arm(args, rank, world, local):
                      "whole_step_algorithmic_bytes": b_whole,
                      "whole_step_frac": (b_whole / (ms / args.steps * 1e-3) / 1e9) / peak},
         "phase_ms_per_step": {k: prof[k] / max(1, prof["steps"])
-                              for k in ("cells", "bonds", "topo", "force", "walls")},
+                              for k in ("cells", "bonds", "topo", "contact", "force", "walls")},
         "clocks": clocks.summary(),
     }
     if args.batch_instances > 0:
@@ -717,7 +717,7 @@ def packed_leg(args, local):
     prof = sim.profile(reset=True)
     sim.close()
     C = stats["active_contacts"]
-    kern_ms = (prof["topo"] + prof["force"]) / max(1, prof["steps"])
+    kern_ms = (prof["topo"] + prof["contact"] + prof["force"]) / max(1, prof["steps"])
     b_step, _, b_tight = algorithmic_bytes(cfg.np, cfg.ncells, C)
     peak, peak_kind = measured_peak_hbm()
     achieved = b_step / (kern_ms * 1e-3) / 1e9
@@ -730,13 +730,13 @@ def packed_leg(args, local):
                     "no normal viscosity",
         "active_contacts": C, "contacts_per_particle": C / cfg.np,
         "cell_rebuilds_timed": stats["cell_rebuilds"] - rebuilds0,
-        "roofline": {"bound": "hbm", "kernel": "k_topo+k_force", "achieved": achieved,
+        "roofline": {"bound": "hbm", "kernel": "k_topo+k_contact+k_force", "achieved": achieved,
                      "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_source": peak_kind, "algorithmic_bytes_per_launch": b_step,
                      "launch_ms": kern_ms, "tight_bytes_per_launch": b_tight,
                      "tight_frac": b_tight / (kern_ms * 1e-3) / 1e9 / peak},
         "phase_ms_per_step": {k: prof[k] / max(1, prof["steps"])
-                              for k in ("cells", "bonds", "topo", "force", "walls")},
+                              for k in ("cells", "bonds", "topo", "contact", "force", "walls")},
         "clocks": clocks.summary(),
     }
 

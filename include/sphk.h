@@ -124,10 +124,11 @@ typedef struct sph_stats {
 #define SPH_PHASE_CELLS 0   /* cell list rebuild (hash histogram, scan, scatter, sort) */
 #define SPH_PHASE_BONDS 1   /* per-bond forces */
 #define SPH_PHASE_TOPO 2    /* contact detection into the slots */
-#define SPH_PHASE_FORCE 3   /* contact and wall forces + integration */
+#define SPH_PHASE_FORCE 3   /* slot sums, wall and bond forces + integration */
 #define SPH_PHASE_WALLS 4   /* wall force reduction + wall integration */
 #define SPH_PHASE_DARCY 5   /* Darcy flow (zero without sph_darcy_upload) */
-#define SPH_NPHASES 6
+#define SPH_PHASE_CONTACT 6 /* force laws of the contact slots (models 2 and 3) */
+#define SPH_NPHASES 7
 
 int sph_version(void);
 int sph_create(const sph_config *cfg, sph_ctx **out);

@@ -12,9 +12,11 @@
 #include <vector>
 
 namespace sphk {
-void launch_step(const Dev &d, uint32_t np, int model, int a, int write_outputs, cudaStream_t st);
+void launch_step(const Dev &d, const Params &hp, uint32_t np, int model, int a, int write_outputs,
+                 cudaStream_t st);
 void launch_topo(const Dev &d, uint32_t np, bool visc, int a, cudaStream_t st);
 void launch_force(const Dev &d, uint32_t np, int model, int a, int write_outputs, cudaStream_t st);
+void launch_contact(const Dev &d, const Params &hp, uint32_t np, int model, int a, cudaStream_t st);
 void launch_bonds(const Dev &d, uint32_t nb0, int a, cudaStream_t st);
 void launch_walls(const Dev &d, uint32_t np, uint32_t nw, cudaStream_t st);
 void launch_cell_init(const Dev &d, uint32_t np, int a, cudaStream_t st);
@@ -359,7 +361,7 @@ int enqueue_one_step(sph_ctx *c, int a, int write_outputs, cudaStream_t st, bool
         launch_darcy(c->d, c->darcy, c->hp, a, a ^ c->dflip, c->darcy_stream);
         CK(cudaEventRecord(c->darcy_join, c->darcy_stream));
     }
-    launch_step(c->d, c->np_all, (int)c->hp.contactmodel, a, write_outputs, st);
+    launch_step(c->d, c->hp, c->np_all, (int)c->hp.contactmodel, a, write_outputs, st);
     if (c->darcy_on && !branch) launch_darcy(c->d, c->darcy, c->hp, a, a ^ c->dflip, st);
     launch_walls(c->d, c->np_all, c->hp.nw, st);
     if (branch) CK(cudaStreamWaitEvent(st, c->darcy_join, 0));
@@ -428,6 +430,10 @@ int profiled_step(sph_ctx *c, int a, int write_outputs, cudaStream_t st)
         c->ev.resize(SPH_NPHASES + 1);
         for (auto &e : c->ev) CK(cudaEventCreate(&e));
     }
+    // the phases in launch order; event k + 1 closes order[k]
+    static const int order[SPH_NPHASES] = {SPH_PHASE_CELLS, SPH_PHASE_BONDS, SPH_PHASE_TOPO,
+                                           SPH_PHASE_CONTACT, SPH_PHASE_FORCE, SPH_PHASE_WALLS,
+                                           SPH_PHASE_DARCY};
     CK(cudaEventRecord(c->ev[0], st));
     launch_rebuild(c->d, c->np_all, c->ncells_all, a, st);
     CK(cudaEventRecord(c->ev[1], st));
@@ -435,18 +441,20 @@ int profiled_step(sph_ctx *c, int a, int write_outputs, cudaStream_t st)
     CK(cudaEventRecord(c->ev[2], st));
     launch_topo(c->d, c->np_all, c->hp.contactmodel == 1, a, st);
     CK(cudaEventRecord(c->ev[3], st));
-    launch_force(c->d, c->np_all, (int)c->hp.contactmodel, a, write_outputs, st);
+    launch_contact(c->d, c->hp, c->np_all, (int)c->hp.contactmodel, a, st);
     CK(cudaEventRecord(c->ev[4], st));
-    launch_walls(c->d, c->np_all, c->hp.nw, st);
+    launch_force(c->d, c->np_all, (int)c->hp.contactmodel, a, write_outputs, st);
     CK(cudaEventRecord(c->ev[5], st));
-    if (c->darcy_on) launch_darcy(c->d, c->darcy, c->hp, a, a ^ c->dflip, st);
+    launch_walls(c->d, c->np_all, c->hp.nw, st);
     CK(cudaEventRecord(c->ev[6], st));
+    if (c->darcy_on) launch_darcy(c->d, c->darcy, c->hp, a, a ^ c->dflip, st);
+    CK(cudaEventRecord(c->ev[7], st));
     CK(cudaGetLastError());
-    CK(cudaEventSynchronize(c->ev[6]));
+    CK(cudaEventSynchronize(c->ev[7]));
     for (int k = 0; k < SPH_NPHASES; ++k) {
         float ms = 0.f;
         CK(cudaEventElapsedTime(&ms, c->ev[k], c->ev[k + 1]));
-        c->prof_ms[k] += ms;
+        c->prof_ms[order[k]] += ms;
     }
     c->prof_steps++;
     return SPH_OK;
@@ -457,6 +465,9 @@ int do_relayout(sph_ctx *c, cudaStream_t st)
     // the cell list must describe the current positions before storage follows it
     launch_rebuild(c->d, c->np_all, c->ncells_all, c->a, st);
     relayout(c->d, c->np_all, c->a, c->scratch, st);
+    // the slot rows moved: every chunk may hold a contact until the next
+    // force pass has looked
+    CK(cudaMemsetAsync(c->d.cflag, 1, div_up(c->np_all, 32), st));
     CK(cudaGetLastError());
     c->relayouts++;
     c->since_relayout = 0;
@@ -589,6 +600,7 @@ int create_impl(const sph_config *cfgs, uint32_t ninst, bool batched, sph_ctx **
     AL(d.force, np); AL(d.torque, np); AL(d.acc, np); AL(d.angacc, np); AL(d.edp, np);
     AL(d.uid, np); AL(d.sidx, np); AL(d.cell, np); AL(d.outside, np);
     AL(d.contacts, np * NC); AL(d.dmc, np); AL(d.delta_t, np * NC); AL(d.cmask, np);
+    AL(d.cflag, div_up(np, 32));
     AL(d.cell_start, ncells + 2); AL(d.cellorder, np); AL(d.pos, np); AL(d.cell_fill, ncells + 1);
     AL(d.scan_tiles, scan_tile_count(c->ncells_all));
     AL(d.alias_any, 1);
@@ -601,7 +613,11 @@ int create_impl(const sph_config *cfgs, uint32_t ninst, bool batched, sph_ctx **
     AL(d.bonds, nb0); AL(d.bonds_delta, nb0); AL(d.bonds_omega, nb0);
     AL(d.bond_f, nb0); AL(d.bond_t, nb0); AL(d.bond_xu, nb0);
     AL(d.bond_ptr, np + 1); AL(d.bond_list, 2 * (size_t)nb0);
-    if (c->hp.contactmodel == 1) AL(d.c1acc, np);
+    if (c->hp.contactmodel == 1) {
+        AL(d.c1acc, np);
+    } else {
+        AL(d.csum_f, np); AL(d.csum_t, np); AL(d.csum_es, np);
+    }
     AL(d.status, 1); AL(d.rebuild, 1); AL(d.prm, ninst);
     if (batched) {
         AL(d.inst, np);
@@ -1211,6 +1227,7 @@ static int restore_ckpt(sph_ctx *c, const sph_ctx::Ckpt &k)
     Dev &d = c->d;
     launch_cell_init(d, c->np_all, k.a, c->stream);
     CK(cudaMemsetAsync(d.dirty, 0, ((size_t)c->ncells_all + 1) * sizeof(uint32_t), c->stream));
+    CK(cudaMemsetAsync(d.cflag, 1, div_up(c->np_all, 32), c->stream));
     CK(cudaStreamSynchronize(c->stream));
     const uint32_t one = 1;
     CK(cudaMemcpy(d.rebuild, &one, 4, cudaMemcpyHostToDevice));
@@ -1384,6 +1401,7 @@ int sph_diff_end(sph_ctx *c)
     CK(cudaDeviceSynchronize());
     free_diff(c);
     drop_graphs(c);
+    CK(cudaMemset(c->d.cflag, 1, div_up(c->np_all, 32)));
     c->diff = false;
     c->relayout_every = c->relayout_saved;
     return SPH_OK;

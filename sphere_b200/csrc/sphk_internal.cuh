@@ -150,6 +150,11 @@ struct Dev {
     ulonglong2 *dmc;      // [np] 4-bit periodic shift code of each of the NC slots
     double4 *delta_t;     // [np][NC]
     uint32_t *cmask;      // [np] occupied-slot bit mask
+    // contact models 2 and 3: each particle's slot sums from k_contact
+    // (F xyz and p; T xyz and ev_dot; es_dot), read by k_force
+    double4 *csum_f, *csum_t;
+    double *csum_es;
+    uint8_t *cflag;       // [ceil(np / 32)] the chunk of 32 storage indices may hold a contact
     // cell list (cell order sorted by uid inside each cell)
     uint32_t *cell_start; // [ncells + 2]
     uint32_t *cellorder;  // [np] cell-list position -> storage index
@@ -211,8 +216,18 @@ __device__ __forceinline__ const Params &prm_at(const Dev &d, uint32_t s)
     else return *d.prm;
 }
 
-// periodic shift code: bits 0-1 x (1: +L, 2: -L), bits 2-3 y
-__device__ __forceinline__ d3 decode_dm(uint32_t code, const Params &P)
+// The force-law constants of one scene (contact models 2 and 3), fixed when
+// a context is created.  Single-scene contexts pass them to the contact
+// kernel by value, where the law reads them as constant operands.
+struct LawParams {
+    double k_n, k_t, gamma_n, gamma_t, gamma_r, mu_s, mu_d, mu_r, kappa, dt;
+    double L[2];
+};
+
+// periodic shift code: bits 0-1 x (1: +L, 2: -L), bits 2-3 y.  PR is Params
+// or LawParams.
+template <class PR>
+__device__ __forceinline__ d3 decode_dm(uint32_t code, const PR &P)
 {
     // reproduces (0,0,0) += (L,0,0) / -= (L,0,0) etc. of findDistMod
     double dx = 0.0, dy = 0.0, dz = 0.0;

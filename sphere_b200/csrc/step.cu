@@ -7,12 +7,15 @@
 //          the 27-cell stencil are three adjacent runs of one array and a
 //          candidate costs one coalesced 16-byte load; the particle's own slot
 //          row is fetched only when an overlap is found.
-// k_force  everything per particle after it (src/device.cu:829-1058):
-//          contact forces over the slots and the walls (interact,
-//          contactsearch.cuh:369-689), the per-bond forces of bondsLinear
-//          (cohesion.cuh:8-233, computed by bonds.cu and gathered here in bond
-//          order), and the half-step leapfrog (integrate, integration.cuh:9-187).
-//          One thread per storage index, so the particle state streams.
+// k_contact the force laws of the occupied slots (interact's slot loop,
+//          src/contactsearch.cuh:468-543), one lane per directed contact;
+//          each particle's sums, in slot order, are left for k_force.
+// k_force  everything per particle after it (src/device.cu:829-1058): the
+//          slot sums, the walls (interact, contactsearch.cuh:578-663), the
+//          per-bond forces of bondsLinear (cohesion.cuh:8-233, computed by
+//          bonds.cu and gathered here in bond order), and the half-step
+//          leapfrog (integrate, integration.cuh:9-187).  One thread per
+//          storage index, so the particle state streams.
 // Kinematics of step n are read from buffer A and step n+1 is written to
 // buffer B, so neighbours always see start-of-step values.
 //
@@ -22,6 +25,8 @@
 // reference's own predicate float_sqrt(dot) - (ra + rb) < 0 decides.  The
 // visiting order is the reference's: stencil cells z, y, x, members of a cell
 // by particle index.
+#include <algorithm>
+
 #include "sphk_internal.cuh"
 #include "diff_step.cuh"
 
@@ -44,12 +49,19 @@ constexpr int FORCE_BLOCK = SPHK_FORCE_BLOCK;
 #ifndef SPHK_FORCE_MIN_BLOCKS
 #define SPHK_FORCE_MIN_BLOCKS 8
 #endif
+#ifndef SPHK_CONTACT_BLOCK
+#define SPHK_CONTACT_BLOCK 128
+#endif
+#ifndef SPHK_CONTACT_MIN_BLOCKS
+#define SPHK_CONTACT_MIN_BLOCKS 4
+#endif
+constexpr int CONTACT_BLOCK = SPHK_CONTACT_BLOCK;
 
-// What one law adds to a particle's sums.  The laws are out of line and
-// return their terms by value, so the caller's sums stay in registers (a
-// reference into them would put them in local memory for the whole
-// kernel).  Each reference update `s += term` is the caller's `s + term`,
-// the same operation.
+// What one law adds to a particle's sums.  The laws return their terms by
+// value and the caller adds them: each reference update `s += term` is the
+// caller's `s + term`, the same operation.  (The wall law is out of line;
+// a reference into the caller's sums would put them in local memory for the
+// whole kernel.)
 struct WallOut {
     d3 f, t;       // F += f, T += t
     double pr;     // p += pr
@@ -63,9 +75,9 @@ struct LawOut {
     double4 dt4;       // the slot's new tangential history
 };
 
-// contactLinear_wall, src/contactmodels.cuh:10-109.  Out of line: six call
-// sites, taken only by particles touching a wall.
-__device__ __noinline__ WallOut contact_wall(const Params &P, double ra, double4 vel_a,
+// contactLinear_wall, src/contactmodels.cuh:10-109.  Inlined into
+// wall_forces, its one caller.
+__device__ __forceinline__ WallOut contact_wall(const Params &P, double ra, double4 vel_a,
                                              double4 angvel_a, d3 n, double delta, double wvel)
 {
     const d3 linvel = xyz(vel_a), angvel = xyz(angvel_a);
@@ -94,9 +106,80 @@ __device__ __noinline__ WallOut contact_wall(const Params &P, double ra, double4
     return o;
 }
 
-// contactLinear, src/contactmodels.cuh:283-493 (contact model 2).  Out of
-// line so that particles without contacts run a lean kernel.
-__device__ __noinline__ LawOut contact_linear(const Params &P, double4 vel_a, d3 angvel_a,
+// The walls interact visits, in its order (src/contactsearch.cuh:578-663,
+// defaults :416-427): 0 the top wall (dynamic wall 0, else z = L.z), 1 the
+// floor at origo.z, then with periodic == 0 the x walls (dynamic walls 1 and
+// 2, else x = L.x and x = 0), and with periodic == 0 or 2 the y walls
+// (dynamic walls 3 and 4, else y = L.y and y = 0).  Wall k's gap, normal and
+// velocity; a dynamic wall replaces the default in order.
+__device__ __forceinline__ double wall_gap(const Params &P, const Walls &W, int k, double4 xa)
+{
+    auto wpos = [&](int j, double dflt) { return ((uint32_t)j < P.nw) ? W.nx[j].w : dflt; };
+    const double ra = xa.w;
+    switch (k) {
+    case 0: return wpos(0, P.L[2]) - (xa.z + ra);
+    case 1: return xa.z - ra - P.origo[2];
+    case 2: return wpos(1, P.L[0]) - (xa.x + ra);
+    case 3: return xa.x - ra - wpos(2, 0.0);
+    case 4: return wpos(3, P.L[1]) - (xa.y + ra);
+    default: return xa.y - ra - wpos(4, 0.0);
+    }
+}
+
+// Bit k: the particle touches wall k (its gap is negative).
+__device__ __forceinline__ uint32_t wall_touch(const Params &P, const Walls &W, double4 xa)
+{
+    const int nwall = (P.periodic == 0) ? 6 : ((P.periodic == 2) ? 6 : 2);
+    uint32_t m = 0;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+        if (k >= nwall || (P.periodic == 2 && (k == 2 || k == 3))) continue;
+        if (wall_gap(P, W, k, xa) < 0.0f) m |= 1u << k;
+    }
+    return m;
+}
+
+struct WallSums {
+    d3 F, T;
+    double p;
+    double w0f;   // the normal force of wall 0 (walls_force_pp)
+};
+
+// The wall terms of the touched walls, added in interact's order to the slot
+// sums (F, T, p).  Out of line: only particles touching a wall call it.
+__device__ __noinline__ WallSums wall_forces(const Params &P, const Walls &W, uint32_t touch,
+                                             double4 xa, double4 vel_a, double4 angvel_a, d3 F,
+                                             d3 T, double p)
+{
+    WallSums r{F, T, p, 0.0};
+    for (int k = 0; k < 6; ++k) {
+        if (!((touch >> k) & 1u)) continue;
+        const int j = (k == 0) ? 0 : k - 1;    // the dynamic wall that replaces wall k
+        const bool dyn = k != 1 && (uint32_t)j < P.nw;
+        d3 n;
+        switch (k) {
+        case 0: n = mk(0.0, 0.0, -1.0); break;
+        case 1: n = mk(0.0, 0.0, 1.0); break;
+        case 2: n = mk(-1.0, 0.0, 0.0); break;
+        case 3: n = mk(1.0, 0.0, 0.0); break;
+        case 4: n = mk(0.0, -1.0, 0.0); break;
+        default: n = mk(0.0, 1.0, 0.0); break;
+        }
+        if (dyn) n = xyz(W.nx[j]);
+        const double wv = dyn ? W.mvfd[j].y : ((k == 1) ? (double)0.0f : 0.0);
+        const WallOut o = contact_wall(P, xa.w, vel_a, angvel_a, n, wall_gap(P, W, k, xa), wv);
+        r.F = add(r.F, o.f);
+        r.T = add(r.T, o.t);
+        r.p += o.pr;
+        if (k == 0) r.w0f = o.fn;
+    }
+    return r;
+}
+
+// contactLinear, src/contactmodels.cuh:283-493 (contact model 2).  Inlined
+// into k_contact, the one kernel that evaluates it.
+template <class PR>
+__device__ __forceinline__ LawOut contact_linear(const PR &P, double4 vel_a, d3 angvel_a,
                                               double4 vel_b4, double4 angvel_b4, double ra,
                                               double rb, d3 x, double x_length, double delta,
                                               double4 dt4)
@@ -211,8 +294,9 @@ __device__ __noinline__ void capillary_exp(const Params &P, d3 &F, double ra, do
 
 // contactHertz, src/contactmodels.cuh:499-666 (contact model 3).  As in the
 // reference, delta is the (negative) overlap, so its fractional powers are
-// NaN and so are the forces of every touching pair.
-__device__ __noinline__ LawOut contact_hertz(const Params &P, double4 vel_a, d3 angvel_a,
+// NaN and so are the forces of every touching pair.  Inlined into k_contact.
+template <class PR>
+__device__ __forceinline__ LawOut contact_hertz(const PR &P, double4 vel_a, d3 angvel_a,
                                              double4 vel_b4, double4 angvel_b4, double ra,
                                              double rb, d3 x, double x_length, double delta,
                                              double4 dt4)
@@ -308,6 +392,43 @@ struct TopoSlots {
     bool dirty;                      // row changed
 };
 
+// Copies the particle's slot row and shift codes to shared memory and
+// registers (once): only the 16-byte pieces of the row that hold an occupied
+// slot, since the other entries are neither searched nor written back.
+__device__ __forceinline__ void topo_load_row(const Dev &d, uint32_t *srow, int tid, uint32_t s,
+                                              TopoSlots &ts)
+{
+    if (ts.loaded) return;
+    if (ts.occ) {
+        const uint4 *row = reinterpret_cast<const uint4 *>(d.contacts + (size_t)s * NC);
+#pragma unroll
+        for (int q = 0; q < NC / 4; ++q) {
+            if (((ts.occ >> (4 * q)) & 0xFu) == 0u) continue;
+            const uint4 v = row[q];
+            srow[(4 * q + 0) * TOPO_BLOCK + tid] = v.x;
+            srow[(4 * q + 1) * TOPO_BLOCK + tid] = v.y;
+            srow[(4 * q + 2) * TOPO_BLOCK + tid] = v.z;
+            srow[(4 * q + 3) * TOPO_BLOCK + tid] = v.w;
+        }
+        const ulonglong2 c2 = d.dmc[s];
+        ts.dm_lo = c2.x;
+        ts.dm_hi = c2.y;
+    }
+    ts.loaded = true;
+}
+
+// Whether candidate t already holds a slot of the (loaded) row through the
+// periodic image `code`.
+__device__ __forceinline__ bool in_slot(const uint32_t *srow, int tid, const TopoSlots &ts,
+                                        uint32_t t, uint32_t code)
+{
+    for (uint32_t m = ts.occ; m; m &= m - 1) {
+        const int i = __ffs(m) - 1;
+        if (srow[i * TOPO_BLOCK + tid] == t) return dm_get(ts.dm_lo, ts.dm_hi, i) == code;
+    }
+    return false;
+}
+
 // Overlapping candidate t (storage index) reached through a stencil cell
 // with shift `code`: the slot choice.  Returns false once nc > NC, which ends
 // the current cell (the reference returns from findContactsInCell).  Kept
@@ -316,23 +437,7 @@ struct TopoSlots {
 __device__ __noinline__ bool topo_insert(const Dev &d, uint32_t *srow, int tid, uint32_t s,
                                          uint32_t t, uint32_t code, TopoSlots &ts)
 {
-    if (!ts.loaded) {
-        if (ts.occ) {
-            const uint4 *row = reinterpret_cast<const uint4 *>(d.contacts + (size_t)s * NC);
-#pragma unroll
-            for (int q = 0; q < NC / 4; ++q) {
-                const uint4 v = row[q];
-                srow[(4 * q + 0) * TOPO_BLOCK + tid] = v.x;
-                srow[(4 * q + 1) * TOPO_BLOCK + tid] = v.y;
-                srow[(4 * q + 2) * TOPO_BLOCK + tid] = v.z;
-                srow[(4 * q + 3) * TOPO_BLOCK + tid] = v.w;
-            }
-            const ulonglong2 c2 = d.dmc[s];
-            ts.dm_lo = c2.x;
-            ts.dm_hi = c2.y;
-        }
-        ts.loaded = true;
-    }
+    topo_load_row(d, srow, tid, s, ts);
     // slot choice, src/contactsearch.cuh:252-271: a slot already holding t
     // wins, else the last empty slot, else position nc
     int cpos = -1;
@@ -340,17 +445,25 @@ __device__ __noinline__ bool topo_insert(const Dev &d, uint32_t *srow, int tid, 
         const int i = __ffs(m) - 1;
         if (srow[i * TOPO_BLOCK + tid] == t) { cpos = i; break; }
     }
-    if (cpos < 0) {
+    if (cpos >= 0) {
+        // already in its slot: the reference writes the slot again, which
+        // changes the row only where the partner is now seen through
+        // another periodic image
+        if (dm_get(ts.dm_lo, ts.dm_hi, cpos) != code) {
+            dm_set(ts.dm_lo, ts.dm_hi, cpos, code);
+            ts.dirty = true;
+        }
+    } else {
         const uint32_t empty = ~ts.occ;
         cpos = empty ? 31 - __clz(empty) : ts.nc;
-    }
-    if (cpos < NC) {
-        ts.occ |= 1u << cpos;
-        srow[cpos * TOPO_BLOCK + tid] = t;
-        dm_set(ts.dm_lo, ts.dm_hi, cpos, code);
-        ts.dirty = true;
-    } else {
-        ts.err |= ST_NC_OVERFLOW;
+        if (cpos < NC) {
+            ts.occ |= 1u << cpos;
+            srow[cpos * TOPO_BLOCK + tid] = t;
+            dm_set(ts.dm_lo, ts.dm_hi, cpos, code);
+            ts.dirty = true;
+        } else {
+            ts.err |= ST_NC_OVERFLOW;
+        }
     }
     return ++ts.nc <= NC;
 }
@@ -478,6 +591,14 @@ k_topo(Dev d, int A)
         // the sectors requested of one entry a load
         const uint4 *vl4 = reinterpret_cast<const uint4 *>(d.vl + (size_t)s * VL_CAP);
         const uint2 *vm4 = reinterpret_cast<const uint2 *>(d.vl_meta + (size_t)s * VL_CAP);
+        // A candidate that already holds a slot through the same image needs
+        // no test: overlapping or not, the reference's topology leaves its
+        // slot as it is (a separated one is freed by the force pass).  The
+        // test only feeds the count nc, which matters once a row fills up;
+        // while the occupied slots plus the list length stay within NC, no
+        // row can fill, so the filter changes nothing.
+        const bool filter = ts.occ != 0u && len + (uint32_t)__popc(ts.occ) <= (uint32_t)NC;
+        if (filter) topo_load_row(d, srow, tid, s, ts);
         int skip_slot = -1;
         for (uint32_t e0 = 0; e0 < len; e0 += 4) {
             const uint4 tq = vl4[e0 >> 2];
@@ -491,6 +612,7 @@ k_topo(Dev d, int A)
                 const int slot = (int)(meta & 31u);
                 if (slot == skip_slot) continue;   // nc > NC: rest of that cell
                 const uint32_t t = tv[j], code = meta >> 5;
+                if (filter && in_slot(srow, tid, ts, t, code)) continue;
                 if (overlaps(P, xr, t, code, xa) && !topo_insert(d, srow, tid, s, t, code, ts))
                     skip_slot = slot;
             }
@@ -664,6 +786,7 @@ k_topo(Dev d, int A)
         }
         d.cmask[s] = occ;
         d.dmc[s] = make_ulonglong2(ts.dm_lo, ts.dm_hi);
+        if (occ) d.cflag[s >> 5] = 1;
     }
     if (ts.err) atomicOr(d.status, ts.err);
 }
@@ -720,7 +843,6 @@ k_force(ForceArgs args)
     const double ra = xa.w;
     const double4 vel_a = ld4(d.vel[A], s);
     const double4 angvel_a4 = ld4(d.angvel[A], s);
-    const d3 angvel_a = xyz(angvel_a4);
     d3 F = mk(0.0, 0.0, 0.0), T = mk(0.0, 0.0, 0.0);
     double es_dot = 0.0f, ev_dot = 0.0f, p = 0.0f;
 
@@ -781,39 +903,14 @@ k_force(ForceArgs args)
         F = mk(c.x, c.y, c.z);
         p = c.w;
     } else if (occ) {
-        const uint32_t occ0 = occ;
-        const ulonglong2 dmw = d.dmc[s];
-        uint32_t *crow = d.contacts + (size_t)s * NC;
-        double4 *dtrow = d.delta_t + (size_t)s * NC;
-        for (uint32_t m = occ0; m; m &= m - 1) {
-            const int i = __ffs(m) - 1;
-            const uint32_t t = crow[i];
-            const d3 dm = decode_dm(dm_get(dmw.x, dmw.y, i), P);
-            const double4 xb = d.xr[A][t];
-            const double rb = xb.w;
-            const d3 xab = mk(xa.x - xb.x + dm.x, xa.y - xb.y + dm.y, xa.z - xb.z + dm.z);
-            const double xlen = flen(xab);
-            const double delta_n = xlen - (ra + rb);
-            if (delta_n < 0.0f) {
-                const LawOut o = (MODEL == 2)
-                    ? contact_linear(P, vel_a, angvel_a, ld4(d.vel[A], t), ld4(d.angvel[A], t), ra,
-                                     rb, xab, xlen, delta_n, dtrow[i])
-                    : contact_hertz(P, vel_a, angvel_a, ld4(d.vel[A], t), ld4(d.angvel[A], t), ra,
-                                    rb, xab, xlen, delta_n, dtrow[i]);
-                F = add(F, o.f);
-                T = add(T, o.t);
-                p += o.pr;
-                ev_dot += o.ev;
-                if (o.es_set) es_dot += o.es;
-                dtrow[i] = o.dt4;
-            } else {
-                // separated: free the slot and zero its history
-                occ &= ~(1u << i);
-                crow[i] = np;
-                dtrow[i] = make_double4(0.0, 0.0, 0.0, 0.0);
-            }
-        }
-        if (occ != occ0) d.cmask[s] = occ;
+        // the slot sums k_contact left for a particle that still holds a
+        // contact (with every slot freed nothing was added: the sums are zero)
+        const double4 cf = d.csum_f[s], ct = d.csum_t[s];
+        F = mk(cf.x, cf.y, cf.z);
+        p = cf.w;
+        T = mk(ct.x, ct.y, ct.z);
+        ev_dot = ct.w;
+        es_dot = d.csum_es[s];
     }
 
     // ---- walls, src/contactsearch.cuh:578-663 (defaults :416-427) ----------
@@ -831,36 +928,15 @@ k_force(ForceArgs args)
             T = add(T, mk(tw.x, tw.y, tw.z));
         }
     } else {
-        // a wall's position only for its test, its normal and velocity only
-        // on contact; dynamic walls replace the defaults (contactsearch.cuh:
-        // 416-427) in order
-        const Walls &W = *d.walls;
-        auto wpos = [&](int k, double dflt) { return ((uint32_t)k < P.nw) ? W.nx[k].w : dflt; };
-        auto wnrm = [&](int k, d3 dflt) { return ((uint32_t)k < P.nw) ? xyz(W.nx[k]) : dflt; };
-        auto wvel = [&](int k) { return ((uint32_t)k < P.nw) ? W.mvfd[k].y : 0.0; };
-        auto wall = [&](d3 n, double dw, double wv) {
-            const WallOut o = contact_wall(P, ra, vel_a, angvel_a4, n, dw, wv);
-            F = add(F, o.f);
-            T = add(T, o.t);
-            p += o.pr;
-            return o.fn;
-        };
-        double dw;
-        dw = wpos(0, P.L[2]) - (xa.z + ra);
-        if (dw < 0.0f) w0f = wall(wnrm(0, mk(0.0, 0.0, -1.0)), dw, wvel(0));
-        dw = xa.z - ra - P.origo[2];
-        if (dw < 0.0f) (void)wall(mk(0.0, 0.0, 1.0), dw, 0.0f);
-        if (P.periodic == 0) {
-            dw = wpos(1, P.L[0]) - (xa.x + ra);
-            if (dw < 0.0f) (void)wall(wnrm(1, mk(-1.0, 0.0, 0.0)), dw, wvel(1));
-            dw = xa.x - ra - wpos(2, 0.0);
-            if (dw < 0.0f) (void)wall(wnrm(2, mk(1.0, 0.0, 0.0)), dw, wvel(2));
-        }
-        if (P.periodic == 0 || P.periodic == 2) {
-            dw = wpos(3, P.L[1]) - (xa.y + ra);
-            if (dw < 0.0f) (void)wall(wnrm(3, mk(0.0, -1.0, 0.0)), dw, wvel(3));
-            dw = xa.y - ra - wpos(4, 0.0);
-            if (dw < 0.0f) (void)wall(wnrm(4, mk(0.0, 1.0, 0.0)), dw, wvel(4));
+        // the six wall gaps first, inline; a particle touching no wall
+        // (nearly all) takes no call
+        const uint32_t touch = wall_touch(P, *d.walls, xa);
+        if (touch) {
+            const WallSums ws = wall_forces(P, *d.walls, touch, xa, vel_a, angvel_a4, F, T, p);
+            F = ws.F;
+            T = ws.T;
+            p = ws.p;
+            w0f = ws.w0f;
         }
     }
 
@@ -1020,6 +1096,221 @@ k_force(ForceArgs args)
     if (err) atomicOr(d.status, err);
 }
 
+
+// Position of the k-th set bit (k = 0 for the lowest) of m; k < popc(m).
+__device__ __forceinline__ uint32_t nth_set_bit(uint32_t m, uint32_t k)
+{
+    uint32_t pos = 0;
+#pragma unroll
+    for (uint32_t w = 16; w; w >>= 1) {
+        const uint32_t lo = m & ((1u << w) - 1u);
+        const uint32_t c = __popc(lo);
+        if (k >= c) {
+            k -= c;
+            m >>= w;
+            pos += w;
+        } else {
+            m = lo;
+        }
+    }
+    return pos;
+}
+
+struct ContactArgs {
+    Dev d;
+    int a;          // read buffer (start of step)
+    LawParams lp;   // single-scene contexts; a batch reads each scene's Params
+};
+
+// Contacts of one chunk whose law terms a warp holds at once.
+constexpr uint32_t CT_CAP = 128;
+
+// k_contact: interact's slot loop (src/contactsearch.cuh:468-543) for
+// contact models 2 and 3, one lane per directed contact.
+//
+// The unit of work is a chunk of 32 consecutive storage indices, and a chunk
+// is visited only while its flag (Dev::cflag) says it may hold a contact:
+// the contact search sets the flag when it writes a row with an occupied
+// slot, and this kernel clears it when the chunk ends without one.  The grid
+// is resident (a few blocks per SM); warp g takes chunks g, g + W, g + 2W,
+// ... of the W warps, reading the flags of 32 of them in one load, so a
+// contact-free scene costs about one memory latency.
+//
+// In a chunk, the occupied slots, particle after particle and each
+// particle's in slot order, form a list of directed contacts, which each
+// particle's lane writes out once into shared memory as (lane, slot) pairs.
+// The list is evaluated 32 contacts at a time, one per lane, so every lane
+// runs a force law whatever the spread of contact counts, and the terms of
+// up to CT_CAP contacts are kept in shared memory.  Then every particle's
+// own lane adds its terms in slot order, the reference's summation order,
+// all lanes at once, and at the end stores the sums for k_force.  A slot
+// whose partner no longer overlaps is freed and its history zeroed, as in
+// the reference.
+template <int MODEL, bool BATCH>
+__global__ void __launch_bounds__(CONTACT_BLOCK, SPHK_CONTACT_MIN_BLOCKS)
+k_contact(ContactArgs args)
+{
+    constexpr uint32_t FULL = 0xffffffffu;
+    constexpr int WARPS = CONTACT_BLOCK / 32;
+    // per warp: the law terms of the contacts held (F xyz, T xyz, p, ev_dot,
+    // es_dot), the chunk's list of (lane | slot << 5), and which held
+    // contacts overlapped (hits) and slipped
+    __shared__ double terms[WARPS][9][CT_CAP];
+    __shared__ uint16_t expand[WARPS][32 * NC];
+    __shared__ uint32_t hitw[WARPS][CT_CAP / 32], slipw[WARPS][CT_CAP / 32];
+    const Dev &d = args.d;
+    const int A = args.a;
+    const uint32_t lane = threadIdx.x & 31u, w = threadIdx.x >> 5;
+    const uint32_t np = d.np_all;
+    const uint32_t nchunk = (np + 31u) >> 5;
+    const uint32_t gw = blockIdx.x * WARPS + w, nwarps = gridDim.x * WARPS;
+    double (*tm)[CT_CAP] = terms[w];
+    uint16_t *ex = expand[w];
+
+    for (uint32_t g = gw; g < nchunk; g += 32u * nwarps) {
+        // the flags of this warp's next 32 chunks: g, g + W, ..., one a lane
+        const uint32_t mine = g + lane * nwarps;
+        uint32_t todo = __ballot_sync(FULL, mine < nchunk && d.cflag[mine] != 0);
+        while (todo) {
+            const uint32_t chunk = g + (uint32_t)(__ffs(todo) - 1) * nwarps;
+            todo &= todo - 1u;
+            const uint32_t s0 = chunk << 5;
+            const uint32_t s = s0 + lane;
+            const uint32_t occ0 = (s < np) ? d.cmask[s] : 0u;
+            const uint32_t n = __popc(occ0);
+            // first contact of each particle in the chunk's list, and its length
+            uint32_t incl = n;
+#pragma unroll
+            for (uint32_t k = 1; k < 32; k <<= 1) {
+                const uint32_t v = __shfl_up_sync(FULL, incl, k);
+                if (lane >= k) incl += v;
+            }
+            const uint32_t total = __shfl_sync(FULL, incl, 31);
+            const uint32_t off = incl - n;
+            {
+                uint32_t k = off;
+                for (uint32_t m = occ0; m; m &= m - 1u)
+                    ex[k++] = (uint16_t)(lane | ((uint32_t)(__ffs(m) - 1) << 5));
+            }
+            __syncwarp();
+
+            d3 F = mk(0.0, 0.0, 0.0), T = mk(0.0, 0.0, 0.0);
+            double p = 0.0f, ev_dot = 0.0f, es_dot = 0.0f;
+            uint32_t occ = occ0;   // slots still held after this step
+            uint32_t rem = occ0;   // slots whose terms are still to be added
+            for (uint32_t pb = 0; pb < total; pb += CT_CAP) {
+                const uint32_t pe = min(total, pb + CT_CAP);
+                for (uint32_t base = pb; base < pe; base += 32u) {
+                    const uint32_t c = base + lane;
+                    bool hit = false, slip = false;
+                    if (c < pe) {
+                        const uint32_t x = ex[c];
+                        const uint32_t sq = s0 + (x & 31u), i = x >> 5;
+                        const size_t e = (size_t)sq * NC + i;
+                        const uint32_t t = d.contacts[e];
+                        const ulonglong2 dmw = d.dmc[sq];
+                        const double4 dt0 = d.delta_t[e];
+                        const double4 xa = d.xr[A][sq];
+                        const double4 vel_a = ld4(d.vel[A], sq);
+                        const d3 angvel_a = xyz(ld4(d.angvel[A], sq));
+                        const double4 xb = d.xr[A][t];
+                        const double4 vel_b = ld4(d.vel[A], t), angvel_b = ld4(d.angvel[A], t);
+                        LawOut o;
+                        bool touch;
+                        auto eval = [&](const auto &P) {
+                            const d3 dm = decode_dm(dm_get(dmw.x, dmw.y, (int)i), P);
+                            const double ra = xa.w, rb = xb.w;
+                            const d3 xab = mk(xa.x - xb.x + dm.x, xa.y - xb.y + dm.y,
+                                              xa.z - xb.z + dm.z);
+                            const double xlen = flen(xab);
+                            const double delta_n = xlen - (ra + rb);
+                            touch = delta_n < 0.0f;
+                            if (touch) {
+                                o = (MODEL == 2)
+                                    ? contact_linear(P, vel_a, angvel_a, vel_b, angvel_b, ra, rb,
+                                                     xab, xlen, delta_n, dt0)
+                                    : contact_hertz(P, vel_a, angvel_a, vel_b, angvel_b, ra, rb,
+                                                    xab, xlen, delta_n, dt0);
+                            }
+                        };
+                        if constexpr (BATCH) eval(prm_at<true>(d, sq));
+                        else eval(args.lp);
+                        if (touch) {
+                            const uint32_t k = c - pb;
+                            d.delta_t[e] = o.dt4;
+                            tm[0][k] = o.f.x;
+                            tm[1][k] = o.f.y;
+                            tm[2][k] = o.f.z;
+                            tm[3][k] = o.t.x;
+                            tm[4][k] = o.t.y;
+                            tm[5][k] = o.t.z;
+                            tm[6][k] = o.pr;
+                            tm[7][k] = o.ev;
+                            tm[8][k] = o.es;
+                            hit = true;
+                            slip = o.es_set;
+                        } else {
+                            // separated: free the slot and zero its history
+                            d.contacts[e] = np;
+                            d.delta_t[e] = make_double4(0.0, 0.0, 0.0, 0.0);
+                        }
+                    }
+                    const uint32_t hb = __ballot_sync(FULL, hit);
+                    const uint32_t sb = __ballot_sync(FULL, slip);
+                    if (lane == 0) {
+                        hitw[w][(base - pb) >> 5] = hb;
+                        slipw[w][(base - pb) >> 5] = sb;
+                    }
+                }
+                __syncwarp();
+                // every particle adds its terms of this pass, in slot order
+                const uint32_t lo = max(off, pb), hi = min(off + n, pe);
+                for (uint32_t j = lo; j < hi; ++j) {
+                    const uint32_t k = j - pb;
+                    const uint32_t i = (uint32_t)(__ffs(rem) - 1);
+                    rem &= rem - 1u;
+                    if ((hitw[w][k >> 5] >> (k & 31u)) & 1u) {
+                        F = add(F, mk(tm[0][k], tm[1][k], tm[2][k]));
+                        T = add(T, mk(tm[3][k], tm[4][k], tm[5][k]));
+                        p += tm[6][k];
+                        ev_dot += tm[7][k];
+                        if ((slipw[w][k >> 5] >> (k & 31u)) & 1u) es_dot += tm[8][k];
+                    } else {
+                        occ &= ~(1u << i);
+                    }
+                }
+                __syncwarp();
+            }
+            if (n) {
+                d.csum_f[s] = make_double4(F.x, F.y, F.z, p);
+                d.csum_t[s] = make_double4(T.x, T.y, T.z, ev_dot);
+                d.csum_es[s] = es_dot;
+                if (occ != occ0) d.cmask[s] = occ;
+            }
+            // no slot left in the chunk: skip it until a search fills one
+            if (!__any_sync(FULL, occ != 0u) && lane == 0) d.cflag[chunk] = 0;
+        }
+    }
+}
+
+// A resident grid of k_contact: the SMs times the blocks of this
+// instantiation that fit on one (looked up once per instantiation).
+template <int MODEL, bool BATCH>
+static unsigned contact_grid(uint32_t np)
+{
+    static int resident = 0;
+    if (resident == 0) {
+        int dev = 0, sms = 0, per_sm = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_contact<MODEL, BATCH>,
+                                                      CONTACT_BLOCK, 0);
+        resident = std::max(1, sms) * std::max(1, per_sm);
+    }
+    const uint64_t chunks = div_up(np, 32);
+    return (unsigned)std::min<uint64_t>((uint64_t)resident, div_up(chunks, CONTACT_BLOCK / 32));
+}
+
 void launch_topo(const Dev &d, uint32_t np, bool visc, int a, cudaStream_t st)
 {
     const unsigned grid = div_up(np, TOPO_BLOCK);
@@ -1054,9 +1345,28 @@ void launch_force_tape(const Dev &d, uint32_t np, int a, int tape_step, cudaStre
     k_force<2, false, true><<<div_up(np, FORCE_BLOCK), FORCE_BLOCK, 0, st>>>(args);
 }
 
-void launch_step(const Dev &d, uint32_t np, int model, int a, int write_outputs, cudaStream_t st)
+// The slot forces of contact models 2 and 3; model 1 has no slots (k_topo
+// sums its forces) and the differentiable step evaluates its own law in
+// k_force, recording the tape.
+void launch_contact(const Dev &d, const Params &hp, uint32_t np, int model, int a,
+                    cudaStream_t st)
+{
+    if (model == 1 || d.mu_p) return;
+    ContactArgs args{d, a, LawParams{hp.k_n, hp.k_t, hp.gamma_n, hp.gamma_t, hp.gamma_r, hp.mu_s,
+                                     hp.mu_d, hp.mu_r, hp.kappa, hp.dt, {hp.L[0], hp.L[1]}}};
+    if (d.inst)   // batched contexts: contact model 2 only
+        k_contact<2, true><<<contact_grid<2, true>(np), CONTACT_BLOCK, 0, st>>>(args);
+    else if (model == 3)
+        k_contact<3, false><<<contact_grid<3, false>(np), CONTACT_BLOCK, 0, st>>>(args);
+    else
+        k_contact<2, false><<<contact_grid<2, false>(np), CONTACT_BLOCK, 0, st>>>(args);
+}
+
+void launch_step(const Dev &d, const Params &hp, uint32_t np, int model, int a,
+                 int write_outputs, cudaStream_t st)
 {
     launch_topo(d, np, model == 1, a, st);
+    launch_contact(d, hp, np, model, a, st);
     launch_force(d, np, model, a, write_outputs, st);
 }
 

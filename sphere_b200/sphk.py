@@ -32,7 +32,7 @@ OPT_RELAYOUT_EVERY = 1
 OPT_GRAPH_STEPS = 2
 OPT_PROFILE = 3
 OPT_VERLET_SKIN = 4
-PHASES = ("cells", "bonds", "topo", "force", "walls", "darcy")
+PHASES = ("cells", "bonds", "topo", "force", "walls", "darcy", "contact")
 
 _dp = C.POINTER(C.c_double)
 _up = C.POINTER(C.c_uint32)
