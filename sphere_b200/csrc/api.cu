@@ -261,7 +261,7 @@ __global__ void k_rows_to_user(Dev d, uint32_t *contacts, double4 *distmod, doub
     const uint32_t s = d.sidx[u];
     const Params &P = prm_of(d, s);
     const bool occ = (d.cmask[s] >> i) & 1u;
-    const uint32_t v = d.contacts[(size_t)s * NC + i];
+    const uint32_t v = d.contacts[tile_at(s, i, NC)];
     // partners as indices within the particle's own scene; np marks empty
     if (contacts) contacts[e] = occ ? d.uid[v] - P.uid_base : P.np;
     if (distmod) {
@@ -274,7 +274,11 @@ __global__ void k_rows_to_user(Dev d, uint32_t *contacts, double4 *distmod, doub
         }
         distmod[e] = o;
     }
-    if (delta_t) delta_t[e] = d.delta_t[(size_t)s * NC + i];
+    if (delta_t) {
+        // the reference writes the history's fourth lane as 0 (contactmodels.cuh:487, :664)
+        const P3 v3 = d.delta_t[tile_at(s, i, NC)];
+        delta_t[e] = occ ? make_double4(v3.x, v3.y, v3.z, 0.0) : make_double4(0.0, 0.0, 0.0, 0.0);
+    }
 }
 
 __global__ void k_cells_out(Dev d, uint32_t *cell_sorted, uint32_t *perm, uint32_t *cstart,
@@ -599,12 +603,14 @@ int create_impl(const sph_config *cfgs, uint32_t ninst, bool batched, sph_ctx **
     AL(d.w_user, WLANES * np); AL(d.fixed, np);
     AL(d.force, np); AL(d.torque, np); AL(d.acc, np); AL(d.angacc, np); AL(d.edp, np);
     AL(d.uid, np); AL(d.sidx, np); AL(d.cell, np); AL(d.outside, np);
-    AL(d.contacts, np * NC); AL(d.dmc, np); AL(d.delta_t, np * NC); AL(d.cmask, np);
+    AL(d.contacts, tiled_size(np, NC)); AL(d.dmc, np); AL(d.delta_t, tiled_size(np, NC));
+    AL(d.cmask, np);
     AL(d.cflag, div_up(np, 32));
     AL(d.cell_start, ncells + 2); AL(d.cellorder, np); AL(d.pos, np); AL(d.cell_fill, ncells + 1);
     AL(d.scan_tiles, scan_tile_count(c->ncells_all));
     AL(d.alias_any, 1);
-    AL(d.vl, np * VL_CAP); AL(d.vl_meta, np * VL_CAP); AL(d.vl_len, np); AL(d.disp, np);
+    AL(d.vl, tiled_size(np, VL_CAP)); AL(d.vl_meta, tiled_size(np, VL_CAP)); AL(d.vl_len, np);
+    AL(d.disp, np);
     AL(d.vl_gap, np);
     AL(d.movers, MOVER_CAP); AL(d.dirty, ncells + 1); AL(d.vs, 1);
     AL(d.wf_pp, np); AL(d.wtouch, np); AL(d.wf_partial, div_up(np, 256));
@@ -625,7 +631,7 @@ int create_impl(const sph_config *cfgs, uint32_t ninst, bool batched, sph_ctx **
         CK(cudaMemcpy(d.inst_cell_base, cell_bases.data(), ((size_t)ninst + 1) * 4,
                       cudaMemcpyHostToDevice));
     }
-    c->scratch_bytes = np * NC * sizeof(double4) + np * sizeof(uint32_t) + 256;
+    c->scratch_bytes = tiled_size(np, NC) * sizeof(P3) + np * sizeof(uint32_t) + 256;
     char *sc = nullptr;
     AL(sc, c->scratch_bytes);
     c->scratch = sc;
@@ -797,22 +803,25 @@ int sph_upload(sph_ctx *c, const sph_host_state *h)
     // contact slots: partners, periodic-shift codes, occupancy, history
     if (!h->contacts) {
         // the reference's initial state: every slot empty, zero history
-        CK(cudaMemset(d.contacts, 0xff, np * NC * 4));   // empty slots are read through cmask only
+        CK(cudaMemset(d.contacts, 0xff, tiled_size(np, NC) * 4));   // empty slots are read through cmask only
         CK(cudaMemset(d.dmc, 0, np * 16));
         CK(cudaMemset(d.cmask, 0, np * 4));
-        CK(cudaMemset(d.delta_t, 0, np * NC * 32));
+        CK(cudaMemset(d.delta_t, 0, tiled_size(np, NC) * sizeof(P3)));
     } else {
-        std::vector<uint32_t> rows(np * NC, (uint32_t)np);
+        // the caller's rows [np][NC] into tiles; the history's fourth lane is
+        // not kept (the reference writes it as 0)
+        std::vector<uint32_t> rows(tiled_size(np, NC), (uint32_t)np);
         std::vector<unsigned long long> dmc(np * 2, 0ull);
         std::vector<uint32_t> cmask(np, 0u);
-        std::vector<double> dts(np * NC * 4, 0.0);
+        std::vector<double> dts(tiled_size(np, NC) * 3, 0.0);
         for (size_t i = 0; i < np; ++i) {
             // partners are indices within the particle's own scene
             const Params &Q = c->hps[inst_of[i]];
             for (int k = 0; k < NC; ++k) {
                 const uint32_t v = h->contacts[i * NC + k];
                 if (v >= Q.np) continue;
-                rows[i * NC + k] = v + Q.uid_base;
+                const size_t at = tile_at((uint32_t)i, (uint32_t)k, NC);
+                rows[at] = v + Q.uid_base;
                 cmask[i] |= 1u << k;
                 uint32_t code = 0;
                 if (h->distmod) {
@@ -825,13 +834,13 @@ int sph_upload(sph_ctx *c, const sph_host_state *h)
                 }
                 dmc[2 * i + (k >> 4)] |= (unsigned long long)code << (4 * (k & 15));
                 if (h->delta_t)
-                    for (int q = 0; q < 4; ++q) dts[(i * NC + k) * 4 + q] = h->delta_t[(i * NC + k) * 4 + q];
+                    for (int q = 0; q < 3; ++q) dts[at * 3 + q] = h->delta_t[(i * NC + k) * 4 + q];
             }
         }
-        CK(cudaMemcpy(d.contacts, rows.data(), np * NC * 4, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(d.contacts, rows.data(), rows.size() * 4, cudaMemcpyHostToDevice));
         CK(cudaMemcpy(d.dmc, dmc.data(), np * 16, cudaMemcpyHostToDevice));
         CK(cudaMemcpy(d.cmask, cmask.data(), np * 4, cudaMemcpyHostToDevice));
-        CK(cudaMemcpy(d.delta_t, dts.data(), np * NC * 32, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(d.delta_t, dts.data(), dts.size() * 8, cudaMemcpyHostToDevice));
     }
     // walls
     {
@@ -1179,8 +1188,9 @@ static std::vector<std::pair<void *, size_t>> ckpt_fields(sph_ctx *c, int a)
     const size_t np = c->np_all;
     return {{d.xr[a], np * 32},       {d.vel[a], np * 24},  {d.angvel[a], np * 24},
             {d.vel0, np * 24},        {d.angvel0, np * 24}, {d.angpos, np * 24},
-            {d.xysum, np * 16},       {d.esv, np * 16},     {d.contacts, np * NC * 4},
-            {d.dmc, np * 16},         {d.cmask, np * 4},    {d.delta_t, np * NC * 32}};
+            {d.xysum, np * 16},       {d.esv, np * 16},     {d.contacts, tiled_size(np, NC) * 4},
+            {d.dmc, np * 16},         {d.cmask, np * 4},
+            {d.delta_t, tiled_size(np, NC) * sizeof(P3)}};
 }
 
 static int save_ckpt(sph_ctx *c, sph_ctx::Ckpt &k)

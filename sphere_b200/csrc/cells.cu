@@ -290,22 +290,34 @@ __global__ void k_gather(const T *__restrict__ src, T *__restrict__ dst, const u
 }
 
 // contact rows: move the row and translate partner indices
+// Tiled slot entries into the new storage order: entry e of the new tiles
+// takes the old particle's entry, partners renamed through `inv` (empty
+// slots keep whatever they held: an empty slot's entry is never read).
+__device__ __forceinline__ bool tile_entry(uint64_t e, uint32_t np, uint32_t &s, uint32_t &i)
+{
+    s = (uint32_t)((e / (32ull * NC)) * 32ull + (e & 31ull));
+    i = (uint32_t)((e >> 5) % NC);
+    return s < np;
+}
+
 __global__ void k_gather_rows(const uint32_t *src, uint32_t *dst, const uint32_t *order,
                               const uint32_t *inv, uint32_t np)
 {
     const uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= (uint64_t)np * NC) return;
-    const uint32_t k = (uint32_t)(e / NC), i = (uint32_t)(e % NC);
-    const uint32_t v = src[(size_t)order[k] * NC + i];
+    if (e >= tiled_size(np, NC)) return;
+    uint32_t s, i;
+    if (!tile_entry(e, np, s, i)) return;
+    const uint32_t v = src[tile_at(order[s], i, NC)];
     dst[e] = (v < np) ? inv[v] : np;
 }
 
-__global__ void k_gather_dt(const double4 *src, double4 *dst, const uint32_t *order, uint32_t np)
+__global__ void k_gather_dt(const P3 *src, P3 *dst, const uint32_t *order, uint32_t np)
 {
     const uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= (uint64_t)np * NC) return;
-    const uint32_t k = (uint32_t)(e / NC), i = (uint32_t)(e % NC);
-    dst[e] = src[(size_t)order[k] * NC + i];
+    if (e >= tiled_size(np, NC)) return;
+    uint32_t s, i;
+    if (!tile_entry(e, np, s, i)) return;
+    dst[e] = src[tile_at(order[s], i, NC)];
 }
 
 __global__ void k_relayout_finish(Dev d, int A)
@@ -334,11 +346,12 @@ static void gather_back(T *arr, void *scratch, const uint32_t *order, uint32_t n
 
 // Permute every per-particle array into the order of d.cellorder (which the
 // rebuild kernels must have brought up to date).  `scratch` holds at least
-// np * NC * sizeof(double4) bytes plus np * sizeof(uint32_t) for the inverse.
+// tiled_size(np, NC) * sizeof(P3) bytes plus np * sizeof(uint32_t) for the
+// inverse.
 void relayout(const Dev &d, uint32_t np, int a, void *scratch, cudaStream_t st)
 {
     uint32_t *inv = reinterpret_cast<uint32_t *>(static_cast<char *>(scratch) +
-                                                 (size_t)np * NC * sizeof(double4));
+                                                 tiled_size(np, NC) * sizeof(P3));
     const uint32_t *order = d.cellorder;
     k_relayout_inv<<<div_up(np, CELL_BLOCK), CELL_BLOCK, 0, st>>>(d, inv);
     gather_back(d.xr[a], scratch, order, np, st);
@@ -362,18 +375,17 @@ void relayout(const Dev &d, uint32_t np, int a, void *scratch, cudaStream_t st)
     gather_back(d.dmc, scratch, order, np, st);
     gather_back(d.wtouch, scratch, order, np, st);
     if (d.inst) gather_back(d.inst, scratch, order, np, st);
-    const unsigned int rows = div_up((unsigned long long)np * NC, CELL_BLOCK);
+    const size_t ntile = tiled_size(np, NC);
+    const unsigned int rows = div_up(ntile, CELL_BLOCK);
     {
         uint32_t *tmp = static_cast<uint32_t *>(scratch);
         k_gather_rows<<<rows, CELL_BLOCK, 0, st>>>(d.contacts, tmp, order, inv, np);
-        cudaMemcpyAsync(d.contacts, tmp, sizeof(uint32_t) * (size_t)np * NC,
-                        cudaMemcpyDeviceToDevice, st);
+        cudaMemcpyAsync(d.contacts, tmp, sizeof(uint32_t) * ntile, cudaMemcpyDeviceToDevice, st);
     }
     {
-        double4 *tmp = static_cast<double4 *>(scratch);
+        P3 *tmp = static_cast<P3 *>(scratch);
         k_gather_dt<<<rows, CELL_BLOCK, 0, st>>>(d.delta_t, tmp, order, np);
-        cudaMemcpyAsync(d.delta_t, tmp, sizeof(double4) * (size_t)np * NC,
-                        cudaMemcpyDeviceToDevice, st);
+        cudaMemcpyAsync(d.delta_t, tmp, sizeof(P3) * ntile, cudaMemcpyDeviceToDevice, st);
     }
     k_relayout_finish<<<div_up(np, CELL_BLOCK), CELL_BLOCK, 0, st>>>(d, a);
 }

@@ -146,9 +146,9 @@ struct Dev {
     uint32_t *cell;       // cell id (calcCellID semantics) of the current positions
     uint8_t *outside;     // the position's floored cell coordinates leave the grid
     // contacts
-    uint32_t *contacts;   // [np][NC]
+    uint32_t *contacts;   // tiled, NC per particle (tile_at)
     ulonglong2 *dmc;      // [np] 4-bit periodic shift code of each of the NC slots
-    double4 *delta_t;     // [np][NC]
+    P3 *delta_t;          // tiled, NC per particle; the reference's fourth lane is always 0
     uint32_t *cmask;      // [np] occupied-slot bit mask
     // contact models 2 and 3: each particle's slot sums from k_contact
     // (F xyz and p; T xyz and ev_dot; es_dot), read by k_force
@@ -163,8 +163,8 @@ struct Dev {
     uint32_t *scan_tiles; // scratch for the scan
     uint32_t *alias_any;  // some particle sits outside its cell's box (set by the rebuild)
     // Verlet lists
-    uint32_t *vl;         // [np][VL_CAP] candidate storage indices, in visiting order
-    uint16_t *vl_meta;    // [np][VL_CAP] stencil cell (0..26) | shift code << 5
+    uint32_t *vl;         // tiled, VL_CAP per particle: candidate storage indices, in visiting order
+    uint16_t *vl_meta;    // tiled, VL_CAP per particle: stencil cell (0..26) | shift code << 5
     uint8_t *vl_len;      // [np] list length or VL_NONE
     float *vl_gap;        // [np] lower bound of the smallest gap to a listed candidate
     float *disp;          // [np] displacement bound since the epoch started
@@ -261,6 +261,48 @@ __device__ __forceinline__ bool cell_outside(const Params &P, double x, double y
     const double f0 = cell_floor(P, 0, x), f1 = cell_floor(P, 1, y), f2 = cell_floor(P, 2, z);
     return !(f0 >= 0.0 && f0 < (double)P.num[0] && f1 >= 0.0 && f1 < (double)P.num[1] &&
              f2 >= 0.0 && f2 < (double)P.num[2]);
+}
+
+// Tiles of 32 storage indices.  The contact slots (partners and tangential
+// history) and the Verlet lists hold `width` entries per particle, stored
+// tile by tile: entry i of particle s sits at ((s / 32) width + i) 32 +
+// s % 32.  The lanes of a warp that touch entry i of their 32 particles touch
+// one contiguous run, and the few entries a particle uses (its occupied
+// slots, its short list) cost no more than their own bytes, where rows of
+// `width` entries per particle cost whole cache lines.
+__host__ __device__ __forceinline__ size_t tile_at(uint32_t s, uint32_t i, uint32_t width)
+{
+    return ((size_t)(s >> 5) * width + i) * 32u + (s & 31u);
+}
+// Asks the copy engine to bring `bytes` at `p` into L2 (a hint: nothing is
+// waited for, no register is held).  `p` and `bytes` are multiples of 16.
+__device__ __forceinline__ void bulk_prefetch_l2(const void *p, uint32_t bytes)
+{
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
+// The slot rule fills the last empty slot first (src/contactsearch.cuh:
+// 252-271), so a particle's few contacts sit in the top slots: the tile rows
+// worth fetching ahead are the top PF_SLOTS.
+constexpr uint32_t PF_SLOTS = 8;
+
+// Entry e of particle s's Verlet list (Dev::vl, Dev::vl_meta): tiled like
+// the slots, or (SPHK_VL_ROWS) one row of VL_CAP entries per particle.
+#ifdef SPHK_VL_ROWS
+__host__ __device__ __forceinline__ size_t vl_at(uint32_t s, uint32_t e)
+{
+    return (size_t)s * VL_CAP + e;
+}
+#else
+__host__ __device__ __forceinline__ size_t vl_at(uint32_t s, uint32_t e)
+{
+    return tile_at(s, e, VL_CAP);
+}
+#endif
+// Entries of a tiled array for np particles (the last tile is padded).
+__host__ __device__ __forceinline__ size_t tiled_size(size_t np, uint32_t width)
+{
+    return ((np + 31) / 32) * 32 * (size_t)width;
 }
 
 inline unsigned int div_up(unsigned long long a, unsigned int b)

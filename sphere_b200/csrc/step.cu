@@ -385,6 +385,7 @@ __device__ __forceinline__ void wrap_axis(int32_t &c, uint32_t num, uint32_t &co
 // Slot state of one particle during contact detection.
 struct TopoSlots {
     uint32_t occ;                    // occupied-slot mask
+    uint32_t occ0;                   // the mask before this step's search
     uint32_t err;
     unsigned long long dm_lo, dm_hi; // periodic shift code of each slot
     int nc;                          // contacts found this step
@@ -392,23 +393,17 @@ struct TopoSlots {
     bool dirty;                      // row changed
 };
 
-// Copies the particle's slot row and shift codes to shared memory and
-// registers (once): only the 16-byte pieces of the row that hold an occupied
-// slot, since the other entries are neither searched nor written back.
+// Copies the partners of the particle's occupied slots to shared memory and
+// its shift codes to registers (once); the other entries are neither
+// searched nor written back.
 __device__ __forceinline__ void topo_load_row(const Dev &d, uint32_t *srow, int tid, uint32_t s,
                                               TopoSlots &ts)
 {
     if (ts.loaded) return;
     if (ts.occ) {
-        const uint4 *row = reinterpret_cast<const uint4 *>(d.contacts + (size_t)s * NC);
-#pragma unroll
-        for (int q = 0; q < NC / 4; ++q) {
-            if (((ts.occ >> (4 * q)) & 0xFu) == 0u) continue;
-            const uint4 v = row[q];
-            srow[(4 * q + 0) * TOPO_BLOCK + tid] = v.x;
-            srow[(4 * q + 1) * TOPO_BLOCK + tid] = v.y;
-            srow[(4 * q + 2) * TOPO_BLOCK + tid] = v.z;
-            srow[(4 * q + 3) * TOPO_BLOCK + tid] = v.w;
+        for (uint32_t m = ts.occ; m; m &= m - 1u) {
+            const uint32_t i = (uint32_t)(__ffs(m) - 1);
+            srow[i * TOPO_BLOCK + tid] = d.contacts[tile_at(s, i, NC)];
         }
         const ulonglong2 c2 = d.dmc[s];
         ts.dm_lo = c2.x;
@@ -568,7 +563,8 @@ k_topo(Dev d, int A)
     const double4 xa = d.xr[A][s];
     const double ra = xa.w;
     const double4 *__restrict__ xr = d.xr[A];
-    TopoSlots ts{d.cmask[s], 0u, 0ull, 0ull, 0, false, false};
+    const uint32_t occ_in = d.cmask[s];
+    TopoSlots ts{occ_in, occ_in, 0u, 0ull, 0ull, 0, false, false};
     const uint32_t nx = P.num[0], ny = P.num[1], nz = P.num[2];
     int32_t gp[3];
     gp[0] = __double2int_rz(cell_floor(P, 0, xa.x));
@@ -581,16 +577,13 @@ k_topo(Dev d, int A)
     double p1 = 0.0f;
 
     if (VISC && list_ok) {
-        const uint32_t *vl = d.vl + (size_t)s * VL_CAP;
-        const uint16_t *vm = d.vl_meta + (size_t)s * VL_CAP;
-        for (uint32_t e = 0; e < len; ++e)
-            visc_pair(d, A, s, vl[e], (uint32_t)vm[e] >> 5, F1, p1);
+        for (uint32_t e = 0; e < len; ++e) {
+            const size_t at = vl_at(s, e);
+            visc_pair(d, A, s, d.vl[at], (uint32_t)d.vl_meta[at] >> 5, F1, p1);
+        }
     } else if (list_ok) {
-        // the list row is read four entries at a time (16 B of candidates,
-        // 8 B of their codes), a quarter of the load instructions and of
-        // the sectors requested of one entry a load
-        const uint4 *vl4 = reinterpret_cast<const uint4 *>(d.vl + (size_t)s * VL_CAP);
-        const uint2 *vm4 = reinterpret_cast<const uint2 *>(d.vl_meta + (size_t)s * VL_CAP);
+        // the list is read four entries at a time, so that their loads are
+        // in flight together
         // A candidate that already holds a slot through the same image needs
         // no test: overlapping or not, the reference's topology leaves its
         // slot as it is (a separated one is freed by the force pass).  The
@@ -601,10 +594,13 @@ k_topo(Dev d, int A)
         if (filter) topo_load_row(d, srow, tid, s, ts);
         int skip_slot = -1;
         for (uint32_t e0 = 0; e0 < len; e0 += 4) {
-            const uint4 tq = vl4[e0 >> 2];
-            const uint2 mq = vm4[e0 >> 2];
-            const uint32_t tv[4] = {tq.x, tq.y, tq.z, tq.w};
-            const uint32_t mv[4] = {mq.x & 0xffffu, mq.x >> 16, mq.y & 0xffffu, mq.y >> 16};
+            uint32_t tv[4], mv[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const size_t at = vl_at(s, min(e0 + (uint32_t)j, (uint32_t)len - 1u));
+                tv[j] = d.vl[at];
+                mv[j] = d.vl_meta[at];
+            }
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
                 if (e0 + (uint32_t)j >= len) break;
@@ -625,8 +621,6 @@ k_topo(Dev d, int A)
         const float eps = P.cull_eps;
         const float skinf = (float)P.skin;
         const float extraf = (float)P.reach_extra;
-        uint32_t *vl = d.vl + (size_t)s * VL_CAP;
-        uint16_t *vm = d.vl_meta + (size_t)s * VL_CAP;
         uint32_t nlist = 0;
         bool list_overflow = false;
         float gmin = 3.0e38f;   // smallest gap to a listed candidate, bounded below
@@ -675,8 +669,9 @@ k_topo(Dev d, int A)
                     const uint32_t slot = slot0 + ((k2 < bnd1) ? 0u : ((k2 < bnd2) ? 1u : 2u));
                     if (!use_lists) {
                     } else if (nlist < VL_CAP) {
-                        vl[nlist] = t;
-                        vm[nlist] = (uint16_t)(slot | (code << 5));
+                        const size_t at = vl_at(s, nlist);
+                        d.vl[at] = t;
+                        d.vl_meta[at] = (uint16_t)(slot | (code << 5));
                         ++nlist;
                     } else {
                         list_overflow = true;
@@ -773,29 +768,19 @@ k_topo(Dev d, int A)
 
     if (VISC) d.c1acc[s] = make_double4(F1.x, F1.y, F1.z, p1);
     if (ts.dirty) {
-        uint4 *row = reinterpret_cast<uint4 *>(d.contacts + (size_t)s * NC);
+        // the search only fills empty slots (and may change a code): the
+        // partners of the newly occupied slots are the entries to write;
+        // an empty slot's entry is never read
         const uint32_t occ = ts.occ;
-#pragma unroll
-        for (int q = 0; q < NC / 4; ++q) {
-            uint4 v;
-            v.x = ((occ >> (4 * q + 0)) & 1u) ? srow[(4 * q + 0) * TOPO_BLOCK + tid] : np;
-            v.y = ((occ >> (4 * q + 1)) & 1u) ? srow[(4 * q + 1) * TOPO_BLOCK + tid] : np;
-            v.z = ((occ >> (4 * q + 2)) & 1u) ? srow[(4 * q + 2) * TOPO_BLOCK + tid] : np;
-            v.w = ((occ >> (4 * q + 3)) & 1u) ? srow[(4 * q + 3) * TOPO_BLOCK + tid] : np;
-            row[q] = v;
+        for (uint32_t m = occ & ~ts.occ0; m; m &= m - 1u) {
+            const uint32_t i = (uint32_t)(__ffs(m) - 1);
+            d.contacts[tile_at(s, i, NC)] = srow[i * TOPO_BLOCK + tid];
         }
         d.cmask[s] = occ;
         d.dmc[s] = make_ulonglong2(ts.dm_lo, ts.dm_hi);
         if (occ) d.cflag[s >> 5] = 1;
     }
     if (ts.err) atomicOr(d.status, ts.err);
-}
-
-// Asks the copy engine to bring `bytes` at `p` into L2 (a hint: nothing is
-// waited for, no register is held).  `p` and `bytes` are multiples of 16.
-__device__ __forceinline__ void bulk_prefetch_l2(const void *p, uint32_t bytes)
-{
-    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
 }
 
 struct ForceArgs {
@@ -853,12 +838,11 @@ k_force(ForceArgs args)
         const size_t row = (j >= 0) ? ((size_t)j * np + s) : 0;
         uint32_t lawmask = 0;
         const ulonglong2 dmw = d.dmc[s];
-        uint32_t *crow = d.contacts + (size_t)s * NC;
-        double4 *dtrow = d.delta_t + (size_t)s * NC;
         const uint32_t occ0 = occ;
         for (uint32_t m = occ0; m; m &= m - 1) {
             const int i = __ffs(m) - 1;
-            const uint32_t t = crow[i];
+            const size_t at = tile_at(s, (uint32_t)i, NC);
+            const uint32_t t = d.contacts[at];
             const d3 dm = decode_dm(dm_get(dmw.x, dmw.y, i), P);
             const double4 xb = d.xr[A][t];
             dl::PairIn in;
@@ -866,7 +850,9 @@ k_force(ForceArgs args)
             in.ra = ra;
             in.rb = xb.w;
             if (dl::len(in.xab) - (ra + xb.w) < 0.0) {
-                const double4 vb = ld4(d.vel[A], t), wb = ld4(d.angvel[A], t), d0 = dtrow[i];
+                const P3 d0p = d.delta_t[at];
+                const double4 vb = ld4(d.vel[A], t), wb = ld4(d.angvel[A], t);
+                const double4 d0 = make_double4(d0p.x, d0p.y, d0p.z, 0.0);
                 in.va = dl::v3(vel_a.x, vel_a.y, vel_a.z);
                 in.vb = dl::v3(vb.x, vb.y, vb.z);
                 in.wa = dl::v3(angvel_a4.x, angvel_a4.y, angvel_a4.z);
@@ -878,7 +864,7 @@ k_force(ForceArgs args)
                 dl::pair_fwd(law, in, o);
                 F = add(F, mk(o.F.x, o.F.y, o.F.z));
                 T = add(T, mk(o.T.x, o.T.y, o.T.z));
-                dtrow[i] = make_double4(o.dtn.x, o.dtn.y, o.dtn.z, 0.0);
+                d.delta_t[at] = P3{o.dtn.x, o.dtn.y, o.dtn.z};
                 lawmask |= 1u << i;
                 if (j >= 0) {
                     d.tp_partner[row * NC + i] = t;
@@ -886,8 +872,8 @@ k_force(ForceArgs args)
                 }
             } else {
                 occ &= ~(1u << i);
-                crow[i] = np;
-                dtrow[i] = make_double4(0.0, 0.0, 0.0, 0.0);
+                d.contacts[at] = np;
+                d.delta_t[at] = P3{0.0, 0.0, 0.0};
             }
         }
         if (occ != occ0) d.cmask[s] = occ;
@@ -1122,8 +1108,11 @@ struct ContactArgs {
     LawParams lp;   // single-scene contexts; a batch reads each scene's Params
 };
 
-// Contacts of one chunk whose law terms a warp holds at once.
-constexpr uint32_t CT_CAP = 128;
+// Contacts of one chunk whose law terms a warp holds at once (a multiple of 32).
+#ifndef SPHK_CONTACT_CAP
+#define SPHK_CONTACT_CAP 96
+#endif
+constexpr uint32_t CT_CAP = SPHK_CONTACT_CAP;
 
 // k_contact: interact's slot loop (src/contactsearch.cuh:468-543) for
 // contact models 2 and 3, one lane per directed contact.
@@ -1136,16 +1125,16 @@ constexpr uint32_t CT_CAP = 128;
 // ... of the W warps, reading the flags of 32 of them in one load, so a
 // contact-free scene costs about one memory latency.
 //
-// In a chunk, the occupied slots, particle after particle and each
-// particle's in slot order, form a list of directed contacts, which each
-// particle's lane writes out once into shared memory as (lane, slot) pairs.
-// The list is evaluated 32 contacts at a time, one per lane, so every lane
-// runs a force law whatever the spread of contact counts, and the terms of
-// up to CT_CAP contacts are kept in shared memory.  Then every particle's
-// own lane adds its terms in slot order, the reference's summation order,
-// all lanes at once, and at the end stores the sums for k_force.  A slot
-// whose partner no longer overlaps is freed and its history zeroed, as in
-// the reference.
+// In a chunk, the occupied slots form a list of directed contacts, written
+// once into shared memory as (lane, slot) pairs in slot-major order.  The
+// list is evaluated 32 contacts at a time, one per lane, so every lane runs
+// a force law whatever the spread of contact counts, and the terms of up to
+// CT_CAP contacts are kept in shared memory.  Then every particle's own lane
+// adds its terms in slot order, the reference's summation order, all lanes
+// at once, and at the end stores the sums for k_force.  A slot whose partner
+// no longer overlaps is freed and its history zeroed, as in the reference.
+// A chunk's rows are contiguous, its slot tiles too, and a round's lanes
+// mostly read one slot of consecutive particles, so their loads coalesce.
 template <int MODEL, bool BATCH>
 __global__ void __launch_bounds__(CONTACT_BLOCK, SPHK_CONTACT_MIN_BLOCKS)
 k_contact(ContactArgs args)
@@ -1158,6 +1147,9 @@ k_contact(ContactArgs args)
     __shared__ double terms[WARPS][9][CT_CAP];
     __shared__ uint16_t expand[WARPS][32 * NC];
     __shared__ uint32_t hitw[WARPS][CT_CAP / 32], slipw[WARPS][CT_CAP / 32];
+    __shared__ double sums[WARPS][9][32];   // each particle's running sums
+    __shared__ uint16_t sbase[WARPS][NC];    // first list entry of each slot
+    __shared__ uint32_t smask[WARPS][NC];    // the particles holding each slot
     const Dev &d = args.d;
     const int A = args.a;
     const uint32_t lane = threadIdx.x & 31u, w = threadIdx.x >> 5;
@@ -1165,126 +1157,185 @@ k_contact(ContactArgs args)
     const uint32_t nchunk = (np + 31u) >> 5;
     const uint32_t gw = blockIdx.x * WARPS + w, nwarps = gridDim.x * WARPS;
     double (*tm)[CT_CAP] = terms[w];
+    double (*sm)[32] = sums[w];
     uint16_t *ex = expand[w];
+    // A chunk's rows are contiguous (its slot tiles too), so one lane asks
+    // the copy engine to bring a chunk that is coming up into L2 while the
+    // warp works: the chain of loads of each round then waits on L2, not on
+    // DRAM.  Only whole chunks, so that no request passes an array's end.
+    auto prefetch_chunk = [&](uint32_t ch) {
+        const uint32_t b = ch << 5;
+        if (lane != 0 || b + 32u > np) return;
+        bulk_prefetch_l2(d.cmask + b, 32 * sizeof(uint32_t));
+        bulk_prefetch_l2(d.dmc + b, 32 * sizeof(ulonglong2));
+        bulk_prefetch_l2(d.xr[A] + b, 32 * sizeof(double4));
+        bulk_prefetch_l2(d.vel[A] + b, 32 * sizeof(P3));
+        bulk_prefetch_l2(d.angvel[A] + b, 32 * sizeof(P3));
+        bulk_prefetch_l2(d.contacts + tile_at(b, NC - PF_SLOTS, NC), PF_SLOTS * 32 * sizeof(uint32_t));
+        bulk_prefetch_l2(d.delta_t + tile_at(b, NC - PF_SLOTS, NC), PF_SLOTS * 32 * sizeof(P3));
+    };
 
     for (uint32_t g = gw; g < nchunk; g += 32u * nwarps) {
         // the flags of this warp's next 32 chunks: g, g + W, ..., one a lane
         const uint32_t mine = g + lane * nwarps;
         uint32_t todo = __ballot_sync(FULL, mine < nchunk && d.cflag[mine] != 0);
+        if (todo) prefetch_chunk(g + (uint32_t)(__ffs(todo) - 1) * nwarps);
         while (todo) {
             const uint32_t chunk = g + (uint32_t)(__ffs(todo) - 1) * nwarps;
             todo &= todo - 1u;
+            if (todo) prefetch_chunk(g + (uint32_t)(__ffs(todo) - 1) * nwarps);
             const uint32_t s0 = chunk << 5;
             const uint32_t s = s0 + lane;
             const uint32_t occ0 = (s < np) ? d.cmask[s] : 0u;
             const uint32_t n = __popc(occ0);
-            // first contact of each particle in the chunk's list, and its length
-            uint32_t incl = n;
-#pragma unroll
-            for (uint32_t k = 1; k < 32; k <<= 1) {
-                const uint32_t v = __shfl_up_sync(FULL, incl, k);
-                if (lane >= k) incl += v;
-            }
-            const uint32_t total = __shfl_sync(FULL, incl, 31);
-            const uint32_t off = incl - n;
+            const uint32_t total = __reduce_add_sync(FULL, n);   // the chunk's contacts
+            // The list in slot-major order: slot by slot, and within a slot
+            // by particle.  The lanes of a round then mostly share a slot and
+            // touch consecutive particles: consecutive entries of the slot
+            // tiles and consecutive particle rows.  A particle's contacts stay
+            // in ascending slot order along the list; slot i's first entry is
+            // sbase[i], and a particle finds its own entry of slot i from
+            // smask[i], the particles holding it.
             {
-                uint32_t k = off;
-                for (uint32_t m = occ0; m; m &= m - 1u)
-                    ex[k++] = (uint16_t)(lane | ((uint32_t)(__ffs(m) - 1) << 5));
+                const uint32_t lt = (1u << lane) - 1u;
+                uint32_t k = 0;
+                for (uint32_t u = __reduce_or_sync(FULL, occ0); u; u &= u - 1u) {
+                    const uint32_t i = (uint32_t)(__ffs(u) - 1);
+                    const uint32_t m = __ballot_sync(FULL, (occ0 >> i) & 1u);
+                    if ((occ0 >> i) & 1u) ex[k + __popc(m & lt)] = (uint16_t)(lane | (i << 5));
+                    if (lane == 0) {
+                        sbase[w][i] = (uint16_t)k;
+                        smask[w][i] = m;
+                    }
+                    k += __popc(m);
+                }
             }
             __syncwarp();
 
-            d3 F = mk(0.0, 0.0, 0.0), T = mk(0.0, 0.0, 0.0);
-            double p = 0.0f, ev_dot = 0.0f, es_dot = 0.0f;
+            // the particle's running sums live in shared memory between the
+            // passes, so no register holds them while the laws run
+            if (n) {
+#pragma unroll
+                for (int f = 0; f < 9; ++f) sm[f][lane] = 0.0;
+            }
             uint32_t occ = occ0;   // slots still held after this step
             uint32_t rem = occ0;   // slots whose terms are still to be added
-            for (uint32_t pb = 0; pb < total; pb += CT_CAP) {
-                const uint32_t pe = min(total, pb + CT_CAP);
-                for (uint32_t base = pb; base < pe; base += 32u) {
-                    const uint32_t c = base + lane;
-                    bool hit = false, slip = false;
-                    if (c < pe) {
-                        const uint32_t x = ex[c];
-                        const uint32_t sq = s0 + (x & 31u), i = x >> 5;
-                        const size_t e = (size_t)sq * NC + i;
-                        const uint32_t t = d.contacts[e];
-                        const ulonglong2 dmw = d.dmc[sq];
-                        const double4 dt0 = d.delta_t[e];
-                        const double4 xa = d.xr[A][sq];
-                        const double4 vel_a = ld4(d.vel[A], sq);
-                        const d3 angvel_a = xyz(ld4(d.angvel[A], sq));
-                        const double4 xb = d.xr[A][t];
-                        const double4 vel_b = ld4(d.vel[A], t), angvel_b = ld4(d.angvel[A], t);
-                        LawOut o;
-                        bool touch;
-                        auto eval = [&](const auto &P) {
-                            const d3 dm = decode_dm(dm_get(dmw.x, dmw.y, (int)i), P);
-                            const double ra = xa.w, rb = xb.w;
-                            const d3 xab = mk(xa.x - xb.x + dm.x, xa.y - xb.y + dm.y,
-                                              xa.z - xb.z + dm.z);
-                            const double xlen = flen(xab);
-                            const double delta_n = xlen - (ra + rb);
-                            touch = delta_n < 0.0f;
-                            if (touch) {
-                                o = (MODEL == 2)
-                                    ? contact_linear(P, vel_a, angvel_a, vel_b, angvel_b, ra, rb,
-                                                     xab, xlen, delta_n, dt0)
-                                    : contact_hertz(P, vel_a, angvel_a, vel_b, angvel_b, ra, rb,
-                                                    xab, xlen, delta_n, dt0);
-                            }
-                        };
-                        if constexpr (BATCH) eval(prm_at<true>(d, sq));
-                        else eval(args.lp);
+            // the partner of this lane's contact, loaded a round ahead
+            uint32_t t_next = 0;
+            if (lane < total) {
+                const uint32_t x = ex[lane];
+                t_next = d.contacts[tile_at(s0 + (x & 31u), x >> 5, NC)];
+            }
+            for (uint32_t base = 0; base < total; base += 32u) {
+                const uint32_t c = base + lane;
+                const uint32_t t = t_next;
+                if (c + 32u < total) {
+                    const uint32_t x = ex[c + 32u];
+                    t_next = d.contacts[tile_at(s0 + (x & 31u), x >> 5, NC)];
+                }
+                const uint32_t pb = base - base % CT_CAP;   // first contact of this pass
+                bool hit = false, slip = false;
+                if (c < total) {
+                    const uint32_t x = ex[c];
+                    const uint32_t sq = s0 + (x & 31u), i = x >> 5;
+                    const size_t e = tile_at(sq, i, NC);
+                    const ulonglong2 dmw = d.dmc[sq];
+                    const P3 dtp = d.delta_t[e];
+                    const double4 dt0 = make_double4(dtp.x, dtp.y, dtp.z, 0.0);
+                    const double4 xa = d.xr[A][sq];
+                    const double4 vel_a = ld4(d.vel[A], sq);
+                    const d3 angvel_a = xyz(ld4(d.angvel[A], sq));
+                    const double4 xb = d.xr[A][t];
+                    const double4 vel_b = ld4(d.vel[A], t), angvel_b = ld4(d.angvel[A], t);
+                    LawOut o;
+                    bool touch;
+                    auto eval = [&](const auto &P) {
+                        const d3 dm = decode_dm(dm_get(dmw.x, dmw.y, (int)i), P);
+                        const double ra = xa.w, rb = xb.w;
+                        const d3 xab = mk(xa.x - xb.x + dm.x, xa.y - xb.y + dm.y,
+                                          xa.z - xb.z + dm.z);
+                        const double xlen = flen(xab);
+                        const double delta_n = xlen - (ra + rb);
+                        touch = delta_n < 0.0f;
                         if (touch) {
-                            const uint32_t k = c - pb;
-                            d.delta_t[e] = o.dt4;
-                            tm[0][k] = o.f.x;
-                            tm[1][k] = o.f.y;
-                            tm[2][k] = o.f.z;
-                            tm[3][k] = o.t.x;
-                            tm[4][k] = o.t.y;
-                            tm[5][k] = o.t.z;
-                            tm[6][k] = o.pr;
-                            tm[7][k] = o.ev;
-                            tm[8][k] = o.es;
-                            hit = true;
-                            slip = o.es_set;
-                        } else {
-                            // separated: free the slot and zero its history
-                            d.contacts[e] = np;
-                            d.delta_t[e] = make_double4(0.0, 0.0, 0.0, 0.0);
+                            o = (MODEL == 2)
+                                ? contact_linear(P, vel_a, angvel_a, vel_b, angvel_b, ra, rb, xab,
+                                                 xlen, delta_n, dt0)
+                                : contact_hertz(P, vel_a, angvel_a, vel_b, angvel_b, ra, rb, xab,
+                                                xlen, delta_n, dt0);
                         }
-                    }
-                    const uint32_t hb = __ballot_sync(FULL, hit);
-                    const uint32_t sb = __ballot_sync(FULL, slip);
-                    if (lane == 0) {
-                        hitw[w][(base - pb) >> 5] = hb;
-                        slipw[w][(base - pb) >> 5] = sb;
+                    };
+                    if constexpr (BATCH) eval(prm_at<true>(d, sq));
+                    else eval(args.lp);
+                    if (touch) {
+                        const uint32_t k = c - pb;
+                        d.delta_t[e] = P3{o.dt4.x, o.dt4.y, o.dt4.z};
+                        tm[0][k] = o.f.x;
+                        tm[1][k] = o.f.y;
+                        tm[2][k] = o.f.z;
+                        tm[3][k] = o.t.x;
+                        tm[4][k] = o.t.y;
+                        tm[5][k] = o.t.z;
+                        tm[6][k] = o.pr;
+                        tm[7][k] = o.ev;
+                        tm[8][k] = o.es;
+                        hit = true;
+                        slip = o.es_set;
+                    } else {
+                        // separated: free the slot and zero its history
+                        d.contacts[e] = np;
+                        d.delta_t[e] = P3{0.0, 0.0, 0.0};
                     }
                 }
+                const uint32_t hb = __ballot_sync(FULL, hit);
+                const uint32_t sb = __ballot_sync(FULL, slip);
+                if (lane == 0) {
+                    hitw[w][(base - pb) >> 5] = hb;
+                    slipw[w][(base - pb) >> 5] = sb;
+                }
+                const uint32_t pe = min(total, pb + CT_CAP);
+                if (base + 32u < pe) continue;
                 __syncwarp();
-                // every particle adds its terms of this pass, in slot order
-                const uint32_t lo = max(off, pb), hi = min(off + n, pe);
-                for (uint32_t j = lo; j < hi; ++j) {
-                    const uint32_t k = j - pb;
-                    const uint32_t i = (uint32_t)(__ffs(rem) - 1);
-                    rem &= rem - 1u;
-                    if ((hitw[w][k >> 5] >> (k & 31u)) & 1u) {
-                        F = add(F, mk(tm[0][k], tm[1][k], tm[2][k]));
-                        T = add(T, mk(tm[3][k], tm[4][k], tm[5][k]));
-                        p += tm[6][k];
-                        ev_dot += tm[7][k];
-                        if ((slipw[w][k >> 5] >> (k & 31u)) & 1u) es_dot += tm[8][k];
-                    } else {
-                        occ &= ~(1u << i);
+                // the pass is complete: every particle adds its terms of the
+                // pass, in slot order
+                const uint32_t lt = (1u << lane) - 1u;
+                auto entry = [&](uint32_t i) { return (uint32_t)sbase[w][i] + __popc(smask[w][i] & lt); };
+                if (rem && entry((uint32_t)(__ffs(rem) - 1)) < pe) {
+                    d3 F = mk(sm[0][lane], sm[1][lane], sm[2][lane]);
+                    d3 T = mk(sm[3][lane], sm[4][lane], sm[5][lane]);
+                    double p = sm[6][lane], ev_dot = sm[7][lane], es_dot = sm[8][lane];
+                    while (rem) {
+                        const uint32_t i = (uint32_t)(__ffs(rem) - 1);
+                        const uint32_t j = entry(i);
+                        if (j >= pe) break;   // in a later pass
+                        const uint32_t k = j - pb;
+                        rem &= rem - 1u;
+                        if ((hitw[w][k >> 5] >> (k & 31u)) & 1u) {
+                            F = add(F, mk(tm[0][k], tm[1][k], tm[2][k]));
+                            T = add(T, mk(tm[3][k], tm[4][k], tm[5][k]));
+                            p += tm[6][k];
+                            ev_dot += tm[7][k];
+                            if ((slipw[w][k >> 5] >> (k & 31u)) & 1u) es_dot += tm[8][k];
+                        } else {
+                            occ &= ~(1u << i);
+                        }
                     }
+                    sm[0][lane] = F.x;
+                    sm[1][lane] = F.y;
+                    sm[2][lane] = F.z;
+                    sm[3][lane] = T.x;
+                    sm[4][lane] = T.y;
+                    sm[5][lane] = T.z;
+                    sm[6][lane] = p;
+                    sm[7][lane] = ev_dot;
+                    sm[8][lane] = es_dot;
                 }
                 __syncwarp();
             }
             if (n) {
-                d.csum_f[s] = make_double4(F.x, F.y, F.z, p);
-                d.csum_t[s] = make_double4(T.x, T.y, T.z, ev_dot);
-                d.csum_es[s] = es_dot;
+                d.csum_f[s] = make_double4(sm[0][lane], sm[1][lane], sm[2][lane], sm[6][lane]);
+                d.csum_t[s] = make_double4(sm[3][lane], sm[4][lane], sm[5][lane], sm[7][lane]);
+                d.csum_es[s] = sm[8][lane];
                 if (occ != occ0) d.cmask[s] = occ;
             }
             // no slot left in the chunk: skip it until a search fills one
