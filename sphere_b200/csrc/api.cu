@@ -16,7 +16,8 @@ void launch_step(const Dev &d, const Params &hp, uint32_t np, int model, int a, 
                  cudaStream_t st);
 void launch_topo(const Dev &d, uint32_t np, bool visc, int a, cudaStream_t st);
 void launch_force(const Dev &d, uint32_t np, int model, int a, int write_outputs, cudaStream_t st);
-void launch_contact(const Dev &d, const Params &hp, uint32_t np, int model, int a, cudaStream_t st);
+void launch_contact(const Dev &d, const Params &hp, uint32_t np, int model, int a, int write_outputs,
+                    cudaStream_t st);
 void launch_bonds(const Dev &d, uint32_t nb0, int a, cudaStream_t st);
 void launch_walls(const Dev &d, uint32_t np, uint32_t nw, cudaStream_t st);
 void launch_cell_init(const Dev &d, uint32_t np, int a, cudaStream_t st);
@@ -445,7 +446,7 @@ int profiled_step(sph_ctx *c, int a, int write_outputs, cudaStream_t st)
     CK(cudaEventRecord(c->ev[2], st));
     launch_topo(c->d, c->np_all, c->hp.contactmodel == 1, a, st);
     CK(cudaEventRecord(c->ev[3], st));
-    launch_contact(c->d, c->hp, c->np_all, (int)c->hp.contactmodel, a, st);
+    launch_contact(c->d, c->hp, c->np_all, (int)c->hp.contactmodel, a, write_outputs, st);
     CK(cudaEventRecord(c->ev[4], st));
     launch_force(c->d, c->np_all, (int)c->hp.contactmodel, a, write_outputs, st);
     CK(cudaEventRecord(c->ev[5], st));

@@ -796,109 +796,20 @@ struct ForceArgs {
 // per-particle friction, implicit walls only, no bonds), recording the tape
 // row args.tape_step when it is >= 0.  Energy rates and pressure are not
 // computed in this variant.
-template <int MODEL, bool BATCH, bool DIFF>
-__global__ void __launch_bounds__(FORCE_BLOCK, SPHK_FORCE_MIN_BLOCKS)
-k_force(ForceArgs args)
+// Everything per particle after the slot sums (F, T, p, ev_dot, es_dot):
+// the walls, the bonds, the energy sums, the half-step leapfrog, the
+// displacement bound and the cell of the new position.  xa, vel_a and
+// angvel_a4 are the particle's start-of-step rows of buffer A; the new state
+// goes to buffer 1 - A.
+template <bool BATCH, bool DIFF>
+__device__ __forceinline__ void particle_tail(const Dev &d, const Params &P, uint32_t s, int A,
+                                              int write_outputs, double4 xa, double4 vel_a,
+                                              double4 angvel_a4, d3 F, d3 T, double p,
+                                              double ev_dot, double es_dot)
 {
-    const Dev &d = args.d;
-    const uint32_t np = d.np_all;
-    const uint32_t s = blockIdx.x * FORCE_BLOCK + threadIdx.x;
-    if (s >= np) return;
-#ifndef SPHK_NO_PREFETCH
-    // The state the integration reads comes after the contact work and
-    // after stores the compiler may not move loads across, so each of its
-    // loads would wait out a full DRAM latency in turn.  Lane 0 of every
-    // warp whose 32 rows all exist asks for the warp's rows of it up front.
-    if ((threadIdx.x & 31u) == 0 && s + 32 <= np) {
-        bulk_prefetch_l2(d.angpos + s, 32 * sizeof(P3));
-        bulk_prefetch_l2(d.angvel0 + s, 32 * sizeof(P3));
-        bulk_prefetch_l2(d.vel0 + s, 32 * sizeof(P3));
-        bulk_prefetch_l2(d.xysum + s, 32 * sizeof(double2));
-        bulk_prefetch_l2(d.pos + s, 32 * sizeof(uint32_t));
-        bulk_prefetch_l2(d.disp + s, 32 * sizeof(float));
-        bulk_prefetch_l2(d.cell + s, 32 * sizeof(uint32_t));
-        bulk_prefetch_l2(d.fixed + s, 32);
-        if (d.wtouch) bulk_prefetch_l2(d.wtouch + s, 32);
-    }
-#endif
-    const Params &P = prm_at<BATCH>(d, s);
-    const int A = args.a, B = 1 - args.a;
-    uint32_t err = 0;
-    const double4 xa = d.xr[A][s];
+    const int B = 1 - A;
     const double ra = xa.w;
-    const double4 vel_a = ld4(d.vel[A], s);
-    const double4 angvel_a4 = ld4(d.angvel[A], s);
-    d3 F = mk(0.0, 0.0, 0.0), T = mk(0.0, 0.0, 0.0);
-    double es_dot = 0.0f, ev_dot = 0.0f, p = 0.0f;
-
-    // ---- interact: occupied slots in slot order ----------------------------
-    uint32_t occ = d.cmask[s];
-    if constexpr (DIFF) {
-        const int j = args.tape_step;
-        const size_t row = (j >= 0) ? ((size_t)j * np + s) : 0;
-        uint32_t lawmask = 0;
-        const ulonglong2 dmw = d.dmc[s];
-        const uint32_t occ0 = occ;
-        for (uint32_t m = occ0; m; m &= m - 1) {
-            const int i = __ffs(m) - 1;
-            const size_t at = tile_at(s, (uint32_t)i, NC);
-            const uint32_t t = d.contacts[at];
-            const d3 dm = decode_dm(dm_get(dmw.x, dmw.y, i), P);
-            const double4 xb = d.xr[A][t];
-            dl::PairIn in;
-            in.xab = dl::v3(xa.x - xb.x + dm.x, xa.y - xb.y + dm.y, xa.z - xb.z + dm.z);
-            in.ra = ra;
-            in.rb = xb.w;
-            if (dl::len(in.xab) - (ra + xb.w) < 0.0) {
-                const P3 d0p = d.delta_t[at];
-                const double4 vb = ld4(d.vel[A], t), wb = ld4(d.angvel[A], t);
-                const double4 d0 = make_double4(d0p.x, d0p.y, d0p.z, 0.0);
-                in.va = dl::v3(vel_a.x, vel_a.y, vel_a.z);
-                in.vb = dl::v3(vb.x, vb.y, vb.z);
-                in.wa = dl::v3(angvel_a4.x, angvel_a4.y, angvel_a4.z);
-                in.wb = dl::v3(wb.x, wb.y, wb.z);
-                in.d0u = dl::v3(d0.x, d0.y, d0.z);
-                const dl::Law law{P.k_n, P.k_t, P.gamma_n, P.gamma_t,
-                                  0.5 * (d.mu_p[s] + d.mu_p[t]), P.kappa, P.dt};
-                dl::PairOut o;
-                dl::pair_fwd(law, in, o);
-                F = add(F, mk(o.F.x, o.F.y, o.F.z));
-                T = add(T, mk(o.T.x, o.T.y, o.T.z));
-                d.delta_t[at] = P3{o.dtn.x, o.dtn.y, o.dtn.z};
-                lawmask |= 1u << i;
-                if (j >= 0) {
-                    d.tp_partner[row * NC + i] = t;
-                    d.tp_dt0[row * NC + i] = d0;
-                }
-            } else {
-                occ &= ~(1u << i);
-                d.contacts[at] = np;
-                d.delta_t[at] = P3{0.0, 0.0, 0.0};
-            }
-        }
-        if (occ != occ0) d.cmask[s] = occ;
-        if (j >= 0) {
-            d.tp_x[row] = xa;
-            d.tp_v[row] = make_double4(vel_a.x, vel_a.y, vel_a.z, d.fixed[s] ? 1.0 : 0.0);
-            d.tp_w[row] = angvel_a4;
-            d.tp_mask[row] = lawmask;
-            d.tp_dmc[row] = dmw;
-        }
-    } else if (MODEL == 1) {
-        const double4 c = d.c1acc[s];
-        F = mk(c.x, c.y, c.z);
-        p = c.w;
-    } else if (occ) {
-        // the slot sums k_contact left for a particle that still holds a
-        // contact (with every slot freed nothing was added: the sums are zero)
-        const double4 cf = d.csum_f[s], ct = d.csum_t[s];
-        F = mk(cf.x, cf.y, cf.z);
-        p = cf.w;
-        T = mk(ct.x, ct.y, ct.z);
-        ev_dot = ct.w;
-        es_dot = d.csum_es[s];
-    }
-
+    uint32_t err = 0;
     // ---- walls, src/contactsearch.cuh:578-663 (defaults :416-427) ----------
     double w0f = 0.0;
     if constexpr (DIFF) {
@@ -994,7 +905,7 @@ k_force(ForceArgs args)
         d.angvel[B][s] = angvel;
         d.angvel0[s] = angvel0;
         d.angpos[s] = angpos;
-        if (args.write_outputs) {
+        if (write_outputs) {
             d.torque[s] = make_double4(T.x, T.y, T.z, 0.0f);
             d.angacc[s] = angacc;
         }
@@ -1045,7 +956,7 @@ k_force(ForceArgs args)
     // float copy for the next step's contact search, at this particle's
     // cell-list position (rewritten by the rebuild when the order changes)
     d.xs[B][d.pos[s]] = make_float4((float)x.x, (float)x.y, (float)x.z, (float)x.w);
-    if (args.write_outputs) {
+    if (write_outputs) {
         d.force[s] = make_double4(F.x, F.y, F.z, 0.0f);
         d.acc[s] = acc;
         d.edp[s] = make_double4(es_dot, ev_dot, p, 0.0);
@@ -1082,30 +993,131 @@ k_force(ForceArgs args)
     if (err) atomicOr(d.status, err);
 }
 
-
-// Position of the k-th set bit (k = 0 for the lowest) of m; k < popc(m).
-__device__ __forceinline__ uint32_t nth_set_bit(uint32_t m, uint32_t k)
+template <int MODEL, bool BATCH, bool DIFF>
+__global__ void __launch_bounds__(FORCE_BLOCK, SPHK_FORCE_MIN_BLOCKS)
+k_force(ForceArgs args)
 {
-    uint32_t pos = 0;
-#pragma unroll
-    for (uint32_t w = 16; w; w >>= 1) {
-        const uint32_t lo = m & ((1u << w) - 1u);
-        const uint32_t c = __popc(lo);
-        if (k >= c) {
-            k -= c;
-            m >>= w;
-            pos += w;
-        } else {
-            m = lo;
+    const Dev &d = args.d;
+    const uint32_t np = d.np_all;
+    const uint32_t s = blockIdx.x * FORCE_BLOCK + threadIdx.x;
+    if (s >= np) return;
+    // A chunk k_contact visited (flag 2: a contact remains, 3: none does)
+    // has the slot sums of its particles in Dev::csum_*; its flag goes back
+    // to 1 or 0 for the next step's search.  A warp is one chunk, so the
+    // flag is the warp's.
+    bool visited = false;
+    if constexpr (MODEL != 1 && !DIFF) {
+        const uint8_t f = d.cflag[s >> 5];
+        visited = f >= 2;
+        if (visited) {
+            __syncwarp(__activemask());
+            if ((s & 31u) == 0) d.cflag[s >> 5] = (f == 2) ? 1 : 0;
         }
     }
-    return pos;
+#ifndef SPHK_NO_PREFETCH
+    // The state the integration reads comes after the contact work and
+    // after stores the compiler may not move loads across, so each of its
+    // loads would wait out a full DRAM latency in turn.  Lane 0 of every
+    // warp whose 32 rows all exist asks for the warp's rows of it up front.
+    if ((threadIdx.x & 31u) == 0 && s + 32 <= np) {
+        bulk_prefetch_l2(d.angpos + s, 32 * sizeof(P3));
+        bulk_prefetch_l2(d.angvel0 + s, 32 * sizeof(P3));
+        bulk_prefetch_l2(d.vel0 + s, 32 * sizeof(P3));
+        bulk_prefetch_l2(d.xysum + s, 32 * sizeof(double2));
+        bulk_prefetch_l2(d.pos + s, 32 * sizeof(uint32_t));
+        bulk_prefetch_l2(d.disp + s, 32 * sizeof(float));
+        bulk_prefetch_l2(d.cell + s, 32 * sizeof(uint32_t));
+        bulk_prefetch_l2(d.fixed + s, 32);
+        if (d.wtouch) bulk_prefetch_l2(d.wtouch + s, 32);
+    }
+#endif
+    const Params &P = prm_at<BATCH>(d, s);
+    const int A = args.a;
+    const double4 xa = d.xr[A][s];
+    const double ra = xa.w;
+    const double4 vel_a = ld4(d.vel[A], s);
+    const double4 angvel_a4 = ld4(d.angvel[A], s);
+    d3 F = mk(0.0, 0.0, 0.0), T = mk(0.0, 0.0, 0.0);
+    double es_dot = 0.0f, ev_dot = 0.0f, p = 0.0f;
+
+    // ---- interact: occupied slots in slot order (the differentiable step;
+    // models 2 and 3 run k_contact, model 1 sums in k_topo) -----------------
+    if constexpr (DIFF) {
+        uint32_t occ = d.cmask[s];
+        const int j = args.tape_step;
+        const size_t row = (j >= 0) ? ((size_t)j * np + s) : 0;
+        uint32_t lawmask = 0;
+        const ulonglong2 dmw = d.dmc[s];
+        const uint32_t occ0 = occ;
+        for (uint32_t m = occ0; m; m &= m - 1) {
+            const int i = __ffs(m) - 1;
+            const size_t at = tile_at(s, (uint32_t)i, NC);
+            const uint32_t t = d.contacts[at];
+            const d3 dm = decode_dm(dm_get(dmw.x, dmw.y, i), P);
+            const double4 xb = d.xr[A][t];
+            dl::PairIn in;
+            in.xab = dl::v3(xa.x - xb.x + dm.x, xa.y - xb.y + dm.y, xa.z - xb.z + dm.z);
+            in.ra = ra;
+            in.rb = xb.w;
+            if (dl::len(in.xab) - (ra + xb.w) < 0.0) {
+                const P3 d0p = d.delta_t[at];
+                const double4 vb = ld4(d.vel[A], t), wb = ld4(d.angvel[A], t);
+                const double4 d0 = make_double4(d0p.x, d0p.y, d0p.z, 0.0);
+                in.va = dl::v3(vel_a.x, vel_a.y, vel_a.z);
+                in.vb = dl::v3(vb.x, vb.y, vb.z);
+                in.wa = dl::v3(angvel_a4.x, angvel_a4.y, angvel_a4.z);
+                in.wb = dl::v3(wb.x, wb.y, wb.z);
+                in.d0u = dl::v3(d0.x, d0.y, d0.z);
+                const dl::Law law{P.k_n, P.k_t, P.gamma_n, P.gamma_t,
+                                  0.5 * (d.mu_p[s] + d.mu_p[t]), P.kappa, P.dt};
+                dl::PairOut o;
+                dl::pair_fwd(law, in, o);
+                F = add(F, mk(o.F.x, o.F.y, o.F.z));
+                T = add(T, mk(o.T.x, o.T.y, o.T.z));
+                d.delta_t[at] = P3{o.dtn.x, o.dtn.y, o.dtn.z};
+                lawmask |= 1u << i;
+                if (j >= 0) {
+                    d.tp_partner[row * NC + i] = t;
+                    d.tp_dt0[row * NC + i] = d0;
+                }
+            } else {
+                occ &= ~(1u << i);
+                d.contacts[at] = np;
+                d.delta_t[at] = P3{0.0, 0.0, 0.0};
+            }
+        }
+        if (occ != occ0) d.cmask[s] = occ;
+        if (j >= 0) {
+            d.tp_x[row] = xa;
+            d.tp_v[row] = make_double4(vel_a.x, vel_a.y, vel_a.z, d.fixed[s] ? 1.0 : 0.0);
+            d.tp_w[row] = angvel_a4;
+            d.tp_mask[row] = lawmask;
+            d.tp_dmc[row] = dmw;
+        }
+    } else if (MODEL == 1) {
+        const double4 c = d.c1acc[s];
+        F = mk(c.x, c.y, c.z);
+        p = c.w;
+    } else if (visited && d.cmask[s] != 0u) {
+        // the sums of a particle that still holds a slot (with every slot
+        // freed nothing was added: the sums are zero)
+        const double4 cf = d.csum_f[s], ct = d.csum_t[s];
+        F = mk(cf.x, cf.y, cf.z);
+        p = cf.w;
+        T = mk(ct.x, ct.y, ct.z);
+        ev_dot = ct.w;
+        es_dot = d.csum_es[s];
+    }
+    particle_tail<BATCH, DIFF>(d, P, s, A, args.write_outputs, xa, vel_a, angvel_a4, F, T, p,
+                               ev_dot, es_dot);
 }
+
 
 struct ContactArgs {
     Dev d;
-    int a;          // read buffer (start of step)
-    LawParams lp;   // single-scene contexts; a batch reads each scene's Params
+    int a;               // read buffer (start of step)
+    int write_outputs;   // store force/torque/acc/angacc/edp of this step
+    LawParams lp;        // single-scene contexts; a batch reads each scene's Params
 };
 
 // Contacts of one chunk whose law terms a warp holds at once (a multiple of 32).
@@ -1338,8 +1350,11 @@ k_contact(ContactArgs args)
                 d.csum_es[s] = sm[8][lane];
                 if (occ != occ0) d.cmask[s] = occ;
             }
-            // no slot left in the chunk: skip it until a search fills one
-            if (!__any_sync(FULL, occ != 0u) && lane == 0) d.cflag[chunk] = 0;
+            // visited (2: a slot is still held, 3: none is); k_force reads
+            // the sums of a visited chunk and sets its flag back to 1 or 0
+            // for the next step's search
+            const bool held = __any_sync(FULL, occ != 0u);
+            if (lane == 0) d.cflag[chunk] = held ? 2 : 3;
         }
     }
 }
@@ -1400,11 +1415,12 @@ void launch_force_tape(const Dev &d, uint32_t np, int a, int tape_step, cudaStre
 // sums its forces) and the differentiable step evaluates its own law in
 // k_force, recording the tape.
 void launch_contact(const Dev &d, const Params &hp, uint32_t np, int model, int a,
-                    cudaStream_t st)
+                    int write_outputs, cudaStream_t st)
 {
     if (model == 1 || d.mu_p) return;
-    ContactArgs args{d, a, LawParams{hp.k_n, hp.k_t, hp.gamma_n, hp.gamma_t, hp.gamma_r, hp.mu_s,
-                                     hp.mu_d, hp.mu_r, hp.kappa, hp.dt, {hp.L[0], hp.L[1]}}};
+    ContactArgs args{d, a, write_outputs,
+                     LawParams{hp.k_n, hp.k_t, hp.gamma_n, hp.gamma_t, hp.gamma_r, hp.mu_s, hp.mu_d,
+                               hp.mu_r, hp.kappa, hp.dt, {hp.L[0], hp.L[1]}}};
     if (d.inst)   // batched contexts: contact model 2 only
         k_contact<2, true><<<contact_grid<2, true>(np), CONTACT_BLOCK, 0, st>>>(args);
     else if (model == 3)
@@ -1417,7 +1433,7 @@ void launch_step(const Dev &d, const Params &hp, uint32_t np, int model, int a,
                  int write_outputs, cudaStream_t st)
 {
     launch_topo(d, np, model == 1, a, st);
-    launch_contact(d, hp, np, model, a, st);
+    launch_contact(d, hp, np, model, a, write_outputs, st);
     launch_force(d, np, model, a, write_outputs, st);
 }
 
