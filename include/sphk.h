@@ -278,14 +278,21 @@ int sph_diff_end(sph_ctx *ctx);
  * output is a device pointer supplied by the caller; the work is enqueued on
  * `stream` (a cudaStream_t; NULL is the default stream).  Only cfg->np,
  * num, origo, L and device are read.
+ * A position outside the grid or not finite goes to one bucket after the
+ * last cell (0xffffffff in cell_sorted), members of every bucket in particle
+ * order; the work is linear in np however the particles spread over cells.
  * Limits: np <= SPHK_NOALLOC_MAX_PARTICLES and num[0]*num[1]*num[2] <=
  * SPHK_NOALLOC_MAX_CELLS, otherwise SPH_ERR_TOO_LARGE and nothing is
  * launched.  It calls no cudaMalloc, cudaFree or allocating library routine:
- * its scratch is one fixed array of about 8 MB inside the library, held by
- * every GPU that loads the library until the process exits.  The first call
- * on a device looks up that array's device address (cudaGetSymbolAddress);
- * make that first call before any stream capture.  All calls share the
- * array, so calls that overlap on the GPU race and give wrong results. */
+ * its scratch is one fixed array of about 9 MB inside the library, held by
+ * every GPU that loads the library until the process exits, and the
+ * caller's cell_sorted and perm serve as scratch until the call's last
+ * kernel writes them.  The first call on a device looks up that array's
+ * device address (cudaGetSymbolAddress); make that first call before any
+ * stream capture.  All calls share the array, so calls that overlap on the
+ * GPU race and give wrong results.  The caller's current device is the same
+ * after the call; a launch error pending from the caller's own earlier work
+ * is reported as SPH_ERR_CUDA (and left pending). */
 #define SPHK_NOALLOC_MAX_PARTICLES 1048576u
 #define SPHK_NOALLOC_MAX_CELLS 524288u
 int sph_cell_list_noalloc(const sph_config *cfg, const double *x_dev, uint32_t *cell_sorted,

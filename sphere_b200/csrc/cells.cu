@@ -33,8 +33,8 @@ __global__ void k_cell_init(Dev d, int A)
     const Params &P = prm_of(d, s);
     const double4 x = d.xr[A][s];
     d.outside[s] = cell_outside(P, x.x, x.y, x.z) ? 1 : 0;
-    uint32_t c = cell_id(P, x.x, x.y, x.z);
-    if (c >= P.ncells || !isfinite(x.x + x.y + x.z)) {
+    uint32_t c;
+    if (!grid_cell(P, x.x, x.y, x.z, c)) {
         atomicOr(d.status, ST_OUT_OF_GRID);
         c = d.ncells_all;
     } else {

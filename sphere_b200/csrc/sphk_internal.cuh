@@ -241,19 +241,34 @@ __device__ __forceinline__ d3 decode_dm(uint32_t code, const PR &P)
     return mk(dx, dy, dz);
 }
 
-// (x - origo) / (L / num), floored (src/sorting.cuh:12-14)
-__device__ __forceinline__ double cell_floor(const Params &P, int d, double v)
+// (x - origo) / (L / num), floored (src/sorting.cuh:12-14).  G is any grid
+// with origo[3], cellsize[3], num[3] and ncells (Params among them).
+template <class G>
+__device__ __forceinline__ double cell_floor(const G &P, int d, double v)
 {
     return floor((v - P.origo[d]) / P.cellsize[d]);
 }
 
 // calcCellID with the device's saturating float->unsigned conversion
-__device__ __forceinline__ uint32_t cell_id(const Params &P, double x, double y, double z)
+template <class G>
+__device__ __forceinline__ uint32_t cell_id(const G &P, double x, double y, double z)
 {
     uint32_t ix = __double2uint_rz(cell_floor(P, 0, x));
     uint32_t iy = __double2uint_rz(cell_floor(P, 1, y));
     uint32_t iz = __double2uint_rz(cell_floor(P, 2, z));
     return (iz * P.num[1]) * P.num[0] + iy * P.num[0] + ix;
+}
+
+// The cell of a position for the cell list: calcCellID's id in c, and
+// whether it lies in the grid.  A position that is not finite is outside
+// whatever its float-to-integer conversion gives; every cell list here puts
+// such a particle, like one whose id is past the grid, in one bucket after
+// the last cell.
+template <class G>
+__device__ __forceinline__ bool grid_cell(const G &P, double x, double y, double z, uint32_t &c)
+{
+    c = cell_id(P, x, y, z);
+    return c < P.ncells && isfinite(x + y + z);
 }
 
 // Whether some floored cell coordinate of the position lies outside

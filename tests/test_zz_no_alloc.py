@@ -13,7 +13,7 @@ import numpy as np
 import pytest
 
 from sphere_b200 import scenes, sphk
-from sphere_b200.sphk import Simulation
+from sphere_b200.sphk import SphError, Simulation
 from sphere_b200.state import config_from_spherebin, state_from_spherebin
 
 pytestmark = pytest.mark.gpu
@@ -30,22 +30,53 @@ def _noalloc(lib, cfg, x_dev, np_, ncells, torch):
     return [o.cpu().numpy().view(np.uint32) for o in outs]
 
 
+def _outside_and_nan():
+    # particles past every face of the grid, a crowd in one far bucket, and
+    # positions that are not finite: they all share the out-of-grid bucket,
+    # members in particle order
+    sb = scenes.collision(n=2000, seed=74, periodic=0)
+    rng = np.random.default_rng(75)
+    sel = rng.choice(sb.np, 400, replace=False)
+    for j, i in enumerate(sel):
+        ax = j % 3
+        sb.x[i, ax] = (sb.L[ax] + 0.01 * (1 + j)) if (j // 3) % 2 == 0 else -0.01 * (1 + j)
+    sb.x[sel[:7], 2] = np.nan
+    sb.x[sel[7], 0] = np.inf
+    return sb
+
+
+def _one_dense_cell():
+    # a coarse grid: most particles in a handful of cells
+    sb = scenes.collision(n=3000, seed=76, periodic=0)
+    sb.num = np.array([2, 1, 2], dtype=sb.num.dtype)
+    return sb
+
+
 @pytest.mark.parametrize("builder", [
     lambda: scenes.collision(n=3000, seed=71, periodic=1),
     lambda: scenes.collision(n=2500, seed=72, periodic=0, nw=1),
-])
+    _outside_and_nan,
+    _one_dense_cell,
+], ids=["periodic", "box_wall", "outside_and_nan", "dense_cells"])
 def test_noalloc_cell_list_matches_context_path(builder):
     torch = pytest.importorskip("torch")
     sb = builder()
     cfg = config_from_spherebin(sb)
     st = state_from_spherebin(sb)
     with Simulation(cfg) as sim:
-        sim.upload(st)
+        try:
+            sim.upload(st)
+        except SphError as e:
+            # the context reports positions outside the grid, and still
+            # holds their cell list
+            assert sphk.ERRORS[e.code] == "SPH_ERR_OUT_OF_GRID"
         want = sim.cells()
     lib = sphk.load_library()
     x_dev = torch.tensor(st.x, dtype=torch.float64, device="cuda").contiguous()
+    dev_before = torch.cuda.current_device()
     first = _noalloc(lib, cfg, x_dev, cfg.np, cfg.ncells, torch)
     second = _noalloc(lib, cfg, x_dev, cfg.np, cfg.ncells, torch)
+    assert torch.cuda.current_device() == dev_before
     for got in (first, second):
         for g, w, name in zip(got, want, ("cell_sorted", "perm", "cell_start", "cell_end")):
             assert np.array_equal(g, w), name
