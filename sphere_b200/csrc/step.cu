@@ -559,11 +559,13 @@ k_topo(Dev d, int A)
     // batch goes on, since its other scenes are still sound.  Tested only
     // here, past the list decision, so that the particles the decision
     // settles do not wait for the status word.
-    if (!BATCH && (*(volatile const uint32_t *)d.status & ST_OUT_OF_GRID)) return;
+    // The slot mask and the position are loaded with the status word, so
+    // the three wait out one memory latency together.
+    const uint32_t occ_in = d.cmask[s];
     const double4 xa = d.xr[A][s];
+    if (!BATCH && (*(volatile const uint32_t *)d.status & ST_OUT_OF_GRID)) return;
     const double ra = xa.w;
     const double4 *__restrict__ xr = d.xr[A];
-    const uint32_t occ_in = d.cmask[s];
     TopoSlots ts{occ_in, occ_in, 0u, 0ull, 0ull, 0, false, false};
     const uint32_t nx = P.num[0], ny = P.num[1], nz = P.num[2];
     int32_t gp[3];
@@ -591,16 +593,20 @@ k_topo(Dev d, int A)
         // while the occupied slots plus the list length stay within NC, no
         // row can fill, so the filter changes nothing.
         const bool filter = ts.occ != 0u && len + (uint32_t)__popc(ts.occ) <= (uint32_t)NC;
-        if (filter) topo_load_row(d, srow, tid, s, ts);
-        int skip_slot = -1;
-        for (uint32_t e0 = 0; e0 < len; e0 += 4) {
-            uint32_t tv[4], mv[4];
+        uint32_t tv[4], mv[4];
+        auto load4 = [&](uint32_t e0) {
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
                 const size_t at = vl_at(s, min(e0 + (uint32_t)j, (uint32_t)len - 1u));
                 tv[j] = d.vl[at];
                 mv[j] = d.vl_meta[at];
             }
+        };
+        load4(0);   // the first four entries are in flight with the slot row
+        if (filter) topo_load_row(d, srow, tid, s, ts);
+        int skip_slot = -1;
+        for (uint32_t e0 = 0; e0 < len; e0 += 4) {
+            if (e0) load4(e0);
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
                 if (e0 + (uint32_t)j >= len) break;
@@ -976,8 +982,8 @@ __device__ __forceinline__ void particle_tail(const Dev &d, const Params &P, uin
     // ---- cell of the new position, for the next step's cell list -----------
     // a position that is not finite (NaN forces, contact model 3) is
     // outside the grid whatever its float-to-integer conversion gives
-    uint32_t c = cell_id(P, x.x, x.y, x.z);
-    if (c >= P.ncells || !isfinite(x.x + x.y + x.z)) { err |= ST_OUT_OF_GRID; c = d.ncells_all; }
+    uint32_t c;
+    if (!grid_cell(P, x.x, x.y, x.z, c)) { err |= ST_OUT_OF_GRID; c = d.ncells_all; }
     else c += P.cell_base;
     d.outside[s] = cell_outside(P, x.x, x.y, x.z) ? 1 : 0;
     const uint32_t c_old = d.cell[s];
