@@ -112,6 +112,9 @@ typedef struct sph_stats {
 /* Options for sph_set_option. */
 #define SPH_OPT_RELAYOUT_EVERY 1  /* re-sort storage every n steps (0: at upload only) */
 #define SPH_OPT_GRAPH_STEPS 2     /* steps captured per CUDA graph (1..64, default 8) */
+#define SPH_OPT_BLOCK_SHAPES 5    /* 0 (default) or 1: the block shapes of the contact
+                                     search and the contact forces; results do not depend
+                                     on it, only their cost does */
 #define SPH_OPT_VERLET_SKIN 4     /* Verlet skin in thousandths of the largest radius
                                      (default 100; 0 sweeps the 27-cell stencil every
                                      step); set before sph_upload.  Results do not depend

@@ -8,6 +8,7 @@ check and bench.py's CPU-baseline leg import this module.
 from __future__ import annotations
 
 import ctypes as C
+import os
 import subprocess
 from pathlib import Path
 
@@ -16,6 +17,9 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 LIB_ORC = HERE / "liborc.so"
 LIB_REF = HERE / "_ref" / "libref.so"
+# the reference checkout's src/: SPHERE_REF_SRC, or a checkout named
+# `reference` beside this repository
+REF_SRC = Path(os.environ.get("SPHERE_REF_SRC", str(HERE.parent.parent / "reference" / "src")))
 
 ERR_NC_OVERFLOW = 1
 ERR_OUT_OF_GRID = 2
@@ -60,7 +64,7 @@ def build(ref: bool = True) -> None:
     reference checkout; it is skipped when that is absent)."""
     subprocess.run(["make", "-s", "-C", str(HERE), "orc"], check=True)
     if ref:
-        subprocess.run(["make", "-s", "-C", str(HERE), "ref"], check=False)
+        subprocess.run(["make", "-s", "-C", str(HERE), "ref", f"REF_SRC={REF_SRC}"], check=False)
 
 
 def load(kind: str = "orc"):

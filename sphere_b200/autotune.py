@@ -1,12 +1,15 @@
 """Autotuner for the batched ensemble: picks the cell size, the neighbour-sweep
-schedule (Verlet skin) and the graph batching by timing short runs.
+schedule (the Verlet skin: 0 sweeps the 27-cell stencil every step, above 0
+tests each particle's candidate list), the graph batching and the block
+shapes of the contact kernels by timing short runs.
 
 Of the knobs, only the cell size changes the scenes themselves: it sets each
 scene's grid, which is part of the input (and decides the reference's
-contact visiting order).  The sweep schedule and graph batching never change
-results -- the parity tests hold them to the same bits -- so the tuner may
-pick any of them freely.  Block shapes are fixed at compile time from an
-offline sweep of register caps and are not tuned here.
+contact visiting order).  The sweep schedule, the graph batching and the
+block shapes never change results -- the parity tests hold them to the same
+bits -- so the tuner may pick any of them freely.  The block shapes are the
+two compiled pairs of the contact search and contact force kernels
+(SPH_OPT_BLOCK_SHAPES, SHAPE_NAMES).
 
 Each candidate is timed on the device with CUDA events on the context's
 stream: `warmup` untimed steps, then `steps` timed steps.
@@ -20,6 +23,9 @@ from dataclasses import dataclass, field
 CELL_FACTORS = (2.0, 2.5, 3.0)
 SKINS = (0.0, 0.05, 0.1, 0.2)
 GRAPH_STEPS = (8, 16)
+SHAPES = (0, 1)
+SHAPE_NAMES = ("contact search 64 x 20, contact forces 128 x 4 (threads x blocks per SM)",
+               "contact search 128 x 10, contact forces 64 x 8 (threads x blocks per SM)")
 
 
 @dataclass
@@ -28,16 +34,18 @@ class Choice:
     verlet_skin: float
     graph_steps: int
     ms_per_step: float
+    shapes: int = 0
     trials: list = field(default_factory=list)
 
 
-def _time_batch(scenes_list, verlet_skin, graph_steps, warmup, steps, device=0):
+def _time_batch(scenes_list, verlet_skin, graph_steps, warmup, steps, device=0, shapes=0):
     import torch
 
     from .sphk import BatchSimulation
     from .state import config_from_spherebin, state_from_spherebin
     with BatchSimulation([config_from_spherebin(sb) for sb in scenes_list], device=device,
-                         graph_steps=graph_steps, verlet_skin=verlet_skin) as sim:
+                         graph_steps=graph_steps, verlet_skin=verlet_skin,
+                         block_shapes=shapes) as sim:
         sim.upload([state_from_spherebin(sb) for sb in scenes_list])
         # a stream of its own: the default stream's handle is 0, which the
         # binding reads as "the context's stream", and events recorded on the
@@ -56,13 +64,15 @@ def _time_batch(scenes_list, verlet_skin, graph_steps, warmup, steps, device=0):
 
 
 def tune(build_scenes, warmup=20, steps=60, cell_factors=CELL_FACTORS, skins=SKINS,
-         graph_steps=GRAPH_STEPS, device=0, log=None) -> Choice:
-    """Time every combination and return the fastest.
+         graph_steps=GRAPH_STEPS, shapes=SHAPES, device=0, log=None) -> Choice:
+    """Time the candidates and return the fastest.
 
     ``build_scenes(cell_factor)`` returns the list of scenes (Spherebin) for
-    that cell size.  The sweep schedule and graph batching are tuned for the
-    cell size that is best with the default schedule, so the number of runs
-    is len(cell_factors) + len(skins) * len(graph_steps)."""
+    that cell size (a cell factor of None: the scenes' own grids).  The
+    sweep schedule and graph batching are tuned for the cell size that is
+    best with the default schedule, then the block shapes for the best of
+    those, so the number of runs is len(cell_factors) + len(skins) *
+    len(graph_steps) - 1 + len(shapes) - 1."""
     trials = []
     best_cf, best_ms = None, float("inf")
     for cf in cell_factors:
@@ -84,6 +94,16 @@ def tune(build_scenes, warmup=20, steps=60, cell_factors=CELL_FACTORS, skins=SKI
             log(f"autotune skin={skin} graph_steps={gs}: {ms:.4f} ms/step")
         if ms < best.ms_per_step:
             best = Choice(best_cf, skin, gs, ms)
+    for sh in shapes:
+        if sh == 0:
+            continue
+        ms = _time_batch(sc, best.verlet_skin, best.graph_steps, warmup, steps, device, sh)
+        trials.append(dict(cell_factor=best_cf, verlet_skin=best.verlet_skin,
+                           graph_steps=best.graph_steps, shapes=sh, ms_per_step=ms))
+        if log:
+            log(f"autotune shapes={sh}: {ms:.4f} ms/step")
+        if ms < best.ms_per_step:
+            best = Choice(best_cf, best.verlet_skin, best.graph_steps, ms, sh)
     best.trials = trials
     return best
 

@@ -140,7 +140,7 @@ int dalloc(sph_ctx *c, T **p, size_t count, std::vector<void *> *owner = nullptr
     void *q = nullptr;
     cudaError_t e = cudaMalloc(&q, bytes);
     if (e != cudaSuccess) return fail(c, SPH_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
-    e = cudaMemset(q, 0, bytes);
+    e = cudaMemsetAsync(q, 0, bytes, c->stream);
     if (e != cudaSuccess) return fail(c, SPH_ERR_CUDA, std::string("cudaMemset: ") + cudaGetErrorString(e));
     (owner ? owner : &c->allocs)->push_back(q);
     (owner ? c->diff_bytes : c->device_bytes) += bytes;
@@ -311,7 +311,7 @@ int sync_status(sph_ctx *c)
 {
     CK(cudaStreamSynchronize(c->stream));
     uint32_t st = 0;
-    CK(cudaMemcpy(&st, c->d.status, sizeof(st), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpyAsync(&st, c->d.status, sizeof(st), cudaMemcpyDeviceToHost, c->stream));
     const int code = status_to_code(st);
     if (code != SPH_OK) return fail(c, code, status_msg(code));
     return SPH_OK;
@@ -629,15 +629,16 @@ int create_impl(const sph_config *cfgs, uint32_t ninst, bool batched, sph_ctx **
     if (batched) {
         AL(d.inst, np);
         AL(d.inst_cell_base, (size_t)ninst + 1);
-        CK(cudaMemcpy(d.inst_cell_base, cell_bases.data(), ((size_t)ninst + 1) * 4,
-                      cudaMemcpyHostToDevice));
+        CK(cudaMemcpyAsync(d.inst_cell_base, cell_bases.data(), ((size_t)ninst + 1) * 4,
+                      cudaMemcpyHostToDevice, c->stream));
     }
     c->scratch_bytes = tiled_size(np, NC) * sizeof(P3) + np * sizeof(uint32_t) + 256;
     char *sc = nullptr;
     AL(sc, c->scratch_bytes);
     c->scratch = sc;
 #undef AL
-    CK(cudaMemcpy(d.prm, c->hps.data(), sizeof(Params) * ninst, cudaMemcpyHostToDevice));
+    CK(cudaMemcpyAsync(d.prm, c->hps.data(), sizeof(Params) * ninst, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
     // The step graphs depend only on what is fixed here (sizes, device
     // pointers, contact model, walls, bonds); every value an upload changes
     // is read from device memory.  Capturing them now puts their cost in
@@ -683,6 +684,17 @@ int sph_set_option(sph_ctx *c, int option, int64_t value)
         c->graph_steps = (int)value;
         return SPH_OK;
     }
+    if (option == SPH_OPT_BLOCK_SHAPES && (value == 0 || value == 1)) {
+        // kernels and graphs take Dev by value: capture again with the shape
+        if (c->d.shape != (uint32_t)value) {
+            CK(cudaSetDevice(c->device));
+            CK(cudaStreamSynchronize(c->stream));
+            c->d.shape = (uint32_t)value;
+            drop_graphs(c);
+            if (!c->batched) return ensure_graphs(c);
+        }
+        return SPH_OK;
+    }
     return fail(c, SPH_ERR_BAD_INPUT, "unknown option or value");
 }
 
@@ -719,9 +731,9 @@ int sph_upload(sph_ctx *c, const sph_host_state *h)
         for (uint32_t i = 0; i < c->ninst; ++i)
             for (uint32_t u = 0; u < c->hps[i].np; ++u) inst_of[c->hps[i].uid_base + u] = i;
     }
-    if (c->batched) CK(cudaMemcpy(d.inst, inst_of.data(), np * 4, cudaMemcpyHostToDevice));
+    if (c->batched) CK(cudaMemcpyAsync(d.inst, inst_of.data(), np * 4, cudaMemcpyHostToDevice, c->stream));
     // kinematics (identity storage order for now)
-    CK(cudaMemcpy(d.xr[A], h->x, np * 32, cudaMemcpyHostToDevice));
+    CK(cudaMemcpyAsync(d.xr[A], h->x, np * 32, cudaMemcpyHostToDevice, c->stream));
     {
         // largest radius of each scene, for the cell-level distance test of
         // contact search; one Verlet skin for the whole context, from the
@@ -743,13 +755,14 @@ int sph_upload(sph_ctx *c, const sph_host_state *h)
                       (h->ev[i] == 0.0 && std::signbit(h->ev[i]));
         for (auto &Q : c->hps) Q.esv_skip = negzero ? 0u : 1u;
         c->hp = c->hps[0];
-        CK(cudaMemcpy(d.prm, c->hps.data(), sizeof(Params) * c->ninst, cudaMemcpyHostToDevice));
+        CK(cudaMemcpyAsync(d.prm, c->hps.data(), sizeof(Params) * c->ninst, cudaMemcpyHostToDevice, c->stream));
         Verlet V{};
         V.step = 1;
         V.all_rebuild = 1;
-        CK(cudaMemcpy(d.vs, &V, sizeof(V), cudaMemcpyHostToDevice));
-        CK(cudaMemset(d.dirty, 0, ((size_t)c->ncells_all + 1) * sizeof(uint32_t)));
-        CK(cudaMemset(d.vl_len, VL_NONE, np));
+        CK(cudaMemcpyAsync(d.vs, &V, sizeof(V), cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemsetAsync(d.dirty, 0, ((size_t)c->ncells_all + 1) * sizeof(uint32_t), c->stream));
+        CK(cudaMemsetAsync(d.vl_len, VL_NONE, np, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
     }
     {
         // vel, angvel, vel0, angvel0, angpos: three doubles on the device, the
@@ -804,10 +817,10 @@ int sph_upload(sph_ctx *c, const sph_host_state *h)
     // contact slots: partners, periodic-shift codes, occupancy, history
     if (!h->contacts) {
         // the reference's initial state: every slot empty, zero history
-        CK(cudaMemset(d.contacts, 0xff, tiled_size(np, NC) * 4));   // empty slots are read through cmask only
-        CK(cudaMemset(d.dmc, 0, np * 16));
-        CK(cudaMemset(d.cmask, 0, np * 4));
-        CK(cudaMemset(d.delta_t, 0, tiled_size(np, NC) * sizeof(P3)));
+        CK(cudaMemsetAsync(d.contacts, 0xff, tiled_size(np, NC) * 4, c->stream));   // empty slots are read through cmask only
+        CK(cudaMemsetAsync(d.dmc, 0, np * 16, c->stream));
+        CK(cudaMemsetAsync(d.cmask, 0, np * 4, c->stream));
+        CK(cudaMemsetAsync(d.delta_t, 0, tiled_size(np, NC) * sizeof(P3), c->stream));
     } else {
         // the caller's rows [np][NC] into tiles; the history's fourth lane is
         // not kept (the reference writes it as 0)
@@ -838,10 +851,11 @@ int sph_upload(sph_ctx *c, const sph_host_state *h)
                     for (int q = 0; q < 3; ++q) dts[at * 3 + q] = h->delta_t[(i * NC + k) * 4 + q];
             }
         }
-        CK(cudaMemcpy(d.contacts, rows.data(), rows.size() * 4, cudaMemcpyHostToDevice));
-        CK(cudaMemcpy(d.dmc, dmc.data(), np * 16, cudaMemcpyHostToDevice));
-        CK(cudaMemcpy(d.cmask, cmask.data(), np * 4, cudaMemcpyHostToDevice));
-        CK(cudaMemcpy(d.delta_t, dts.data(), dts.size() * 8, cudaMemcpyHostToDevice));
+        CK(cudaMemcpyAsync(d.contacts, rows.data(), rows.size() * 4, cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemcpyAsync(d.dmc, dmc.data(), np * 16, cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemcpyAsync(d.cmask, cmask.data(), np * 4, cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemcpyAsync(d.delta_t, dts.data(), dts.size() * 8, cudaMemcpyHostToDevice, c->stream));
+        CK(cudaStreamSynchronize(c->stream));   // the host rows above go out of scope
     }
     // walls
     {
@@ -853,11 +867,12 @@ int sph_upload(sph_ctx *c, const sph_host_state *h)
         }
         W.t_current = h->t_current;
         W.done_blocks = 0;
-        CK(cudaMemcpy(d.walls, &W, sizeof(W), cudaMemcpyHostToDevice));
+        CK(cudaMemcpyAsync(d.walls, &W, sizeof(W), cudaMemcpyHostToDevice, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
     }
-    CK(cudaMemset(d.wf_pp, 0, np * sizeof(double)));
-    CK(cudaMemset(d.wtouch, 0, np));
-    CK(cudaMemset(d.wf_flag, 0, div_up(np, 256)));
+    CK(cudaMemsetAsync(d.wf_pp, 0, np * sizeof(double), c->stream));
+    CK(cudaMemsetAsync(d.wtouch, 0, np, c->stream));
+    CK(cudaMemsetAsync(d.wf_flag, 0, div_up(np, 256), c->stream));
     // bonds and their per-particle lists (by user index, in bond order)
     if (nb0 > 0) {
         std::vector<uint32_t> ptr(np + 1, 0), list;
@@ -875,16 +890,17 @@ int sph_upload(sph_ctx *c, const sph_host_state *h)
             if (x < np) list[fill[x]++] = (uint32_t)(b << 1);
             list[fill[y]++] = (uint32_t)((b << 1) | 1u);
         }
-        CK(cudaMemcpy(d.bond_ptr, ptr.data(), (np + 1) * 4, cudaMemcpyHostToDevice));
+        CK(cudaMemcpyAsync(d.bond_ptr, ptr.data(), (np + 1) * 4, cudaMemcpyHostToDevice, c->stream));
         if (!list.empty())
-            CK(cudaMemcpy(d.bond_list, list.data(), list.size() * 4, cudaMemcpyHostToDevice));
-        CK(cudaMemcpy(d.bonds, h->bonds, nb0 * 8, cudaMemcpyHostToDevice));
-        CK(cudaMemcpy(d.bonds_delta, h->bonds_delta, nb0 * 32, cudaMemcpyHostToDevice));
-        CK(cudaMemcpy(d.bonds_omega, h->bonds_omega, nb0 * 32, cudaMemcpyHostToDevice));
+            CK(cudaMemcpyAsync(d.bond_list, list.data(), list.size() * 4, cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemcpyAsync(d.bonds, h->bonds, nb0 * 8, cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemcpyAsync(d.bonds_delta, h->bonds_delta, nb0 * 32, cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemcpyAsync(d.bonds_omega, h->bonds_omega, nb0 * 32, cudaMemcpyHostToDevice, c->stream));
+        CK(cudaStreamSynchronize(c->stream));   // the CSR built above goes out of scope
     }
-    CK(cudaMemset(d.status, 0, 4));
+    CK(cudaMemsetAsync(d.status, 0, 4, c->stream));
     const uint32_t one = 1;
-    CK(cudaMemcpy(d.rebuild, &one, 4, cudaMemcpyHostToDevice));
+    CK(cudaMemcpyAsync(d.rebuild, &one, 4, cudaMemcpyHostToDevice, c->stream));
     c->sticky = SPH_OK;
     c->err.clear();
     c->t_host = h->t_current;
@@ -1059,18 +1075,19 @@ int sph_download(sph_ctx *c, sph_host_state *h)
         if (rc != SPH_OK) return rc;
     }
     if (P.nb0 > 0) {
-        if (h->bonds) CK(cudaMemcpy(h->bonds, d.bonds, (size_t)P.nb0 * 8, cudaMemcpyDeviceToHost));
-        if (h->bonds_delta) CK(cudaMemcpy(h->bonds_delta, d.bonds_delta, (size_t)P.nb0 * 32, cudaMemcpyDeviceToHost));
-        if (h->bonds_omega) CK(cudaMemcpy(h->bonds_omega, d.bonds_omega, (size_t)P.nb0 * 32, cudaMemcpyDeviceToHost));
+        if (h->bonds) CK(cudaMemcpyAsync(h->bonds, d.bonds, (size_t)P.nb0 * 8, cudaMemcpyDeviceToHost, c->stream));
+        if (h->bonds_delta) CK(cudaMemcpyAsync(h->bonds_delta, d.bonds_delta, (size_t)P.nb0 * 32, cudaMemcpyDeviceToHost, c->stream));
+        if (h->bonds_omega) CK(cudaMemcpyAsync(h->bonds_omega, d.bonds_omega, (size_t)P.nb0 * 32, cudaMemcpyDeviceToHost, c->stream));
     }
     Walls W{};
-    CK(cudaMemcpy(&W, d.walls, sizeof(W), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpyAsync(&W, d.walls, sizeof(W), cudaMemcpyDeviceToHost, c->stream));
     for (uint32_t k = 0; k < P.nw; ++k) {
         if (h->walls_nx) memcpy(&h->walls_nx[4 * k], &W.nx[k], 32);
         if (h->walls_mvfd) memcpy(&h->walls_mvfd[4 * k], &W.mvfd[k], 32);
         if (h->walls_vel0) h->walls_vel0[k] = W.vel0[k];
     }
     h->t_current = c->t_host;
+    CK(cudaStreamSynchronize(c->stream));   // the caller's arrays are complete
     return SPH_OK;
 }
 
@@ -1124,7 +1141,8 @@ int sph_get_wall_forces(sph_ctx *c, double *wall0_force)
     if (!c || !c->uploaded || !wall0_force) return fail(c, SPH_ERR_BAD_INPUT, "bad arguments");
     CK(cudaSetDevice(c->device));
     CK(cudaDeviceSynchronize());
-    CK(cudaMemcpy(wall0_force, c->d.wf_pp, (size_t)c->np_all * 8, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpyAsync(wall0_force, c->d.wf_pp, (size_t)c->np_all * 8, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));   // the caller's arrays are complete
     return SPH_OK;
 }
 
@@ -1146,13 +1164,14 @@ int sph_get_stats(sph_ctx *c, sph_stats *out)
     }
     if (c->uploaded) {
         Verlet V{};
-        CK(cudaMemcpy(&V, c->d.vs, sizeof(V), cudaMemcpyDeviceToHost));
+        CK(cudaMemcpyAsync(&V, c->d.vs, sizeof(V), cudaMemcpyDeviceToHost, c->stream));
         out->cell_rebuilds = V.rebuilds;
     }
     out->steps = c->steps;
     out->relayouts = c->relayouts;
     out->device_bytes = c->device_bytes + c->diff_bytes +
                         (c->ckpts.size() + c->ckpt_pool.size()) * c->ckpt_bytes;
+    CK(cudaStreamSynchronize(c->stream));   // the caller's arrays are complete
     return SPH_OK;
 }
 
@@ -1241,11 +1260,12 @@ static int restore_ckpt(sph_ctx *c, const sph_ctx::Ckpt &k)
     CK(cudaMemsetAsync(d.cflag, 1, div_up(c->np_all, 32), c->stream));
     CK(cudaStreamSynchronize(c->stream));
     const uint32_t one = 1;
-    CK(cudaMemcpy(d.rebuild, &one, 4, cudaMemcpyHostToDevice));
+    CK(cudaMemcpyAsync(d.rebuild, &one, 4, cudaMemcpyHostToDevice, c->stream));
     Verlet V{};
     V.step = 1;
     V.all_rebuild = 1;
-    CK(cudaMemcpy(d.vs, &V, sizeof(V), cudaMemcpyHostToDevice));
+    CK(cudaMemcpyAsync(d.vs, &V, sizeof(V), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));   // one and V go out of scope
     return SPH_OK;
 }
 
@@ -1330,7 +1350,7 @@ int sph_diff_begin(sph_ctx *c, const double *mu, uint32_t checkpoint_every)
     double *tmp = nullptr;
     ALD(tmp, np);
 #undef ALD
-    if (mu) CK(cudaMemcpy(tmp, mu, np * 8, cudaMemcpyHostToDevice));
+    if (mu) CK(cudaMemcpyAsync(tmp, mu, np * 8, cudaMemcpyHostToDevice, c->stream));
     launch_user_to_storage1(mu ? tmp : nullptr, d.mu_p, d.uid, P.mu_s, (uint32_t)np, c->stream);
     CK(cudaStreamSynchronize(c->stream));
     // kernels and graphs take Dev by value: capture again with the new arrays
@@ -1343,6 +1363,7 @@ int sph_diff_begin(sph_ctx *c, const double *mu, uint32_t checkpoint_every)
     sph_ctx::Ckpt k{};
     if ((rc = save_ckpt(c, k)) != SPH_OK) return rc;
     c->ckpts.push_back(k);
+    CK(cudaStreamSynchronize(c->stream));   // the caller's arrays are complete
     return SPH_OK;
 }
 
@@ -1369,8 +1390,8 @@ int sph_diff_backward(sph_ctx *c, const double *x_bar, const double *v_bar, doub
     double *hx = c->bwd_scratch;
     double *out = c->bwd_scratch + 6 * (size_t)np;
     {
-        if (x_bar) CK(cudaMemcpy(hx, x_bar, (size_t)np * 24, cudaMemcpyHostToDevice));
-        if (v_bar) CK(cudaMemcpy(hx + 3 * (size_t)np, v_bar, (size_t)np * 24, cudaMemcpyHostToDevice));
+        if (x_bar) CK(cudaMemcpyAsync(hx, x_bar, (size_t)np * 24, cudaMemcpyHostToDevice, c->stream));
+        if (v_bar) CK(cudaMemcpyAsync(hx + 3 * (size_t)np, v_bar, (size_t)np * 24, cudaMemcpyHostToDevice, c->stream));
         launch_user_to_storage3(x_bar ? hx : nullptr, A.xb, d.uid, np, st);
         launch_user_to_storage3(v_bar ? hx + 3 * (size_t)np : nullptr, A.vb, d.uid, np, st);
     }
@@ -1396,10 +1417,11 @@ int sph_diff_backward(sph_ctx *c, const double *x_bar, const double *v_bar, doub
     launch_storage_to_user3(A.xb, nullptr, out + np, d.sidx, np, st);
     launch_storage_to_user3(A.vb, A.v0b, out + 4 * (size_t)np, d.sidx, np, st);
     CK(cudaStreamSynchronize(st));
-    if (grad_params) CK(cudaMemcpy(grad_params, A.theta_b, 24, cudaMemcpyDeviceToHost));
-    if (grad_mu) CK(cudaMemcpy(grad_mu, out, (size_t)np * 8, cudaMemcpyDeviceToHost));
-    if (x0_bar) CK(cudaMemcpy(x0_bar, out + np, (size_t)np * 24, cudaMemcpyDeviceToHost));
-    if (v0_bar) CK(cudaMemcpy(v0_bar, out + 4 * (size_t)np, (size_t)np * 24, cudaMemcpyDeviceToHost));
+    if (grad_params) CK(cudaMemcpyAsync(grad_params, A.theta_b, 24, cudaMemcpyDeviceToHost, c->stream));
+    if (grad_mu) CK(cudaMemcpyAsync(grad_mu, out, (size_t)np * 8, cudaMemcpyDeviceToHost, c->stream));
+    if (x0_bar) CK(cudaMemcpyAsync(x0_bar, out + np, (size_t)np * 24, cudaMemcpyDeviceToHost, c->stream));
+    if (v0_bar) CK(cudaMemcpyAsync(v0_bar, out + 4 * (size_t)np, (size_t)np * 24, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));   // the caller's arrays are complete
     ckpt_release(c, fin.buf);   // the final-state copy goes back to the pool
     return SPH_OK;
 }
@@ -1412,7 +1434,7 @@ int sph_diff_end(sph_ctx *c)
     CK(cudaDeviceSynchronize());
     free_diff(c);
     drop_graphs(c);
-    CK(cudaMemset(c->d.cflag, 1, div_up(c->np_all, 32)));
+    CK(cudaMemsetAsync(c->d.cflag, 1, div_up(c->np_all, 32), c->stream));
     c->diff = false;
     c->relayout_every = c->relayout_saved;
     return SPH_OK;
@@ -1446,11 +1468,11 @@ int sph_darcy_upload(sph_ctx *c, double nu, const sph_darcy_state *h)
     const std::pair<double *, const double *> one[] = {
         {f.H[0], h->H}, {f.H[1], h->H_new}, {f.K, h->K}, {f.Ss, h->Ss},
         {f.W, h->W},    {f.phi, h->phi},    {f.dphi, h->dphi}};
-    for (const auto &p : one) CK(cudaMemcpy(p.first, p.second, n * 8, cudaMemcpyHostToDevice));
+    for (const auto &p : one) CK(cudaMemcpyAsync(p.first, p.second, n * 8, cudaMemcpyHostToDevice, c->stream));
     const std::pair<double *, const double *> three[] = {{f.V, h->V}, {f.dH, h->dH}, {f.T, h->T}};
-    for (const auto &p : three) CK(cudaMemcpy(p.first, p.second, 3 * n * 8, cudaMemcpyHostToDevice));
+    for (const auto &p : three) CK(cudaMemcpyAsync(p.first, p.second, 3 * n * 8, cudaMemcpyHostToDevice, c->stream));
     const uint32_t one_u = 1u;
-    CK(cudaMemcpy(f.first, &one_u, 4, cudaMemcpyHostToDevice));
+    CK(cudaMemcpyAsync(f.first, &one_u, 4, cudaMemcpyHostToDevice, c->stream));
     f.nu = nu;
     // src/device.cu:673-678
     const double r_bar2 = c->mean_radius * 2.0;
@@ -1462,6 +1484,7 @@ int sph_darcy_upload(sph_ctx *c, double nu, const sph_darcy_state *h)
     }
     c->darcy_on = true;
     drop_graphs(c);   // the step graphs gain the Darcy kernels
+    CK(cudaStreamSynchronize(c->stream));   // the caller's arrays are complete
     return SPH_OK;
 }
 
@@ -1478,10 +1501,11 @@ int sph_darcy_download(sph_ctx *c, sph_darcy_state *h)
         {h->H, f.H[hs]}, {h->H_new, f.H[hs ^ 1]}, {h->K, f.K},      {h->Ss, f.Ss},
         {h->W, f.W},     {h->phi, f.phi},         {h->dphi, f.dphi}};
     for (const auto &p : one)
-        if (p.first) CK(cudaMemcpy(p.first, p.second, n * 8, cudaMemcpyDeviceToHost));
+        if (p.first) CK(cudaMemcpyAsync(p.first, p.second, n * 8, cudaMemcpyDeviceToHost, c->stream));
     const std::pair<double *, const double *> three[] = {{h->V, f.V}, {h->dH, f.dH}, {h->T, f.T}};
     for (const auto &p : three)
-        if (p.first) CK(cudaMemcpy(p.first, p.second, 3 * n * 8, cudaMemcpyDeviceToHost));
+        if (p.first) CK(cudaMemcpyAsync(p.first, p.second, 3 * n * 8, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));   // the caller's arrays are complete
     return SPH_OK;
 }
 

@@ -122,6 +122,7 @@ __device__ __forceinline__ P3 p3of(double4 v) { return P3{v.x, v.y, v.z}; }
 struct Dev {
     // sizes of the whole context: one scene, or every instance of a batch
     uint32_t np_all, ncells_all, ninst;
+    uint32_t shape;       // block shapes of the contact search and forces (SPH_OPT_BLOCK_SHAPES)
     // batched contexts: instance of each storage index and the first global
     // cell id of each instance (ninst + 1 entries); nullptr for one scene
     uint32_t *inst;

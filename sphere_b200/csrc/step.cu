@@ -35,27 +35,23 @@ namespace sphk {
 // Threads per block, and resident blocks per SM that the register
 // allocation must allow (the __launch_bounds__ minimum), from sweeps of
 // block shapes and caps at 1M spheres.
-#ifndef SPHK_TOPO_BLOCK
-#define SPHK_TOPO_BLOCK 64
-#endif
 #ifndef SPHK_FORCE_BLOCK
 #define SPHK_FORCE_BLOCK 128
 #endif
-constexpr int TOPO_BLOCK = SPHK_TOPO_BLOCK;
 constexpr int FORCE_BLOCK = SPHK_FORCE_BLOCK;
-#ifndef SPHK_TOPO_MIN_BLOCKS
-#define SPHK_TOPO_MIN_BLOCKS 20
-#endif
 #ifndef SPHK_FORCE_MIN_BLOCKS
 #define SPHK_FORCE_MIN_BLOCKS 8
 #endif
-#ifndef SPHK_CONTACT_BLOCK
-#define SPHK_CONTACT_BLOCK 128
-#endif
-#ifndef SPHK_CONTACT_MIN_BLOCKS
-#define SPHK_CONTACT_MIN_BLOCKS 4
-#endif
-constexpr int CONTACT_BLOCK = SPHK_CONTACT_BLOCK;
+// The contact search and the contact forces are compiled in two block
+// shapes each, and a context picks one pair (Dev::shape, SPH_OPT_BLOCK_SHAPES;
+// the ensemble's autotuner times both).  Shape 0, the default: k_topo in
+// blocks of 64 threads, 20 per SM, whose threads leave at different times;
+// k_contact in blocks of 4 warps, 4 per SM.  Shape 1: k_topo in 128 x 10,
+// k_contact in 2 warps x 8.  The threads resident per SM are the same.
+constexpr int TOPO_THREADS_PER_SM = 1280;
+constexpr int CONTACT_THREADS_PER_SM = 512;
+__host__ __device__ constexpr int topo_block(uint32_t shape) { return shape ? 128 : 64; }
+__host__ __device__ constexpr int contact_block(uint32_t shape) { return shape ? 64 : 128; }
 
 // What one law adds to a particle's sums.  The laws return their terms by
 // value and the caller adds them: each reference update `s += term` is the
@@ -396,6 +392,7 @@ struct TopoSlots {
 // Copies the partners of the particle's occupied slots to shared memory and
 // its shift codes to registers (once); the other entries are neither
 // searched nor written back.
+template <int TB>
 __device__ __forceinline__ void topo_load_row(const Dev &d, uint32_t *srow, int tid, uint32_t s,
                                               TopoSlots &ts)
 {
@@ -403,7 +400,7 @@ __device__ __forceinline__ void topo_load_row(const Dev &d, uint32_t *srow, int 
     if (ts.occ) {
         for (uint32_t m = ts.occ; m; m &= m - 1u) {
             const uint32_t i = (uint32_t)(__ffs(m) - 1);
-            srow[i * TOPO_BLOCK + tid] = d.contacts[tile_at(s, i, NC)];
+            srow[i * TB + tid] = d.contacts[tile_at(s, i, NC)];
         }
         const ulonglong2 c2 = d.dmc[s];
         ts.dm_lo = c2.x;
@@ -414,12 +411,13 @@ __device__ __forceinline__ void topo_load_row(const Dev &d, uint32_t *srow, int 
 
 // Whether candidate t already holds a slot of the (loaded) row through the
 // periodic image `code`.
+template <int TB>
 __device__ __forceinline__ bool in_slot(const uint32_t *srow, int tid, const TopoSlots &ts,
                                         uint32_t t, uint32_t code)
 {
     for (uint32_t m = ts.occ; m; m &= m - 1) {
         const int i = __ffs(m) - 1;
-        if (srow[i * TOPO_BLOCK + tid] == t) return dm_get(ts.dm_lo, ts.dm_hi, i) == code;
+        if (srow[i * TB + tid] == t) return dm_get(ts.dm_lo, ts.dm_hi, i) == code;
     }
     return false;
 }
@@ -429,16 +427,17 @@ __device__ __forceinline__ bool in_slot(const uint32_t *srow, int tid, const Top
 // the current cell (the reference returns from findContactsInCell).  Kept
 // out of line: it runs for the few overlaps of a particle, and inlining it
 // would raise the register count of the whole candidate loop.
+template <int TB>
 __device__ __noinline__ bool topo_insert(const Dev &d, uint32_t *srow, int tid, uint32_t s,
                                          uint32_t t, uint32_t code, TopoSlots &ts)
 {
-    topo_load_row(d, srow, tid, s, ts);
+    topo_load_row<TB>(d, srow, tid, s, ts);
     // slot choice, src/contactsearch.cuh:252-271: a slot already holding t
     // wins, else the last empty slot, else position nc
     int cpos = -1;
     for (uint32_t m = ts.occ; m; m &= m - 1) {
         const int i = __ffs(m) - 1;
-        if (srow[i * TOPO_BLOCK + tid] == t) { cpos = i; break; }
+        if (srow[i * TB + tid] == t) { cpos = i; break; }
     }
     if (cpos >= 0) {
         // already in its slot: the reference writes the slot again, which
@@ -453,7 +452,7 @@ __device__ __noinline__ bool topo_insert(const Dev &d, uint32_t *srow, int tid, 
         cpos = empty ? 31 - __clz(empty) : ts.nc;
         if (cpos < NC) {
             ts.occ |= 1u << cpos;
-            srow[cpos * TOPO_BLOCK + tid] = t;
+            srow[cpos * TB + tid] = t;
             dm_set(ts.dm_lo, ts.dm_hi, cpos, code);
             ts.dirty = true;
         } else {
@@ -522,14 +521,14 @@ __device__ __forceinline__ float moved_bound(const Dev &d, uint32_t s, const Ver
 // VISC (contact model 1): no slots; every candidate within ra + rb + db is
 // processed in visiting order and the contact force and pressure sums are
 // left in Dev::c1acc for k_force.
-template <bool VISC, bool BATCH>
-__global__ void __launch_bounds__(TOPO_BLOCK, SPHK_TOPO_MIN_BLOCKS)
+template <bool VISC, bool BATCH, int TB>
+__global__ void __launch_bounds__(TB, TOPO_THREADS_PER_SM / TB)
 k_topo(Dev d, int A)
 {
-    __shared__ uint32_t srow[NC * TOPO_BLOCK];
+    __shared__ uint32_t srow[NC * TB];
     const uint32_t np = d.np_all;
     const int tid = threadIdx.x;
-    const uint32_t s = blockIdx.x * TOPO_BLOCK + tid;
+    const uint32_t s = blockIdx.x * TB + tid;
     if (s == 0) {
         // the movers of the last step have been consumed by the rebuild
         d.vs->nmovers = 0u;
@@ -603,7 +602,7 @@ k_topo(Dev d, int A)
             }
         };
         load4(0);   // the first four entries are in flight with the slot row
-        if (filter) topo_load_row(d, srow, tid, s, ts);
+        if (filter) topo_load_row<TB>(d, srow, tid, s, ts);
         int skip_slot = -1;
         for (uint32_t e0 = 0; e0 < len; e0 += 4) {
             if (e0) load4(e0);
@@ -614,8 +613,8 @@ k_topo(Dev d, int A)
                 const int slot = (int)(meta & 31u);
                 if (slot == skip_slot) continue;   // nc > NC: rest of that cell
                 const uint32_t t = tv[j], code = meta >> 5;
-                if (filter && in_slot(srow, tid, ts, t, code)) continue;
-                if (overlaps(P, xr, t, code, xa) && !topo_insert(d, srow, tid, s, t, code, ts))
+                if (filter && in_slot<TB>(srow, tid, ts, t, code)) continue;
+                if (overlaps(P, xr, t, code, xa) && !topo_insert<TB>(d, srow, tid, s, t, code, ts))
                     skip_slot = slot;
             }
         }
@@ -686,7 +685,7 @@ k_topo(Dev d, int A)
                         if ((hit >> j) & 1u) visc_pair(d, A, s, t, code, F1, p1);
                     } else if ((hit >> j) & 1u) {
                         if (overlaps(P, xr, t, code, xa) &&
-                            !topo_insert(d, srow, tid, s, t, code, ts)) {
+                            !topo_insert<TB>(d, srow, tid, s, t, code, ts)) {
                             // nc > NC: skip the rest of this cell; the list
                             // would not describe the skipped part
                             next = (k2 < bnd1) ? bnd1 : ((k2 < bnd2) ? bnd2 : end);
@@ -780,7 +779,7 @@ k_topo(Dev d, int A)
         const uint32_t occ = ts.occ;
         for (uint32_t m = occ & ~ts.occ0; m; m &= m - 1u) {
             const uint32_t i = (uint32_t)(__ffs(m) - 1);
-            d.contacts[tile_at(s, i, NC)] = srow[i * TOPO_BLOCK + tid];
+            d.contacts[tile_at(s, i, NC)] = srow[i * TB + tid];
         }
         d.cmask[s] = occ;
         d.dmc[s] = make_ulonglong2(ts.dm_lo, ts.dm_hi);
@@ -1153,12 +1152,12 @@ constexpr uint32_t CT_CAP = SPHK_CONTACT_CAP;
 // no longer overlaps is freed and its history zeroed, as in the reference.
 // A chunk's rows are contiguous, its slot tiles too, and a round's lanes
 // mostly read one slot of consecutive particles, so their loads coalesce.
-template <int MODEL, bool BATCH>
-__global__ void __launch_bounds__(CONTACT_BLOCK, SPHK_CONTACT_MIN_BLOCKS)
+template <int MODEL, bool BATCH, int CB>
+__global__ void __launch_bounds__(CB, CONTACT_THREADS_PER_SM / CB)
 k_contact(ContactArgs args)
 {
     constexpr uint32_t FULL = 0xffffffffu;
-    constexpr int WARPS = CONTACT_BLOCK / 32;
+    constexpr int WARPS = CB / 32;
     // per warp: the law terms of the contacts held (F xyz, T xyz, p, ev_dot,
     // es_dot), the chunk's list of (lane | slot << 5), and which held
     // contacts overlapped (hits) and slipped
@@ -1367,7 +1366,7 @@ k_contact(ContactArgs args)
 
 // A resident grid of k_contact: the SMs times the blocks of this
 // instantiation that fit on one (looked up once per instantiation).
-template <int MODEL, bool BATCH>
+template <int MODEL, bool BATCH, int CB>
 static unsigned contact_grid(uint32_t np)
 {
     static int resident = 0;
@@ -1375,23 +1374,40 @@ static unsigned contact_grid(uint32_t np)
         int dev = 0, sms = 0, per_sm = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_contact<MODEL, BATCH>,
-                                                      CONTACT_BLOCK, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_contact<MODEL, BATCH, CB>, CB, 0);
         resident = std::max(1, sms) * std::max(1, per_sm);
     }
     const uint64_t chunks = div_up(np, 32);
-    return (unsigned)std::min<uint64_t>((uint64_t)resident, div_up(chunks, CONTACT_BLOCK / 32));
+    return (unsigned)std::min<uint64_t>((uint64_t)resident, div_up(chunks, CB / 32));
+}
+
+template <int TB>
+static void launch_topo_as(const Dev &d, uint32_t np, bool visc, int a, cudaStream_t st)
+{
+    const unsigned grid = div_up(np, TB);
+    if (d.inst)   // batched contexts: contact model 2 only
+        k_topo<false, true, TB><<<grid, TB, 0, st>>>(d, a);
+    else if (visc)
+        k_topo<true, false, TB><<<grid, TB, 0, st>>>(d, a);
+    else
+        k_topo<false, false, TB><<<grid, TB, 0, st>>>(d, a);
+}
+
+template <int CB>
+static void launch_contact_as(const ContactArgs &args, uint32_t np, int model, cudaStream_t st)
+{
+    if (args.d.inst)   // batched contexts: contact model 2 only
+        k_contact<2, true, CB><<<contact_grid<2, true, CB>(np), CB, 0, st>>>(args);
+    else if (model == 3)
+        k_contact<3, false, CB><<<contact_grid<3, false, CB>(np), CB, 0, st>>>(args);
+    else
+        k_contact<2, false, CB><<<contact_grid<2, false, CB>(np), CB, 0, st>>>(args);
 }
 
 void launch_topo(const Dev &d, uint32_t np, bool visc, int a, cudaStream_t st)
 {
-    const unsigned grid = div_up(np, TOPO_BLOCK);
-    if (d.inst)   // batched contexts: contact model 2 only
-        k_topo<false, true><<<grid, TOPO_BLOCK, 0, st>>>(d, a);
-    else if (visc)
-        k_topo<true, false><<<grid, TOPO_BLOCK, 0, st>>>(d, a);
-    else
-        k_topo<false, false><<<grid, TOPO_BLOCK, 0, st>>>(d, a);
+    if (d.shape) launch_topo_as<topo_block(1)>(d, np, visc, a, st);
+    else launch_topo_as<topo_block(0)>(d, np, visc, a, st);
 }
 
 void launch_force(const Dev &d, uint32_t np, int model, int a, int write_outputs, cudaStream_t st)
@@ -1427,12 +1443,8 @@ void launch_contact(const Dev &d, const Params &hp, uint32_t np, int model, int 
     ContactArgs args{d, a, write_outputs,
                      LawParams{hp.k_n, hp.k_t, hp.gamma_n, hp.gamma_t, hp.gamma_r, hp.mu_s, hp.mu_d,
                                hp.mu_r, hp.kappa, hp.dt, {hp.L[0], hp.L[1]}}};
-    if (d.inst)   // batched contexts: contact model 2 only
-        k_contact<2, true><<<contact_grid<2, true>(np), CONTACT_BLOCK, 0, st>>>(args);
-    else if (model == 3)
-        k_contact<3, false><<<contact_grid<3, false>(np), CONTACT_BLOCK, 0, st>>>(args);
-    else
-        k_contact<2, false><<<contact_grid<2, false>(np), CONTACT_BLOCK, 0, st>>>(args);
+    if (d.shape) launch_contact_as<contact_block(1)>(args, np, model, st);
+    else launch_contact_as<contact_block(0)>(args, np, model, st);
 }
 
 void launch_step(const Dev &d, const Params &hp, uint32_t np, int model, int a,

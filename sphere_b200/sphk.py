@@ -32,6 +32,7 @@ OPT_RELAYOUT_EVERY = 1
 OPT_GRAPH_STEPS = 2
 OPT_PROFILE = 3
 OPT_VERLET_SKIN = 4
+OPT_BLOCK_SHAPES = 5
 PHASES = ("cells", "bonds", "topo", "force", "walls", "darcy", "contact")
 
 _dp = C.POINTER(C.c_double)
@@ -209,9 +210,11 @@ class Simulation:
     """One DEM simulation resident on a GPU."""
 
     def __init__(self, cfg: SceneConfig, device: int = 0, graph_steps: int | None = None,
-                 relayout_every: int | None = None, verlet_skin: float | None = None):
+                 relayout_every: int | None = None, verlet_skin: float | None = None,
+                 block_shapes: int | None = None):
         """``verlet_skin``: Verlet-list skin as a fraction of the largest radius
-        (default 0.1; 0 sweeps the full stencil every step)."""
+        (default 0.1; 0 sweeps the full stencil every step).  ``block_shapes``:
+        0 or 1, the compiled block shapes of the contact kernels to use."""
         self.lib = load_library()
         self.cfg = cfg
         self._ctx = C.c_void_p()
@@ -225,6 +228,8 @@ class Simulation:
         if verlet_skin is not None:
             self._check(self.lib.sph_set_option(self._ctx, OPT_VERLET_SKIN,
                                                 int(round(verlet_skin * 1000))))
+        if block_shapes is not None:
+            self._check(self.lib.sph_set_option(self._ctx, OPT_BLOCK_SHAPES, int(block_shapes)))
 
     def _check(self, rc):
         if rc != SPH_OK:
@@ -412,7 +417,8 @@ class BatchSimulation(Simulation):
     of a Simulation of that scene alone."""
 
     def __init__(self, cfgs, device: int = 0, graph_steps: int | None = None,
-                 relayout_every: int | None = None, verlet_skin: float | None = None):
+                 relayout_every: int | None = None, verlet_skin: float | None = None,
+                 block_shapes: int | None = None):
         self.lib = load_library()
         self.cfgs = list(cfgs)
         self.nps = [c.np for c in self.cfgs]
@@ -431,6 +437,8 @@ class BatchSimulation(Simulation):
         if verlet_skin is not None:
             self._check(self.lib.sph_set_option(self._ctx, OPT_VERLET_SKIN,
                                                 int(round(verlet_skin * 1000))))
+        if block_shapes is not None:
+            self._check(self.lib.sph_set_option(self._ctx, OPT_BLOCK_SHAPES, int(block_shapes)))
 
     def upload(self, states):
         super().upload(pack_states(states))

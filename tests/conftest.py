@@ -23,7 +23,7 @@ def pytest_configure(config):
 @pytest.fixture(scope="session")
 def oracle_libs():
     import pyoracle
-    if not pyoracle.LIB_ORC.exists() or (not pyoracle.LIB_REF.exists() and Path("/root/reference/src").exists()):
+    if not pyoracle.LIB_ORC.exists() or (not pyoracle.LIB_REF.exists() and pyoracle.REF_SRC.exists()):
         pyoracle.build(ref=True)
     libs = {"orc": pyoracle.load("orc")}
     if pyoracle.LIB_REF.exists():

@@ -55,8 +55,9 @@ def test_pack_and_split_are_inverse():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("kw", [dict(), dict(verlet_skin=0.0), dict(relayout_every=5, graph_steps=3)],
-                         ids=["default", "sweep_every_step", "relayout_graphs"])
+@pytest.mark.parametrize("kw", [dict(), dict(verlet_skin=0.0), dict(relayout_every=5, graph_steps=3),
+                                dict(block_shapes=1)],
+                         ids=["default", "sweep_every_step", "relayout_graphs", "block_shapes_1"])
 def test_batch_matches_each_scene_alone(oracle_libs, kw):
     sbs = _mixed()
     want = []

@@ -104,6 +104,18 @@ def test_contact_detection_modes_agree_with_oracle(oracle_libs, name, skin):
     assert mismatches(got, want, ALL) == []
 
 
+@pytest.mark.parametrize("name", ["packed", "polydisperse_small", "box_wall", "periodic_crossing"])
+def test_second_block_shapes_agree_with_oracle(oracle_libs, name):
+    """The contact search and contact force kernels in their second compiled
+    block shapes (SPH_OPT_BLOCK_SHAPES = 1) give the oracle's results bit for
+    bit."""
+    sb = SCENES[name]()
+    rc, want, _ = run_oracle(oracle_libs["orc"], sb, 30)
+    assert rc == 0
+    got, _, _ = run_gpu(sb, (11, 19), block_shapes=1)
+    assert mismatches(got, want, ALL) == []
+
+
 @pytest.mark.parametrize("name", ["box", "periodic_xy"])
 def test_verlet_epochs_restart_exactly(oracle_libs, name):
     """300 steps: the displacement bound restarts the list epoch several
@@ -288,6 +300,22 @@ def test_bonded_tension_breaks_bonds_exactly(oracle_libs):
     assert mismatches(got, want, ALL + BOND_FIELDS) == []
     broken = int((got.bonds[:, 0] == sb.nb0).sum())
     assert 0 < broken < sb.nb0
+
+
+def test_stretched_bar_breaks_two_thirds_of_its_bonds_exactly(oracle_libs):
+    """The bonded-tension workload's bar (FCC, every lattice neighbour
+    bonded) at 5,324 spheres and 29,106 bonds, stretched as a whole so that
+    bonds throughout the bar break within the run (about two thirds of them,
+    all that lie along the pull); bit for bit over 120 steps in two calls,
+    bond history and breaks included."""
+    sb = scenes.tension(nx=11, ny=11, nz=11, pull=0.2)
+    assert sb.np == 5324 and sb.nb0 > 5 * sb.np
+    rc, want, _ = run_oracle(oracle_libs["orc"], sb, 120)
+    assert rc == 0
+    got, _, _ = run_gpu(sb, (45, 75))
+    assert mismatches(got, want, ALL + BOND_FIELDS) == []
+    broken = int((got.bonds[:, 0] >= sb.np).sum())
+    assert 0.5 * sb.nb0 < broken < sb.nb0
 
 
 def _ensemble_stats(sb, st):
