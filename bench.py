@@ -59,10 +59,14 @@ def parse():
     ap.add_argument("--batch-sample", type=int, default=16,
                     help="members run one by one for the per-instance baseline")
     ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--no-jammed", action="store_true",
+                    help="skip the contact-laden (jammed) batched ensemble")
     ap.add_argument("--adjoint-n", type=int, default=100_000,
                     help="spheres of the calibration column (0: skip the adjoint leg)")
     ap.add_argument("--adjoint-steps", type=int, default=4000)
     ap.add_argument("--adjoint-checkpoint", type=int, default=100)
+    ap.add_argument("--adjoint-fd-steps", type=int, default=40,
+                    help="steps of the central-difference check on the jammed column")
     ap.add_argument("--no-darcy", action="store_true",
                     help="skip the Darcy-flow leg (the 1M workload with the fluid grid on)")
     ap.add_argument("--darcy-steps", type=int, default=400)
@@ -74,6 +78,12 @@ def parse():
     ap.add_argument("--packed-steps", type=int, default=1000)
     ap.add_argument("--packed-side", type=int, default=100,
                     help="spheres per lattice edge of the packed column (default: 100^3 = 1M)")
+    ap.add_argument("--no-bonded", action="store_true",
+                    help="skip the bonded-tension leg (253,952 spheres, ~1.3M bonds)")
+    ap.add_argument("--bonded-steps", type=int, default=1000)
+    ap.add_argument("--no-settling", action="store_true",
+                    help="skip the 10k settling leg (the reference's CPU-runnable case)")
+    ap.add_argument("--settling-steps", type=int, default=1000)
     return ap.parse_args()
 
 
@@ -121,10 +131,15 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
-                 "-lms", "200", "-i", str(self.gpu)],
+                 "-lms", "100", "-i", str(self.gpu)],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            # nvidia-smi takes a moment to start: wait for its first sample
+            # so that the region it brackets is covered
+            t0 = time.perf_counter()
+            while not self.lines and time.perf_counter() - t0 < 5.0:
+                time.sleep(0.02)
         except FileNotFoundError:
             self.proc = None
         return self
@@ -141,7 +156,13 @@ class ClockSampler:
             except subprocess.TimeoutExpired:
                 self.proc.kill()
 
-    def summary(self):
+    def summary(self, window=None):
+        out = self._summary()
+        if window:
+            out["window"] = window
+        return out
+
+    def _summary(self):
         sm, mx, reasons = [], None, set()
         names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
         for ln in self.lines:
@@ -168,18 +189,6 @@ def measured_peak_hbm():
     if p.exists():
         return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
     return 6650.0, "fallback"
-
-
-def ncu_traffic(np_):
-    """DRAM bytes per launch of the step kernel from the committed ncu summary
-    (profiles/), scaled to this particle count; None when absent."""
-    p = ROOT / "profiles" / "k_force_polydisperse_1m_dram.md"
-    if not p.exists():
-        return None
-    for ln in p.read_text().splitlines():
-        if ln.startswith("dram_bytes_per_particle:"):
-            return float(ln.split(":")[1]) * np_
-    return None
 
 
 def algorithmic_bytes(np_, ncells, contacts, nbonds=0):
@@ -264,6 +273,10 @@ def gpu_arm(args, rank, world, local):
     stream = torch.cuda.Stream()
     sim = Simulation(cfg, device=local)
     sim.upload(st0)
+    # The clock samples (every 100 ms) cover the warm-up, the timed steps and
+    # the profiled steps: a timed region of a few milliseconds falls between
+    # two samples, the GPU's clocks under this load do not.
+    clocks = ClockSampler(local).__enter__()
     sim.step(args.warmup, stream=stream.cuda_stream)
     torch.cuda.synchronize()
     sim.sync()
@@ -272,18 +285,17 @@ def gpu_arm(args, rank, world, local):
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     rebuilds0 = sim.stats()["cell_rebuilds"]
     barrier()
-    with ClockSampler(local) as clocks:
-        start.record(stream)
-        sim.step(args.steps, stream=stream.cuda_stream)
-        end.record(stream)
-        end.synchronize()
+    start.record(stream)
+    sim.step(args.steps, stream=stream.cuda_stream)
+    end.record(stream)
+    end.synchronize()
     barrier()
     sim.sync()
     ms = max_over_ranks(start.elapsed_time(end))
     stats = sim.stats()
 
     # ---- per-phase device time (profile mode, events between phases) ------
-    nprof = min(args.steps, 200)
+    nprof = min(max(args.steps, 50), 200)
     sim.set_profile(True)
     sim.profile(reset=True)
     sim.step(nprof)
@@ -291,6 +303,7 @@ def gpu_arm(args, rank, world, local):
     prof = sim.profile(reset=True)
     sim.set_profile(False)
     sim.close()
+    clocks.__exit__(None, None, None)
 
     # ---- end to end through the C ABI with pinned host buffers ------------
     def pinned(a):
@@ -354,7 +367,8 @@ def gpu_arm(args, rank, world, local):
         "gpu_launches": launches, "cell_rebuilds_timed": rebuilt,
         "roofline": {"bound": "hbm", "kernel": "k_topo+k_contact+k_force", "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
-                     "traffic": ncu_traffic(cfg.np),
+                     "traffic": (profiled_traffic("polydisperse_1m") or {}).get("bytes_per_step")
+                                if cfg.np == 1_000_000 else None,
                      "algorithmic_bytes_per_launch": b_step,
                      "launch_ms": step_ms,
                      "tight_bytes_per_launch": b_tight,
@@ -363,14 +377,23 @@ def gpu_arm(args, rank, world, local):
                      "whole_step_frac": (b_whole / (ms / args.steps * 1e-3) / 1e9) / peak},
         "phase_ms_per_step": {k: prof[k] / max(1, prof["steps"])
                               for k in ("cells", "bonds", "topo", "contact", "force", "walls")},
-        "clocks": clocks.summary(),
+        "clocks": clocks.summary("warm-up, timed and profiled steps of this workload"),
     }
     if args.batch_instances > 0:
         out["batched"] = batched_leg(args, rank, world, local, barrier, max_over_ranks)
+        if not args.no_jammed:
+            out["batched_jammed"] = batched_leg(args, rank, world, local, barrier,
+                                                max_over_ranks, kind="jammed")
     if args.adjoint_n > 0 and rank == 0:
         out["adjoint"] = adjoint_leg(args, local)
+        if not args.no_jammed:
+            out["adjoint_contacts"] = adjoint_contacts_leg(args, local)
+    if not args.no_settling and rank == 0:
+        out["settling"] = settling_leg(args, local)
     if not args.no_packed and rank == 0:
         out["packed"] = packed_leg(args, local)
+    if not args.no_bonded and rank == 0:
+        out["bonded"] = bonded_leg(args, local)
     if not args.no_darcy and rank == 0:
         out["darcy"] = darcy_leg(args, local, sb)
     if not args.no_render and rank == 0:
@@ -396,29 +419,42 @@ def binpack(nps, world):
     return [sorted(b) for b in bins]
 
 
-def batched_leg(args, rank, world, local, barrier, max_over_ranks):
-    """The batched settling ensemble: every member this rank holds, stepped
-    together by one context, against the same members run one by one."""
+def batched_leg(args, rank, world, local, barrier, max_over_ranks, kind="settling"):
+    """A batched ensemble: every member this rank holds, stepped together by
+    one context, against the same members run one by one.
+
+    kind "settling": the configs' ensemble (``scenes.ensemble_member``),
+    members that start apart and settle; the autotuner also picks their
+    cell size.  kind "jammed": the same counts, stiffnesses and frictions
+    with every member a jammed lattice (``scenes.jammed_member``, about six
+    contacts per sphere from the first step), so the force laws run in every
+    timed step."""
     import torch
     from sphere_b200 import autotune, scenes
     from sphere_b200.sphk import BatchSimulation, Simulation
     from sphere_b200.state import config_from_spherebin, state_from_spherebin
 
     n_inst = args.batch_instances
-    nps = [scenes.ensemble_member(i).np for i in range(n_inst)]
+    if kind == "jammed":
+        build = lambda i, cf=None: scenes.jammed_member(i)
+        cell_factors = (None,)
+    else:
+        build = lambda i, cf=2.0: scenes.ensemble_member(i, cell_factor=cf)
+        cell_factors = autotune.CELL_FACTORS
+    nps = [build(i).np for i in range(n_inst)]
     mine = binpack(nps, world)[rank]
     tuned = None
     if args.no_autotune:
-        cell_factor, skin, gsteps = 2.0, 0.1, 8
+        cell_factor, skin, gsteps, shapes = (2.0 if kind != "jammed" else None), 0.1, 8, 0
     else:
         sub = mine[:: max(1, len(mine) // 64)][:64]
         t0 = time.perf_counter()
-        ch = autotune.tune(lambda cf: [scenes.ensemble_member(i, cell_factor=cf) for i in sub],
-                           warmup=10, steps=40, device=local)
-        cell_factor, skin, gsteps = ch.cell_factor, ch.verlet_skin, ch.graph_steps
+        ch = autotune.tune(lambda cf: [build(i, cf) for i in sub], warmup=10, steps=40,
+                           device=local, cell_factors=cell_factors)
+        cell_factor, skin, gsteps, shapes = ch.cell_factor, ch.verlet_skin, ch.graph_steps, ch.shapes
         tuned = {"members": len(sub), "seconds": time.perf_counter() - t0,
                  "trials": ch.trials}
-    members = [scenes.ensemble_member(i, cell_factor=cell_factor) for i in mine]
+    members = [build(i, cell_factor) for i in mine]
     cfgs = [config_from_spherebin(sb) for sb in members]
     states = [state_from_spherebin(sb) for sb in members]
     stream = torch.cuda.Stream()   # not the default stream (handle 0)
@@ -426,7 +462,8 @@ def batched_leg(args, rank, world, local, barrier, max_over_ranks):
 
     # ---- batched: all members in one context, inputs resident ---------------
     t_e2e = time.perf_counter()
-    sim = BatchSimulation(cfgs, device=local, graph_steps=gsteps, verlet_skin=skin)
+    sim = BatchSimulation(cfgs, device=local, graph_steps=gsteps, verlet_skin=skin,
+                          block_shapes=shapes)
     sim.upload(states)
     sim.step(args.warmup, stream=stream.cuda_stream)
     sim.sync()
@@ -469,14 +506,17 @@ def batched_leg(args, rank, world, local, barrier, max_over_ranks):
                "instances_per_s": len(members) / (est_ms * 1e-3),
                "speedup_batched_vs_per_instance": est_ms / ms_batch}
     n_part = sum(nps)
+    what = ("settling members (N log-uniform 500-20000)" if kind != "jammed" else
+            "jammed members (counts, k_n, mu of the settling members; r 1 mm simple-cubic "
+            "lattices at a 20 kPa overlap, periodic x/y)")
     return {
         "metric": "batched instances/s", "value": n_inst / (ms_batch * 1e-3), "unit": "instances/s",
-        "workload": f"{n_inst} settling members (N log-uniform 500-20000, {n_part} spheres), "
-                    f"{K} steps each, one context per GPU",
+        "workload": f"{n_inst} {what}, {n_part} spheres, {K} steps each, one context per GPU",
         "particles": n_part, "steps": K, "ms": ms_batch, "scaling": "strong",
         "particle_steps_per_s": n_part * K / (ms_batch * 1e-3),
         "active_contacts_end": contacts,
-        "choice": {"cell_factor": cell_factor, "verlet_skin": skin, "graph_steps": gsteps},
+        "choice": {"cell_factor": cell_factor, "verlet_skin": skin, "graph_steps": gsteps,
+                   "block_shapes": autotune.SHAPE_NAMES[shapes]},
         "autotune": tuned,
         "e2e": {"value": n_inst / e2e_s, "unit": "instances/s", "seconds": e2e_s,
                 "note": "create + upload + warm-up + timed steps + download"},
@@ -559,24 +599,11 @@ def adjoint_leg(args, local):
         iters.append((t_fwd, t_bwd))
     sim.close()
 
-    # finite-difference check of dL/dk_n, h = 1e-6 relative, on a dense scene
+    # central differences of every gradient on a dense colliding scene
     fsb = scenes.collision(n=2000, seed=args.seed + 3, periodic=0, vmax=0.2, wmax=50.0)
-    w = np.random.default_rng(args.seed + 4).normal(size=(fsb.np, 3))
     fsteps = 60
-
-    def floss(kn):
-        s_, st_ = adjoint.run_forward(fsb, fsteps, kn, fsb.k_t, fsb.gamma_n, None,
-                                      checkpoint_every=20, device=local)
-        return s_, float(np.sum(w * (st_.x[:, :3] - fsb.x)))
-    s_, _ = floss(fsb.k_n)
-    gk = s_.diff_backward(w)["k_n"]
-    s_.close()
-    h = 1e-6 * fsb.k_n
-    sp, lp = floss(fsb.k_n + h)
-    sp.close()
-    sm, lm = floss(fsb.k_n - h)
-    sm.close()
-    fd = (lp - lm) / (2 * h)
+    fd = fd_checks(fsb, fsteps, 20, local, args.seed + 4)
+    fd["scene"] = f"collision, {fsb.np} spheres, {fsteps} steps, checkpoints every 20"
     return {
         "metric": "adjoint/forward time ratio",
         "value": float(np.median([b / f for f, b in iters[1:]])), "unit": "ratio",
@@ -593,9 +620,125 @@ def adjoint_leg(args, local):
                                "mu_global": float(g["mu"].sum()),
                                "mu_particles_nonzero": int(np.count_nonzero(g["mu"]))},
         "device_bytes": stats["device_bytes"],
-        "fd_check": {"scene": f"collision, {fsb.np} spheres, {fsteps} steps",
-                     "param": "k_n", "adjoint": gk, "central_difference": fd,
-                     "rel_error": abs(gk - fd) / abs(fd) if fd else None},
+        "fd_check": fd,
+    }
+
+
+def fd_checks(sb, fsteps, fK, local, seed):
+    """Central differences (h = 1e-6 relative) of a seeded linear loss of the
+    final positions and velocities, L = w.x + u.v, against the adjoint's
+    gradients with respect to k_n, k_t, gamma_n, the global mu and the mu of
+    the three particles with the largest adjoint: one list entry per
+    parameter."""
+    import numpy as np
+    from sphere_b200 import adjoint
+
+    rng = np.random.default_rng(seed)
+    wx = rng.normal(size=(sb.np, 3))
+    wv = rng.normal(size=(sb.np, 3)) * 1e-3
+    mu0 = np.full(sb.np, float(sb.mu_s))
+    base = dict(k_n=float(sb.k_n), k_t=float(sb.k_t), gamma_n=float(sb.gamma_n))
+
+    def run(k_n, k_t, gamma_n, mu):
+        s_, st_ = adjoint.run_forward(sb, fsteps, k_n, k_t, gamma_n, mu, checkpoint_every=fK,
+                                      device=local)
+        return s_, float(np.sum(wx * st_.x[:, :3]) + np.sum(wv * st_.vel[:, :3]))
+
+    s_, _ = run(base["k_n"], base["k_t"], base["gamma_n"], mu0)
+    ga = s_.diff_backward(wx, wv)
+    s_.close()
+    checks = []
+
+    def central(name, adj, plus, minus, h):
+        sp, lp = plus()
+        sp.close()
+        sm, lm = minus()
+        sm.close()
+        fd = (lp - lm) / (2.0 * h)
+        checks.append({"param": name, "adjoint": adj, "central_difference": fd,
+                       "rel_error": abs(adj - fd) / abs(fd) if fd else None})
+
+    for name in ("k_n", "k_t", "gamma_n"):
+        h = 1e-6 * base[name]
+        pp, pm = dict(base), dict(base)
+        pp[name] += h
+        pm[name] -= h
+        central(name, float(ga[name]), lambda p=pp: run(**p, mu=mu0),
+                lambda p=pm: run(**p, mu=mu0), h)
+    h = 1e-6 * float(sb.mu_s)
+    central("mu", float(ga["mu"].sum()), lambda: run(**base, mu=mu0 + h),
+            lambda: run(**base, mu=mu0 - h), h)
+    for i in np.argsort(-np.abs(ga["mu"]))[:3]:
+        e = np.zeros(sb.np)
+        e[i] = h
+        central(f"mu[{int(i)}]", float(ga["mu"][i]), lambda e=e: run(**base, mu=mu0 + e),
+                lambda e=e: run(**base, mu=mu0 - e), h)
+    return {"h": "1e-6 relative", "loss": "w.x + u.v, seeded normal weights (u scaled 1e-3)",
+            "checks": checks, "max_rel_error": max(c["rel_error"] or 0.0 for c in checks)}
+
+
+def adjoint_contacts_leg(args, local):
+    """The adjoint where the contacts do the work: the calibration column
+    replaced by a jammed, stirred block (``scenes.jammed_column``: 100,800
+    spheres of r 1 mm held at a 20 kPa overlap by the six implicit walls,
+    seeded velocities and spins, so contacts stick and slide from the first
+    step).  Reports the adjoint/forward time ratio over the full run with the
+    height-profile loss, every gradient, and a central-difference check (h =
+    1e-6 relative) of the gradients with respect to k_n, k_t, gamma_n, the
+    global mu and three particles' mu on a short run of the same block, with
+    a seeded linear loss of the final positions and velocities."""
+    import numpy as np
+    import torch
+    from sphere_b200 import adjoint, scenes
+    from sphere_b200.sphk import Simulation
+    from sphere_b200.state import config_from_spherebin, state_from_spherebin
+
+    sb = scenes.jammed_column()
+    steps, K = args.adjoint_steps, args.adjoint_checkpoint
+    cfg = config_from_spherebin(sb)
+    st0 = state_from_spherebin(sb)
+    target = np.random.default_rng(args.seed + 17).uniform(0.12, 0.13, 64)
+    sim = Simulation(cfg, device=local)
+    iters = []
+    for _ in range(3):
+        sim.upload(st0)
+        sim.diff_begin(mu=None, checkpoint_every=K)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        sim.step(steps)
+        sim.sync()
+        t_fwd = time.perf_counter() - t0
+        st = sim.download()
+        C = sim.stats()["active_contacts"]
+        loss, xbar = height_profile_loss(st.x[:, :3], st.x[:, 3], 0.0, float(sb.L[0]), target)
+        t0 = time.perf_counter()
+        g = sim.diff_backward(xbar)
+        t_bwd = time.perf_counter() - t0
+        sim.diff_end()
+        iters.append((t_fwd, t_bwd))
+    sim.close()
+
+    # central differences on a short run of the same block
+    fsteps = args.adjoint_fd_steps
+    fd = fd_checks(sb, fsteps, 10, local, args.seed + 18)
+    fd["scene"] = f"the same block, {fsteps} steps, checkpoints every 10"
+    ratios = [b / f for f, b in iters[1:]]
+    return {
+        "metric": "adjoint/forward time ratio", "value": float(np.median(ratios)), "unit": "ratio",
+        "higher_is_better": False,
+        "workload": f"jammed, stirred column: {sb.np} spheres of r 1 mm, simple-cubic block "
+                    "40x40x63 at a 20 kPa overlap held by the six implicit walls, velocities "
+                    "U(+-0.005) m/s, spins U(+-20) rad/s, k_n = k_t = 1e6, mu 0.3, gamma_n 1e-3 of "
+                    f"critical, FP64, dt 5e-7 s, {steps} steps, checkpoints every {K}",
+        "active_contacts_end": C,
+        "forward_s": float(np.median([f for f, _ in iters[1:]])),
+        "backward_s": float(np.median([b for _, b in iters[1:]])),
+        "iterations": [{"forward_s": f, "backward_s": b, "ratio": b / f} for f, b in iters],
+        "loss": loss,
+        "grad": {"k_n": g["k_n"], "k_t": g["k_t"], "gamma_n": g["gamma_n"],
+                 "mu_global": float(g["mu"].sum()),
+                 "mu_particles_nonzero": int(np.count_nonzero(g["mu"]))},
+        "fd_check": fd,
     }
 
 
@@ -671,14 +814,167 @@ def darcy_leg(args, local, sb):
     }
 
 
+def profiled_traffic(workload_key):
+    """DRAM bytes per step of the step kernels of one workload, from the
+    committed ncu summary of the 1M workloads (profiles/
+    step_kernels_1m_dram.md: one line `traffic <workload> <kernel> <bytes>`
+    per kernel, a capture of the current code), or None when absent."""
+    p = ROOT / "profiles" / "step_kernels_1m_dram.md"
+    if not p.exists():
+        return None
+    out = {}
+    for ln in p.read_text().splitlines():
+        f = ln.strip().strip("`").split()
+        if len(f) == 4 and f[0] == "traffic" and f[1] == workload_key:
+            out[f[2]] = float(f[3])
+    if not out:
+        return None
+    return {"bytes_per_step": sum(out.values()), "per_kernel": out,
+            "source": "profiles/step_kernels_1m_dram.md"}
+
+
+def timed_steps(sim, K, warmup, local, stream, nprof=200):
+    """Warm-up, then exactly K steps between CUDA events on `stream`, then
+    per-phase times from up to `nprof` profile-mode steps; the clock samples
+    cover all three.  Returns (ms per step, phases per step, clocks)."""
+    import torch
+    clocks = ClockSampler(local).__enter__()
+    sim.step(warmup, stream=stream.cuda_stream)
+    sim.sync()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    sim.step(K, stream=stream.cuda_stream)
+    b.record(stream)
+    b.synchronize()
+    sim.sync()
+    ms = a.elapsed_time(b) / K
+    prof = None
+    if nprof:
+        sim.set_profile(True)
+        sim.profile(reset=True)
+        sim.step(min(K, nprof))
+        sim.sync()
+        prof = sim.profile(reset=True)
+        sim.set_profile(False)
+        prof = {k: prof[k] / max(1, prof["steps"])
+                for k in ("cells", "bonds", "topo", "contact", "force", "walls")}
+    clocks.__exit__(None, None, None)
+    return ms, prof, clocks.summary("warm-up, timed and profiled steps of this workload")
+
+
+def settling_leg(args, local):
+    """The plain settling scene (``scenes.settling``: 10,000 spheres of r =
+    0.01 m on a jittered lattice in a 0.5 x 0.5 x 2 m box, dt = 1e-6 s,
+    1000 steps), the reference's own CPU-runnable case: particle-steps/s on
+    the GPU through the whole run, and beside it the reference's kernel
+    bodies on the host cores over the same 1000 steps."""
+    import torch
+    from sphere_b200 import scenes
+    from sphere_b200.sphk import Simulation
+    from sphere_b200.state import config_from_spherebin, state_from_spherebin
+
+    sb = scenes.settling()
+    cfg = config_from_spherebin(sb)
+    K = args.settling_steps
+    stream = torch.cuda.Stream()
+    with Simulation(cfg, device=local) as sim:
+        sim.upload(state_from_spherebin(sb))
+        ms, prof, clocks = timed_steps(sim, K, 0, local, stream, nprof=0)
+        C = sim.stats()["active_contacts"]
+    out = {
+        "metric": "particle-steps/s, 10k settling", "value": cfg.np / (ms * 1e-3),
+        "unit": UNIT, "higher_is_better": True, "ms_per_step": ms, "steps": K,
+        "workload": "plain settling: 10,000 spheres, r 0.01 m, rho 2600, jittered cubic lattice "
+                    "(2.2 r, +-0.1 r) in a 0.5x0.5x2 m box, frictional walls, g -9.81, kn = kt = "
+                    "1e6, gamma_n 100, mu 0.5, FP64, dt 1e-6 s, grid 24x24x96, from rest",
+        "active_contacts_end": C, "clocks": clocks,
+    }
+    if not args.no_cpu_baseline:
+        base = cpu_reference_run(sb, 0, K, 120.0)
+        out["cpu_baseline"] = base
+        out["speedup_vs_cpu_baseline"] = out["value"] / base["value"]
+    return out
+
+
+def bonded_leg(args, local):
+    """The bonded-tension workload (``scenes.tension``: 253,952 spheres on an
+    FCC bar along x, a bond between every pair of lattice neighbours, about
+    5 bonds per sphere counted once, stretched at 0.01 m/s end to end): the
+    step with bond forces, breaking and bond-order force gathering.  The K
+    timed steps start from the unbroken bar and run past half of its bonds
+    breaking; reports particle-steps/s, the bond share of the step, the
+    whole step against the measured HBM bandwidth with 136 B per bond, and
+    the reference's kernel bodies on the host cores over a bounded sample."""
+    import numpy as np
+    import torch
+    from sphere_b200 import scenes
+    from sphere_b200.sphk import Simulation
+    from sphere_b200.state import config_from_spherebin, state_from_spherebin
+
+    sb = scenes.tension()
+    cfg = config_from_spherebin(sb)
+    st0 = state_from_spherebin(sb)
+    K = args.bonded_steps
+    stream = torch.cuda.Stream()
+    with Simulation(cfg, device=local) as sim:
+        sim.upload(st0)
+        sim.step(args.warmup, stream=stream.cuda_stream)   # warm-up, then back to the start
+        sim.sync()
+        sim.upload(st0)
+        ms, _, clocks = timed_steps(sim, K, 0, local, stream, nprof=0)
+        st = sim.download()
+        C = sim.stats()["active_contacts"]
+        broken = int((st.bonds[:, 0] >= cfg.np).sum())
+        # the per-phase times over the same steps, from the start again
+        sim.upload(st0)
+        sim.set_profile(True)
+        sim.profile(reset=True)
+        sim.step(min(K, 400))
+        sim.sync()
+        prof = sim.profile(reset=True)
+    nb = cfg.nb0
+    phases = {k: prof[k] / max(1, prof["steps"])
+              for k in ("cells", "bonds", "topo", "contact", "force", "walls")}
+    _, b_whole, _ = algorithmic_bytes(cfg.np, cfg.ncells, C, nb)
+    peak, peak_kind = measured_peak_hbm()
+    achieved = b_whole / (ms * 1e-3) / 1e9
+    b_bonds = 136 * nb
+    out = {
+        "metric": "particle-steps/s, bonded tension", "value": cfg.np / (ms * 1e-3), "unit": UNIT,
+        "higher_is_better": True, "ms_per_step": ms, "steps": K,
+        "workload": f"bonded tension: {cfg.np:,} spheres, r U(0.9, 1.1) mm, FCC bar along x "
+                    f"(62x32x32 cells, spacing 2.25 mm), {nb:,} bonds (every lattice neighbour), "
+                    "homogeneous stretch at 0.01 m/s end to end, end layers held, sigma_b = tau_b "
+                    "= 0.003, FP64, dt 1e-7 s, from the unbroken bar",
+        "bonds": nb, "bonds_per_particle": nb / cfg.np,
+        "broken_fraction_end": broken / nb, "active_contacts_end": C,
+        "phase_ms_per_step": phases,
+        "bond_share_of_step": phases["bonds"] / max(1e-12, sum(phases.values())),
+        "roofline": {"bound": "hbm", "kernel": "whole step", "achieved": achieved, "peak": peak,
+                     "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
+                     "algorithmic_bytes_per_step": b_whole,
+                     "k_bonds_achieved": b_bonds / (phases["bonds"] * 1e-3) / 1e9
+                     if phases["bonds"] > 0 else None,
+                     "k_bonds_algorithmic_bytes": b_bonds},
+        "clocks": clocks,
+    }
+    if not args.no_cpu_baseline:
+        base = cpu_reference_run(sb, 0, 1000, args.cpu_seconds)
+        out["cpu_baseline"] = base
+        out["speedup_vs_cpu_baseline"] = out["value"] / base["value"]
+    return out
+
+
 def packed_leg(args, local):
     """The contact-heavy workload: a jammed simple-cubic column of 1M spheres
     (``scenes.packed``: 100 x 100 x 100, r = 1 mm, periodic x/y, 20 kPa top
     wall), where every sphere holds about six contacts through the run.  It
     measures the force laws and the 52 B per directed contact that the
     headline workload, whose spheres barely touch, leaves out.  Reports
-    particle-steps/s over K graph steps and the k_topo + k_force pair against
-    the measured HBM bandwidth with the measured contact count."""
+    particle-steps/s over K graph steps, the contact search, contact force
+    and integration kernels against the measured HBM bandwidth with the
+    measured contact count, and the reference's kernel bodies on the host
+    cores over a bounded sample of the same steps."""
     import numpy as np
     import torch
     from sphere_b200 import scenes
@@ -701,27 +997,16 @@ def packed_leg(args, local):
         sim.close()
         return {"unavailable": f"packed column not jammed after warm-up (max speed {vmax:.3g} m/s)"}
     rebuilds0 = sim.stats()["cell_rebuilds"]
-    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local) as clocks:
-        a.record(stream)
-        sim.step(K, stream=stream.cuda_stream)
-        b.record(stream)
-        b.synchronize()
-    sim.sync()
-    ms = a.elapsed_time(b) / K
+    ms, prof, clocks = timed_steps(sim, K, 0, local, stream)
     stats = sim.stats()
-    sim.set_profile(True)
-    sim.profile(reset=True)
-    sim.step(min(K, 200))
-    sim.sync()
-    prof = sim.profile(reset=True)
     sim.close()
     C = stats["active_contacts"]
-    kern_ms = (prof["topo"] + prof["contact"] + prof["force"]) / max(1, prof["steps"])
+    kern_ms = prof["topo"] + prof["contact"] + prof["force"]
     b_step, _, b_tight = algorithmic_bytes(cfg.np, cfg.ncells, C)
     peak, peak_kind = measured_peak_hbm()
     achieved = b_step / (kern_ms * 1e-3) / 1e9
-    return {
+    traffic = profiled_traffic("packed_1m") if side == 100 else None
+    out = {
         "metric": METRIC, "value": cfg.np / (ms * 1e-3), "unit": UNIT, "higher_is_better": True,
         "ms_per_step": ms, "steps": K,
         "workload": f"packed column: {cfg.np:,} spheres of r 1 mm on a jammed simple-cubic "
@@ -734,11 +1019,17 @@ def packed_leg(args, local):
                      "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_source": peak_kind, "algorithmic_bytes_per_launch": b_step,
                      "launch_ms": kern_ms, "tight_bytes_per_launch": b_tight,
-                     "tight_frac": b_tight / (kern_ms * 1e-3) / 1e9 / peak},
-        "phase_ms_per_step": {k: prof[k] / max(1, prof["steps"])
-                              for k in ("cells", "bonds", "topo", "contact", "force", "walls")},
-        "clocks": clocks.summary(),
+                     "tight_frac": b_tight / (kern_ms * 1e-3) / 1e9 / peak,
+                     "traffic": traffic["bytes_per_step"] if traffic else None,
+                     "traffic_per_kernel": traffic["per_kernel"] if traffic else None},
+        "phase_ms_per_step": prof,
+        "clocks": clocks,
     }
+    if not args.no_cpu_baseline:
+        base = cpu_reference_run(sb, 1, 1000, args.cpu_seconds)
+        out["cpu_baseline"] = base
+        out["speedup_vs_cpu_baseline"] = out["value"] / base["value"]
+    return out
 
 
 def render_leg(args, local, sb):

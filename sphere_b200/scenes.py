@@ -193,13 +193,15 @@ def packed(nx=100, ny=100, nz=100, r=1e-3, sigma=20e3, seed=0, height=0.4,
 
 
 def bonded(seed=0, nx=40, ny=20, nz=20, r_lo=0.9e-3, r_hi=1.1e-3, pull=0.01,
-           sigma_b=2e7, tau_b=2e7, sid="bonded") -> Spherebin:
-    """FCC lattice with the nearest-neighbour distance equal to the mean
-    diameter (a close packing: pairs with ri + rj above it overlap), bonds
-    between all pairs closer than 1.05 (ri + rj); the first and last x layer
-    move apart at +-pull/2."""
+           sigma_b=2e7, tau_b=2e7, spacing=None, bond_all=False, sid="bonded") -> Spherebin:
+    """FCC lattice with the nearest-neighbour distance `spacing` (default the
+    mean diameter: a close packing, where pairs with ri + rj above it
+    overlap), bonds between all pairs closer than 1.05 (ri + rj), or with
+    `bond_all` between every pair of lattice neighbours; the first and last x
+    layer move apart at +-pull/2."""
     rng = np.random.default_rng(seed)
-    a = (r_lo + r_hi) * math.sqrt(2.0)   # cubic FCC cell edge; neighbour distance r_lo + r_hi
+    nn_dist = (r_lo + r_hi) if spacing is None else float(spacing)
+    a = nn_dist * math.sqrt(2.0)   # cubic FCC cell edge
     basis = np.array([[0, 0, 0], [0.5, 0.5, 0], [0.5, 0, 0.5], [0, 0.5, 0.5]])
     cells = np.stack(np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij"),
                      axis=-1).reshape(-1, 3)
@@ -239,8 +241,9 @@ def bonded(seed=0, nx=40, ny=20, nz=20, r_lo=0.9e-3, r_hi=1.1e-3, pull=0.01,
                 sel = oth > src
                 src, oth = src[sel], oth[sel]
                 d = np.linalg.norm(sb.x[src] - sb.x[oth], axis=1)
-                ok = d < 1.05 * (sb.radius[src] + sb.radius[oth])
-                ok &= d < 1.2 * nn
+                ok = d < 1.2 * nn
+                if not bond_all:
+                    ok &= d < 1.05 * (sb.radius[src] + sb.radius[oth])
                 pairs.append(np.stack([src[ok], oth[ok]], axis=1))
     bonds = np.unique(np.concatenate(pairs), axis=0).astype(np.uint32)
     sb.bonds = bonds
@@ -262,6 +265,41 @@ def bonded(seed=0, nx=40, ny=20, nz=20, r_lo=0.9e-3, r_hi=1.1e-3, pull=0.01,
     sb.time_total = 1000 * sb.time_dt
     sb.time_file_dt = sb.time_total
     _ = m_min
+    return sb
+
+
+def tension(nx=62, ny=32, nz=32, seed=0, pull=0.01, sigma_b=0.003, tau_b=0.003,
+            sid="tension") -> Spherebin:
+    """The bonded-tension workload: a bar of nx x ny x nz FCC cells (4
+    spheres each; 253,952 at the default 62 x 32 x 32, 0.20 x 0.10 x 0.10 m)
+    laid along x, radii U(0.9, 1.1) mm, a bond between every pair of lattice
+    neighbours (12 per sphere, about 6 per sphere counted once), both x end
+    layers pulled apart at pull/2 each, dt = 1e-7 s, no gravity.
+
+    The lattice spacing is 2.25 mm, the largest diameter plus the jitter
+    of the positions on both sides, so no pair overlaps
+    at the start: the reference's bonds are as stiff as k_n A (a few N/m at
+    k_n = 1e6 N/m and the bond section A = pi (0.9 mm)^2), against the
+    contacts' 1e6 N/m, so a packing whose neighbours overlap flies apart
+    under its contact forces before any pull acts.  Bond stiffness is the
+    reference's k_n A and k_t A (contact k_n = k_t = 1e6 N/m).
+
+    The bar starts in homogeneous stretch: x velocities linear in x, from
+    -pull/2 at one end layer to +pull/2 at the other.  Pulled at its ends
+    from rest, the bar (whose longitudinal wave speed with these bonds is
+    about 1 m/s) would tear at the end layers and nowhere else within the
+    run; stretched as a whole, every bond lengthens at 0.05 / s times its
+    length, and the breaking strengths sigma_b = tau_b = 0.003 (the
+    reference's units: k_n times the stretch, plus bending) are reached
+    throughout the bar after about 600 steps, where about 70% of the bonds
+    (those along the pull) break."""
+    sb = bonded(seed=seed, nx=nx, ny=ny, nz=nz, pull=pull, sigma_b=sigma_b, tau_b=tau_b,
+                spacing=2.25e-3, bond_all=True, sid=sid)
+    x = sb.x[:, 0]
+    lo, hi = float(x.min()), float(x.max())
+    sb.vel[:, 0] = pull * ((x - lo) / (hi - lo) - 0.5)
+    ends = sb.fixvel > 0
+    sb.vel[ends, 0] = np.where(x[ends] < 0.5 * (lo + hi), -0.5 * pull, 0.5 * pull)
     return sb
 
 
@@ -354,6 +392,97 @@ def ensemble_member(i, cell_factor=2.0, n_range=(500, 20000), sid=None) -> Spher
     m_min = 4.0 / 3.0 * math.pi * float(radii.min()) ** 3 * sb.rho
     sb.time_dt = 0.075 * math.sqrt(m_min / k)
     sb.time_total = 2000 * sb.time_dt
+    sb.time_file_dt = sb.time_total
+    return sb
+
+
+def jammed_member(i, n_range=(500, 20000), r=1e-3, sigma=20e3, sid=None) -> Spherebin:
+    """Member i of the contact-laden ensemble: ``packed`` at the member's
+    size, so that every sphere holds about six contacts from the first step.
+
+    - the particle count and the stiffness and friction draws of
+      ``ensemble_member`` i (seed 1000 + i): N log-uniform in 500-20,000,
+      k_n = k_t log-uniform in 1e5-1e7 N/m, mu ~ U(0.2, 0.8);
+    - a simple-cubic lattice nx x nx x nz (nx ~ (N / 1.25)^(1/3)) of spheres
+      of radius r = 1 mm (one radius: a lattice of unequal spheres cannot be
+      jammed evenly), spacing 2 r - delta with delta = sigma (2 r)^2 / k_n,
+      the overlap that carries a 20 kPa stress;
+    - periodic x/y with the lattice's period; the floor and the top of the
+      box (the reference's implicit walls, no dynamic wall: batched scenes
+      have none) each overlap their layer by delta;
+    - no normal viscosity (contact model 2's normal viscosity drives a
+      vibrating lattice apart, see ``packed``), wall viscosities 0.48 of
+      critical, dt = 0.075 sqrt(m / k_n) (python/sphere.py:1371), gravity
+      -9.81 m/s^2."""
+    rng = np.random.default_rng(1000 + i)
+    n_draw = int(round(math.exp(rng.uniform(math.log(n_range[0]), math.log(n_range[1])))))
+    rng.uniform(0.9e-3, 1.1e-3, n_draw)   # the radii draw of ensemble_member, unused
+    mu = float(rng.uniform(0.2, 0.8))
+    k = float(math.exp(rng.uniform(math.log(1e5), math.log(1e7))))
+    nx = max(6, int(round((n_draw / 1.25) ** (1.0 / 3.0))))
+    nz = max(2, int(round(n_draw / (nx * nx))))
+    n = nx * nx * nz
+    m = 2600.0 * float(V_sphere(r))
+    s0 = 2.0 * r
+    delta = sigma * s0 * s0 / k
+    spacing = s0 - delta
+    sb = Spherebin(np_=n, nw=0, sid=sid or f"jammed{i:04d}")
+    idx = np.arange(n)
+    lat = np.stack([idx % nx, (idx // nx) % nx, idx // (nx * nx)], axis=1).astype(float)
+    sb.x = lat * spacing + np.array([0.5 * spacing, 0.5 * spacing, r - delta])
+    sb.x += rng.uniform(-0.01 * delta, 0.01 * delta, size=(n, 3))
+    sb.radius = np.full(n, r)
+    sb.origo = np.zeros(3)
+    top = r - delta + (nz - 1) * spacing
+    sb.L = np.array([nx * spacing, nx * spacing, top + r - delta])
+    sb.num = np.array([nx // 2, nx // 2, max(1, int(sb.L[2] / (2.2 * r)))], dtype=np.uint32)
+    sb.periodic = 1
+    sb.g = np.array([0.0, 0.0, -9.81])
+    gamma_w = 0.48 * 2.0 * math.sqrt(k * m)
+    _contact_params(sb, k_n=k, k_t=k, gamma_n=0.0, gamma_t=0.0, mu=mu, gamma_w=gamma_w)
+    sb.time_dt = 0.075 * math.sqrt(m / k)
+    sb.time_total = 2000 * sb.time_dt
+    sb.time_file_dt = sb.time_total
+    return sb
+
+
+def jammed_column(nx=40, ny=40, nz=63, r=1e-3, sigma=20e3, k=1e6, mu=0.3, vmax=0.005,
+                  wmax=20.0, gamma_frac=1e-3, dt=5e-7, seed=0, sid="jammed_column") -> Spherebin:
+    """The calibration column in contact from the first step: a jammed
+    simple-cubic block of nx x ny x nz spheres (100,800 at the default, 8 x 8
+    x 12.6 cm), r = 1 mm, spacing 2 r - delta (delta = sigma (2 r)^2 / k, the
+    overlap that carries a 20 kPa stress), held in a box of its own size by
+    the reference's six implicit frictional walls, each overlapping its layer
+    by delta (a free block would spring apart: its contacts only push).  It
+    is stirred: seeded velocities U(+-vmax) and spins U(+-wmax), small against
+    the overlap's rate, so that contacts hold, stick and slide from the
+    start.  k_n = k_t = k, mu_s = mu_d = mu, dt = 5e-7 s, gravity -9.81
+    m/s^2.  gamma_n is gamma_frac of critical: contact model 2's normal
+    viscosity feeds a vibrating packing (see ``packed``), slowly at this
+    value."""
+    rng = np.random.default_rng(seed)
+    n = nx * ny * nz
+    m = 2600.0 * float(V_sphere(r))
+    s0 = 2.0 * r
+    delta = sigma * s0 * s0 / k
+    spacing = s0 - delta
+    sb = Spherebin(np_=n, nw=0, sid=sid)
+    idx = np.arange(n)
+    lat = np.stack([idx % nx, (idx // nx) % ny, idx // (nx * ny)], axis=1).astype(float)
+    sb.x = lat * spacing + (r - delta)
+    sb.x += rng.uniform(-0.01 * delta, 0.01 * delta, size=(n, 3))
+    sb.radius = np.full(n, r)
+    sb.vel = rng.uniform(-vmax, vmax, size=(n, 3))
+    sb.angvel = rng.uniform(-wmax, wmax, size=(n, 3))
+    sb.origo = np.zeros(3)
+    sb.L = np.array([nx, ny, nz], dtype=float) * spacing - spacing + 2.0 * (r - delta)
+    sb.num = np.floor(sb.L / (2.2 * r)).astype(np.uint32)
+    sb.periodic = 0
+    sb.g = np.array([0.0, 0.0, -9.81])
+    gamma = gamma_frac * 2.0 * math.sqrt(k * m)
+    _contact_params(sb, k_n=k, k_t=k, gamma_n=gamma, gamma_t=0.0, mu=mu, gamma_w=gamma)
+    sb.time_dt = dt
+    sb.time_total = 4000 * dt
     sb.time_file_dt = sb.time_total
     return sb
 
