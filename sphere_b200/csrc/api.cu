@@ -473,6 +473,7 @@ int do_relayout(sph_ctx *c, cudaStream_t st)
     // the slot rows moved: every chunk may hold a contact until the next
     // force pass has looked
     CK(cudaMemsetAsync(c->d.cflag, 1, div_up(c->np_all, 32), st));
+    CK(cudaMemsetAsync(c->d.settled, 0, c->np_all, st));
     CK(cudaGetLastError());
     c->relayouts++;
     c->since_relayout = 0;
@@ -612,7 +613,7 @@ int create_impl(const sph_config *cfgs, uint32_t ninst, bool batched, sph_ctx **
     AL(d.alias_any, 1);
     AL(d.vl, tiled_size(np, VL_CAP)); AL(d.vl_meta, tiled_size(np, VL_CAP)); AL(d.vl_len, np);
     AL(d.disp, np);
-    AL(d.vl_gap, np);
+    AL(d.vl_gap, np); AL(d.settled, np);
     AL(d.movers, MOVER_CAP); AL(d.dirty, ncells + 1); AL(d.vs, 1);
     AL(d.wf_pp, np); AL(d.wtouch, np); AL(d.wf_partial, div_up(np, 256));
     AL(d.wf_flag, div_up(np, 256));
@@ -1258,6 +1259,7 @@ static int restore_ckpt(sph_ctx *c, const sph_ctx::Ckpt &k)
     launch_cell_init(d, c->np_all, k.a, c->stream);
     CK(cudaMemsetAsync(d.dirty, 0, ((size_t)c->ncells_all + 1) * sizeof(uint32_t), c->stream));
     CK(cudaMemsetAsync(d.cflag, 1, div_up(c->np_all, 32), c->stream));
+    CK(cudaMemsetAsync(d.settled, 0, c->np_all, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     const uint32_t one = 1;
     CK(cudaMemcpyAsync(d.rebuild, &one, 4, cudaMemcpyHostToDevice, c->stream));
@@ -1435,6 +1437,7 @@ int sph_diff_end(sph_ctx *c)
     free_diff(c);
     drop_graphs(c);
     CK(cudaMemsetAsync(c->d.cflag, 1, div_up(c->np_all, 32), c->stream));
+    CK(cudaMemsetAsync(c->d.settled, 0, c->np_all, c->stream));
     c->diff = false;
     c->relayout_every = c->relayout_saved;
     return SPH_OK;

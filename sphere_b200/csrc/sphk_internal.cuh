@@ -172,6 +172,8 @@ struct Dev {
     uint8_t *vl_len;      // [np] list length or VL_NONE
     float *vl_gap;        // [np] lower bound of the smallest gap to a listed candidate
     float *disp;          // [np] displacement bound since the epoch started
+    uint8_t *settled;     // [np] every candidate of the valid list holds its slot (k_topo sets
+                          // it; a freed slot, a new list, upload or relayout clears it)
     uint2 *movers;        // [MOVER_CAP] (old cell, new cell) of the last step
     uint32_t *dirty;      // [ncells + 1] step stamp: a neighbour cell changed members
     Verlet *vs;

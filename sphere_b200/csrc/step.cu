@@ -544,10 +544,15 @@ k_topo(Dev d, int A)
     const uint8_t len = d.vl_len[s];
     const uint8_t outs = d.outside[s];
     const float gap = d.vl_gap[s];
+    const uint8_t held = VISC ? 0 : d.settled[s];
     const float bound = moved_bound(d, s, V);
     bool list_ok = P.skin > 0.0 && !V.all_rebuild && len != VL_NONE && outs == 0;
     if (list_ok && V.dirty_step == V.step) list_ok = d.dirty[d.cell[s]] != V.step;
-    if (list_ok && gap > bound) {
+    // A valid list whose candidates all hold their slots (Dev::settled) is
+    // settled too: the reference's topology would find every overlap among
+    // them (the list holds every possible one) already in its slot and
+    // change nothing.
+    if (list_ok && (gap > bound || held)) {
         if (VISC) d.c1acc[s] = make_double4(0.0, 0.0, 0.0, 0.0);
         return;
     }
@@ -604,6 +609,7 @@ k_topo(Dev d, int A)
         load4(0);   // the first four entries are in flight with the slot row
         if (filter) topo_load_row<TB>(d, srow, tid, s, ts);
         int skip_slot = -1;
+        uint32_t found = 0;   // candidates found in their slots
         for (uint32_t e0 = 0; e0 < len; e0 += 4) {
             if (e0) load4(e0);
 #pragma unroll
@@ -613,12 +619,19 @@ k_topo(Dev d, int A)
                 const int slot = (int)(meta & 31u);
                 if (slot == skip_slot) continue;   // nc > NC: rest of that cell
                 const uint32_t t = tv[j], code = meta >> 5;
-                if (filter && in_slot<TB>(srow, tid, ts, t, code)) continue;
+                if (filter && in_slot<TB>(srow, tid, ts, t, code)) {
+                    ++found;
+                    continue;
+                }
                 if (overlaps(P, xr, t, code, xa) && !topo_insert<TB>(d, srow, tid, s, t, code, ts))
                     skip_slot = slot;
             }
         }
+        // every candidate already held its slot: settled until a slot is
+        // freed (k_contact) or the list is recorded again
+        if (!VISC && filter && found == len && len != 0) d.settled[s] = 1;
     } else {
+        if (held) d.settled[s] = 0;   // the list is recorded again
         const float4 *__restrict__ xs = d.xs[A];
         const uint32_t k = d.pos[s];
         const float4 xaf = xs[k];
@@ -1091,7 +1104,10 @@ k_force(ForceArgs args)
                 d.delta_t[at] = P3{0.0, 0.0, 0.0};
             }
         }
-        if (occ != occ0) d.cmask[s] = occ;
+        if (occ != occ0) {
+            d.cmask[s] = occ;
+            d.settled[s] = 0;   // a listed candidate left its slot
+        }
         if (j >= 0) {
             d.tp_x[row] = xa;
             d.tp_v[row] = make_double4(vel_a.x, vel_a.y, vel_a.z, d.fixed[s] ? 1.0 : 0.0);
@@ -1353,7 +1369,10 @@ k_contact(ContactArgs args)
                 d.csum_f[s] = make_double4(sm[0][lane], sm[1][lane], sm[2][lane], sm[6][lane]);
                 d.csum_t[s] = make_double4(sm[3][lane], sm[4][lane], sm[5][lane], sm[7][lane]);
                 d.csum_es[s] = sm[8][lane];
-                if (occ != occ0) d.cmask[s] = occ;
+                if (occ != occ0) {
+                    d.cmask[s] = occ;
+                    d.settled[s] = 0;   // a listed candidate left its slot
+                }
             }
             // visited (2: a slot is still held, 3: none is); k_force reads
             // the sums of a visited chunk and sets its flag back to 1 or 0
