@@ -81,6 +81,8 @@ def parse():
     ap.add_argument("--no-bonded", action="store_true",
                     help="skip the bonded-tension leg (253,952 spheres, ~1.3M bonds)")
     ap.add_argument("--bonded-steps", type=int, default=1000)
+    ap.add_argument("--profile-workload", choices=("polydisperse", "packed", "tension"),
+                    help="only run one workload in profile mode (direct launches, for ncu)")
     ap.add_argument("--no-settling", action="store_true",
                     help="skip the 10k settling leg (the reference's CPU-runnable case)")
     ap.add_argument("--settling-steps", type=int, default=1000)
@@ -1099,9 +1101,49 @@ def reference_arm(args, rank, world):
     }
 
 
+def profile_workload(args):
+    """One workload in profile mode only (every kernel a direct launch, one
+    step after another with events between the phases), for ncu: a profiler
+    cannot follow the kernels of the step graphs.  `warmup` steps, then
+    `steps` steps; prints the phase times per step.  Per step the launches
+    are the cell-list kernels, k_bonds (with bonds), k_topo, k_contact (models
+    2 and 3), k_force and the wall kernel, in that order."""
+    import torch
+    from sphere_b200 import scenes
+    from sphere_b200.sphk import Simulation
+    from sphere_b200.state import config_from_spherebin, state_from_spherebin
+
+    w = args.profile_workload
+    if w == "packed":
+        side = args.packed_side
+        sb = scenes.packed(nx=side, ny=side, nz=side)
+    elif w == "tension":
+        sb = scenes.tension()
+    else:
+        sb = scene(args.n, args.seed)
+    with Simulation(config_from_spherebin(sb), device=0) as sim:
+        sim.upload(state_from_spherebin(sb))
+        sim.set_profile(True)
+        sim.step(args.warmup)
+        sim.sync()
+        sim.profile(reset=True)
+        sim.step(args.steps)
+        sim.sync()
+        prof = sim.profile(reset=True)
+    torch.cuda.synchronize()
+    return {"profile_workload": w, "particles": sb.np, "steps": args.steps,
+            "phase_ms_per_step": {k: prof[k] / max(1, prof["steps"])
+                                  for k in ("cells", "bonds", "topo", "contact", "force", "walls")}}
+
+
 def main():
     args = parse()
     rank, world, local = dist_env()
+    if args.profile_workload:
+        from sphere_b200 import build
+        build.build()
+        print(json.dumps(profile_workload(args)))
+        return
     if args.impl == "reference":
         out = reference_arm(args, rank, world)
     else:

@@ -885,6 +885,12 @@ __device__ __forceinline__ void particle_tail(const Dev &d, const Params &P, uin
         const double2 e = d.esv[s];
         d.esv[s] = make_double2(e.x + es_dot * dt, e.y + ev_dot * dt);
     }
+    // the outputs of the call's last step, each stored once it is final, so
+    // that no sum stays live through the integration for them
+    if (write_outputs) {
+        d.force[s] = make_double4(F.x, F.y, F.z, 0.0f);
+        d.edp[s] = make_double4(es_dot, ev_dot, p, 0.0);
+    }
     if (P.nw > 0) {
         const uint8_t touched = d.wtouch[s];
         if (w0f != 0.0 || touched) {
@@ -943,6 +949,7 @@ __device__ __forceinline__ void particle_tail(const Dev &d, const Params &P, uin
         acc.y = 0.0;
         acc.z -= P.g[2];
     }
+    if (write_outputs) d.acc[s] = acc;
     if (P.periodic == 1) {
         if (x.x < P.origo[0]) x.x += P.L[0];
         if (x.x > P.L[0]) x.x -= P.L[0];
@@ -974,11 +981,6 @@ __device__ __forceinline__ void particle_tail(const Dev &d, const Params &P, uin
     // float copy for the next step's contact search, at this particle's
     // cell-list position (rewritten by the rebuild when the order changes)
     d.xs[B][d.pos[s]] = make_float4((float)x.x, (float)x.y, (float)x.z, (float)x.w);
-    if (write_outputs) {
-        d.force[s] = make_double4(F.x, F.y, F.z, 0.0f);
-        d.acc[s] = acc;
-        d.edp[s] = make_double4(es_dot, ev_dot, p, 0.0);
-    }
 
     // ---- displacement bound since the Verlet epoch started ----------------
     Verlet &V = *d.vs;
