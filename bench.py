@@ -957,7 +957,11 @@ def bonded_leg(args, local):
                      "algorithmic_bytes_per_step": b_whole,
                      "k_bonds_achieved": b_bonds / (phases["bonds"] * 1e-3) / 1e9
                      if phases["bonds"] > 0 else None,
-                     "k_bonds_algorithmic_bytes": b_bonds},
+                     "k_bonds_algorithmic_bytes": b_bonds,
+                     "traffic": (profiled_traffic("tension_254k") or {}).get("bytes_per_step")
+                                if cfg.np == 253_952 else None,
+                     "traffic_per_kernel": (profiled_traffic("tension_254k") or {}).get("per_kernel")
+                                           if cfg.np == 253_952 else None},
         "clocks": clocks,
     }
     if not args.no_cpu_baseline:

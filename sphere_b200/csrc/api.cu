@@ -12,14 +12,14 @@
 #include <vector>
 
 namespace sphk {
-void launch_step(const Dev &d, const Params &hp, uint32_t np, int model, int a, int write_outputs,
-                 cudaStream_t st);
 void launch_topo(const Dev &d, uint32_t np, bool visc, int a, cudaStream_t st);
 void launch_force(const Dev &d, uint32_t np, int model, int a, int write_outputs, cudaStream_t st);
 void launch_contact(const Dev &d, const Params &hp, uint32_t np, int model, int a, int write_outputs,
                     cudaStream_t st);
 void launch_bonds(const Dev &d, uint32_t nb0, int a, cudaStream_t st);
 void launch_walls(const Dev &d, uint32_t np, uint32_t nw, cudaStream_t st);
+void launch_wall_motion(const Dev &d, uint32_t np, cudaStream_t st);
+void launch_tail(const Dev &d, cudaStream_t st);
 void launch_cell_init(const Dev &d, uint32_t np, int a, cudaStream_t st);
 void launch_rebuild(const Dev &d, uint32_t np, uint32_t ncells, int a, cudaStream_t st);
 unsigned int scan_tile_count(uint32_t ncells);
@@ -99,6 +99,12 @@ struct sph_ctx {
     // and wall kernels: forked after the cell list, joined at the step's end
     cudaStream_t darcy_stream = nullptr;
     cudaEvent_t darcy_fork = nullptr, darcy_join = nullptr;
+    // in the step graphs the wall reduction and integration of a step run on
+    // a branch forked after its force kernel and joined before the next
+    // step's force kernel (or the graph's end); wall_pending: a fork is open
+    cudaStream_t wall_stream = nullptr;
+    cudaEvent_t wall_fork = nullptr, wall_join = nullptr;
+    bool wall_pending = false;
     int dflip = 0;
     double mean_radius = 0.0;        // of the uploaded particles, summed in caller order
     // ray tracer scratch: per-pixel keys and image, per-particle values
@@ -366,9 +372,27 @@ int enqueue_one_step(sph_ctx *c, int a, int write_outputs, cudaStream_t st, bool
         launch_darcy(c->d, c->darcy, c->hp, a, a ^ c->dflip, c->darcy_stream);
         CK(cudaEventRecord(c->darcy_join, c->darcy_stream));
     }
-    launch_step(c->d, c->hp, c->np_all, (int)c->hp.contactmodel, a, write_outputs, st);
+    const int model = (int)c->hp.contactmodel;
+    launch_topo(c->d, c->np_all, model == 1, a, st);
+    launch_contact(c->d, c->hp, c->np_all, model, a, write_outputs, st);
+    if (c->wall_pending) {
+        // the walls moved by the previous step's branch, before this step's
+        // wall forces read them
+        CK(cudaStreamWaitEvent(st, c->wall_join, 0));
+        c->wall_pending = false;
+    }
+    launch_force(c->d, c->np_all, model, a, write_outputs, st);
     if (c->darcy_on && !branch) launch_darcy(c->d, c->darcy, c->hp, a, a ^ c->dflip, st);
-    launch_walls(c->d, c->np_all, c->hp.nw, st);
+    if (capturing && c->hp.nw > 0 && !c->batched) {
+        CK(cudaEventRecord(c->wall_fork, st));
+        CK(cudaStreamWaitEvent(c->wall_stream, c->wall_fork, 0));
+        launch_wall_motion(c->d, c->np_all, c->wall_stream);
+        CK(cudaEventRecord(c->wall_join, c->wall_stream));
+        c->wall_pending = true;
+        launch_tail(c->d, st);
+    } else {
+        launch_walls(c->d, c->np_all, c->hp.nw, st);
+    }
     if (branch) CK(cudaStreamWaitEvent(st, c->darcy_join, 0));
     return SPH_OK;
 }
@@ -379,10 +403,19 @@ int capture(sph_ctx *c, cudaGraphExec_t *out, int a, int nsteps, int write_last)
     CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
     int aa = a;
     int rc = SPH_OK;
+    c->wall_pending = false;
     for (int i = 0; i < nsteps && rc == SPH_OK; ++i) {
         rc = enqueue_one_step(c, aa, (write_last && i == nsteps - 1) ? 1 : 0, c->stream, true);
         aa ^= 1;
     }
+    if (c->wall_pending) {
+        // the last step's walls are part of the graph's work (and a capture
+        // that failed ends with its branch joined)
+        const cudaError_t e = cudaStreamWaitEvent(c->stream, c->wall_join, 0);
+        if (e != cudaSuccess && rc == SPH_OK)
+            rc = fail(c, SPH_ERR_CUDA, std::string("wall join: ") + cudaGetErrorString(e));
+    }
+    c->wall_pending = false;
     if (rc != SPH_OK) {
         // conditional nodes unavailable: end the broken capture and capture
         // the plain rebuild instead
@@ -589,6 +622,9 @@ int create_impl(const sph_config *cfgs, uint32_t ninst, bool batched, sph_ctx **
     CK(cudaSetDevice(c->device));
     CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
     CK(cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&c->wall_stream, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&c->wall_fork, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&c->wall_join, cudaEventDisableTiming));
 
     const size_t np = c->np_all;
     const size_t ncells = c->ncells_all;
@@ -1568,6 +1604,9 @@ int sph_destroy(sph_ctx *c)
     if (c->darcy_fork) cudaEventDestroy(c->darcy_fork);
     if (c->darcy_join) cudaEventDestroy(c->darcy_join);
     if (c->darcy_stream) cudaStreamDestroy(c->darcy_stream);
+    if (c->wall_fork) cudaEventDestroy(c->wall_fork);
+    if (c->wall_join) cudaEventDestroy(c->wall_join);
+    if (c->wall_stream) cudaStreamDestroy(c->wall_stream);
     for (void *p : c->allocs) cudaFree(p);
     if (c->stream) cudaStreamDestroy(c->stream);
     if (c->side) cudaStreamDestroy(c->side);

@@ -1468,12 +1468,4 @@ void launch_contact(const Dev &d, const Params &hp, uint32_t np, int model, int 
     else launch_contact_as<contact_block(0)>(args, np, model, st);
 }
 
-void launch_step(const Dev &d, const Params &hp, uint32_t np, int model, int a,
-                 int write_outputs, cudaStream_t st)
-{
-    launch_topo(d, np, model == 1, a, st);
-    launch_contact(d, hp, np, model, a, write_outputs, st);
-    launch_force(d, np, model, a, write_outputs, st);
-}
-
 }  // namespace sphk

@@ -1,6 +1,13 @@
 // walls.cu -- wall-force reduction and wall integration (summation and
 // integrateWalls, src/integration.cuh:191-295), in one launch.
 //
+// The launch also ends the step's Verlet bookkeeping (step_tail) when it
+// runs on the step's own stream.  In the step graphs it runs on a branch
+// instead, forked after the force kernel and joined before the next step's
+// force kernel (the only reader of the wall rows), so that its serial tail
+// overlaps the next step's contact search; the bookkeeping, which that
+// search reads, is then a one-thread launch on the step's stream (k_tail).
+//
 // The wall-0 force of every particle is summed in the reference's exact
 // order: 256-particle blocks in particle-index order reduced by a halving
 // tree (integration.cuh:197-216), then the block partials added one after
@@ -38,6 +45,7 @@ constexpr int REF_BLOCK = 256;               // the reference's summation block
 constexpr int WARPS = WALL_BLOCK / 32;        // reference blocks per CUDA block
 constexpr int FOLD = 16;                      // partials per thread in the fold
 
+template <bool TAIL>
 __global__ void __launch_bounds__(WALL_BLOCK)
 k_walls(Dev d)
 {
@@ -150,7 +158,7 @@ k_walls(Dev d)
     if (t == 0) {
         W.t_current += P.dt;
         W.done_blocks = 0;
-        step_tail(d);
+        if (TAIL) step_tail(d);
     }
 }
 
@@ -167,7 +175,20 @@ void launch_walls(const Dev &d, uint32_t np, uint32_t nw, cudaStream_t st)
         return;
     }
     const unsigned int nref = div_up(np, REF_BLOCK);
-    k_walls<<<div_up(nref, WARPS), WALL_BLOCK, 0, st>>>(d);
+    k_walls<true><<<div_up(nref, WARPS), WALL_BLOCK, 0, st>>>(d);
+}
+
+// The wall reduction and integration alone (nw > 0), for a graph branch.
+void launch_wall_motion(const Dev &d, uint32_t np, cudaStream_t st)
+{
+    const unsigned int nref = div_up(np, REF_BLOCK);
+    k_walls<false><<<div_up(nref, WARPS), WALL_BLOCK, 0, st>>>(d);
+}
+
+// The Verlet bookkeeping alone.
+void launch_tail(const Dev &d, cudaStream_t st)
+{
+    k_tail<<<1, 32, 0, st>>>(d);
 }
 
 }  // namespace sphk
