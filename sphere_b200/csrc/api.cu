@@ -13,7 +13,8 @@
 
 namespace sphk {
 void launch_topo(const Dev &d, uint32_t np, bool visc, int a, cudaStream_t st);
-void launch_force(const Dev &d, uint32_t np, int model, int a, int write_outputs, cudaStream_t st);
+void launch_force(const Dev &d, const Params &hp, uint32_t np, int model, int a, int write_outputs,
+                  cudaStream_t st);
 void launch_contact(const Dev &d, const Params &hp, uint32_t np, int model, int a, int write_outputs,
                     cudaStream_t st);
 void launch_bonds(const Dev &d, uint32_t nb0, int a, cudaStream_t st);
@@ -105,6 +106,7 @@ struct sph_ctx {
     cudaStream_t wall_stream = nullptr;
     cudaEvent_t wall_fork = nullptr, wall_join = nullptr;
     bool wall_pending = false;
+    ForceConsts graph_fc{};          // the force kernel's constants in the step graphs
     int dflip = 0;
     double mean_radius = 0.0;        // of the uploaded particles, summed in caller order
     // ray tracer scratch: per-pixel keys and image, per-particle values
@@ -381,7 +383,7 @@ int enqueue_one_step(sph_ctx *c, int a, int write_outputs, cudaStream_t st, bool
         CK(cudaStreamWaitEvent(st, c->wall_join, 0));
         c->wall_pending = false;
     }
-    launch_force(c->d, c->np_all, model, a, write_outputs, st);
+    launch_force(c->d, c->hp, c->np_all, model, a, write_outputs, st);
     if (c->darcy_on && !branch) launch_darcy(c->d, c->darcy, c->hp, a, a ^ c->dflip, st);
     if (capturing && c->hp.nw > 0 && !c->batched) {
         CK(cudaEventRecord(c->wall_fork, st));
@@ -449,7 +451,12 @@ void drop_graphs(sph_ctx *c)
 
 int ensure_graphs(sph_ctx *c)
 {
-    if (c->graphs_for_k == c->graph_steps && c->g_single[0][0]) return SPH_OK;
+    // graphs carry the force kernel's constants: an upload that changed one
+    // (the skin, esv_skip) captures them again
+    const ForceConsts fc = force_consts(c->hp);
+    if (c->graphs_for_k == c->graph_steps && c->g_single[0][0] &&
+        std::memcmp(&fc, &c->graph_fc, sizeof(fc)) == 0)
+        return SPH_OK;
     drop_graphs(c);
     for (int a = 0; a < 2; ++a) {
         int rc;
@@ -458,6 +465,7 @@ int ensure_graphs(sph_ctx *c)
             if ((rc = capture(c, &c->g_single[a][w], a, 1, w)) != SPH_OK) return rc;
     }
     c->graphs_for_k = c->graph_steps;
+    c->graph_fc = force_consts(c->hp);
     return SPH_OK;
 }
 
@@ -481,7 +489,7 @@ int profiled_step(sph_ctx *c, int a, int write_outputs, cudaStream_t st)
     CK(cudaEventRecord(c->ev[3], st));
     launch_contact(c->d, c->hp, c->np_all, (int)c->hp.contactmodel, a, write_outputs, st);
     CK(cudaEventRecord(c->ev[4], st));
-    launch_force(c->d, c->np_all, (int)c->hp.contactmodel, a, write_outputs, st);
+    launch_force(c->d, c->hp, c->np_all, (int)c->hp.contactmodel, a, write_outputs, st);
     CK(cudaEventRecord(c->ev[5], st));
     launch_walls(c->d, c->np_all, c->hp.nw, st);
     CK(cudaEventRecord(c->ev[6], st));
@@ -634,24 +642,26 @@ int create_impl(const sph_config *cfgs, uint32_t ninst, bool batched, sph_ctx **
     d.ninst = ninst;
     int rc = SPH_OK;
 #define AL(ptr, n) if ((rc = dalloc(c, &(ptr), (n))) != SPH_OK) return rc;
+    // the rows the force kernel copies in tiles, in whole tiles
+    const size_t npad = padded_rows(np);
     for (int b = 0; b < 2; ++b) {
-        AL(d.xr[b], np); AL(d.vel[b], np); AL(d.angvel[b], np); AL(d.xs[b], np);
+        AL(d.xr[b], npad); AL(d.vel[b], npad); AL(d.angvel[b], npad); AL(d.xs[b], np);
     }
-    AL(d.vel0, np); AL(d.angvel0, np); AL(d.angpos, np); AL(d.xysum, np); AL(d.esv, np);
-    AL(d.w_user, WLANES * np); AL(d.fixed, np);
+    AL(d.vel0, npad); AL(d.angvel0, npad); AL(d.angpos, npad); AL(d.xysum, npad); AL(d.esv, np);
+    AL(d.w_user, WLANES * np); AL(d.fixed, npad);
     AL(d.force, np); AL(d.torque, np); AL(d.acc, np); AL(d.angacc, np); AL(d.edp, np);
-    AL(d.uid, np); AL(d.sidx, np); AL(d.cell, np); AL(d.outside, np);
+    AL(d.uid, np); AL(d.sidx, np); AL(d.cell, npad); AL(d.outside, np);
     AL(d.contacts, tiled_size(np, NC)); AL(d.dmc, np); AL(d.delta_t, tiled_size(np, NC));
     AL(d.cmask, np);
     AL(d.cflag, div_up(np, 32));
-    AL(d.cell_start, ncells + 2); AL(d.cellorder, np); AL(d.pos, np); AL(d.cell_fill, ncells + 1);
+    AL(d.cell_start, ncells + 2); AL(d.cellorder, np); AL(d.pos, npad); AL(d.cell_fill, ncells + 1);
     AL(d.scan_tiles, scan_tile_count(c->ncells_all));
     AL(d.alias_any, 1);
     AL(d.vl, tiled_size(np, VL_CAP)); AL(d.vl_meta, tiled_size(np, VL_CAP)); AL(d.vl_len, np);
-    AL(d.disp, np);
+    AL(d.disp, npad);
     AL(d.vl_gap, np); AL(d.settled, np);
     AL(d.movers, MOVER_CAP); AL(d.dirty, ncells + 1); AL(d.vs, 1);
-    AL(d.wf_pp, np); AL(d.wtouch, np); AL(d.wf_partial, div_up(np, 256));
+    AL(d.wf_pp, np); AL(d.wtouch, npad); AL(d.wf_partial, div_up(np, 256));
     AL(d.wf_flag, div_up(np, 256));
     AL(d.walls, 1);
     AL(d.bonds, nb0); AL(d.bonds_delta, nb0); AL(d.bonds_omega, nb0);

@@ -70,6 +70,42 @@ struct Params {
     uint32_t uid_base;  // batched contexts: first global particle index of this instance
 };
 
+// The scene constants the force kernel reads for every particle, passed by
+// value to single-scene launches (read from the constant bank, never
+// reloaded after a store); the same fields as in Params.  skin and esv_skip
+// change at upload: a context captures its step graphs again when any field
+// changes.
+struct ForceConsts {
+    uint32_t nw, nb0, ncells, cell_base;
+    int32_t periodic;
+    uint32_t num[3];
+    uint32_t esv_skip;
+    uint32_t pad;
+    double origo[3], L[3], cellsize[3];
+    double dt, g[3], rho, skin;
+};
+inline ForceConsts force_consts(const Params &P)
+{
+    ForceConsts c{};
+    c.nw = P.nw;
+    c.nb0 = P.nb0;
+    c.ncells = P.ncells;
+    c.cell_base = P.cell_base;
+    c.periodic = P.periodic;
+    c.esv_skip = P.esv_skip;
+    for (int i = 0; i < 3; ++i) {
+        c.num[i] = P.num[i];
+        c.origo[i] = P.origo[i];
+        c.L[i] = P.L[i];
+        c.cellsize[i] = P.cellsize[i];
+        c.g[i] = P.g[i];
+    }
+    c.dt = P.dt;
+    c.rho = P.rho;
+    c.skin = P.skin;
+    return c;
+}
+
 constexpr int VL_CAP = 32;              // candidates kept per particle
 constexpr uint8_t VL_NONE = 0xff;       // no usable list: sweep the stencil
 constexpr uint32_t MOVER_CAP = 1u << 16;
@@ -277,7 +313,8 @@ __device__ __forceinline__ bool grid_cell(const G &P, double x, double y, double
 // Whether some floored cell coordinate of the position lies outside
 // [0, num): the particle is not inside its own cell's box (contact search
 // takes the reference's stencil from the floored coordinates, not the id).
-__device__ __forceinline__ bool cell_outside(const Params &P, double x, double y, double z)
+template <class G>
+__device__ __forceinline__ bool cell_outside(const G &P, double x, double y, double z)
 {
     const double f0 = cell_floor(P, 0, x), f1 = cell_floor(P, 1, y), f2 = cell_floor(P, 2, z);
     return !(f0 >= 0.0 && f0 < (double)P.num[0] && f1 >= 0.0 && f1 < (double)P.num[1] &&
@@ -301,6 +338,75 @@ __device__ __forceinline__ void bulk_prefetch_l2(const void *p, uint32_t bytes)
 {
     asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
 }
+
+// Bulk copies into shared memory that complete on an mbarrier (the copy
+// engine moves the bytes; the issuing thread holds no register for them).
+// Addresses and sizes are multiples of 16 bytes.
+__device__ __forceinline__ uint32_t smem_u32(const void *p)
+{
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+// makes initialised barriers visible to the copy engine
+__device__ __forceinline__ void mbar_init_fence()
+{
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+// the issuing thread's arrival, announcing `bytes` of copies to complete
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes, uint64_t *bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+// orders this thread's earlier shared-memory accesses (and those a barrier
+// made it wait for) before the copies it issues next
+__device__ __forceinline__ void fence_proxy_async_smem()
+{
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
+{
+    uint32_t done;
+    asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+                 " selp.u32 %0, 1, 0, p;\n}"
+                 : "=r"(done)
+                 : "r"(smem_u32(bar)), "r"(parity)
+                 : "memory");
+    return done != 0;
+}
+__device__ __forceinline__ uint64_t global_ns()
+{
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+// Waits until phase `parity` of `bar` completes, for at most limit_ns
+// nanoseconds; false when it gave up.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint64_t limit_ns)
+{
+    if (mbar_try_wait(bar, parity)) return true;
+    const uint64_t t0 = global_ns();
+    while (!mbar_try_wait(bar, parity))
+        if (global_ns() - t0 > limit_ns) return false;
+    return true;
+}
+// The per-particle arrays that the force kernel copies in tiles are
+// allocated in whole multiples of ROW_PAD rows, so that a tile's copy never
+// reads past its array.
+constexpr uint32_t ROW_PAD = 128;
+__host__ __device__ constexpr size_t padded_rows(size_t n) { return (n + ROW_PAD - 1) / ROW_PAD * ROW_PAD; }
+
+// How long a kernel waits for a bulk copy before it reports ST_TIMEOUT.
+constexpr uint64_t BULK_WAIT_NS = 1000000000ull;
 
 // The slot rule fills the last empty slot first (src/contactsearch.cuh:
 // 252-271), so a particle's few contacts sit in the top slots: the tile rows

@@ -108,7 +108,8 @@ __device__ __forceinline__ WallOut contact_wall(const Params &P, double ra, doub
 // 2, else x = L.x and x = 0), and with periodic == 0 or 2 the y walls
 // (dynamic walls 3 and 4, else y = L.y and y = 0).  Wall k's gap, normal and
 // velocity; a dynamic wall replaces the default in order.
-__device__ __forceinline__ double wall_gap(const Params &P, const Walls &W, int k, double4 xa)
+template <class PS>
+__device__ __forceinline__ double wall_gap(const PS &P, const Walls &W, int k, double4 xa)
 {
     auto wpos = [&](int j, double dflt) { return ((uint32_t)j < P.nw) ? W.nx[j].w : dflt; };
     const double ra = xa.w;
@@ -123,7 +124,8 @@ __device__ __forceinline__ double wall_gap(const Params &P, const Walls &W, int 
 }
 
 // Bit k: the particle touches wall k (its gap is negative).
-__device__ __forceinline__ uint32_t wall_touch(const Params &P, const Walls &W, double4 xa)
+template <class PS>
+__device__ __forceinline__ uint32_t wall_touch(const PS &P, const Walls &W, double4 xa)
 {
     const int nwall = (P.periodic == 0) ? 6 : ((P.periodic == 2) ? 6 : 2);
     uint32_t m = 0;
@@ -806,6 +808,76 @@ struct ForceArgs {
     int a;              // read buffer (start of step); the kernel writes buffer 1-a
     int write_outputs;  // store force/torque/acc/angacc/edp of this step
     int tape_step;      // differentiable step: tape row to record, or -1
+    ForceConsts fc;     // single-scene contexts: the scene's constants
+};
+
+// Where the force kernels read a particle's own start-of-step rows: global
+// memory (GlobalRows) or a tile of rows staged in shared memory (TileRows).
+struct GlobalRows {
+    const Dev &d;
+    int A;
+    uint32_t s;
+    __device__ double4 xr() const { return d.xr[A][s]; }
+    __device__ double4 vel() const { return ld4(d.vel[A], s); }
+    __device__ double4 angvel() const { return ld4(d.angvel[A], s); }
+    __device__ P3 angpos() const { return d.angpos[s]; }
+    __device__ P3 angvel0() const { return d.angvel0[s]; }
+    __device__ P3 vel0() const { return d.vel0[s]; }
+    __device__ double2 xysum() const { return d.xysum[s]; }
+    __device__ uint32_t pos() const { return d.pos[s]; }
+    __device__ float disp() const { return d.disp[s]; }
+    __device__ uint32_t cell() const { return d.cell[s]; }
+    __device__ uint8_t fixed() const { return d.fixed[s]; }
+    __device__ uint8_t wtouch() const { return d.wtouch[s]; }
+};
+
+// Particles per tile of the tiled force kernel (one thread each), a multiple
+// of 32; the per-particle arrays it stages are allocated in whole tiles.
+#ifndef SPHK_FORCE_TILE
+#define SPHK_FORCE_TILE 128
+#endif
+constexpr uint32_t FT_TILE = SPHK_FORCE_TILE;
+static_assert(FT_TILE % 32 == 0 && ROW_PAD % FT_TILE == 0, "force tiles are whole warps of a padded array");
+// Resident tiles per SM: two stages of a tile are ~45.5 KB of shared memory.
+#ifndef SPHK_FORCE_TILE_BLOCKS
+#define SPHK_FORCE_TILE_BLOCKS (512 / SPHK_FORCE_TILE)
+#endif
+
+// The start-of-step rows of FT_TILE consecutive particles, each array one
+// bulk copy (every member a multiple of 16 bytes).
+struct __align__(16) ForceTile {
+    double4 xr[FT_TILE];
+    P3 vel[FT_TILE], angvel[FT_TILE], angpos[FT_TILE], angvel0[FT_TILE], vel0[FT_TILE];
+    double2 xysum[FT_TILE];
+    uint32_t pos[FT_TILE], cell[FT_TILE];
+    float disp[FT_TILE];
+    uint8_t fixed[FT_TILE], wtouch[FT_TILE];
+};
+static_assert(sizeof(ForceTile) % 16 == 0 && (FT_TILE % 16) == 0, "bulk copies are multiples of 16 bytes");
+
+struct TileRows {
+    const ForceTile &T;
+    uint32_t r;
+    __device__ double4 xr() const { return T.xr[r]; }
+    __device__ double4 vel() const
+    {
+        const P3 v = T.vel[r];
+        return make_double4(v.x, v.y, v.z, 0.0);
+    }
+    __device__ double4 angvel() const
+    {
+        const P3 v = T.angvel[r];
+        return make_double4(v.x, v.y, v.z, 0.0);
+    }
+    __device__ P3 angpos() const { return T.angpos[r]; }
+    __device__ P3 angvel0() const { return T.angvel0[r]; }
+    __device__ P3 vel0() const { return T.vel0[r]; }
+    __device__ double2 xysum() const { return T.xysum[r]; }
+    __device__ uint32_t pos() const { return T.pos[r]; }
+    __device__ float disp() const { return T.disp[r]; }
+    __device__ uint32_t cell() const { return T.cell[r]; }
+    __device__ uint8_t fixed() const { return T.fixed[r]; }
+    __device__ uint8_t wtouch() const { return T.wtouch[r]; }
 };
 
 // MODEL: the contact model (1, 2 or 3), a template argument so that each
@@ -817,13 +889,16 @@ struct ForceArgs {
 // Everything per particle after the slot sums (F, T, p, ev_dot, es_dot):
 // the walls, the bonds, the energy sums, the half-step leapfrog, the
 // displacement bound and the cell of the new position.  xa, vel_a and
-// angvel_a4 are the particle's start-of-step rows of buffer A; the new state
-// goes to buffer 1 - A.
-template <bool BATCH, bool DIFF>
-__device__ __forceinline__ void particle_tail(const Dev &d, const Params &P, uint32_t s, int A,
-                                              int write_outputs, double4 xa, double4 vel_a,
-                                              double4 angvel_a4, d3 F, d3 T, double p,
-                                              double ev_dot, double es_dot)
+// angvel_a4 are the particle's start-of-step rows of buffer A, R reads its
+// other rows; the new state goes to buffer 1 - A.
+// P: the particle's scene constants (Params, or a launch's ForceConsts);
+// restart: this step starts a Verlet epoch (Verlet::all_rebuild).
+template <bool BATCH, bool DIFF, class Rows, class PS>
+__device__ __forceinline__ void particle_tail(const Dev &d, const PS &P, uint32_t s, int A,
+                                              int write_outputs, bool restart, double4 xa,
+                                              double4 vel_a, double4 angvel_a4, d3 F, d3 T,
+                                              double p, double ev_dot, double es_dot,
+                                              const Rows &R)
 {
     const int B = 1 - A;
     const double ra = xa.w;
@@ -847,7 +922,8 @@ __device__ __forceinline__ void particle_tail(const Dev &d, const Params &P, uin
         // (nearly all) takes no call
         const uint32_t touch = wall_touch(P, *d.walls, xa);
         if (touch) {
-            const WallSums ws = wall_forces(P, *d.walls, touch, xa, vel_a, angvel_a4, F, T, p);
+            const WallSums ws = wall_forces(prm_at<BATCH>(d, s), *d.walls, touch, xa, vel_a,
+                                            angvel_a4, F, T, p);
             F = ws.F;
             T = ws.T;
             p = ws.p;
@@ -892,7 +968,7 @@ __device__ __forceinline__ void particle_tail(const Dev &d, const Params &P, uin
         d.edp[s] = make_double4(es_dot, ev_dot, p, 0.0);
     }
     if (P.nw > 0) {
-        const uint8_t touched = d.wtouch[s];
+        const uint8_t touched = R.wtouch();
         if (w0f != 0.0 || touched) {
             const uint32_t u = d.uid[s];
             d.wf_pp[u] = w0f;
@@ -907,9 +983,9 @@ __device__ __forceinline__ void particle_tail(const Dev &d, const Params &P, uin
     // Every expression keeps the reference's operands and order.
     const double radius = xa.w;
     const double m = 4.0 / 3.0 * REF_PI * radius * radius * radius * P.rho;
-    const bool fixed = d.fixed[s] != 0;   // fixvel > 0
+    const bool fixed = R.fixed() != 0;   // fixvel > 0
     {
-        P3 angpos = d.angpos[s], angvel0 = d.angvel0[s];
+        P3 angpos = R.angpos(), angvel0 = R.angvel0();
         double4 angacc;
         angacc.x = T.x * 1.0 / (2.0 / 5.0 * m * radius * radius);
         angacc.y = T.y * 1.0 / (2.0 / 5.0 * m * radius * radius);
@@ -935,7 +1011,7 @@ __device__ __forceinline__ void particle_tail(const Dev &d, const Params &P, uin
         }
     }
     double4 x = xa, vel = vel_a;
-    P3 vel0 = d.vel0[s];
+    P3 vel0 = R.vel0();
     double4 acc;
     acc.x = F.x / m;
     acc.y = F.y / m;
@@ -972,7 +1048,7 @@ __device__ __forceinline__ void particle_tail(const Dev &d, const Params &P, uin
     xys.x += vel.x * dt;
     xys.y += vel.y * dt;
     {
-        const double2 o = d.xysum[s];
+        const double2 o = R.xysum();
         d.xysum[s] = make_double2(o.x + xys.x, o.y + xys.y);
     }
     d.xr[B][s] = x;
@@ -980,14 +1056,14 @@ __device__ __forceinline__ void particle_tail(const Dev &d, const Params &P, uin
     d.vel0[s] = vel0;
     // float copy for the next step's contact search, at this particle's
     // cell-list position (rewritten by the rebuild when the order changes)
-    d.xs[B][d.pos[s]] = make_float4((float)x.x, (float)x.y, (float)x.z, (float)x.w);
+    d.xs[B][R.pos()] = make_float4((float)x.x, (float)x.y, (float)x.z, (float)x.w);
 
     // ---- displacement bound since the Verlet epoch started ----------------
     Verlet &V = *d.vs;
     if (P.skin > 0.0) {
         const double ix = vel0.x * dt, iy = vel0.y * dt, iz = vel0.z * dt;
         const float inc = __fadd_ru(__fmul_ru((float)sqrt(ix * ix + iy * iy + iz * iz), 1.0001f), 1e-15f);
-        const float dnew = __fadd_ru(V.all_rebuild ? 0.0f : d.disp[s], inc);
+        const float dnew = __fadd_ru(restart ? 0.0f : R.disp(), inc);
         d.disp[s] = dnew;
         const uint32_t bits = __reduce_max_sync(__activemask(), __float_as_uint(dnew));
         if ((threadIdx.x & 31u) == (uint32_t)(__ffs(__activemask()) - 1)) atomicMax(&V.dmax_bits, bits);
@@ -1000,7 +1076,7 @@ __device__ __forceinline__ void particle_tail(const Dev &d, const Params &P, uin
     if (!grid_cell(P, x.x, x.y, x.z, c)) { err |= ST_OUT_OF_GRID; c = d.ncells_all; }
     else c += P.cell_base;
     d.outside[s] = cell_outside(P, x.x, x.y, x.z) ? 1 : 0;
-    const uint32_t c_old = d.cell[s];
+    const uint32_t c_old = R.cell();
     if (c != c_old) {
         d.cell[s] = c;
         *d.rebuild = 1u;
@@ -1013,27 +1089,64 @@ __device__ __forceinline__ void particle_tail(const Dev &d, const Params &P, uin
     if (err) atomicOr(d.status, err);
 }
 
-template <int MODEL, bool BATCH, bool DIFF>
-__global__ void __launch_bounds__(FORCE_BLOCK, SPHK_FORCE_MIN_BLOCKS)
-k_force(ForceArgs args)
+// Everything of one particle s after the contact search, outside the
+// differentiable step: its slot sums (k_contact's, or k_topo's for model 1)
+// and particle_tail.  f: the chunk flag of s (Dev::cflag[s / 32], read by
+// the caller ahead of the rows); restart: Verlet::all_rebuild.
+template <int MODEL, bool BATCH, class Rows>
+__device__ __forceinline__ void force_row(const ForceArgs &args, uint32_t s, const Rows &R,
+                                          uint8_t f, bool restart)
 {
     const Dev &d = args.d;
-    const uint32_t np = d.np_all;
-    const uint32_t s = blockIdx.x * FORCE_BLOCK + threadIdx.x;
-    if (s >= np) return;
     // A chunk k_contact visited (flag 2: a contact remains, 3: none does)
     // has the slot sums of its particles in Dev::csum_*; its flag goes back
     // to 1 or 0 for the next step's search.  A warp is one chunk, so the
     // flag is the warp's.
     bool visited = false;
-    if constexpr (MODEL != 1 && !DIFF) {
-        const uint8_t f = d.cflag[s >> 5];
+    if constexpr (MODEL != 1) {
         visited = f >= 2;
         if (visited) {
             __syncwarp(__activemask());
             if ((s & 31u) == 0) d.cflag[s >> 5] = (f == 2) ? 1 : 0;
         }
     }
+    const double4 xa = R.xr();
+    const double4 vel_a = R.vel();
+    const double4 angvel_a4 = R.angvel();
+    d3 F = mk(0.0, 0.0, 0.0), T = mk(0.0, 0.0, 0.0);
+    double es_dot = 0.0f, ev_dot = 0.0f, p = 0.0f;
+    if (MODEL == 1) {
+        const double4 c = d.c1acc[s];
+        F = mk(c.x, c.y, c.z);
+        p = c.w;
+    } else if (visited && d.cmask[s] != 0u) {
+        // the sums of a particle that still holds a slot (with every slot
+        // freed nothing was added: the sums are zero)
+        const double4 cf = d.csum_f[s], ct = d.csum_t[s];
+        F = mk(cf.x, cf.y, cf.z);
+        p = cf.w;
+        T = mk(ct.x, ct.y, ct.z);
+        ev_dot = ct.w;
+        es_dot = d.csum_es[s];
+    }
+    if constexpr (BATCH)
+        particle_tail<true, false>(d, prm_at<true>(d, s), s, args.a, args.write_outputs, restart, xa,
+                                   vel_a, angvel_a4, F, T, p, ev_dot, es_dot, R);
+    else
+        particle_tail<false, false>(d, args.fc, s, args.a, args.write_outputs, restart, xa, vel_a,
+                                    angvel_a4, F, T, p, ev_dot, es_dot, R);
+}
+
+// The differentiable step's force kernel: one thread per particle, rows
+// read from global memory, its own slot laws (contact model 2 in exact FP64
+// with per-particle friction), recording the tape.
+__global__ void __launch_bounds__(FORCE_BLOCK, SPHK_FORCE_MIN_BLOCKS)
+k_force_diff(ForceArgs args)
+{
+    const Dev &d = args.d;
+    const uint32_t np = d.np_all;
+    const uint32_t s = blockIdx.x * FORCE_BLOCK + threadIdx.x;
+    if (s >= np) return;
 #ifndef SPHK_NO_PREFETCH
     // The state the integration reads comes after the contact work and
     // after stores the compiler may not move loads across, so each of its
@@ -1048,21 +1161,21 @@ k_force(ForceArgs args)
         bulk_prefetch_l2(d.disp + s, 32 * sizeof(float));
         bulk_prefetch_l2(d.cell + s, 32 * sizeof(uint32_t));
         bulk_prefetch_l2(d.fixed + s, 32);
-        if (d.wtouch) bulk_prefetch_l2(d.wtouch + s, 32);
+        bulk_prefetch_l2(d.wtouch + s, 32);
     }
 #endif
-    const Params &P = prm_at<BATCH>(d, s);
-    const int A = args.a;
-    const double4 xa = d.xr[A][s];
-    const double ra = xa.w;
-    const double4 vel_a = ld4(d.vel[A], s);
-    const double4 angvel_a4 = ld4(d.angvel[A], s);
-    d3 F = mk(0.0, 0.0, 0.0), T = mk(0.0, 0.0, 0.0);
-    double es_dot = 0.0f, ev_dot = 0.0f, p = 0.0f;
-
-    // ---- interact: occupied slots in slot order (the differentiable step;
-    // models 2 and 3 run k_contact, model 1 sums in k_topo) -----------------
-    if constexpr (DIFF) {
+    const GlobalRows R{d, args.a, s};
+    const bool restart = d.vs->all_rebuild != 0u;
+    {
+        const Params &P = *d.prm;
+        const int A = args.a;
+        const double4 xa = d.xr[A][s];
+        const double ra = xa.w;
+        const double4 vel_a = ld4(d.vel[A], s);
+        const double4 angvel_a4 = ld4(d.angvel[A], s);
+        d3 F = mk(0.0, 0.0, 0.0), T = mk(0.0, 0.0, 0.0);
+        double es_dot = 0.0f, ev_dot = 0.0f, p = 0.0f;
+        // ---- interact: occupied slots in slot order ----------------------
         uint32_t occ = d.cmask[s];
         const int j = args.tape_step;
         const size_t row = (j >= 0) ? ((size_t)j * np + s) : 0;
@@ -1117,24 +1230,83 @@ k_force(ForceArgs args)
             d.tp_mask[row] = lawmask;
             d.tp_dmc[row] = dmw;
         }
-    } else if (MODEL == 1) {
-        const double4 c = d.c1acc[s];
-        F = mk(c.x, c.y, c.z);
-        p = c.w;
-    } else if (visited && d.cmask[s] != 0u) {
-        // the sums of a particle that still holds a slot (with every slot
-        // freed nothing was added: the sums are zero)
-        const double4 cf = d.csum_f[s], ct = d.csum_t[s];
-        F = mk(cf.x, cf.y, cf.z);
-        p = cf.w;
-        T = mk(ct.x, ct.y, ct.z);
-        ev_dot = ct.w;
-        es_dot = d.csum_es[s];
+        particle_tail<false, true>(d, P, s, A, args.write_outputs, restart, xa, vel_a, angvel_a4, F,
+                                   T, p, ev_dot, es_dot, R);
     }
-    particle_tail<BATCH, DIFF>(d, P, s, A, args.write_outputs, xa, vel_a, angvel_a4, F, T, p,
-                               ev_dot, es_dot);
 }
 
+// Issues the bulk copies of tile t's rows into T, completing on `bar`.
+__device__ __forceinline__ void stage_force_tile(const Dev &d, int A, uint32_t t, ForceTile &T,
+                                                 uint64_t *bar)
+{
+    const size_t s0 = (size_t)t * FT_TILE;
+    mbar_expect_tx(bar, (uint32_t)sizeof(ForceTile));
+    bulk_load(T.xr, d.xr[A] + s0, sizeof(T.xr), bar);
+    bulk_load(T.vel, d.vel[A] + s0, sizeof(T.vel), bar);
+    bulk_load(T.angvel, d.angvel[A] + s0, sizeof(T.angvel), bar);
+    bulk_load(T.angpos, d.angpos + s0, sizeof(T.angpos), bar);
+    bulk_load(T.angvel0, d.angvel0 + s0, sizeof(T.angvel0), bar);
+    bulk_load(T.vel0, d.vel0 + s0, sizeof(T.vel0), bar);
+    bulk_load(T.xysum, d.xysum + s0, sizeof(T.xysum), bar);
+    bulk_load(T.pos, d.pos + s0, sizeof(T.pos), bar);
+    bulk_load(T.cell, d.cell + s0, sizeof(T.cell), bar);
+    bulk_load(T.disp, d.disp + s0, sizeof(T.disp), bar);
+    bulk_load(T.fixed, d.fixed + s0, sizeof(T.fixed), bar);
+    bulk_load(T.wtouch, d.wtouch + s0, sizeof(T.wtouch), bar);
+}
+
+// k_force_tiles: force_row over tiles of FT_TILE particles, a resident grid
+// of blocks (one thread per particle of a tile), each taking tiles
+// blockIdx.x, blockIdx.x + gridDim.x, ...  The particle's own rows (372 of
+// the 372 + 189 bytes a particle moves) arrive by bulk copies into one of
+// two shared-memory stages: while a block integrates one tile, the copy
+// engine fetches its next, so the bytes in flight do not depend on how many
+// threads are resident.  The per-particle arrays are allocated in whole
+// tiles (ROW_PAD), so every copy is a whole tile.  A copy that has not
+// landed after BULK_WAIT_NS stops the block with ST_TIMEOUT.
+template <int MODEL, bool BATCH>
+__global__ void __launch_bounds__(FT_TILE, SPHK_FORCE_TILE_BLOCKS)
+k_force_tiles(ForceArgs args)
+{
+    __shared__ ForceTile tiles[2];
+    __shared__ uint64_t full[2];
+    const Dev &d = args.d;
+    const uint32_t np = d.np_all;
+    const uint32_t ntiles = (np + FT_TILE - 1) / FT_TILE;
+    const uint32_t tid = threadIdx.x;
+    const int A = args.a;
+    if (tid == 0) {
+        mbar_init(&full[0], 1);
+        mbar_init(&full[1], 1);
+        mbar_init_fence();
+    }
+    __syncthreads();
+    uint32_t t = blockIdx.x;
+    if (tid == 0 && t < ntiles) stage_force_tile(d, A, t, tiles[0], &full[0]);
+    const bool restart = d.vs->all_rebuild != 0u;
+    for (uint32_t it = 0; t < ntiles; t += gridDim.x, ++it) {
+        const uint32_t k = it & 1u;
+        const uint32_t tn = t + gridDim.x;
+        // stage k ^ 1 was read in the previous round, which ended at a barrier
+        if (tid == 0 && tn < ntiles) {
+            fence_proxy_async_smem();
+            stage_force_tile(d, A, tn, tiles[k ^ 1u], &full[k ^ 1u]);
+        }
+        const uint32_t s = t * FT_TILE + tid;
+        // the chunk flag comes from global memory: asked for before the wait
+        const uint8_t f = (MODEL != 1 && s < np) ? d.cflag[s >> 5] : (uint8_t)0;
+        const bool ready = mbar_wait(&full[k], (it >> 1) & 1u, BULK_WAIT_NS);
+        if (ready && s < np) force_row<MODEL, BATCH>(args, s, TileRows{tiles[k], tid}, f, restart);
+        if (__syncthreads_or(!ready)) {
+            if (tid == 0) {
+                atomicOr(d.status, ST_TIMEOUT);
+                // the copies of the next tile land before the block leaves
+                if (tn < ntiles) mbar_wait(&full[k ^ 1u], ((it + 1) >> 1) & 1u, BULK_WAIT_NS);
+            }
+            return;
+        }
+    }
+}
 
 struct ContactArgs {
     Dev d;
@@ -1431,27 +1603,46 @@ void launch_topo(const Dev &d, uint32_t np, bool visc, int a, cudaStream_t st)
     else launch_topo_as<topo_block(0)>(d, np, visc, a, st);
 }
 
-void launch_force(const Dev &d, uint32_t np, int model, int a, int write_outputs, cudaStream_t st)
+// Blocks of k_force_tiles: as many as fit on the device at once, no more
+// than there are tiles.
+template <int MODEL, bool BATCH>
+static void launch_force_tiles(const ForceArgs &args, uint32_t np, cudaStream_t st)
 {
-    ForceArgs args{d, a, write_outputs, -1};
-    const unsigned grid = div_up(np, FORCE_BLOCK);
-    if (d.inst)   // batched contexts: contact model 2 only
-        k_force<2, true, false><<<grid, FORCE_BLOCK, 0, st>>>(args);
-    else if (d.mu_p)   // the differentiable step
-        k_force<2, false, true><<<grid, FORCE_BLOCK, 0, st>>>(args);
-    else if (model == 1)
-        k_force<1, false, false><<<grid, FORCE_BLOCK, 0, st>>>(args);
-    else if (model == 3)
-        k_force<3, false, false><<<grid, FORCE_BLOCK, 0, st>>>(args);
-    else
-        k_force<2, false, false><<<grid, FORCE_BLOCK, 0, st>>>(args);
+    static int per_sm = 0, nsm = 0;
+    if (per_sm == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_force_tiles<MODEL, BATCH>, FT_TILE, 0);
+        if (per_sm < 1) per_sm = 1;
+    }
+    const uint32_t ntiles = div_up(np, FT_TILE);
+    const uint32_t grid = std::min<uint32_t>(ntiles, (uint32_t)(per_sm * nsm));
+    if (grid) k_force_tiles<MODEL, BATCH><<<grid, FT_TILE, 0, st>>>(args);
+}
+
+void launch_force(const Dev &d, const Params &hp, uint32_t np, int model, int a, int write_outputs,
+                  cudaStream_t st)
+{
+    ForceArgs args{d, a, write_outputs, -1, force_consts(hp)};
+    if (d.inst) {   // batched contexts: contact model 2 only
+        launch_force_tiles<2, true>(args, np, st);
+    } else if (d.mu_p) {   // the differentiable step
+        k_force_diff<<<div_up(np, FORCE_BLOCK), FORCE_BLOCK, 0, st>>>(args);
+    } else if (model == 1) {
+        launch_force_tiles<1, false>(args, np, st);
+    } else if (model == 3) {
+        launch_force_tiles<3, false>(args, np, st);
+    } else {
+        launch_force_tiles<2, false>(args, np, st);
+    }
 }
 
 // The differentiable step, recording tape row `tape_step`.
 void launch_force_tape(const Dev &d, uint32_t np, int a, int tape_step, cudaStream_t st)
 {
-    ForceArgs args{d, a, 0, tape_step};
-    k_force<2, false, true><<<div_up(np, FORCE_BLOCK), FORCE_BLOCK, 0, st>>>(args);
+    ForceArgs args{d, a, 0, tape_step, ForceConsts{}};
+    k_force_diff<<<div_up(np, FORCE_BLOCK), FORCE_BLOCK, 0, st>>>(args);
 }
 
 // The slot forces of contact models 2 and 3; model 1 has no slots (k_topo
