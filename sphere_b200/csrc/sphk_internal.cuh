@@ -204,7 +204,7 @@ struct Dev {
     uint32_t *alias_any;  // some particle sits outside its cell's box (set by the rebuild)
     // Verlet lists
     uint32_t *vl;         // tiled, VL_CAP per particle: candidate storage indices, in visiting order
-    uint16_t *vl_meta;    // tiled, VL_CAP per particle: stencil cell (0..26) | shift code << 5
+    uint32_t *vl_meta;    // tiled, VL_CAP per particle: vl_meta_of(stencil cell, shift code, gap)
     uint8_t *vl_len;      // [np] list length or VL_NONE
     float *vl_gap;        // [np] lower bound of the smallest gap to a listed candidate
     float *disp;          // [np] displacement bound since the epoch started
@@ -412,6 +412,18 @@ constexpr uint64_t BULK_WAIT_NS = 1000000000ull;
 // 252-271), so a particle's few contacts sit in the top slots: the tile rows
 // worth fetching ahead are the top PF_SLOTS.
 constexpr uint32_t PF_SLOTS = 8;
+
+// The metadata of a Verlet-list entry: bits 0-4 the stencil cell (0..26),
+// 5-15 the periodic shift code, 16-31 the top half of the float gap to the
+// candidate when the list was recorded (a lower bound: the float's low half
+// is dropped, toward zero, and a negative gap is kept as 0).
+__device__ __forceinline__ uint32_t vl_meta_of(uint32_t slot, uint32_t code, float gap)
+{
+    const uint32_t g = __float_as_uint(fmaxf(gap, 0.0f)) & 0xffff0000u;
+    return slot | (code << 5) | g;
+}
+__device__ __forceinline__ uint32_t vl_code(uint32_t meta) { return (meta & 0xffffu) >> 5; }
+__device__ __forceinline__ float vl_gap_of(uint32_t meta) { return __uint_as_float(meta & 0xffff0000u); }
 
 // Entry e of particle s's Verlet list (Dev::vl, Dev::vl_meta): tiled like
 // the slots, or (SPHK_VL_ROWS) one row of VL_CAP entries per particle.

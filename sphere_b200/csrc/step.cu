@@ -45,10 +45,13 @@ constexpr int FORCE_BLOCK = SPHK_FORCE_BLOCK;
 // The contact search and the contact forces are compiled in two block
 // shapes each, and a context picks one pair (Dev::shape, SPH_OPT_BLOCK_SHAPES;
 // the ensemble's autotuner times both).  Shape 0, the default: k_topo in
-// blocks of 64 threads, 20 per SM, whose threads leave at different times;
-// k_contact in blocks of 4 warps, 4 per SM.  Shape 1: k_topo in 128 x 10,
+// blocks of 64 threads, 16 per SM, whose threads leave at different times;
+// k_contact in blocks of 4 warps, 4 per SM.  Shape 1: k_topo in 128 x 8,
 // k_contact in 2 warps x 8.  The threads resident per SM are the same.
-constexpr int TOPO_THREADS_PER_SM = 1280;
+#ifndef SPHK_TOPO_THREADS_PER_SM
+#define SPHK_TOPO_THREADS_PER_SM 1024
+#endif
+constexpr int TOPO_THREADS_PER_SM = SPHK_TOPO_THREADS_PER_SM;
 constexpr int CONTACT_THREADS_PER_SM = 512;
 __host__ __device__ constexpr int topo_block(uint32_t shape) { return shape ? 128 : 64; }
 __host__ __device__ constexpr int contact_block(uint32_t shape) { return shape ? 64 : 128; }
@@ -523,41 +526,14 @@ __device__ __forceinline__ float moved_bound(const Dev &d, uint32_t s, const Ver
 // VISC (contact model 1): no slots; every candidate within ra + rb + db is
 // processed in visiting order and the contact force and pressure sums are
 // left in Dev::c1acc for k_force.
+// The contact search of one particle s whose list decision (k_topo) did not
+// settle it: list_ok, its Verlet list is valid; held, Dev::settled[s].
 template <bool VISC, bool BATCH, int TB>
-__global__ void __launch_bounds__(TB, TOPO_THREADS_PER_SM / TB)
-k_topo(Dev d, int A)
+__device__ __forceinline__ void topo_search(const Dev &d, int A, uint32_t s, int tid, uint32_t *srow,
+                                            bool list_ok, bool held)
 {
-    __shared__ uint32_t srow[NC * TB];
-    const uint32_t np = d.np_all;
-    const int tid = threadIdx.x;
-    const uint32_t s = blockIdx.x * TB + tid;
-    if (s == 0) {
-        // the movers of the last step have been consumed by the rebuild
-        d.vs->nmovers = 0u;
-        d.vs->movers_overflow = 0u;
-    }
-    if (s >= np) return;
     const Params &P = prm_at<BATCH>(d, s);
-    const Verlet &V = *d.vs;
-    // The list decision first, from a few bytes: a valid list whose gap
-    // bound rules out every contact ends the particle's work here.  Its four
-    // per-particle loads are unconditional so that they are in flight
-    // together, one memory latency instead of a chain of them.
-    const uint8_t len = d.vl_len[s];
-    const uint8_t outs = d.outside[s];
-    const float gap = d.vl_gap[s];
-    const uint8_t held = VISC ? 0 : d.settled[s];
-    const float bound = moved_bound(d, s, V);
-    bool list_ok = P.skin > 0.0 && !V.all_rebuild && len != VL_NONE && outs == 0;
-    if (list_ok && V.dirty_step == V.step) list_ok = d.dirty[d.cell[s]] != V.step;
-    // A valid list whose candidates all hold their slots (Dev::settled) is
-    // settled too: the reference's topology would find every overlap among
-    // them (the list holds every possible one) already in its slot and
-    // change nothing.
-    if (list_ok && (gap > bound || held)) {
-        if (VISC) d.c1acc[s] = make_double4(0.0, 0.0, 0.0, 0.0);
-        return;
-    }
+    const uint32_t len = d.vl_len[s];
     // After a position left the grid (the step reports SPH_ERR_OUT_OF_GRID)
     // the scene has come apart: saturated cell ids pile its particles into
     // the edge cells, where the stencil sweep grows with the square of their
@@ -587,7 +563,7 @@ k_topo(Dev d, int A)
     if (VISC && list_ok) {
         for (uint32_t e = 0; e < len; ++e) {
             const size_t at = vl_at(s, e);
-            visc_pair(d, A, s, d.vl[at], (uint32_t)d.vl_meta[at] >> 5, F1, p1);
+            visc_pair(d, A, s, d.vl[at], vl_code(d.vl_meta[at]), F1, p1);
         }
     } else if (list_ok) {
         // the list is read four entries at a time, so that their loads are
@@ -599,6 +575,11 @@ k_topo(Dev d, int A)
         // while the occupied slots plus the list length stay within NC, no
         // row can fill, so the filter changes nothing.
         const bool filter = ts.occ != 0u && len + (uint32_t)__popc(ts.occ) <= (uint32_t)NC;
+        // A candidate whose own recorded gap exceeds the displacement bound
+        // cannot overlap (nor hold a slot taken since the list was
+        // recorded): its position is not fetched.  Skipping it leaves the
+        // order of the others, and so the slot choice, unchanged.
+        const float bound = moved_bound(d, s, *d.vs);
         uint32_t tv[4], mv[4];
         auto load4 = [&](uint32_t e0) {
 #pragma unroll
@@ -620,11 +601,12 @@ k_topo(Dev d, int A)
                 const uint32_t meta = mv[j];
                 const int slot = (int)(meta & 31u);
                 if (slot == skip_slot) continue;   // nc > NC: rest of that cell
-                const uint32_t t = tv[j], code = meta >> 5;
+                const uint32_t t = tv[j], code = vl_code(meta);
                 if (filter && in_slot<TB>(srow, tid, ts, t, code)) {
                     ++found;
                     continue;
                 }
+                if (vl_gap_of(meta) > bound) continue;
                 if (overlaps(P, xr, t, code, xa) && !topo_insert<TB>(d, srow, tid, s, t, code, ts))
                     skip_slot = slot;
             }
@@ -660,6 +642,7 @@ k_topo(Dev d, int A)
 #pragma unroll
                 for (int j = 0; j < 4; ++j) c[j] = __ldg(&xs[min(base + (uint32_t)j, last)]);
                 uint32_t near = 0, hit = 0;
+                float gj[4];
 #pragma unroll
                 for (int j = 0; j < 4; ++j) {
                     const float fx = (xaf.x - c[j].x) + sx;
@@ -675,8 +658,8 @@ k_topo(Dev d, int A)
                         near |= 1u << j;
                         // the gap, with the cull's float slack taken against
                         // it (over every near candidate: at least the listed)
-                        gmin = fminf(gmin, __fsub_rd(__fmul_rd(__fsqrt_rd(d2), 0.999996f),
-                                                     rr));
+                        gj[j] = __fsub_rd(__fmul_rd(__fsqrt_rd(d2), 0.999996f), rr);
+                        gmin = fminf(gmin, gj[j]);
                     }
                     if (ok && d2 < rr * rr) hit |= 1u << j;
                 }
@@ -691,7 +674,7 @@ k_topo(Dev d, int A)
                     } else if (nlist < VL_CAP) {
                         const size_t at = vl_at(s, nlist);
                         d.vl[at] = t;
-                        d.vl_meta[at] = (uint16_t)(slot | (code << 5));
+                        d.vl_meta[at] = vl_meta_of(slot, code, gj[j]);
                         ++nlist;
                     } else {
                         list_overflow = true;
@@ -801,6 +784,114 @@ k_topo(Dev d, int A)
         if (occ) d.cflag[s >> 5] = 1;
     }
     if (ts.err) atomicOr(d.status, ts.err);
+}
+
+// Particles whose list decision each lane of k_topo makes in one go.
+#ifndef SPHK_TOPO_SPAN
+#define SPHK_TOPO_SPAN 4
+#endif
+constexpr uint32_t TOPO_SPAN = SPHK_TOPO_SPAN;
+
+// k_topo: the contact search, one warp per TOPO_SPAN x 32 consecutive
+// storage indices (storage order, which relayout keeps close to cell order).
+// First every lane makes the list decision of its TOPO_SPAN particles
+// (particle base + 32 j + lane), their loads in flight together; the
+// particles it does not settle are then dealt to the warp's lanes in order,
+// 32 at a time, each searched by topo_search.
+//
+// List mode: while the particle's Verlet list is valid (no epoch restart, no
+// cell of its neighbourhood changed members this step) only the listed
+// candidates are tested, in their recorded order.  The list holds, in the
+// reference's visiting order, every member of the stencil cells that was
+// within ra + rb + skin when it was recorded; a pair missing from it is at
+// least skin - 4 dmax > 0 apart now, so it cannot overlap.
+//
+// Sweep mode: the 27 stencil cells are scanned as in the reference (z, y, x;
+// members by particle index) and the list is recorded on the way.
+//
+// VISC (contact model 1): no slots; every candidate within ra + rb + db is
+// processed in visiting order and the contact force and pressure sums are
+// left in Dev::c1acc for k_force.
+template <bool VISC, bool BATCH, int TB>
+__global__ void __launch_bounds__(TB, TOPO_THREADS_PER_SM / TB)
+k_topo(Dev d, int A)
+{
+    constexpr uint32_t FULL = 0xffffffffu;
+    __shared__ uint32_t srow[NC * TB];
+    const uint32_t np = d.np_all;
+    const int tid = threadIdx.x;
+    const uint32_t lane = (uint32_t)tid & 31u;
+    const uint32_t base = ((blockIdx.x * TB + (uint32_t)tid) >> 5) * (32u * TOPO_SPAN);
+    if (blockIdx.x == 0 && tid == 0) {
+        // the movers of the last step have been consumed by the rebuild
+        d.vs->nmovers = 0u;
+        d.vs->movers_overflow = 0u;
+    }
+    const Verlet &V = *d.vs;
+    // bit j: particle base + 32 j + lane needs the search / has a valid
+    // list / is marked settled
+    uint32_t need = 0, lok = 0, hld = 0;
+#pragma unroll
+    for (uint32_t j = 0; j < TOPO_SPAN; ++j) {
+        const uint32_t s = base + 32u * j + lane;
+        if (s >= np) continue;
+        const Params &P = prm_at<BATCH>(d, s);
+        // The list decision, from a few bytes: a valid list whose gap bound
+        // rules out every contact ends the particle's work here.  Its
+        // per-particle loads are unconditional so that they (and those of
+        // the lane's other particles) are in flight together.
+        const uint8_t len = d.vl_len[s];
+        const uint8_t outs = d.outside[s];
+        const float gap = d.vl_gap[s];
+        const uint8_t held = VISC ? 0 : d.settled[s];
+        const float bound = moved_bound(d, s, V);
+        bool list_ok = P.skin > 0.0 && !V.all_rebuild && len != VL_NONE && outs == 0;
+        if (list_ok && V.dirty_step == V.step) list_ok = d.dirty[d.cell[s]] != V.step;
+        // A valid list whose candidates all hold their slots (Dev::settled) is
+        // settled too: the reference's topology would find every overlap among
+        // them (the list holds every possible one) already in its slot and
+        // change nothing.
+        if (list_ok && (gap > bound || held)) {
+            if (VISC) d.c1acc[s] = make_double4(0.0, 0.0, 0.0, 0.0);
+            continue;
+        }
+        need |= 1u << j;
+        if (list_ok) lok |= 1u << j;
+        if (held) hld |= 1u << j;
+    }
+    // the warp's particles that need the search, in (j, lane) order: the
+    // k-th goes to lane k % 32 in round k / 32
+    uint32_t m[TOPO_SPAN], ml[TOPO_SPAN], mh[TOPO_SPAN];
+    uint32_t total = 0;
+#pragma unroll
+    for (uint32_t j = 0; j < TOPO_SPAN; ++j) {
+        m[j] = __ballot_sync(FULL, (need >> j) & 1u);
+        ml[j] = __ballot_sync(FULL, (lok >> j) & 1u);
+        mh[j] = __ballot_sync(FULL, (hld >> j) & 1u);
+        total += (uint32_t)__popc(m[j]);
+    }
+    for (uint32_t k = lane; k < total; k += 32u) {
+        uint32_t rem = k, sel = 0, selj = 0, sel_l = 0, sel_h = 0;
+        bool got = false;
+#pragma unroll
+        for (uint32_t j = 0; j < TOPO_SPAN; ++j) {
+            const uint32_t c = (uint32_t)__popc(m[j]);
+            if (!got) {
+                if (rem < c) {
+                    sel = m[j];
+                    sel_l = ml[j];
+                    sel_h = mh[j];
+                    selj = j;
+                    got = true;
+                } else {
+                    rem -= c;
+                }
+            }
+        }
+        const uint32_t bit = __fns(sel, 0, (int)rem + 1);
+        const uint32_t s = base + 32u * selj + bit;
+        topo_search<VISC, BATCH, TB>(d, A, s, tid, srow, (sel_l >> bit) & 1u, (sel_h >> bit) & 1u);
+    }
 }
 
 struct ForceArgs {
@@ -1577,7 +1668,8 @@ static unsigned contact_grid(uint32_t np)
 template <int TB>
 static void launch_topo_as(const Dev &d, uint32_t np, bool visc, int a, cudaStream_t st)
 {
-    const unsigned grid = div_up(np, TB);
+    // one warp per TOPO_SPAN x 32 particles
+    const unsigned grid = div_up(div_up(np, 32u * TOPO_SPAN), (uint32_t)TB / 32u);
     if (d.inst)   // batched contexts: contact model 2 only
         k_topo<false, true, TB><<<grid, TB, 0, st>>>(d, a);
     else if (visc)
