@@ -122,6 +122,10 @@ typedef struct sph_stats {
 #define SPH_OPT_PROFILE 3         /* 1: launch kernels one by one with CUDA events around
                                      each phase (the reference's PROFILING switch,
                                      src/debug.h:7, src/device.cu:86-102); 0: graphs */
+#define SPH_OPT_TOPO_SPAN 6       /* particles whose list decision each thread of the contact
+                                     search makes at once: 0 (default) chooses from the
+                                     particle count (4 at 1M on a B200, 1 below ~300k), or
+                                     1, 2, 4; results do not depend on it, only its cost */
 
 /* Phases timed in profile mode. */
 #define SPH_PHASE_CELLS 0   /* cell list rebuild (hash histogram, scan, scatter, sort) */

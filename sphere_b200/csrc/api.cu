@@ -742,6 +742,16 @@ int sph_set_option(sph_ctx *c, int option, int64_t value)
         }
         return SPH_OK;
     }
+    if (option == SPH_OPT_TOPO_SPAN && (value == 0 || value == 1 || value == 2 || value == 4)) {
+        if (c->d.topo_span != (uint32_t)value) {
+            CK(cudaSetDevice(c->device));
+            CK(cudaStreamSynchronize(c->stream));
+            c->d.topo_span = (uint32_t)value;
+            drop_graphs(c);
+            if (!c->batched) return ensure_graphs(c);
+        }
+        return SPH_OK;
+    }
     return fail(c, SPH_ERR_BAD_INPUT, "unknown option or value");
 }
 
@@ -958,6 +968,10 @@ int sph_upload(sph_ctx *c, const sph_host_state *h)
     int rc = do_relayout(c, c->stream);
     if (rc != SPH_OK) return rc;
     c->uploaded = true;
+    // the step graphs carry the force kernel's constants, which the upload
+    // may have changed (the skin): capture them here rather than in the
+    // first sph_step
+    if (!c->batched && (rc = ensure_graphs(c)) != SPH_OK) return rc;
     return sync_status(c);
 }
 

@@ -159,6 +159,7 @@ struct Dev {
     // sizes of the whole context: one scene, or every instance of a batch
     uint32_t np_all, ncells_all, ninst;
     uint32_t shape;       // block shapes of the contact search and forces (SPH_OPT_BLOCK_SHAPES)
+    uint32_t topo_span;   // list decisions per thread of the contact search (0: by size)
     // batched contexts: instance of each storage index and the first global
     // cell id of each instance (ninst + 1 entries); nullptr for one scene
     uint32_t *inst;

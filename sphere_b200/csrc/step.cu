@@ -786,18 +786,15 @@ __device__ __forceinline__ void topo_search(const Dev &d, int A, uint32_t s, int
     if (ts.err) atomicOr(d.status, ts.err);
 }
 
-// Particles whose list decision each lane of k_topo makes in one go.
-#ifndef SPHK_TOPO_SPAN
-#define SPHK_TOPO_SPAN 4
-#endif
-constexpr uint32_t TOPO_SPAN = SPHK_TOPO_SPAN;
+// Most particles whose list decision each lane of k_topo makes in one go.
+constexpr uint32_t TOPO_SPAN_MAX = 4;
 
-// k_topo: the contact search, one warp per TOPO_SPAN x 32 consecutive
-// storage indices (storage order, which relayout keeps close to cell order).
-// First every lane makes the list decision of its TOPO_SPAN particles
-// (particle base + 32 j + lane), their loads in flight together; the
-// particles it does not settle are then dealt to the warp's lanes in order,
-// 32 at a time, each searched by topo_search.
+// k_topo: the contact search, one warp per span x 32 consecutive storage
+// indices (storage order, which relayout keeps close to cell order), span
+// <= TOPO_SPAN_MAX.  First every lane makes the list decision of its span
+// particles (particle base + 32 j + lane), their loads in flight together;
+// the particles it does not settle are then dealt to the warp's lanes in
+// order, 32 at a time, each searched by topo_search.
 //
 // List mode: while the particle's Verlet list is valid (no epoch restart, no
 // cell of its neighbourhood changed members this step) only the listed
@@ -814,14 +811,14 @@ constexpr uint32_t TOPO_SPAN = SPHK_TOPO_SPAN;
 // left in Dev::c1acc for k_force.
 template <bool VISC, bool BATCH, int TB>
 __global__ void __launch_bounds__(TB, TOPO_THREADS_PER_SM / TB)
-k_topo(Dev d, int A)
+k_topo(Dev d, int A, uint32_t span)
 {
     constexpr uint32_t FULL = 0xffffffffu;
     __shared__ uint32_t srow[NC * TB];
     const uint32_t np = d.np_all;
     const int tid = threadIdx.x;
     const uint32_t lane = (uint32_t)tid & 31u;
-    const uint32_t base = ((blockIdx.x * TB + (uint32_t)tid) >> 5) * (32u * TOPO_SPAN);
+    const uint32_t base = ((blockIdx.x * TB + (uint32_t)tid) >> 5) * (32u * span);
     if (blockIdx.x == 0 && tid == 0) {
         // the movers of the last step have been consumed by the rebuild
         d.vs->nmovers = 0u;
@@ -832,8 +829,9 @@ k_topo(Dev d, int A)
     // list / is marked settled
     uint32_t need = 0, lok = 0, hld = 0;
 #pragma unroll
-    for (uint32_t j = 0; j < TOPO_SPAN; ++j) {
+    for (uint32_t j = 0; j < TOPO_SPAN_MAX; ++j) {
         const uint32_t s = base + 32u * j + lane;
+        if (j >= span) break;
         if (s >= np) continue;
         const Params &P = prm_at<BATCH>(d, s);
         // The list decision, from a few bytes: a valid list whose gap bound
@@ -861,10 +859,11 @@ k_topo(Dev d, int A)
     }
     // the warp's particles that need the search, in (j, lane) order: the
     // k-th goes to lane k % 32 in round k / 32
-    uint32_t m[TOPO_SPAN], ml[TOPO_SPAN], mh[TOPO_SPAN];
+    uint32_t m[TOPO_SPAN_MAX], ml[TOPO_SPAN_MAX], mh[TOPO_SPAN_MAX];
     uint32_t total = 0;
 #pragma unroll
-    for (uint32_t j = 0; j < TOPO_SPAN; ++j) {
+    for (uint32_t j = 0; j < TOPO_SPAN_MAX; ++j) {
+        // need, lok and hld have no bit j >= span: those masks are zero
         m[j] = __ballot_sync(FULL, (need >> j) & 1u);
         ml[j] = __ballot_sync(FULL, (lok >> j) & 1u);
         mh[j] = __ballot_sync(FULL, (hld >> j) & 1u);
@@ -874,7 +873,7 @@ k_topo(Dev d, int A)
         uint32_t rem = k, sel = 0, selj = 0, sel_l = 0, sel_h = 0;
         bool got = false;
 #pragma unroll
-        for (uint32_t j = 0; j < TOPO_SPAN; ++j) {
+        for (uint32_t j = 0; j < TOPO_SPAN_MAX; ++j) {
             const uint32_t c = (uint32_t)__popc(m[j]);
             if (!got) {
                 if (rem < c) {
@@ -1665,17 +1664,35 @@ static unsigned contact_grid(uint32_t np)
     return (unsigned)std::min<uint64_t>((uint64_t)resident, div_up(chunks, CB / 32));
 }
 
+// Particles per lane of k_topo's list decisions: 4 once the scene is four
+// times the threads the device holds at once (one decision round then
+// hides the latency of four), 2 from twice, else 1, so that a smaller
+// scene's searches run on as many lanes as it has particles.
+static uint32_t topo_span(uint32_t np)
+{
+    static int nsm = 0;
+    if (nsm == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+        if (nsm < 1) nsm = 1;
+    }
+    const uint64_t resident = (uint64_t)nsm * TOPO_THREADS_PER_SM;
+    return (uint64_t)np >= 4 * resident ? 4u : ((uint64_t)np >= 2 * resident ? 2u : 1u);
+}
+
 template <int TB>
 static void launch_topo_as(const Dev &d, uint32_t np, bool visc, int a, cudaStream_t st)
 {
-    // one warp per TOPO_SPAN x 32 particles
-    const unsigned grid = div_up(div_up(np, 32u * TOPO_SPAN), (uint32_t)TB / 32u);
+    // one warp per span x 32 particles
+    const uint32_t span = d.topo_span ? d.topo_span : topo_span(np);
+    const unsigned grid = div_up(div_up(np, 32u * span), (uint32_t)TB / 32u);
     if (d.inst)   // batched contexts: contact model 2 only
-        k_topo<false, true, TB><<<grid, TB, 0, st>>>(d, a);
+        k_topo<false, true, TB><<<grid, TB, 0, st>>>(d, a, span);
     else if (visc)
-        k_topo<true, false, TB><<<grid, TB, 0, st>>>(d, a);
+        k_topo<true, false, TB><<<grid, TB, 0, st>>>(d, a, span);
     else
-        k_topo<false, false, TB><<<grid, TB, 0, st>>>(d, a);
+        k_topo<false, false, TB><<<grid, TB, 0, st>>>(d, a, span);
 }
 
 template <int CB>

@@ -33,6 +33,7 @@ OPT_GRAPH_STEPS = 2
 OPT_PROFILE = 3
 OPT_VERLET_SKIN = 4
 OPT_BLOCK_SHAPES = 5
+OPT_TOPO_SPAN = 6
 PHASES = ("cells", "bonds", "topo", "force", "walls", "darcy", "contact")
 
 _dp = C.POINTER(C.c_double)
@@ -211,10 +212,12 @@ class Simulation:
 
     def __init__(self, cfg: SceneConfig, device: int = 0, graph_steps: int | None = None,
                  relayout_every: int | None = None, verlet_skin: float | None = None,
-                 block_shapes: int | None = None):
+                 block_shapes: int | None = None, topo_span: int | None = None):
         """``verlet_skin``: Verlet-list skin as a fraction of the largest radius
         (default 0.1; 0 sweeps the full stencil every step).  ``block_shapes``:
-        0 or 1, the compiled block shapes of the contact kernels to use."""
+        0 or 1, the compiled block shapes of the contact kernels to use.
+        ``topo_span``: list decisions per thread of the contact search (0:
+        chosen from the particle count; 1, 2 or 4)."""
         self.lib = load_library()
         self.cfg = cfg
         self._ctx = C.c_void_p()
@@ -230,6 +233,8 @@ class Simulation:
                                                 int(round(verlet_skin * 1000))))
         if block_shapes is not None:
             self._check(self.lib.sph_set_option(self._ctx, OPT_BLOCK_SHAPES, int(block_shapes)))
+        if topo_span is not None:
+            self._check(self.lib.sph_set_option(self._ctx, OPT_TOPO_SPAN, int(topo_span)))
 
     def _check(self, rc):
         if rc != SPH_OK:
@@ -418,7 +423,7 @@ class BatchSimulation(Simulation):
 
     def __init__(self, cfgs, device: int = 0, graph_steps: int | None = None,
                  relayout_every: int | None = None, verlet_skin: float | None = None,
-                 block_shapes: int | None = None):
+                 block_shapes: int | None = None, topo_span: int | None = None):
         self.lib = load_library()
         self.cfgs = list(cfgs)
         self.nps = [c.np for c in self.cfgs]
@@ -439,6 +444,8 @@ class BatchSimulation(Simulation):
                                                 int(round(verlet_skin * 1000))))
         if block_shapes is not None:
             self._check(self.lib.sph_set_option(self._ctx, OPT_BLOCK_SHAPES, int(block_shapes)))
+        if topo_span is not None:
+            self._check(self.lib.sph_set_option(self._ctx, OPT_TOPO_SPAN, int(topo_span)))
 
     def upload(self, states):
         super().upload(pack_states(states))

@@ -116,6 +116,19 @@ def test_second_block_shapes_agree_with_oracle(oracle_libs, name):
     assert mismatches(got, want, ALL) == []
 
 
+@pytest.mark.parametrize("span", [2, 4])
+@pytest.mark.parametrize("name", ["packed", "polydisperse_small", "box_wall", "periodic_crossing"])
+def test_contact_search_spans_agree_with_oracle(oracle_libs, name, span):
+    """The contact search making the list decisions of 2 or 4 particles per
+    thread and dealing the ones that need a search to the warp's lanes (the
+    layout chosen at 1M spheres) gives the oracle's results bit for bit."""
+    sb = SCENES[name]()
+    rc, want, _ = run_oracle(oracle_libs["orc"], sb, 30)
+    assert rc == 0
+    got, _, _ = run_gpu(sb, (11, 19), topo_span=span)
+    assert mismatches(got, want, ALL) == []
+
+
 @pytest.mark.parametrize("name", ["box", "periodic_xy"])
 def test_verlet_epochs_restart_exactly(oracle_libs, name):
     """300 steps: the displacement bound restarts the list epoch several
