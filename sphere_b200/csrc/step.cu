@@ -928,7 +928,7 @@ struct GlobalRows {
 #endif
 constexpr uint32_t FT_TILE = SPHK_FORCE_TILE;
 static_assert(FT_TILE % 32 == 0 && ROW_PAD % FT_TILE == 0, "force tiles are whole warps of a padded array");
-// Resident tiles per SM: two stages of a tile are ~45.5 KB of shared memory.
+// Resident blocks per SM: two stages of a tile are ~45.5 KB of shared memory.
 #ifndef SPHK_FORCE_TILE_BLOCKS
 #define SPHK_FORCE_TILE_BLOCKS (512 / SPHK_FORCE_TILE)
 #endif
@@ -1345,55 +1345,72 @@ __device__ __forceinline__ void stage_force_tile(const Dev &d, int A, uint32_t t
     bulk_load(T.wtouch, d.wtouch + s0, sizeof(T.wtouch), bar);
 }
 
+// Shared-memory stages of k_force_tiles: tiles a block has in flight.
+#ifndef SPHK_FORCE_STAGES
+#define SPHK_FORCE_STAGES 2
+#endif
+constexpr uint32_t FT_STAGES = SPHK_FORCE_STAGES;
+
 // k_force_tiles: force_row over tiles of FT_TILE particles, a resident grid
 // of blocks (one thread per particle of a tile), each taking tiles
 // blockIdx.x, blockIdx.x + gridDim.x, ...  The particle's own rows (372 of
-// the 372 + 189 bytes a particle moves) arrive by bulk copies into one of
-// two shared-memory stages: while a block integrates one tile, the copy
-// engine fetches its next, so the bytes in flight do not depend on how many
-// threads are resident.  The per-particle arrays are allocated in whole
-// tiles (ROW_PAD), so every copy is a whole tile.  A copy that has not
-// landed after BULK_WAIT_NS stops the block with ST_TIMEOUT.
+// the 372 + 189 bytes a particle moves) arrive by bulk copies into a ring of
+// FT_STAGES shared-memory stages: while a block integrates one tile, the
+// copy engine fetches its next ones, so the bytes in flight do not depend on
+// how many threads are resident.  A stage is refilled, FT_STAGES tiles
+// ahead, once the block's barrier shows its tile consumed.  The
+// per-particle arrays are allocated in whole tiles (ROW_PAD), so every copy
+// is a whole tile.  A copy that has not landed after BULK_WAIT_NS stops the
+// block with ST_TIMEOUT, after the copies it issued have landed.
 template <int MODEL, bool BATCH>
 __global__ void __launch_bounds__(FT_TILE, SPHK_FORCE_TILE_BLOCKS)
 k_force_tiles(ForceArgs args)
 {
-    __shared__ ForceTile tiles[2];
-    __shared__ uint64_t full[2];
+    __shared__ ForceTile tiles[FT_STAGES];
+    __shared__ uint64_t full[FT_STAGES];
     const Dev &d = args.d;
     const uint32_t np = d.np_all;
     const uint32_t ntiles = (np + FT_TILE - 1) / FT_TILE;
     const uint32_t tid = threadIdx.x;
     const int A = args.a;
     if (tid == 0) {
-        mbar_init(&full[0], 1);
-        mbar_init(&full[1], 1);
+        for (uint32_t k = 0; k < FT_STAGES; ++k) mbar_init(&full[k], 1);
         mbar_init_fence();
+        // the block's first FT_STAGES tiles
+        for (uint32_t k = 0; k < FT_STAGES; ++k) {
+            const uint32_t tk = blockIdx.x + k * gridDim.x;
+            if (tk < ntiles) stage_force_tile(d, A, tk, tiles[k], &full[k]);
+        }
     }
     __syncthreads();
-    uint32_t t = blockIdx.x;
-    if (tid == 0 && t < ntiles) stage_force_tile(d, A, t, tiles[0], &full[0]);
     const bool restart = d.vs->all_rebuild != 0u;
+    uint32_t t = blockIdx.x;
     for (uint32_t it = 0; t < ntiles; t += gridDim.x, ++it) {
-        const uint32_t k = it & 1u;
-        const uint32_t tn = t + gridDim.x;
-        // stage k ^ 1 was read in the previous round, which ended at a barrier
-        if (tid == 0 && tn < ntiles) {
-            fence_proxy_async_smem();
-            stage_force_tile(d, A, tn, tiles[k ^ 1u], &full[k ^ 1u]);
-        }
+        const uint32_t k = it % FT_STAGES;
         const uint32_t s = t * FT_TILE + tid;
         // the chunk flag comes from global memory: asked for before the wait
         const uint8_t f = (MODEL != 1 && s < np) ? d.cflag[s >> 5] : (uint8_t)0;
-        const bool ready = mbar_wait(&full[k], (it >> 1) & 1u, BULK_WAIT_NS);
+        const bool ready = mbar_wait(&full[k], (it / FT_STAGES) & 1u, BULK_WAIT_NS);
         if (ready && s < np) force_row<MODEL, BATCH>(args, s, TileRows{tiles[k], tid}, f, restart);
         if (__syncthreads_or(!ready)) {
             if (tid == 0) {
                 atomicOr(d.status, ST_TIMEOUT);
-                // the copies of the next tile land before the block leaves
-                if (tn < ntiles) mbar_wait(&full[k ^ 1u], ((it + 1) >> 1) & 1u, BULK_WAIT_NS);
+                // this tile's copies and those issued for the next ones land
+                // before the block leaves
+                for (uint32_t q = 0; q < FT_STAGES; ++q) {
+                    const uint32_t iq = it + q;
+                    if (t + q * gridDim.x < ntiles)
+                        mbar_wait(&full[iq % FT_STAGES], (iq / FT_STAGES) & 1u, BULK_WAIT_NS);
+                }
             }
             return;
+        }
+        // every thread is past its reads of stage k: it takes the tile
+        // FT_STAGES rounds ahead
+        const uint32_t tn = t + FT_STAGES * gridDim.x;
+        if (tid == 0 && tn < ntiles) {
+            fence_proxy_async_smem();
+            stage_force_tile(d, A, tn, tiles[k], &full[k]);
         }
     }
 }
