@@ -25,6 +25,10 @@
 namespace sphk {
 
 constexpr int REV_BLOCK = 128;
+// Resident blocks per SM that k_rev_contacts' register allocation must allow.
+#ifndef SPHK_REV_MIN_BLOCKS
+#define SPHK_REV_MIN_BLOCKS 2
+#endif
 
 __device__ __forceinline__ dl::V3 v3of(double4 a) { return dl::v3(a.x, a.y, a.z); }
 __device__ __forceinline__ double4 d4of(dl::V3 a) { return make_double4(a.x, a.y, a.z, 0.0); }
@@ -72,7 +76,7 @@ __global__ void k_rev_integ(Dev d, AdjDev a, int j)
     a.wb[s] = make_double4(0.0, 0.0, 0.0, 0.0);
 }
 
-__global__ void __launch_bounds__(REV_BLOCK)
+__global__ void __launch_bounds__(REV_BLOCK, SPHK_REV_MIN_BLOCKS)
 k_rev_contacts(Dev d, AdjDev a, int j)
 {
     const uint32_t np = d.np_all;
@@ -85,6 +89,7 @@ k_rev_contacts(Dev d, AdjDev a, int j)
         const dl::V3 va = v3of(va4), wa = v3of(wa4);
         const dl::V3 Fb = v3of(a.Fb[s]), Tb = v3of(a.Tb[s]);
         dl::V3 xbs = dl::v3(0.0, 0.0, 0.0), vbs = xbs, wbs = xbs;
+        double mubs = 0.0;   // the particle's own share of its contacts' friction adjoints
 
         // walls
         WallHits wh;
@@ -108,13 +113,14 @@ k_rev_contacts(Dev d, AdjDev a, int j)
         // -- only where an earlier (later-in-time) step left one
         const uint32_t mask = d.tp_mask[row];
         const ulonglong2 dmw = d.tp_dmc[row];
-        double4 *dtb = a.dtb + (size_t)s * NC;
         for (uint32_t m = a.dtb_mask[s] & ~mask; m; m &= m - 1)
-            dtb[__ffs(m) - 1] = make_double4(0.0, 0.0, 0.0, 0.0);
+            a.dtb[tile_at(s, (uint32_t)(__ffs(m) - 1), NC)] = P3{0.0, 0.0, 0.0};
         if (a.dtb_mask[s] != mask) a.dtb_mask[s] = mask;
         for (uint32_t m = mask; m; m &= m - 1) {
             const int i = __ffs(m) - 1;
-            const uint32_t t = d.tp_partner[row * NC + i];
+            const size_t ts = tape_slot_at((uint32_t)j, np, s, (uint32_t)i);
+            const size_t si = tile_at(s, (uint32_t)i, NC);
+            const uint32_t t = d.tp_partner[ts];
             const size_t rt = (size_t)j * np + t;
             const double4 xb = d.tp_x[rt];
             const uint32_t code = (uint32_t)((i < 16 ? (dmw.x >> (4 * i)) : (dmw.y >> (4 * (i - 16)))) & 0xFull);
@@ -127,23 +133,25 @@ k_rev_contacts(Dev d, AdjDev a, int j)
             in.vb = v3of(d.tp_v[rt]);
             in.wa = wa;
             in.wb = v3of(d.tp_w[rt]);
-            in.d0u = v3of(d.tp_dt0[row * NC + i]);
+            const P3 d0 = d.tp_dt0[ts];
+            in.d0u = dl::v3(d0.x, d0.y, d0.z);
             const dl::Law law{P.k_n, P.k_t, P.gamma_n, P.gamma_t, 0.5 * (d.mu_p[s] + d.mu_p[t]),
                               P.kappa, P.dt};
             dl::PairBar ib;
             dl::LawBar lb{0.0, 0.0, 0.0, 0.0};
-            dl::pair_rev(law, in, Fb, Tb, v3of(dtb[i]), ib, lb);
+            const P3 dtbi = a.dtb[si];
+            dl::pair_rev(law, in, Fb, Tb, dl::v3(dtbi.x, dtbi.y, dtbi.z), ib, lb);
             xbs += ib.xab;
             vbs += ib.va;
             wbs += ib.wa;
             atomic_add3(&a.xb[t], -ib.xab);
             atomic_add3(&a.vb[t], ib.vb);
             atomic_add3(&a.wb[t], ib.wb);
-            dtb[i] = d4of(ib.d0u);
+            a.dtb[si] = P3{ib.d0u.x, ib.d0u.y, ib.d0u.z};
             knb += lb.kn;
             ktb += lb.kt;
             gnb += lb.gn;
-            atomicAdd(&a.mub[s], 0.5 * lb.mu);
+            mubs += 0.5 * lb.mu;
             atomicAdd(&a.mub[t], 0.5 * lb.mu);
         }
         if (mask != 0u || wh.count > 0) {   // nothing to add otherwise
@@ -151,6 +159,7 @@ k_rev_contacts(Dev d, AdjDev a, int j)
             atomic_add3(&a.vb[s], vbs);
             atomic_add3(&a.wb[s], wbs);
         }
+        if (mask != 0u) atomicAdd(&a.mub[s], mubs);
     }
     // parameter adjoints: warp sums, one atomic per warp
 #pragma unroll

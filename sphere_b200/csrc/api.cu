@@ -22,6 +22,7 @@ void launch_walls(const Dev &d, uint32_t np, uint32_t nw, cudaStream_t st);
 void launch_wall_motion(const Dev &d, uint32_t np, cudaStream_t st);
 void launch_tail(const Dev &d, cudaStream_t st);
 void launch_cell_init(const Dev &d, uint32_t np, int a, cudaStream_t st);
+void launch_epoch_reset(const Dev &d, cudaStream_t st);
 void launch_rebuild(const Dev &d, uint32_t np, uint32_t ncells, int a, cudaStream_t st);
 unsigned int scan_tile_count(uint32_t ncells);
 void relayout(const Dev &d, uint32_t np, int a, void *scratch, cudaStream_t st);
@@ -1320,14 +1321,9 @@ static int restore_ckpt(sph_ctx *c, const sph_ctx::Ckpt &k)
     CK(cudaMemsetAsync(d.dirty, 0, ((size_t)c->ncells_all + 1) * sizeof(uint32_t), c->stream));
     CK(cudaMemsetAsync(d.cflag, 1, div_up(c->np_all, 32), c->stream));
     CK(cudaMemsetAsync(d.settled, 0, c->np_all, c->stream));
-    CK(cudaStreamSynchronize(c->stream));
-    const uint32_t one = 1;
-    CK(cudaMemcpyAsync(d.rebuild, &one, 4, cudaMemcpyHostToDevice, c->stream));
-    Verlet V{};
-    V.step = 1;
-    V.all_rebuild = 1;
-    CK(cudaMemcpyAsync(d.vs, &V, sizeof(V), cudaMemcpyHostToDevice, c->stream));
-    CK(cudaStreamSynchronize(c->stream));   // one and V go out of scope
+    // stream-ordered: the host enqueues the next work without waiting
+    launch_epoch_reset(d, c->stream);
+    CK(cudaGetLastError());
     return SPH_OK;
 }
 
@@ -1379,7 +1375,8 @@ static void free_diff(sph_ctx *c)
     c->adj = AdjDev{};
     Dev &d = c->d;
     d.mu_p = nullptr;
-    d.tp_x = d.tp_v = d.tp_w = d.tp_dt0 = nullptr;
+    d.tp_x = d.tp_v = d.tp_w = nullptr;
+    d.tp_dt0 = nullptr;
     d.tp_mask = d.tp_partner = nullptr;
     d.tp_dmc = nullptr;
 }
@@ -1405,9 +1402,9 @@ int sph_diff_begin(sph_ctx *c, const double *mu, uint32_t checkpoint_every)
     ALD(d.mu_p, np);
     ALD(d.tp_x, K * np); ALD(d.tp_v, K * np); ALD(d.tp_w, K * np);
     ALD(d.tp_mask, K * np); ALD(d.tp_dmc, K * np);
-    ALD(d.tp_partner, K * np * NC); ALD(d.tp_dt0, K * np * NC);
+    ALD(d.tp_partner, K * tiled_size(np, NC)); ALD(d.tp_dt0, K * tiled_size(np, NC));
     ALD(A.xb, np); ALD(A.vb, np); ALD(A.wb, np); ALD(A.v0b, np); ALD(A.w0b, np);
-    ALD(A.Fb, np); ALD(A.Tb, np); ALD(A.dtb, np * NC); ALD(A.mub, np); ALD(A.theta_b, 3);
+    ALD(A.Fb, np); ALD(A.Tb, np); ALD(A.dtb, tiled_size(np, NC)); ALD(A.mub, np); ALD(A.theta_b, 3);
     ALD(A.dtb_mask, np);
     double *tmp = nullptr;
     ALD(tmp, np);
@@ -1458,7 +1455,7 @@ int sph_diff_backward(sph_ctx *c, const double *x_bar, const double *v_bar, doub
         launch_user_to_storage3(v_bar ? hx + 3 * (size_t)np : nullptr, A.vb, d.uid, np, st);
     }
     for (double4 *p : {A.wb, A.v0b, A.w0b}) CK(cudaMemsetAsync(p, 0, (size_t)np * 32, st));
-    CK(cudaMemsetAsync(A.dtb, 0, (size_t)np * NC * 32, st));
+    CK(cudaMemsetAsync(A.dtb, 0, tiled_size(np, NC) * sizeof(P3), st));
     CK(cudaMemsetAsync(A.dtb_mask, 0, (size_t)np * 4, st));
     CK(cudaMemsetAsync(A.mub, 0, (size_t)np * 8, st));
     CK(cudaMemsetAsync(A.theta_b, 0, 24, st));
@@ -1470,7 +1467,6 @@ int sph_diff_backward(sph_ctx *c, const double *x_bar, const double *v_bar, doub
         cudaGraphExec_t &gx = c->diff_graphs[{len, c->a}];
         if (!gx && (rc = capture_segment(c, len, c->a, &gx)) != SPH_OK) return rc;
         CK(cudaGraphLaunch(gx, st));
-        CK(cudaStreamSynchronize(st));
     }
     if ((rc = restore_ckpt(c, fin)) != SPH_OK) return rc;
     if ((rc = sync_status(c)) != SPH_OK) return rc;

@@ -254,6 +254,22 @@ void launch_cell_init(const Dev &d, uint32_t np, int a, cudaStream_t st)
     k_cell_init<<<div_up(np, CELL_BLOCK), CELL_BLOCK, 0, st>>>(d, a);
 }
 
+// A Verlet epoch from scratch after a state was put back: the cell list is
+// rebuilt and every particle sweeps in the next step.
+__global__ void k_epoch_reset(Dev d)
+{
+    Verlet V{};
+    V.step = 1;
+    V.all_rebuild = 1;
+    *d.vs = V;
+    *d.rebuild = 1u;
+}
+
+void launch_epoch_reset(const Dev &d, cudaStream_t st)
+{
+    k_epoch_reset<<<1, 1, 0, st>>>(d);
+}
+
 void launch_rebuild(const Dev &d, uint32_t np, uint32_t ncells, int a, cudaStream_t st)
 {
     const unsigned int ntiles = div_up((unsigned long long)ncells + 1, SCAN_TILE);

@@ -49,7 +49,7 @@ __device__ __forceinline__ void implicit_walls(const Params &P, double4 xa, Wall
 struct AdjDev {
     double4 *xb, *vb, *wb, *v0b, *w0b;  // adjoints of the state, xyz used
     double4 *Fb, *Tb;                   // adjoints of force and torque, per step
-    double4 *dtb;                       // [np][NC] adjoint of the slot history
+    P3 *dtb;                            // adjoint of the slot history, tiled (tile_at)
     uint32_t *dtb_mask;                 // [np] slots whose dtb entry may be nonzero
     double *mub;                        // [np] adjoint of per-particle friction
     double *theta_b;                    // [3] adjoints of k_n, k_t, gamma_n

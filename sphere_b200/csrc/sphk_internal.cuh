@@ -233,8 +233,9 @@ struct Dev {
     // ([step][np] rows; partner and history rows [step][np][NC], written for
     // evaluated slots only)
     double *mu_p;
-    double4 *tp_x, *tp_v, *tp_w, *tp_dt0;
-    uint32_t *tp_mask, *tp_partner;
+    double4 *tp_x, *tp_v, *tp_w;
+    P3 *tp_dt0;             // tape_slot_at: starting history of each evaluated slot
+    uint32_t *tp_mask, *tp_partner;   // tp_partner: tape_slot_at
     ulonglong2 *tp_dmc;
     // status
     uint32_t *status;
@@ -443,6 +444,14 @@ __host__ __device__ __forceinline__ size_t vl_at(uint32_t s, uint32_t e)
 __host__ __device__ __forceinline__ size_t tiled_size(size_t np, uint32_t width)
 {
     return ((np + 31) / 32) * 32 * (size_t)width;
+}
+
+// Slot i of particle s in row j of the differentiable step's tape: the slot
+// tiles of every step one after another, so that a warp's accesses to one
+// slot of its 32 particles are one contiguous run, as in the state's slots.
+__host__ __device__ __forceinline__ size_t tape_slot_at(uint32_t j, uint32_t np, uint32_t s, uint32_t i)
+{
+    return (size_t)j * tiled_size(np, NC) + tile_at(s, i, NC);
 }
 
 inline unsigned int div_up(unsigned long long a, unsigned int b)

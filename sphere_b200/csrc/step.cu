@@ -1300,8 +1300,9 @@ k_force_diff(ForceArgs args)
                 d.delta_t[at] = P3{o.dtn.x, o.dtn.y, o.dtn.z};
                 lawmask |= 1u << i;
                 if (j >= 0) {
-                    d.tp_partner[row * NC + i] = t;
-                    d.tp_dt0[row * NC + i] = d0;
+                    const size_t ts = tape_slot_at((uint32_t)j, np, s, (uint32_t)i);
+                    d.tp_partner[ts] = t;
+                    d.tp_dt0[ts] = d0p;
                 }
             } else {
                 occ &= ~(1u << i);
