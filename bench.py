@@ -626,25 +626,30 @@ def adjoint_leg(args, local):
     }
 
 
-def fd_checks(sb, fsteps, fK, local, seed):
-    """Central differences (h = 1e-6 relative) of a seeded linear loss of the
-    final positions and velocities, L = w.x + u.v, against the adjoint's
-    gradients with respect to k_n, k_t, gamma_n, the global mu and the mu of
-    the three particles with the largest adjoint: one list entry per
-    parameter."""
+def fd_checks(sb, fsteps, fK, local, seed, h_rel=1e-6, v_weight=1e-3):
+    """Central differences (step h_rel of each parameter) of a seeded linear
+    loss of the final positions and velocities, L = w.x + u.v, against the
+    adjoint's gradients with respect to k_n, k_t, gamma_n, the global mu and
+    the mu of the three particles with the largest adjoint: one list entry
+    per parameter (u: normal weights scaled by v_weight).  The difference
+    L(+h) - L(-h) is summed from the
+    elementwise differences of the two final states, w.(x+ - x-) + u.(v+ -
+    v-): the loss itself is of the order of the positions (centimetres
+    times sqrt(N)), and rounding its two sums would bury the change of
+    order h that the difference measures."""
     import numpy as np
     from sphere_b200 import adjoint
 
     rng = np.random.default_rng(seed)
     wx = rng.normal(size=(sb.np, 3))
-    wv = rng.normal(size=(sb.np, 3)) * 1e-3
+    wv = rng.normal(size=(sb.np, 3)) * v_weight
     mu0 = np.full(sb.np, float(sb.mu_s))
     base = dict(k_n=float(sb.k_n), k_t=float(sb.k_t), gamma_n=float(sb.gamma_n))
 
     def run(k_n, k_t, gamma_n, mu):
         s_, st_ = adjoint.run_forward(sb, fsteps, k_n, k_t, gamma_n, mu, checkpoint_every=fK,
                                       device=local)
-        return s_, float(np.sum(wx * st_.x[:, :3]) + np.sum(wv * st_.vel[:, :3]))
+        return s_, (np.array(st_.x[:, :3]), np.array(st_.vel[:, :3]))
 
     s_, _ = run(base["k_n"], base["k_t"], base["gamma_n"], mu0)
     ga = s_.diff_backward(wx, wv)
@@ -652,22 +657,22 @@ def fd_checks(sb, fsteps, fK, local, seed):
     checks = []
 
     def central(name, adj, plus, minus, h):
-        sp, lp = plus()
+        sp, (xp, vp) = plus()
         sp.close()
-        sm, lm = minus()
+        sm, (xm, vm) = minus()
         sm.close()
-        fd = (lp - lm) / (2.0 * h)
+        fd = (float(np.sum(wx * (xp - xm))) + float(np.sum(wv * (vp - vm)))) / (2.0 * h)
         checks.append({"param": name, "adjoint": adj, "central_difference": fd,
                        "rel_error": abs(adj - fd) / abs(fd) if fd else None})
 
     for name in ("k_n", "k_t", "gamma_n"):
-        h = 1e-6 * base[name]
+        h = h_rel * base[name]
         pp, pm = dict(base), dict(base)
         pp[name] += h
         pm[name] -= h
         central(name, float(ga[name]), lambda p=pp: run(**p, mu=mu0),
                 lambda p=pm: run(**p, mu=mu0), h)
-    h = 1e-6 * float(sb.mu_s)
+    h = h_rel * float(sb.mu_s)
     central("mu", float(ga["mu"].sum()), lambda: run(**base, mu=mu0 + h),
             lambda: run(**base, mu=mu0 - h), h)
     for i in np.argsort(-np.abs(ga["mu"]))[:3]:
@@ -675,7 +680,9 @@ def fd_checks(sb, fsteps, fK, local, seed):
         e[i] = h
         central(f"mu[{int(i)}]", float(ga["mu"][i]), lambda e=e: run(**base, mu=mu0 + e),
                 lambda e=e: run(**base, mu=mu0 - e), h)
-    return {"h": "1e-6 relative", "loss": "w.x + u.v, seeded normal weights (u scaled 1e-3)",
+    return {"h": f"{h_rel:g} relative",
+            "loss": f"w.x + u.v, seeded normal weights (u scaled {v_weight:g})",
+            "difference": "elementwise, w.(x+ - x-) + u.(v+ - v-)",
             "checks": checks, "max_rel_error": max(c["rel_error"] or 0.0 for c in checks)}
 
 
@@ -685,10 +692,17 @@ def adjoint_contacts_leg(args, local):
     spheres of r 1 mm held at a 20 kPa overlap by the six implicit walls,
     seeded velocities and spins, so contacts stick and slide from the first
     step).  Reports the adjoint/forward time ratio over the full run with the
-    height-profile loss, every gradient, and a central-difference check (h =
-    1e-6 relative) of the gradients with respect to k_n, k_t, gamma_n, the
-    global mu and three particles' mu on a short run of the same block, with
-    a seeded linear loss of the final positions and velocities."""
+    height-profile loss, every gradient, and a central-difference check of
+    the gradients with respect to k_n, k_t, gamma_n and the global mu on a
+    jammed block of the same kind where the loss is smooth in the
+    parameters over the difference's step: 16^3 spheres at k_n = k_t = 1e4,
+    gamma_n 0.1 of critical, stirred 100 times more gently, so that every
+    contact holds and sticks through the 40 steps (h = 1e-3 relative,
+    velocity-weighted linear loss).  On the timed block itself a central
+    difference measures no derivative: its stirring opens contacts and
+    moves them across the stick/slip limit within the run (kinks a step h
+    can cross), and at k_n = 1e6 the locked lattice's response to a small
+    h is near the FP64 resolution of its trajectories."""
     import numpy as np
     import torch
     from sphere_b200 import adjoint, scenes
@@ -720,10 +734,13 @@ def adjoint_contacts_leg(args, local):
         iters.append((t_fwd, t_bwd))
     sim.close()
 
-    # central differences on a short run of the same block
+    # central differences on a smooth block of the same kind
     fsteps = args.adjoint_fd_steps
-    fd = fd_checks(sb, fsteps, 10, local, args.seed + 18)
-    fd["scene"] = f"the same block, {fsteps} steps, checkpoints every 10"
+    fsb = scenes.jammed_column(nx=16, ny=16, nz=16, k=1e4, gamma_frac=0.1, vmax=5e-5, wmax=0.2)
+    fd = fd_checks(fsb, fsteps, 10, local, args.seed + 18, h_rel=1e-3, v_weight=1e3)
+    fd["scene"] = (f"jammed block 16x16x16 ({fsb.np} spheres, r 1 mm, six implicit walls), "
+                   "k_n = k_t = 1e4, gamma_n 0.1 of critical, velocities U(+-5e-5) m/s, spins "
+                   f"U(+-0.2) rad/s, every contact sticking; {fsteps} steps, checkpoints every 10")
     ratios = [b / f for f, b in iters[1:]]
     return {
         "metric": "adjoint/forward time ratio", "value": float(np.median(ratios)), "unit": "ratio",
