@@ -11,6 +11,7 @@
 #include "sphere.h"
 
 #include <chrono>
+#include <cmath>
 #include <fstream>
 #include <cstdio>
 #include <cstdlib>
@@ -102,26 +103,74 @@ void DEM::initDarcy()
 }
 
 // endDarcy (src/darcy.cpp:826-836): porosity and conductivity of every cell
-// as text, as printDarcyArray lays them out (src/darcy.cpp:483-495)
 void DEM::endDarcy()
 {
-    const std::pair<const char *, const std::vector<double> *> out[] = {{"d_phi.txt", &d_phi_},
-                                                                       {"d_K.txt", &d_K_}};
-    for (const auto &o : out) {
-        FILE *f = fopen(o.first, "w");
-        if (!f) {
-            fprintf(stderr, "Error, could not open %s.\n", o.first);
-            continue;
+    writeDarcyArray(d_phi_.data(), "d_phi.txt");
+    writeDarcyArray(d_K_.data(), "d_K.txt");
+}
+
+// printDarcyArray (src/darcy.cpp:483-528): the cells of the grid, x fastest,
+// a tab after each value, a line per (y, z) row and an empty line per z
+// slice; the ghost nodes are not printed.  The described forms write their
+// heading to standard output whatever the stream, as the reference's do.
+void DEM::printDarcyArray(FILE *stream, double *arr)
+{
+    for (uint32_t z = 0; z < cfg_.num[2]; ++z) {
+        for (uint32_t y = 0; y < cfg_.num[1]; ++y) {
+            for (uint32_t x = 0; x < cfg_.num[0]; ++x)
+                fprintf(stream, "%f\t", arr[darcyNode((int)x, (int)y, (int)z)]);
+            fprintf(stream, "\n");
         }
-        for (uint32_t z = 0; z < cfg_.num[2]; ++z) {
-            for (uint32_t y = 0; y < cfg_.num[1]; ++y) {
-                for (uint32_t x = 0; x < cfg_.num[0]; ++x)
-                    fprintf(f, "%f\t", (*o.second)[darcyNode((int)x, (int)y, (int)z)]);
-                fprintf(f, "\n");
+        fprintf(stream, "\n");
+    }
+}
+
+void DEM::printDarcyArray(FILE *stream, double *arr, std::string desc)
+{
+    std::cout << "\n" << desc << ":\n";
+    printDarcyArray(stream, arr);
+}
+
+void DEM::printDarcyArray(FILE *stream, Float3 *arr)
+{
+    for (uint32_t z = 0; z < cfg_.num[2]; ++z) {
+        for (uint32_t y = 0; y < cfg_.num[1]; ++y) {
+            for (uint32_t x = 0; x < cfg_.num[0]; ++x) {
+                const Float3 &v = arr[darcyNode((int)x, (int)y, (int)z)];
+                fprintf(stream, "%f,%f,%f\t", v.x, v.y, v.z);
             }
-            fprintf(f, "\n");
+            fprintf(stream, "\n");
         }
-        fclose(f);
+        fprintf(stream, "\n");
+    }
+}
+
+void DEM::printDarcyArray(FILE *stream, Float3 *arr, std::string desc)
+{
+    std::cout << "\n" << desc << ":\n";
+    printDarcyArray(stream, arr);
+}
+
+// writeDarcyArray (src/darcy.cpp:801-824)
+void DEM::writeDarcyArray(double *array, const char *filename)
+{
+    FILE *file = fopen(filename, "w");
+    if (file) {
+        printDarcyArray(file, array);
+        fclose(file);
+    } else {
+        fprintf(stderr, "Error, could not open %s.\n", filename);
+    }
+}
+
+void DEM::writeDarcyArray(Float3 *array, const char *filename)
+{
+    FILE *file = fopen(filename, "w");
+    if (file) {
+        printDarcyArray(file, array);
+        fclose(file);
+    } else {
+        fprintf(stderr, "Error, could not open %s.\n", filename);
     }
 }
 
@@ -403,19 +452,129 @@ void DEM::render(const int method, const float maxval, const float lower_cutoff,
     o.lower_cutoff = lower_cutoff;
     o.width = img_width;
     o.height = img_height;
-    std::vector<unsigned char> img((size_t)img_width * img_height * 4);
-    const int rc = sph_render(ctx_, &o, img.data());
+    img_.assign((size_t)img_width * img_height * 4, 0);
+    width_ = img_width;
+    height_ = img_height;
+    const int rc = sph_render(ctx_, &o, img_.data());
     if (rc != SPH_OK) fail(rc, "sph_render");
-    const std::string target = "img_out/" + sid_ + ".ppm";
+    writePPM(("img_out/" + sid_ + ".ppm").c_str());
+}
+
+// writePPM (src/file_io.cpp:493-516): header, then r, g, b of every pixel
+void DEM::writePPM(const char *target)
+{
     std::ofstream ofs(target, std::ios_base::binary);
     if (!ofs) {
         std::cerr << "Could not create output PPM file '" << target << std::endl;
         exit(1);
     }
     if (verbose_ == 1) std::cout << "  Saving image: " << target << std::endl;
-    ofs << "P6 " << img_width << " " << img_height << " 255\n";
-    for (size_t i = 0; i < (size_t)img_width * img_height; ++i)
-        ofs << img[4 * i] << img[4 * i + 1] << img[4 * i + 2];
+    ofs << "P6 " << width_ << " " << height_ << " 255\n";
+    for (size_t i = 0; i < (size_t)width_ * height_; ++i)
+        ofs << img_[4 * i] << img_[4 * i + 1] << img_[4 * i + 2];
+}
+
+// minPos / maxPos (src/sphere.cpp:487-551): the reference reduces per
+// thread and then across threads, every partial starting from 0, with
+// std::min / std::max (a NaN coordinate is never taken, and 0 and -0
+// compare equal, so the first value kept stays): the order of the
+// comparisons does not change the result.
+Float3 DEM::minPos()
+{
+    Float3 m{0.0, 0.0, 0.0};
+    for (uint32_t i = 0; i < cfg_.np; ++i) {
+        m.x = std::min(m.x, x_[4 * (size_t)i]);
+        m.y = std::min(m.y, x_[4 * (size_t)i + 1]);
+        m.z = std::min(m.z, x_[4 * (size_t)i + 2]);
+    }
+    return m;
+}
+
+Float3 DEM::maxPos()
+{
+    Float3 m{0.0, 0.0, 0.0};
+    for (uint32_t i = 0; i < cfg_.np; ++i) {
+        m.x = std::max(m.x, x_[4 * (size_t)i]);
+        m.y = std::max(m.y, x_[4 * (size_t)i + 1]);
+        m.z = std::max(m.z, x_[4 * (size_t)i + 2]);
+    }
+    return m;
+}
+
+// findOverlaps (src/sphere.cpp:556-602).  The reference tests all pairs
+// i < j.  A pair overlaps only when it is closer than r_i + r_j <= 2 r_max,
+// so the candidates here come from a grid of cells a little wider than
+// 2 r_max (two such particles lie in the same or adjacent cells); each is
+// tested with the reference's arithmetic (x_j - x_i, the squares summed x,
+// y, z, sqrt, less r_i + r_j) and the pairs are put in the reference's
+// (i, j) order.  A particle with a coordinate or radius that is not finite
+// overlaps nothing there (delta_n is NaN) and is left out.
+void DEM::findOverlaps(std::vector<std::vector<unsigned int>> &ij, std::vector<double> &delta_n_ij)
+{
+    const uint32_t n = cfg_.np;
+    auto finite = [&](uint32_t i) {
+        const double *p = &x_[4 * (size_t)i];
+        return std::isfinite(p[0]) && std::isfinite(p[1]) && std::isfinite(p[2]) &&
+               std::isfinite(p[3]);
+    };
+    double rmax = 0.0, lo[3] = {0.0, 0.0, 0.0};
+    bool any = false;
+    for (uint32_t i = 0; i < n; ++i) {
+        if (!finite(i)) continue;
+        const double *p = &x_[4 * (size_t)i];
+        rmax = std::max(rmax, p[3]);
+        for (int d = 0; d < 3; ++d) lo[d] = any ? std::min(lo[d], p[d]) : p[d];
+        any = true;
+    }
+    // r_i + r_j <= 0 leaves delta_n = |x_ij| - (r_i + r_j) >= 0
+    if (!any || !(rmax > 0.0)) return;
+    const double edge = 2.0 * rmax * (1.0 + 1e-6);
+    std::vector<std::pair<uint64_t, uint32_t>> keyed;   // (cell key, particle)
+    std::vector<int64_t> cell(3 * (size_t)n);
+    auto key_of = [](int64_t cx, int64_t cy, int64_t cz) {
+        return ((uint64_t)(cx & 0x1fffff) << 42) | ((uint64_t)(cy & 0x1fffff) << 21) |
+               (uint64_t)(cz & 0x1fffff);
+    };
+    for (uint32_t i = 0; i < n; ++i) {
+        if (!finite(i)) continue;
+        const double *p = &x_[4 * (size_t)i];
+        for (int d = 0; d < 3; ++d) cell[3 * (size_t)i + d] = (int64_t)std::floor((p[d] - lo[d]) / edge);
+        keyed.emplace_back(key_of(cell[3 * (size_t)i], cell[3 * (size_t)i + 1], cell[3 * (size_t)i + 2]), i);
+    }
+    std::sort(keyed.begin(), keyed.end());
+    std::vector<std::pair<std::pair<uint32_t, uint32_t>, double>> found;
+    for (const auto &ki : keyed) {
+        const uint32_t i = ki.second;
+        const double *xi = &x_[4 * (size_t)i];
+        for (int64_t dz = -1; dz <= 1; ++dz)
+            for (int64_t dy = -1; dy <= 1; ++dy)
+                for (int64_t dx = -1; dx <= 1; ++dx) {
+                    const uint64_t k = key_of(cell[3 * (size_t)i] + dx, cell[3 * (size_t)i + 1] + dy,
+                                              cell[3 * (size_t)i + 2] + dz);
+                    auto it = std::lower_bound(keyed.begin(), keyed.end(),
+                                               std::make_pair(k, (uint32_t)0));
+                    for (; it != keyed.end() && it->first == k; ++it) {
+                        const uint32_t j = it->second;
+                        if (j <= i) continue;
+                        const double *xj = &x_[4 * (size_t)j];
+                        // the 21-bit keys wrap; a far particle sharing a key is no neighbour
+                        if (std::abs(cell[3 * (size_t)j] - cell[3 * (size_t)i]) > 1 ||
+                            std::abs(cell[3 * (size_t)j + 1] - cell[3 * (size_t)i + 1]) > 1 ||
+                            std::abs(cell[3 * (size_t)j + 2] - cell[3 * (size_t)i + 2]) > 1)
+                            continue;
+                        const double ax = xj[0] - xi[0], ay = xj[1] - xi[1], az = xj[2] - xi[2];
+                        const double len = std::sqrt(ax * ax + ay * ay + az * az);
+                        const double delta_n = len - (xi[3] + xj[3]);
+                        if (delta_n < 0.0) found.push_back({{i, j}, delta_n});
+                    }
+                }
+    }
+    std::sort(found.begin(), found.end(),
+              [](const auto &a, const auto &b) { return a.first < b.first; });
+    for (const auto &f : found) {
+        ij.push_back({f.first.first, f.first.second});
+        delta_n_ij.push_back(f.second);
+    }
 }
 
 void DEM::porosity(const int)

@@ -10,18 +10,26 @@
 // nu > 0 the Darcy flow runs with the step (src/darcy.cpp, src/darcy.cuh):
 // its grid is read from and written to the files' fluid section, set up by
 // sph_darcy_init and stepped on the device.  render() draws the current
-// state with the reference's ray tracer (sph_render) into img_out/<sid>.ppm.
-// The lattice-Boltzmann coupling (nu > 0 without darcyflow) and the
-// porosity and force-chain tools are not part of this build: they report
-// that and exit.
+// state with the reference's ray tracer (sph_render) and writePPM saves it
+// into img_out/<sid>.ppm.  The analysis members minPos, maxPos and
+// findOverlaps and the Darcy array printers (src/sphere.cpp:487-602,
+// src/darcy.cpp:483-528,801-824) work on the host state.  The
+// lattice-Boltzmann coupling (nu > 0 without darcyflow) and the porosity and
+// force-chain tools are not part of this build: they report that and exit.
 #ifndef SPHERE_B200_SPHERE_H_
 #define SPHERE_B200_SPHERE_H_
 
 #include <cstdint>
+#include <cstdio>
 #include <string>
 #include <vector>
 
 #include "sphk.h"
+
+// The reference's Float3 in its double-precision build (src/datatypes.h).
+struct Float3 {
+    double x, y, z;
+};
 
 class DEM {
   public:
@@ -48,6 +56,27 @@ class DEM {
     void porosity(const int z_slices = 10);
     void forcechains(const std::string format = "interactive", const int threedim = 1,
                      const double lower_cutoff = 0.0, const double upper_cutoff = 1.0e9);
+
+    // the image of the last render() as binary PPM, src/file_io.cpp:493-516
+    void writePPM(const char *target);
+
+    // smallest / largest particle coordinate in each dimension, each
+    // starting from 0 as the reference's do (src/sphere.cpp:487-551)
+    Float3 minPos();
+    Float3 maxPos();
+
+    // every overlapping pair i < j in (i, j) order with its delta_n < 0,
+    // src/sphere.cpp:556-602
+    void findOverlaps(std::vector<std::vector<unsigned int>> &ij, std::vector<double> &delta_n_ij);
+
+    // a field over the Darcy cell grid (ghost nodes included, the layout of
+    // the fluid section) as text, src/darcy.cpp:483-528,801-824
+    void printDarcyArray(FILE *stream, double *arr);
+    void printDarcyArray(FILE *stream, double *arr, std::string desc);
+    void printDarcyArray(FILE *stream, Float3 *arr);
+    void printDarcyArray(FILE *stream, Float3 *arr, std::string desc);
+    void writeDarcyArray(double *array, const char *filename);
+    void writeDarcyArray(Float3 *array, const char *filename);
 
   private:
     std::string inputbin_, sid_;
@@ -78,6 +107,10 @@ class DEM {
     sph_darcy_state darcyState();
 
     sph_ctx *ctx_ = nullptr;
+
+    // the last render(): RGBA bytes, width_ x height_
+    std::vector<unsigned char> img_;
+    unsigned int width_ = 0, height_ = 0;
 
     void initDevice();
     void upload();
