@@ -350,11 +350,14 @@ def gpu_arm(args, rank, world, local):
     b_step, b_whole, b_tight = algorithmic_bytes(cfg.np, cfg.ncells, C, cfg.nb0)
     peak, peak_kind = measured_peak_hbm()
     achieved = b_step / (step_ms * 1e-3) / 1e9
-    # per step: the rebuild gate, k_bonds (with bonds), k_topo, k_force and
-    # the wall kernel (k_walls, or k_tail without walls); the 7 cell-list
-    # kernels only in steps whose cell list changed (a conditional graph node)
+    # per step: the rebuild gate, k_bonds (with bonds), k_topo, k_contact
+    # (contact models 2 and 3), k_force_tiles, k_tail, and with dynamic walls
+    # k_walls on its graph branch; the 7 cell-list kernels only in steps
+    # whose cell list changed (a conditional graph node)
     rebuilt = stats["cell_rebuilds"] - rebuilds0
-    launches = args.steps * (4 + (1 if cfg.nb0 else 0)) + 7 * rebuilt
+    per_step = (4 + (1 if cfg.nb0 else 0) + (1 if cfg.contactmodel in (2, 3) else 0)
+                + (1 if cfg.nw else 0))
+    launches = args.steps * per_step + 7 * rebuilt
     out = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
