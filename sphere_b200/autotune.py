@@ -24,8 +24,8 @@ CELL_FACTORS = (2.0, 2.5, 3.0)
 SKINS = (0.0, 0.05, 0.1, 0.2)
 GRAPH_STEPS = (8, 16)
 SHAPES = (0, 1)
-SHAPE_NAMES = ("contact search 64 x 16, contact forces 128 x 4 (threads x blocks per SM)",
-               "contact search 128 x 8, contact forces 64 x 8 (threads x blocks per SM)")
+SHAPE_NAMES = ("contact search 64 x 16, contact forces 128 x 5 (threads x blocks per SM)",
+               "contact search 128 x 8, contact forces 64 x 10 (threads x blocks per SM)")
 
 
 @dataclass

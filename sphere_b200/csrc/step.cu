@@ -46,13 +46,16 @@ constexpr int FORCE_BLOCK = SPHK_FORCE_BLOCK;
 // shapes each, and a context picks one pair (Dev::shape, SPH_OPT_BLOCK_SHAPES;
 // the ensemble's autotuner times both).  Shape 0, the default: k_topo in
 // blocks of 64 threads, 16 per SM, whose threads leave at different times;
-// k_contact in blocks of 4 warps, 4 per SM.  Shape 1: k_topo in 128 x 8,
-// k_contact in 2 warps x 8.  The threads resident per SM are the same.
+// k_contact in blocks of 4 warps, 5 per SM.  Shape 1: k_topo in 128 x 8,
+// k_contact in 2 warps x 10.  The threads resident per SM are the same.
 #ifndef SPHK_TOPO_THREADS_PER_SM
 #define SPHK_TOPO_THREADS_PER_SM 1024
 #endif
 constexpr int TOPO_THREADS_PER_SM = SPHK_TOPO_THREADS_PER_SM;
-constexpr int CONTACT_THREADS_PER_SM = 512;
+#ifndef SPHK_CONTACT_THREADS_PER_SM
+#define SPHK_CONTACT_THREADS_PER_SM 640
+#endif
+constexpr int CONTACT_THREADS_PER_SM = SPHK_CONTACT_THREADS_PER_SM;
 __host__ __device__ constexpr int topo_block(uint32_t shape) { return shape ? 128 : 64; }
 __host__ __device__ constexpr int contact_block(uint32_t shape) { return shape ? 64 : 128; }
 
@@ -1425,7 +1428,7 @@ struct ContactArgs {
 
 // Contacts of one chunk whose law terms a warp holds at once (a multiple of 32).
 #ifndef SPHK_CONTACT_CAP
-#define SPHK_CONTACT_CAP 96
+#define SPHK_CONTACT_CAP 64
 #endif
 constexpr uint32_t CT_CAP = SPHK_CONTACT_CAP;
 
