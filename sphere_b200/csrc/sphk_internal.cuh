@@ -412,8 +412,14 @@ constexpr uint64_t BULK_WAIT_NS = 1000000000ull;
 
 // The slot rule fills the last empty slot first (src/contactsearch.cuh:
 // 252-271), so a particle's few contacts sit in the top slots: the tile rows
-// worth fetching ahead are the top PF_SLOTS.
-constexpr uint32_t PF_SLOTS = 8;
+// worth fetching ahead are the top PF_SLOTS.  Six: a dense packing holds
+// four to six contacts a sphere (the jammed column exactly six), and rows
+// fetched for empty slots only take L2 bandwidth from the ones used
+// (4, 5, 6 and 8 slots measured on the 1M column: 6 fastest).
+#ifndef SPHK_PF_SLOTS
+#define SPHK_PF_SLOTS 6
+#endif
+constexpr uint32_t PF_SLOTS = SPHK_PF_SLOTS;
 
 // The metadata of a Verlet-list entry: bits 0-4 the stencil cell (0..26),
 // 5-15 the periodic shift code, 16-31 the top half of the float gap to the
