@@ -17,7 +17,8 @@ void launch_force(const Dev &d, const Params &hp, uint32_t np, int model, int a,
                   cudaStream_t st);
 void launch_contact(const Dev &d, const Params &hp, uint32_t np, int model, int a, int write_outputs,
                     cudaStream_t st);
-void launch_bonds(const Dev &d, uint32_t nb0, int a, cudaStream_t st);
+void launch_bonds(const Dev &d, const Params &hp, uint32_t nb0, int a, cudaStream_t st);
+void launch_bond_storage(const Dev &d, uint32_t nb0, uint32_t np, cudaStream_t st);
 void launch_walls(const Dev &d, uint32_t np, uint32_t nw, cudaStream_t st);
 void launch_wall_motion(const Dev &d, uint32_t np, cudaStream_t st);
 void launch_tail(const Dev &d, cudaStream_t st);
@@ -363,7 +364,7 @@ int enqueue_one_step(sph_ctx *c, int a, int write_outputs, cudaStream_t st, bool
     } else {
         launch_rebuild(c->d, c->np_all, c->ncells_all, a, st);
     }
-    launch_bonds(c->d, c->hp.nb0, a, st);
+    launch_bonds(c->d, c->hp, c->hp.nb0, a, st);
     // The Darcy block reads the step's start positions (buffer a) and its
     // cell list, which nothing changes before the next step's rebuild, and
     // writes only the fluid grid: in a graph it runs beside the force and
@@ -484,7 +485,7 @@ int profiled_step(sph_ctx *c, int a, int write_outputs, cudaStream_t st)
     CK(cudaEventRecord(c->ev[0], st));
     launch_rebuild(c->d, c->np_all, c->ncells_all, a, st);
     CK(cudaEventRecord(c->ev[1], st));
-    launch_bonds(c->d, c->hp.nb0, a, st);
+    launch_bonds(c->d, c->hp, c->hp.nb0, a, st);
     CK(cudaEventRecord(c->ev[2], st));
     launch_topo(c->d, c->np_all, c->hp.contactmodel == 1, a, st);
     CK(cudaEventRecord(c->ev[3], st));
@@ -512,6 +513,8 @@ int do_relayout(sph_ctx *c, cudaStream_t st)
     // the cell list must describe the current positions before storage follows it
     launch_rebuild(c->d, c->np_all, c->ncells_all, c->a, st);
     relayout(c->d, c->np_all, c->a, c->scratch, st);
+    // the bonds follow their particles' new storage indices
+    if (!c->batched) launch_bond_storage(c->d, c->hp.nb0, c->np_all, st);
     // the slot rows moved: every chunk may hold a contact until the next
     // force pass has looked
     CK(cudaMemsetAsync(c->d.cflag, 1, div_up(c->np_all, 32), st));
@@ -666,7 +669,7 @@ int create_impl(const sph_config *cfgs, uint32_t ninst, bool batched, sph_ctx **
     AL(d.wf_flag, div_up(np, 256));
     AL(d.walls, 1);
     AL(d.bonds, nb0); AL(d.bonds_delta, nb0); AL(d.bonds_omega, nb0);
-    AL(d.bond_f, nb0); AL(d.bond_t, nb0); AL(d.bond_xu, nb0);
+    AL(d.bond_f, nb0); AL(d.bond_t, nb0); AL(d.bond_xu, nb0); AL(d.bond_s, nb0);
     AL(d.bond_ptr, np + 1); AL(d.bond_list, 2 * (size_t)nb0);
     if (c->hp.contactmodel == 1) {
         AL(d.c1acc, np);

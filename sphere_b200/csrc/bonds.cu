@@ -12,16 +12,37 @@ namespace sphk {
 
 constexpr int BOND_BLOCK = 256;
 
-__global__ void __launch_bounds__(BOND_BLOCK)
-k_bonds(Dev d, int A)
+// The constants of bondsLinear, fixed when a context is created: passed by
+// value (the constant bank) rather than read through Params after a store.
+struct BondConsts {
+    uint32_t nb0, np;
+    double dt, lambda_bar, k_n, k_t, gamma_n, gamma_t, sigma_b, tau_b;
+};
+
+// The bonds' particles as storage indices: bond_s follows bonds (by caller
+// index) through sidx.  Storage order changes only at a relayout, after
+// which this runs; a bond already broken (marker x >= np) keeps a pair that
+// is never read.
+__global__ void k_bond_storage(Dev d, uint32_t nb0, uint32_t np)
 {
-    const Params &P = *d.prm;
+    const uint32_t b = blockIdx.x * BOND_BLOCK + threadIdx.x;
+    if (b >= nb0) return;
+    const uint2 bond = d.bonds[b];
+    d.bond_s[b] = make_uint2(bond.x < np ? d.sidx[bond.x] : 0u, d.sidx[bond.y]);
+}
+
+__global__ void __launch_bounds__(BOND_BLOCK)
+k_bonds(Dev d, int A, BondConsts P)
+{
     const uint32_t idx = blockIdx.x * BOND_BLOCK + threadIdx.x;
     if (idx >= P.nb0) return;
+    // the bond and its storage pair before any store, so that the two loads
+    // and then the particle rows are each one memory latency
     const uint2 bond = d.bonds[idx];
+    const uint2 bs = d.bond_s[idx];
     d.bond_xu[idx] = 0xffffffffu;
     if (!(bond.x < P.np)) return;     // erased bond (marker nb0 >= np)
-    const uint32_t si = d.sidx[bond.x], sj = d.sidx[bond.y];
+    const uint32_t si = bs.x, sj = bs.y;
     const double dt = P.dt;
     const double4 d0 = d.bonds_delta[idx], o0 = d.bonds_omega[idx];
     d3 delta0_t = xyz(d0);
@@ -77,10 +98,18 @@ k_bonds(Dev d, int A)
     d.bond_xu[idx] = bond.x;
 }
 
-void launch_bonds(const Dev &d, uint32_t nb0, int a, cudaStream_t st)
+void launch_bonds(const Dev &d, const Params &hp, uint32_t nb0, int a, cudaStream_t st)
 {
     if (nb0 == 0) return;
-    k_bonds<<<div_up(nb0, BOND_BLOCK), BOND_BLOCK, 0, st>>>(d, a);
+    const BondConsts bc{hp.nb0,     hp.np,     hp.dt,      hp.lambda_bar, hp.k_n,
+                        hp.k_t,     hp.gamma_n, hp.gamma_t, hp.sigma_b,   hp.tau_b};
+    k_bonds<<<div_up(nb0, BOND_BLOCK), BOND_BLOCK, 0, st>>>(d, a, bc);
+}
+
+void launch_bond_storage(const Dev &d, uint32_t nb0, uint32_t np, cudaStream_t st)
+{
+    if (nb0 == 0) return;
+    k_bond_storage<<<div_up(nb0, BOND_BLOCK), BOND_BLOCK, 0, st>>>(d, nb0, np);
 }
 
 }  // namespace sphk

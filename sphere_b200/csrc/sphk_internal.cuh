@@ -225,6 +225,7 @@ struct Dev {
     double4 *bonds_delta, *bonds_omega;
     double4 *bond_f, *bond_t;   // per-bond force on x and torque on y
     uint32_t *bond_xu;          // user index that received +f this step, or ~0u
+    uint2 *bond_s;              // the bond's particles as storage indices (set at relayout)
     uint32_t *bond_ptr;         // [np + 1] CSR by uid
     uint32_t *bond_list;        // [2 nb0] (bond << 1) | role (0: x, 1: y)
     // contact model 1: contact force xyz and pressure summed by k_topo
