@@ -11,7 +11,7 @@ sequential placement in a periodic-x/y 0.2 x 0.2 x 0.4 m domain, top wall at
 
 A step is one time step of the whole scene.  ``value`` is device-timed
 throughput with the state resident in HBM (CUDA events on the launching
-stream around exactly K steps; the ~1.5 GB state exceeds the 126 MB L2, so no
+stream around exactly K steps; the ~2.5 GB state exceeds the 126 MB L2, so no
 flush is needed).  ``e2e`` is the same metric through the C ABI with host
 buffers: upload of the pinned host state, K steps, download of the state.
 With N > 1 every rank runs an independent replica (own seed): the DEM step of
@@ -1131,7 +1131,7 @@ def profile_workload(args):
     cannot follow the kernels of the step graphs.  `warmup` steps, then
     `steps` steps; prints the phase times per step.  Per step the launches
     are the cell-list kernels, k_bonds (with bonds), k_topo, k_contact (models
-    2 and 3), k_force and the wall kernel, in that order."""
+    2 and 3), k_force_tiles and the wall kernel, in that order."""
     import torch
     from sphere_b200 import scenes
     from sphere_b200.sphk import Simulation

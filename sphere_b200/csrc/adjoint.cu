@@ -1,7 +1,7 @@
 // adjoint.cu -- the reverse pass of the differentiable step.
 //
 // The differentiable step is contact model 2 in exact FP64 with
-// per-particle friction (k_force's DIFF variant, step.cu).  Going backwards
+// per-particle friction (k_force_diff, step.cu).  Going backwards
 // through one step j needs the step's inputs, which the forward re-run of a
 // checkpoint segment records in the tape (Dev::tp_*): positions, velocities
 // and spins of every particle, and for each contact slot the law was
@@ -40,7 +40,7 @@ __device__ __forceinline__ void atomic_add3(double4 *p, dl::V3 v)
     atomicAdd(&p->z, v.z);
 }
 
-// The leapfrog of k_force (src/integration.cuh:9-187) is linear in force,
+// The leapfrog of the force kernels (src/integration.cuh:9-187) is linear in force,
 // torque and the carried state:
 //   acc = F / m + g, angacc = T / (2/5 m r^2)   (zero under fixvel, except acc.z)
 //   vel0' = vel0 + acc dt,  x' = x + vel0' dt,  vel' = vel0' + acc dt / 2

@@ -1,5 +1,5 @@
-// diff_step.cuh -- shared pieces of the differentiable step (k_force's DIFF
-// variant in step.cu) and of its reverse (adjoint.cu).
+// diff_step.cuh -- shared pieces of the differentiable step (k_force_diff in
+// step.cu) and of its reverse (adjoint.cu).
 #ifndef SPHK_DIFF_STEP_CUH_
 #define SPHK_DIFF_STEP_CUH_
 

@@ -188,11 +188,11 @@ struct Dev {
     ulonglong2 *dmc;      // [np] 4-bit periodic shift code of each of the NC slots
     P3 *delta_t;          // tiled, NC per particle; the reference's fourth lane is always 0
     uint32_t *cmask;      // [np] occupied-slot bit mask
-    // [ceil(np / 32)] the chunk of 32 storage indices may hold a contact (1),
-    // or, between k_contact and k_force, was visited by k_contact (2: a slot
-    // is still held, 3: none is)
+    // [ceil(np / 32)] the chunk of 32 storage indices may hold a contact
+    // (1), or, between k_contact and k_force_tiles, was visited by k_contact
+    // (2: a slot is still held, 3: none is)
     uint8_t *cflag;
-    // contact models 2 and 3: the slot sums k_contact leaves for k_force (F
+    // contact models 2 and 3: the slot sums k_contact leaves for k_force_tiles (F
     // xyz and p; T xyz and ev_dot; es_dot)
     double4 *csum_f, *csum_t;
     double *csum_es;

@@ -1,21 +1,24 @@
-// step.cu -- the per-particle DEM step of libsphk, in two launches.
+// step.cu -- the per-particle DEM step of libsphk, in three launches.
 //
 // k_topo   contact detection into the persistent slots (topology,
-//          src/contactsearch.cuh:181-355).  One thread per cell-list
-//          position.  Candidates come from a float copy of the positions kept
+//          src/contactsearch.cuh:181-355): a lane's list decisions for one
+//          to four particles, then a search for each particle they do not
+//          settle.  Candidates come from a float copy of the positions kept
 //          in cell-list order (Dev::xs), so the three cells of each x-row of
 //          the 27-cell stencil are three adjacent runs of one array and a
 //          candidate costs one coalesced 16-byte load; the particle's own slot
 //          row is fetched only when an overlap is found.
 // k_contact the force laws of the occupied slots (interact's slot loop,
 //          src/contactsearch.cuh:468-543), one lane per directed contact;
-//          each particle's sums, in slot order, are left for k_force.
-// k_force  everything per particle after it (src/device.cu:829-1058): the
-//          slot sums, the walls (interact, contactsearch.cuh:578-663), the
-//          per-bond forces of bondsLinear (cohesion.cuh:8-233, computed by
-//          bonds.cu and gathered here in bond order), and the half-step
-//          leapfrog (integrate, integration.cuh:9-187).  One thread per
-//          storage index, so the particle state streams.
+//          each particle's sums, in slot order, are left for k_force_tiles.
+// k_force_tiles  everything per particle after it (src/device.cu:829-1058):
+//          the slot sums, the walls (interact, contactsearch.cuh:578-663),
+//          the per-bond forces of bondsLinear (cohesion.cuh:8-233, computed
+//          by bonds.cu and gathered here in bond order), and the half-step
+//          leapfrog (integrate, integration.cuh:9-187).  A resident grid over
+//          tiles of 128 particles whose rows arrive by bulk copies.  The
+//          differentiable step runs k_force_diff instead of k_contact and
+//          k_force_tiles.
 // Kinematics of step n are read from buffer A and step n+1 is written to
 // buffer B, so neighbours always see start-of-step values.
 //
@@ -528,7 +531,7 @@ __device__ __forceinline__ float moved_bound(const Dev &d, uint32_t s, const Ver
 //
 // VISC (contact model 1): no slots; every candidate within ra + rb + db is
 // processed in visiting order and the contact force and pressure sums are
-// left in Dev::c1acc for k_force.
+// left in Dev::c1acc for k_force_tiles.
 // The contact search of one particle s whose list decision (k_topo) did not
 // settle it: list_ok, its Verlet list is valid; held, Dev::settled[s].
 template <bool VISC, bool BATCH, int TB>
@@ -811,7 +814,7 @@ constexpr uint32_t TOPO_SPAN_MAX = 4;
 //
 // VISC (contact model 1): no slots; every candidate within ra + rb + db is
 // processed in visiting order and the contact force and pressure sums are
-// left in Dev::c1acc for k_force.
+// left in Dev::c1acc for k_force_tiles.
 template <bool VISC, bool BATCH, int TB>
 __global__ void __launch_bounds__(TB, TOPO_THREADS_PER_SM / TB)
 k_topo(Dev d, int A, uint32_t span)
@@ -1449,7 +1452,7 @@ constexpr uint32_t CT_CAP = SPHK_CONTACT_CAP;
 // a force law whatever the spread of contact counts, and the terms of up to
 // CT_CAP contacts are kept in shared memory.  Then every particle's own lane
 // adds its terms in slot order, the reference's summation order, all lanes
-// at once, and at the end stores the sums for k_force.  A slot whose partner
+// at once, and at the end stores the sums for k_force_tiles.  A slot whose partner
 // no longer overlaps is freed and its history zeroed, as in the reference.
 // A chunk's rows are contiguous, its slot tiles too, and a round's lanes
 // mostly read one slot of consecutive particles, so their loads coalesce.
@@ -1659,7 +1662,7 @@ k_contact(ContactArgs args)
                     d.settled[s] = 0;   // a listed candidate left its slot
                 }
             }
-            // visited (2: a slot is still held, 3: none is); k_force reads
+            // visited (2: a slot is still held, 3: none is); k_force_tiles reads
             // the sums of a visited chunk and sets its flag back to 1 or 0
             // for the next step's search
             const bool held = __any_sync(FULL, occ != 0u);
@@ -1777,7 +1780,7 @@ void launch_force_tape(const Dev &d, uint32_t np, int a, int tape_step, cudaStre
 
 // The slot forces of contact models 2 and 3; model 1 has no slots (k_topo
 // sums its forces) and the differentiable step evaluates its own law in
-// k_force, recording the tape.
+// k_force_diff, recording the tape.
 void launch_contact(const Dev &d, const Params &hp, uint32_t np, int model, int a,
                     int write_outputs, cudaStream_t st)
 {
