@@ -169,6 +169,18 @@ def test_relayout_does_not_change_results(oracle_libs):
     assert mismatches(a, b, ALL) == []
 
 
+def test_relayout_keeps_bonds_on_their_particles():
+    """Re-sorting storage every 7 steps of a stretched bar leaves its bonds,
+    their history and their breaks exactly as a run without relayouts: each
+    bond's storage pair follows its particles to their new places."""
+    sb = scenes.tension(nx=6, ny=6, nz=6, pull=0.2)
+    a, _, _ = run_gpu(sb, (120,))
+    b, _, stats = run_gpu(sb, (120,), relayout_every=7)
+    assert stats["relayouts"] >= 17
+    assert mismatches(a, b, ALL + BOND_FIELDS) == []
+    assert int((a.bonds[:, 0] >= sb.np).sum()) > 0
+
+
 @pytest.mark.parametrize("graph_steps", [1, 3, 16])
 def test_graph_batching_does_not_change_results(graph_steps):
     sb = scenes.collision(n=800, seed=42, periodic=0, nw=1)
